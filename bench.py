@@ -1,0 +1,480 @@
+#!/usr/bin/env python
+"""Time-step throughput of the dnsjax hot path on B200.
+
+Default workload: plane Couette, nx = nz = 128 Fourier modes, ny = 129 CGL
+points, fd_order 6, Re 1000, dt 0.01, c 0.5, corrector tolerance 1e-10
+(Lx = 2 pi, Lz = pi); seeded synthetic initial perturbation (spectrum
+exp(-(kx^2+kz^2)/32) (1-y^2)^2, energy 5e-2).  One "step" is one full time
+step with the reference's semantics: predictor + corrector iterations until
+the correction norm is below the tolerance (the cap is raised to 60
+iterations so steps converge) + correct_velocity.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload couette128|couette64|kolmogorov32|kolmogorov128]
+
+Under torchrun each rank advances its own trajectory (replicas, no data
+exchange; "scaling": "weak"); timing is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from math import pi
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "steps/s at 128^3: learned+mixed vs plain FP64 on same B200, KE err ≤1e-6"
+
+WORKLOADS = {
+    "couette128": dict(system="plane-couette", nx=128, ny=129, nz=128, p=6,
+                       re=1000.0, dt=0.01, lx=2 * pi, lz=pi, tol=1e-10,
+                       max_iter=60, energy=5e-2, kscale=32.0, seed=4),
+    "couette64": dict(system="plane-couette", nx=64, ny=65, nz=64, p=4,
+                      re=400.0, dt=0.02, lx=2 * pi, lz=pi, tol=1e-10,
+                      max_iter=60, energy=1e-3, kscale=8.0, seed=1),
+    "kolmogorov32": dict(system="kolmogorov", nx=32, ny=32, nz=32, re=40.0,
+                         dt=0.01, lx=2 * pi, lz=2 * pi, ly=2 * pi, tol=1e-10,
+                         max_iter=10, energy=1e-2, spectrum="cfg0", seed=0),
+    "kolmogorov128": dict(system="kolmogorov", nx=128, ny=128, nz=128,
+                          re=100.0, dt=0.005, lx=2 * pi, lz=2 * pi, ly=2 * pi,
+                          tol=1e-10, max_iter=10, energy=0.5, spectrum="k53",
+                          seed=2),
+}
+
+# Corrector iterations per step of the plain method on each workload's
+# first steps (deterministic; measured by the CUDA path and equal to the
+# oracle's).  Used only to turn the reference arm's bounded per-iteration
+# sample into steps/s.
+PLAIN_ITERS_PER_STEP = {"couette128": 36, "couette64": 21, "kolmogorov32": 3,
+                        "kolmogorov128": 3}
+
+
+def params_for(w):
+    from dnsjax_b200.parameters import Parameters
+
+    res = dict(nx=w["nx"], ny=w["ny"], nz=w["nz"])
+    if "p" in w:
+        res["fd_order"] = w["p"]
+    return Parameters(phys=dict(system=w["system"], re=w["re"]),
+                      geo=dict(lx=w["lx"], lz=w["lz"]), res=res,
+                      step=dict(dt=w["dt"], corrector_tolerance=w["tol"],
+                                max_corrector_iterations=w["max_iter"]))
+
+
+def initial_state(w, seed):
+    from dnsjax_b200 import initial
+
+    if w["system"] == "plane-couette":
+        return initial.couette_field(w["nx"], w["ny"], w["nz"], w["lx"], w["lz"],
+                                     w["p"], seed, w["kscale"], w["energy"])
+    spec = (initial.kolmogorov_spectrum_cfg0 if w["spectrum"] == "cfg0"
+            else initial.kolmogorov_spectrum_k53)
+    return initial.periodic_field(w["nx"], w["ny"], w["nz"], w["lx"], w["ly"],
+                                  w["lz"], seed, spec, w["energy"])
+
+
+def grid_points(w):
+    nxp, nzp = 3 * w["nx"] // 2, 3 * w["nz"] // 2
+    nyp = w["ny"] if w["system"] == "plane-couette" else 3 * w["ny"] // 2
+    return nxp * nyp * nzp
+
+
+def op_bytes(w):
+    """Algorithmic HBM bytes of one RHS and one corrector IMM launch."""
+    cb = 16
+    nkx, ny, nz = w["nx"] // 2, w["ny"], w["nz"]
+    if w["system"] == "plane-couette":
+        nkz, mz, p = nz - 1, 3 * nz // 2, w["p"]
+        K = nkz * nkx
+        rhs = cb * nkx * ny * (6 * nkz + 18 * mz)
+        imm = K * ny * (12 * cb + 2 * (3 * p + 1) * 8 + 2 * 4 + 4 * 8 + 3 * cb) + 32 * K
+        return {"rhs": rhs, "imm": imm}
+    ny1, nz1 = ny - 1, nz - 1
+    my, mz = 3 * ny // 2, 3 * nz // 2
+    S, A1, A2 = ny1 * nz1 * nkx, my * nz1 * nkx, my * mz * nkx
+    return {"rhs": cb * (6 * S + 18 * A1 + 18 * A2), "correct": cb * 12 * S}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        return None
+
+
+class Timed:
+    """Wraps a flow so each RHS / corrector call is bracketed by CUDA events."""
+
+    def __init__(self, flow):
+        self.flow = flow
+        self.on = False
+        self.events = {"rhs": [], "imm": []}
+
+    def _rec(self, key, fn, *a, **k):
+        import torch
+
+        if not self.on:
+            return fn(*a, **k)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        out = fn(*a, **k)
+        e.record()
+        self.events[key].append((s, e))
+        return out
+
+    def get_rhs(self, state, out=None):
+        return self._rec("rhs", self.flow.get_rhs, state, out)
+
+    def predict(self, state, rhs):
+        return self.flow.predict(state, rhs)
+
+    def correct_fused(self, *a, **k):
+        return self._rec("imm", self.flow.correct_fused, *a, **k)
+
+    def correct_velocity(self, state):
+        return self.flow.correct_velocity(state)
+
+    @property
+    def params(self):
+        return self.flow.params
+
+    def make_stepper(self, fused=True):
+        from dnsjax_b200.timestep import make_fused_stepper
+
+        return make_fused_stepper(self)
+
+    def durations_ms(self, key):
+        return [s.elapsed_time(e) for s, e in self.events[key]]
+
+
+def run_ours(a, w, rank, world):
+    import torch
+
+    from dnsjax_b200 import _lib, driver
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    p = params_for(w)
+    if w["system"] == "plane-couette":
+        from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
+
+        flow = PlaneCouetteFlow(p)
+    else:
+        from dnsjax_b200.flows.monochromatic import TriplyPeriodicFlow
+
+        flow = TriplyPeriodicFlow(p, ly=w["ly"])
+    u0 = initial_state(w, w["seed"] + rank)
+    tf = Timed(flow)
+    steppers = tf.make_stepper()
+    tol, mi = w["tol"], w["max_iter"]
+    state = torch.as_tensor(u0, device="cuda")
+    for _ in range(a.warmup):
+        state, c, e = driver.step(tf, steppers, state, tol, mi)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    iters = []
+    errs = []
+    tf.on = True
+    n0 = _lib.launch_count()
+    barrier()
+    with ClockSampler(local) as clk:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(a.steps):
+            state, c, e = driver.step(tf, steppers, state, tol, mi)
+            iters.append(c)
+            errs.append(e)
+        t1.record()
+        barrier()
+    launches = _lib.launch_count() - n0
+    tf.on = False
+    ms = t0.elapsed_time(t1)
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # End to end through the public API: pinned host state in, new state out.
+    host_in = torch.empty(state.shape, dtype=state.dtype, pin_memory=True)
+    host_in.copy_(torch.as_tensor(u0))
+    host_out = torch.empty_like(host_in, pin_memory=True)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        d_state = host_in.to("cuda", non_blocking=True)
+        d_state, c, e = driver.step(tf, steppers, d_state, tol, mi)
+        host_out.copy_(d_state, non_blocking=True)
+        host_in, host_out = host_out, host_in
+    e1.record()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    state_bytes = state.numel() * state.element_size()
+
+    # Roofline of the dominant op (events inside the timed region).
+    ob = op_bytes(w)
+    rhs_ms = tf.durations_ms("rhs")
+    imm_ms = tf.durations_ms("imm")
+    tot = {"rhs": sum(rhs_ms), "imm": sum(imm_ms)}
+    dom = max(tot, key=tot.get)
+    dur = (sum(imm_ms) / len(imm_ms)) if dom == "imm" else (sum(rhs_ms) / len(rhs_ms))
+    corr_bytes = ob.get("imm", ob.get("correct"))
+    bytes_ = corr_bytes if dom == "imm" else ob["rhs"]
+    peaks = measured_peaks()
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    achieved = bytes_ / (dur * 1e-3) / 1e9
+    nsteps = a.steps * world
+    value = nsteps / (ms * 1e-3)
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "steps/s",
+        "n_gpus": world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": ms / a.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded divergence-free spectral field)",
+        "config": {
+            "workload": a.workload,
+            "form": "plain-fp64",
+            "grid": [w["nx"], w["ny"], w["nz"]],
+            "fd_order": w.get("p"),
+            "re": w["re"], "dt": w["dt"], "tol": w["tol"],
+            "max_corrector_iterations": w["max_iter"],
+            "corrector_iterations_per_step": sum(iters) / len(iters),
+            "last_error": errs[-1],
+            "grid_points_steps_per_s": value * grid_points(w),
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": "working set (state, operators, workspace) > 126 MB L2",
+            "op_ms": {"rhs": sum(rhs_ms) / max(1, len(rhs_ms)),
+                      "imm_or_correct": sum(imm_ms) / max(1, len(imm_ms))},
+            "op_share": {k: v / ms for k, v in tot.items()},
+        },
+        "roofline": {
+            "bound": "hbm",
+            "kernel": "imm_kernel (+1-block norm finalize)" if dom == "imm"
+                      else "rhs passes (3 kernels)",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": None,
+            "peak_source": "measured" if peaks else "fallback",
+            "algorithmic_bytes_per_launch": bytes_,
+            "avg_launch_ms": dur,
+        },
+        "e2e": {
+            "value": nsteps / (e2e_ms * 1e-3),
+            "unit": "steps/s",
+            "h2d_bytes_per_step": state_bytes,
+            "d2h_bytes_per_step": state_bytes,
+        },
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not a.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_sample(w, flow, u0, sum(iters) / len(iters))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def cpu_sample(w, flow, u0, iters_per_step, imm=None):
+    """Oracle (NumPy FP64 port) timed on one host core: one RHS + one
+    corrector evaluation of the same workload, turned into steps/s with the
+    iterations per step."""
+    import numpy as np
+
+    from oracle.config import Config
+
+    cfg = Config(system=w["system"], nx=w["nx"], ny=w["ny"], nz=w["nz"],
+                 lx=w["lx"], lz=w["lz"], re=w["re"], dt=w["dt"],
+                 corrector_tolerance=w["tol"], **({"ly": w["ly"]} if "ly" in w else {}),
+                 **({"fd_order": w["p"]} if "p" in w else {}))
+    if w["system"] == "plane-couette":
+        from oracle.couette import CouetteSetup
+
+        if imm is None:
+            imm = {k: v.detach().cpu().numpy() for k, v in flow.imm.items()}
+            imm["D1"], imm["D2"] = flow.D1, flow.D2
+        S = CouetteSetup(cfg, imm=imm)
+    else:
+        from oracle.periodic import PeriodicSetup
+
+        S = PeriodicSetup(cfg)
+    t0 = time.perf_counter()
+    r0 = S.get_rhs(u0)
+    t1 = time.perf_counter()
+    new, corr = S.correct(u0, u0, r0, r0)
+    S.norm(corr)
+    t2 = time.perf_counter()
+    per_iter = t2 - t0
+    per_step = per_iter * (2 + iters_per_step)
+    return {"value": 1.0 / per_step, "unit": "steps/s", "cores": 1,
+            "kind": "port",
+            "sample": f"1 RHS ({t1 - t0:.2f} s) + 1 corrector ({t2 - t1:.2f} s) "
+                      f"of the workload on 1 core, x(2 + {iters_per_step:.1f}) "
+                      "iterations per step"}
+
+
+def run_reference(a, w, rank, world):
+    """The oracle port of the reference's CPU path, on the host cores."""
+    if rank != 0:
+        return
+    import numpy as np
+
+    from oracle.config import Config
+
+    cfg = Config(system=w["system"], nx=w["nx"], ny=w["ny"], nz=w["nz"],
+                 lx=w["lx"], lz=w["lz"], re=w["re"], dt=w["dt"],
+                 corrector_tolerance=w["tol"], **({"ly": w["ly"]} if "ly" in w else {}),
+                 **({"fd_order": w["p"]} if "p" in w else {}))
+    if w["system"] == "plane-couette":
+        from oracle.couette import CouetteSetup
+
+        S = CouetteSetup(cfg)
+    else:
+        from oracle.periodic import PeriodicSetup
+
+        S = PeriodicSetup(cfg)
+    u0 = initial_state(w, w["seed"])
+    iters = PLAIN_ITERS_PER_STEP[a.workload]
+
+    def sample():
+        r0 = S.get_rhs(u0)
+        new, corr = S.correct(u0, u0, r0, r0)
+        return S.norm(corr)
+
+    for _ in range(a.warmup):
+        sample()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        sample()
+    dt_iter = (time.perf_counter() - t0) / a.steps
+    per_step = dt_iter * (2 + iters)
+    value = 1.0 / per_step
+    out = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": per_step * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded divergence-free spectral field)",
+        "impl": "reference",
+        "config": {"workload": a.workload, "form": "plain-fp64",
+                   "grid": [w["nx"], w["ny"], w["nz"]]},
+        "cpu_baseline": {
+            "value": value, "unit": "steps/s", "cores": 1, "kind": "port",
+            "sample": f"each step = 1 RHS + 1 corrector of the workload "
+                      f"({dt_iter:.2f} s), scaled by 2 + {iters} iterations/step; "
+                      "NumPy FP64 restatement of the reference (JAX absent)"},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="couette128", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    w = WORKLOADS[a.workload]
+    if a.impl == "reference":
+        run_reference(a, w, rank, world)
+    else:
+        run_ours(a, w, rank, world)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,830 @@
+// C ABI of libdnsb.so (include/dnsb.h): contexts, workspace, and the
+// launch sequences of the time-step operations.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dnsb.h"
+#include "passes.cuh"
+#include "solver.cuh"
+
+using namespace dnsb;
+
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<long long> g_launches{0};
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define DNSB_CUDA(call)                                                     \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess)                                                  \
+      return fail(DNSB_ERR_CUDA, std::string(#call) + ": " +               \
+                                     cudaGetErrorString(e_));               \
+  } while (0)
+
+// Counts one kernel launch and checks its launch status.
+#define DNSB_LAUNCH(call)                                                   \
+  do {                                                                      \
+    g_launches.fetch_add(1, std::memory_order_relaxed);                     \
+    DNSB_CUDA(call);                                                        \
+  } while (0)
+
+template <typename T>
+int upload(T** dst, const T* src, size_t n) {
+  *dst = nullptr;
+  if (n == 0) return 0;
+  if (!src) return fail(DNSB_ERR_ARG, "null host array");
+  DNSB_CUDA(cudaMalloc((void**)dst, n * sizeof(T)));
+  DNSB_CUDA(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+// tw[m] = exp(-2 pi i m / L), evaluated in long double.
+int make_twiddles(double2** dst, int L) {
+  std::vector<double2> h(L);
+  const long double pi = 3.14159265358979323846264338327950288L;
+  for (int m = 0; m < L; ++m) {
+    const long double a = 2.0L * pi * (long double)m / (long double)L;
+    h[m] = make_double2((double)cosl(a), (double)(-sinl(a)));
+  }
+  return upload(dst, h.data(), (size_t)L);
+}
+
+bool fft_size_ok(int L) { return L >= 1 && make_plan(L).nst > 0; }
+
+int max_smem_optin() {
+  int dev = 0, v = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return v;
+}
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace
+
+// ===========================================================================
+// Triply periodic
+// ===========================================================================
+struct dnsb_periodic {
+  int NY1, NZ1, NKX, My, Mz, Mx, S;
+  double c;
+  FFTPlan py, pz, px;
+  double2 *twy = nullptr, *twz = nullptr, *twx = nullptr;
+  double *kx = nullptr, *ky = nullptr, *kz = nullptr;
+  double *U = nullptr, *cU = nullptr, *nU = nullptr;
+  double *ldt1 = nullptr, *ildt2 = nullptr, *lapl = nullptr, *inv_lapl = nullptr;
+  double2 *A = nullptr, *B = nullptr;
+  double* partials = nullptr;
+  size_t ws_bytes = 0;
+
+  PeriodicPointArgs point() const {
+    PeriodicPointArgs a;
+    a.S = S;
+    a.NY1 = NY1;
+    a.NZ1 = NZ1;
+    a.NKX = NKX;
+    a.ldt_1 = ldt1;
+    a.ildt_2 = ildt2;
+    a.kx = kx;
+    a.ky = ky;
+    a.kz = kz;
+    a.inv_lapl = inv_lapl;
+    a.lapl = lapl;
+    a.c = c;
+    return a;
+  }
+};
+
+static void periodic_free(dnsb_periodic* p) {
+  void* ptrs[] = {p->twy, p->twz, p->twx, p->kx, p->ky, p->kz, p->U, p->cU,
+                  p->nU, p->ldt1, p->ildt2, p->lapl, p->inv_lapl, p->A, p->B,
+                  p->partials};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  delete p;
+}
+
+extern "C" int dnsb_version(void) { return 1; }
+extern "C" const char* dnsb_last_error(void) { return g_last_error.c_str(); }
+extern "C" long long dnsb_launch_count(void) { return g_launches.load(); }
+
+extern "C" int dnsb_periodic_create(const dnsb_periodic_desc* d,
+                                    dnsb_periodic** out) {
+  if (!d || !out) return fail(DNSB_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (d->nx < 2 || d->ny < 2 || d->nz < 2 || d->nx % 2 || d->ny % 2 || d->nz % 2)
+    return fail(DNSB_ERR_ARG, "nx, ny, nz must be even and >= 2");
+  if (!fft_size_ok(d->nx_p) || !fft_size_ok(d->ny_p) || !fft_size_ok(d->nz_p))
+    return fail(DNSB_ERR_ARG, "padded sizes must be of the form 2^a 3^b");
+  if (d->nx_p % 2 || d->nx_p < d->nx || d->ny_p < d->ny || d->nz_p < d->nz ||
+      (d->ny_p - d->ny) % 2 || (d->nz_p - d->nz) % 2)
+    return fail(DNSB_ERR_ARG, "padded sizes incompatible with the 3/2 rule");
+  dnsb_periodic* p = new dnsb_periodic();
+  p->NY1 = d->ny - 1;
+  p->NZ1 = d->nz - 1;
+  p->NKX = d->nx / 2;
+  p->My = d->ny_p;
+  p->Mz = d->nz_p;
+  p->Mx = d->nx_p;
+  p->S = p->NY1 * p->NZ1 * p->NKX;
+  p->c = d->implicitness;
+  p->py = make_plan(p->My);
+  p->pz = make_plan(p->Mz);
+  p->px = make_plan(p->Mx);
+  const int smax = max_smem_optin();
+  const size_t need[] = {col_pass_smem(p->Mz), x_pass_smem(p->Mx),
+                         x_phys_smem(p->Mx), x_fwd_smem(p->Mx),
+                         yinv_smem(p->My, p->NY1), yfwd_smem(p->My, p->NY1)};
+  for (size_t n : need)
+    if ((int)n > smax) {
+      periodic_free(p);
+      return fail(DNSB_ERR_ARG, "grid too large for shared-memory tiles");
+    }
+  int rc = 0;
+  auto chk = [&](int r) {
+    if (r && !rc) rc = r;
+  };
+  chk(make_twiddles(&p->twy, p->My));
+  chk(make_twiddles(&p->twz, p->Mz));
+  chk(make_twiddles(&p->twx, p->Mx));
+  chk(upload(&p->kx, d->kx, p->NKX));
+  chk(upload(&p->ky, d->ky, p->NY1));
+  chk(upload(&p->kz, d->kz, p->NZ1));
+  chk(upload(&p->U, d->base_flow, 3 * (size_t)p->My));
+  chk(upload(&p->cU, d->curl_base_flow, 3 * (size_t)p->My));
+  chk(upload(&p->nU, d->nonlin_base_flow, 3 * (size_t)p->My));
+  chk(upload(&p->ldt1, d->ldt_1, p->S));
+  chk(upload(&p->ildt2, d->ildt_2, p->S));
+  if (!rc) {
+    // lapl = -(kx^2 + ky^2 + kz^2), inv_lapl = 1/lapl off the mean mode
+    // (triply_periodic.py:59-67).
+    std::vector<double> l(p->S), il(p->S);
+    for (int iy = 0; iy < p->NY1; ++iy)
+      for (int iz = 0; iz < p->NZ1; ++iz)
+        for (int ix = 0; ix < p->NKX; ++ix) {
+          const double a = d->kx[ix], b = d->ky[iy], cc = d->kz[iz];
+          const double v = -(a * a + b * b + cc * cc);
+          const int s = (iy * p->NZ1 + iz) * p->NKX + ix;
+          l[s] = v;
+          il[s] = v < 0 ? 1.0 / v : 0.0;
+        }
+    chk(upload(&p->lapl, l.data(), p->S));
+    chk(upload(&p->inv_lapl, il.data(), p->S));
+  }
+  const size_t nA = 6ull * p->My * p->NZ1 * p->NKX;
+  const size_t nB = 6ull * p->My * p->Mz * p->NKX;
+  if (!rc) {
+    cudaError_t e1 = cudaMalloc(&p->A, nA * sizeof(double2));
+    cudaError_t e2 = cudaMalloc(&p->B, nB * sizeof(double2));
+    cudaError_t e3 = cudaMalloc(&p->partials, 2 * kRedBlocks * sizeof(double));
+    if (e1 || e2 || e3) rc = fail(DNSB_ERR_CUDA, "workspace allocation failed");
+  }
+  if (!rc) {
+    cudaError_t e = set_pass_attributes(smax);
+    if (e == cudaSuccess) e = set_solver_attributes(smax);
+    if (e != cudaSuccess)
+      rc = fail(DNSB_ERR_CUDA, std::string("cudaFuncSetAttribute: ") +
+                                   cudaGetErrorString(e));
+  }
+  if (rc) {
+    periodic_free(p);
+    return rc;
+  }
+  p->ws_bytes = (nA + nB) * sizeof(double2) + 2 * kRedBlocks * sizeof(double);
+  *out = p;
+  return 0;
+}
+
+extern "C" int dnsb_periodic_destroy(dnsb_periodic* p) {
+  if (p) periodic_free(p);
+  return 0;
+}
+
+extern "C" size_t dnsb_periodic_workspace_bytes(const dnsb_periodic* p) {
+  return p ? p->ws_bytes : 0;
+}
+
+// Inverse z pass over nf fields: A[f][y][kz][kx] -> B[f][y][z][kx].
+static ColPassArgs periodic_zinv(const dnsb_periodic* p) {
+  ColPassArgs a{};
+  a.in = p->A;
+  a.out = p->B;
+  a.in_fs = (long long)p->My * p->NZ1 * p->NKX;
+  a.out_fs = (long long)p->My * p->Mz * p->NKX;
+  a.in_os = (long long)p->NZ1 * p->NKX;
+  a.out_os = (long long)p->Mz * p->NKX;
+  a.in_ts = p->NKX;
+  a.out_ts = p->NKX;
+  a.nI = p->NKX;
+  a.nstored = p->NZ1;
+  a.inverse = 1;
+  a.plan = p->pz;
+  a.tw = p->twz;
+  return a;
+}
+
+// Forward z pass over 3 fields: B[f][y][z][kx] -> A[f][y][kz][kx].
+static ColPassArgs periodic_zfwd(const dnsb_periodic* p) {
+  ColPassArgs a{};
+  a.in = p->B;
+  a.out = p->A;
+  a.in_fs = (long long)p->My * p->Mz * p->NKX;
+  a.out_fs = (long long)p->My * p->NZ1 * p->NKX;
+  a.in_os = (long long)p->Mz * p->NKX;
+  a.out_os = (long long)p->NZ1 * p->NKX;
+  a.in_ts = p->NKX;
+  a.out_ts = p->NKX;
+  a.nI = p->NKX;
+  a.nstored = p->NZ1;
+  a.inverse = 0;
+  a.plan = p->pz;
+  a.tw = p->twz;
+  return a;
+}
+
+extern "C" int dnsb_periodic_rhs(dnsb_periodic* p, const void* state,
+                                 void* rhs, void* stream) {
+  if (!p || !state || !rhs) return fail(DNSB_ERR_ARG, "null argument");
+  cudaStream_t st = as_stream(stream);
+  YInvArgs yi{};
+  yi.u = (const double2*)state;
+  yi.out = p->A;
+  yi.NY1 = p->NY1;
+  yi.NZ1 = p->NZ1;
+  yi.NKX = p->NKX;
+  yi.curl = 1;
+  yi.kx = p->kx;
+  yi.ky = p->ky;
+  yi.kz = p->kz;
+  yi.plan = p->py;
+  yi.tw = p->twy;
+  DNSB_LAUNCH(launch_yinv(yi, st));
+  DNSB_LAUNCH(launch_col_pass(periodic_zinv(p), 6, p->My, st));
+  XPassArgs xa{};
+  xa.in = p->B;
+  xa.out = p->B;
+  xa.in_fs = xa.out_fs = (long long)p->My * p->Mz * p->NKX;
+  xa.nrows = p->My * p->Mz;
+  xa.inner_n = p->Mz;
+  xa.so = (long long)p->Mz * p->NKX;
+  xa.si = p->NKX;
+  xa.ks = 1;
+  xa.nkx = p->NKX;
+  xa.y_outer = 1;
+  xa.rows_fast = 0;
+  xa.U = p->U;
+  xa.cU = p->cU;
+  xa.nU = p->nU;
+  xa.ny_grid = p->My;
+  xa.plan = p->px;
+  xa.tw = p->twx;
+  DNSB_LAUNCH(launch_x_pass(xa, st));
+  DNSB_LAUNCH(launch_col_pass(periodic_zfwd(p), 3, p->My, st));
+  YFwdArgs yf{};
+  yf.in = p->A;
+  yf.out = (double2*)rhs;
+  yf.NY1 = p->NY1;
+  yf.NZ1 = p->NZ1;
+  yf.NKX = p->NKX;
+  yf.project = 1;
+  yf.kx = p->kx;
+  yf.ky = p->ky;
+  yf.kz = p->kz;
+  yf.inv_lapl = p->inv_lapl;
+  yf.plan = p->py;
+  yf.tw = p->twy;
+  DNSB_LAUNCH(launch_yfwd(yf, st));
+  return 0;
+}
+
+extern "C" int dnsb_periodic_predict(dnsb_periodic* p, const void* state,
+                                     const void* rhs, void* out,
+                                     void* stream) {
+  if (!p || !state || !rhs || !out) return fail(DNSB_ERR_ARG, "null argument");
+  DNSB_LAUNCH(launch_periodic_predict(p->point(), (const double2*)state,
+                                      (const double2*)rhs, (double2*)out,
+                                      as_stream(stream)));
+  return 0;
+}
+
+extern "C" int dnsb_periodic_correct(dnsb_periodic* p, const void* pred,
+                                     const void* rhs_prev,
+                                     const void* rhs_next, void* pred_out,
+                                     void* corr_out, double* err_dev,
+                                     void* stream) {
+  if (!p || !pred || !rhs_prev || !rhs_next || !pred_out)
+    return fail(DNSB_ERR_ARG, "null argument");
+  cudaStream_t st = as_stream(stream);
+  DNSB_LAUNCH(launch_periodic_correct(
+      p->point(), (const double2*)pred, (const double2*)rhs_prev,
+      (const double2*)rhs_next, (double2*)pred_out, (double2*)corr_out,
+      err_dev ? p->partials : nullptr, st));
+  if (err_dev)
+    DNSB_LAUNCH(launch_finalize(p->partials, kRedBlocks, err_dev, 1.0, 1, st));
+  return 0;
+}
+
+extern "C" int dnsb_periodic_norm(dnsb_periodic* p, const void* v,
+                                  double* out_dev, void* stream) {
+  if (!p || !v || !out_dev) return fail(DNSB_ERR_ARG, "null argument");
+  cudaStream_t st = as_stream(stream);
+  DNSB_LAUNCH(launch_periodic_norm2(p->point(), (const double2*)v, p->partials, st));
+  DNSB_LAUNCH(launch_finalize(p->partials, kRedBlocks, out_dev, 1.0, 1, st));
+  return 0;
+}
+
+extern "C" int dnsb_periodic_correct_velocity(dnsb_periodic* p, const void* v,
+                                              void* out, int divergence,
+                                              void* stream) {
+  if (!p || !v || !out) return fail(DNSB_ERR_ARG, "null argument");
+  DNSB_LAUNCH(launch_periodic_correct_velocity(p->point(), (const double2*)v,
+                                               (double2*)out, divergence,
+                                               as_stream(stream)));
+  return 0;
+}
+
+extern "C" int dnsb_periodic_energy_sums(dnsb_periodic* p, const void* v,
+                                         double* out_dev, void* stream) {
+  if (!p || !v || !out_dev) return fail(DNSB_ERR_ARG, "null argument");
+  cudaStream_t st = as_stream(stream);
+  DNSB_LAUNCH(launch_periodic_stats(p->point(), (const double2*)v, p->partials, st));
+  DNSB_LAUNCH(launch_finalize(p->partials, kRedBlocks, out_dev, 1.0, 0, st));
+  DNSB_LAUNCH(launch_finalize(p->partials + kRedBlocks, kRedBlocks, out_dev + 1,
+                              1.0, 0, st));
+  return 0;
+}
+
+extern "C" int dnsb_periodic_spec_to_phys(dnsb_periodic* p, const void* spec,
+                                          double* phys, void* stream) {
+  if (!p || !spec || !phys) return fail(DNSB_ERR_ARG, "null argument");
+  cudaStream_t st = as_stream(stream);
+  YInvArgs yi{};
+  yi.u = (const double2*)spec;
+  yi.out = p->A;
+  yi.NY1 = p->NY1;
+  yi.NZ1 = p->NZ1;
+  yi.NKX = p->NKX;
+  yi.curl = 0;
+  yi.kx = p->kx;
+  yi.ky = p->ky;
+  yi.kz = p->kz;
+  yi.plan = p->py;
+  yi.tw = p->twy;
+  DNSB_LAUNCH(launch_yinv(yi, st));
+  DNSB_LAUNCH(launch_col_pass(periodic_zinv(p), 3, p->My, st));
+  XPhysArgs xa{};
+  xa.in = p->B;
+  xa.out = phys;
+  xa.in_fs = (long long)p->My * p->Mz * p->NKX;
+  xa.out_fs = (long long)p->My * p->Mz * p->Mx;
+  xa.nrows = p->My * p->Mz;
+  xa.inner_n = p->Mz;
+  xa.so = (long long)p->Mz * p->NKX;
+  xa.si = p->NKX;
+  xa.ks = 1;
+  xa.pso = (long long)p->Mz * p->Mx;
+  xa.psi = p->Mx;
+  xa.nkx = p->NKX;
+  xa.rows_fast = 0;
+  xa.plan = p->px;
+  xa.tw = p->twx;
+  DNSB_LAUNCH(launch_x_phys(xa, st));
+  return 0;
+}
+
+extern "C" int dnsb_periodic_phys_to_spec(dnsb_periodic* p, const double* phys,
+                                          void* spec, void* stream) {
+  if (!p || !spec || !phys) return fail(DNSB_ERR_ARG, "null argument");
+  cudaStream_t st = as_stream(stream);
+  XPhysArgs xa{};
+  xa.in_fs = (long long)p->My * p->Mz * p->NKX;
+  xa.out_fs = (long long)p->My * p->Mz * p->Mx;
+  xa.nrows = p->My * p->Mz;
+  xa.inner_n = p->Mz;
+  xa.so = (long long)p->Mz * p->NKX;
+  xa.si = p->NKX;
+  xa.ks = 1;
+  xa.pso = (long long)p->Mz * p->Mx;
+  xa.psi = p->Mx;
+  xa.nkx = p->NKX;
+  xa.rows_fast = 0;
+  xa.plan = p->px;
+  xa.tw = p->twx;
+  DNSB_LAUNCH(launch_x_fwd(xa, phys, p->B, st));
+  DNSB_LAUNCH(launch_col_pass(periodic_zfwd(p), 3, p->My, st));
+  YFwdArgs yf{};
+  yf.in = p->A;
+  yf.out = (double2*)spec;
+  yf.NY1 = p->NY1;
+  yf.NZ1 = p->NZ1;
+  yf.NKX = p->NKX;
+  yf.project = 0;
+  yf.kx = p->kx;
+  yf.ky = p->ky;
+  yf.kz = p->kz;
+  yf.inv_lapl = p->inv_lapl;
+  yf.plan = p->py;
+  yf.tw = p->twy;
+  DNSB_LAUNCH(launch_yfwd(yf, st));
+  return 0;
+}
+
+// ===========================================================================
+// Plane Couette
+// ===========================================================================
+struct dnsb_couette {
+  int NZ1, NKX, Ny, Mz, Mx, p, s1, s2, span_max, NM;
+  double dt, c, nu, ly;
+  FFTPlan pz, px;
+  double2 *twz = nullptr, *twx = nullptr;
+  double *kx = nullptr, *kz = nullptr, *d1w = nullptr, *d2w = nullptr;
+  int *d1j0 = nullptr, *d2j0 = nullptr;
+  double *U = nullptr, *cU = nullptr, *nU = nullptr, *simpson = nullptr;
+  double2* B = nullptr;
+  double* partials = nullptr;
+  int* status = nullptr;
+  dnsb_imm_ops ops{};
+  bool bound = false;
+  size_t ws_bytes = 0;
+
+  ImmArgs imm() const {
+    ImmArgs a{};
+    a.NZ1 = NZ1;
+    a.NKX = NKX;
+    a.Ny = Ny;
+    a.kl = a.ku = p;
+    a.s1 = s1;
+    a.s2 = s2;
+    a.d1_j0 = d1j0;
+    a.d1_w = d1w;
+    a.d2_j0 = d2j0;
+    a.d2_w = d2w;
+    a.kx = kx;
+    a.kz = kz;
+    a.simpson = simpson;
+    a.dt = dt;
+    a.c = c;
+    a.nu = nu;
+    a.Lk_ab = ops.Lk_ab;
+    a.Lk_piv = ops.Lk_piv;
+    a.Hk_ab = ops.Hk_ab;
+    a.Hk_piv = ops.Hk_piv;
+    a.v1 = ops.v1;
+    a.v2 = ops.v2;
+    a.q1 = ops.q1;
+    a.q2 = ops.q2;
+    a.M_inv = ops.M_inv;
+    a.status = status;
+    return a;
+  }
+};
+
+static void couette_free(dnsb_couette* p) {
+  void* ptrs[] = {p->twz, p->twx, p->kx, p->kz, p->d1w, p->d2w, p->d1j0,
+                  p->d2j0, p->U, p->cU, p->nU, p->simpson, p->B, p->partials,
+                  p->status};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  delete p;
+}
+
+// Composite Simpson weights on non-uniform panels (cartesian.py:106-140),
+// expressed as the linear functional sum_y W_y f_y.
+static std::vector<double> simpson_weights(const double* ys, int n) {
+  std::vector<double> W(n, 0.0);
+  for (int i = 0; i + 2 < n; i += 2) {
+    const double h0 = ys[i + 1] - ys[i], h1 = ys[i + 2] - ys[i + 1];
+    const double hs = h0 + h1, hp = h0 * h1, r = h0 / h1;
+    W[i] += (hs / 6) * (2 - 1 / r);
+    W[i + 1] += (hs / 6) * (hs * hs / hp);
+    W[i + 2] += (hs / 6) * (2 - r);
+  }
+  return W;
+}
+
+static bool stencil_ok(const int* j0, int n, int s) {
+  for (int i = 0; i < n; ++i) {
+    if (j0[i] < 0 || j0[i] > i || j0[i] + s > n || j0[i] + s <= i) return false;
+    if (i > 0 && (j0[i] < j0[i - 1] || j0[i] > j0[i - 1] + 1)) return false;
+  }
+  return true;
+}
+
+extern "C" int dnsb_couette_create(const dnsb_couette_desc* d,
+                                   dnsb_couette** out) {
+  if (!d || !out) return fail(DNSB_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (d->nx < 2 || d->nz < 2 || d->nx % 2 || d->nz % 2)
+    return fail(DNSB_ERR_ARG, "nx, nz must be even and >= 2");
+  if (d->ny < 3 || d->ny % 2 == 0)
+    return fail(DNSB_ERR_ARG, "ny must be odd and >= 3 (Simpson rule)");
+  if (d->fd_order < 2 || d->fd_order + 2 > d->ny)
+    return fail(DNSB_ERR_ARG, "fd_order out of range");
+  if (!fft_size_ok(d->nx_p) || !fft_size_ok(d->nz_p) || d->nx_p % 2 ||
+      d->nx_p < d->nx || d->nz_p < d->nz || (d->nz_p - d->nz) % 2)
+    return fail(DNSB_ERR_ARG, "padded sizes must be 2^a 3^b and >= modes");
+  const int pord = d->fd_order;
+  if (!d->d1_j0 || !d->d2_j0 || !stencil_ok(d->d1_j0, d->ny, pord + 1) ||
+      !stencil_ok(d->d2_j0, d->ny, pord + 2))
+    return fail(DNSB_ERR_ARG, "invalid FD stencil start columns");
+  dnsb_couette* p = new dnsb_couette();
+  p->NZ1 = d->nz - 1;
+  p->NKX = d->nx / 2;
+  p->Ny = d->ny;
+  p->Mz = d->nz_p;
+  p->Mx = d->nx_p;
+  p->p = pord;
+  p->s1 = pord + 1;
+  p->s2 = pord + 2;
+  p->span_max = kZTile + pord;
+  p->NM = p->NZ1 * p->NKX;
+  p->dt = d->dt;
+  p->c = d->implicitness;
+  p->nu = d->nu;
+  p->ly = d->ly;
+  p->pz = make_plan(p->Mz);
+  p->px = make_plan(p->Mx);
+  const int smax = max_smem_optin();
+  const size_t need[] = {col_pass_smem(p->Mz), x_pass_smem(p->Mx),
+                         x_phys_smem(p->Mx), x_fwd_smem(p->Mx),
+                         zinv_curl_smem(p->Mz, p->NZ1, p->span_max),
+                         imm_smem(p->Ny)};
+  for (size_t n : need)
+    if ((int)n > smax) {
+      couette_free(p);
+      return fail(DNSB_ERR_ARG, "grid too large for shared-memory tiles");
+    }
+  int rc = 0;
+  auto chk = [&](int r) {
+    if (r && !rc) rc = r;
+  };
+  chk(make_twiddles(&p->twz, p->Mz));
+  chk(make_twiddles(&p->twx, p->Mx));
+  chk(upload(&p->kx, d->kx, p->NKX));
+  chk(upload(&p->kz, d->kz, p->NZ1));
+  chk(upload(&p->d1j0, d->d1_j0, p->Ny));
+  chk(upload(&p->d2j0, d->d2_j0, p->Ny));
+  chk(upload(&p->d1w, d->d1_w, (size_t)p->Ny * p->s1));
+  chk(upload(&p->d2w, d->d2_w, (size_t)p->Ny * p->s2));
+  chk(upload(&p->U, d->base_flow, 3 * (size_t)p->Ny));
+  chk(upload(&p->cU, d->curl_base_flow, 3 * (size_t)p->Ny));
+  chk(upload(&p->nU, d->nonlin_base_flow, 3 * (size_t)p->Ny));
+  if (!rc) {
+    if (!d->ys) rc = fail(DNSB_ERR_ARG, "null ys");
+    else {
+      std::vector<double> W = simpson_weights(d->ys, p->Ny);
+      chk(upload(&p->simpson, W.data(), W.size()));
+    }
+  }
+  const size_t nB = 6ull * p->Mz * p->NKX * p->Ny;
+  const size_t npart = (size_t)std::max(p->NM, kRedBlocks);
+  if (!rc) {
+    cudaError_t e1 = cudaMalloc(&p->B, nB * sizeof(double2));
+    cudaError_t e2 = cudaMalloc(&p->partials, npart * sizeof(double));
+    cudaError_t e3 = cudaMalloc(&p->status, sizeof(int));
+    if (e1 || e2 || e3) rc = fail(DNSB_ERR_CUDA, "workspace allocation failed");
+    else if (cudaMemset(p->status, 0, sizeof(int)) != cudaSuccess)
+      rc = fail(DNSB_ERR_CUDA, "cudaMemset failed");
+  }
+  if (!rc) {
+    cudaError_t e = set_pass_attributes(smax);
+    if (e == cudaSuccess) e = set_solver_attributes(smax);
+    if (e != cudaSuccess)
+      rc = fail(DNSB_ERR_CUDA, std::string("cudaFuncSetAttribute: ") +
+                                   cudaGetErrorString(e));
+  }
+  if (rc) {
+    couette_free(p);
+    return rc;
+  }
+  p->ws_bytes = nB * sizeof(double2) + npart * sizeof(double) + sizeof(int);
+  *out = p;
+  return 0;
+}
+
+extern "C" int dnsb_couette_destroy(dnsb_couette* p) {
+  if (p) couette_free(p);
+  return 0;
+}
+
+extern "C" size_t dnsb_couette_workspace_bytes(const dnsb_couette* p) {
+  return p ? p->ws_bytes : 0;
+}
+
+extern "C" int dnsb_couette_bind_imm(dnsb_couette* p, const dnsb_imm_ops* ops) {
+  if (!p || !ops) return fail(DNSB_ERR_ARG, "null argument");
+  if (!ops->Lk_ab || !ops->Lk_piv || !ops->Hk_ab || !ops->Hk_piv || !ops->v1 ||
+      !ops->v2 || !ops->q1 || !ops->q2 || !ops->M_inv)
+    return fail(DNSB_ERR_ARG, "null IMM operator");
+  p->ops = *ops;
+  p->bound = true;
+  return 0;
+}
+
+extern "C" int dnsb_couette_rhs(dnsb_couette* p, const void* state, void* rhs,
+                                void* stream) {
+  if (!p || !state || !rhs) return fail(DNSB_ERR_ARG, "null argument");
+  cudaStream_t st = as_stream(stream);
+  ZInvCurlArgs zi{};
+  zi.u = (const double2*)state;
+  zi.out = p->B;
+  zi.NZ1 = p->NZ1;
+  zi.NKX = p->NKX;
+  zi.Ny = p->Ny;
+  zi.curl = 1;
+  zi.s1 = p->s1;
+  zi.d1_j0 = p->d1j0;
+  zi.d1_w = p->d1w;
+  zi.kx = p->kx;
+  zi.kz = p->kz;
+  zi.plan = p->pz;
+  zi.tw = p->twz;
+  DNSB_LAUNCH(launch_zinv_curl(zi, p->span_max, st));
+  XPassArgs xa{};
+  xa.in = p->B;
+  xa.out = p->B;
+  xa.in_fs = xa.out_fs = (long long)p->Mz * p->NKX * p->Ny;
+  xa.nrows = p->Mz * p->Ny;
+  xa.inner_n = p->Ny;
+  xa.so = (long long)p->NKX * p->Ny;
+  xa.si = 1;
+  xa.ks = p->Ny;
+  xa.nkx = p->NKX;
+  xa.y_outer = 0;
+  xa.rows_fast = 1;
+  xa.U = p->U;
+  xa.cU = p->cU;
+  xa.nU = p->nU;
+  xa.ny_grid = p->Ny;
+  xa.plan = p->px;
+  xa.tw = p->twx;
+  DNSB_LAUNCH(launch_x_pass(xa, st));
+  ColPassArgs zf{};
+  zf.in = p->B;
+  zf.out = (double2*)rhs;
+  zf.in_fs = (long long)p->Mz * p->NKX * p->Ny;
+  zf.out_fs = (long long)p->NZ1 * p->NKX * p->Ny;
+  zf.in_os = p->Ny;
+  zf.out_os = p->Ny;
+  zf.in_ts = (long long)p->NKX * p->Ny;
+  zf.out_ts = (long long)p->NKX * p->Ny;
+  zf.nI = p->Ny;
+  zf.nstored = p->NZ1;
+  zf.inverse = 0;
+  zf.plan = p->pz;
+  zf.tw = p->twz;
+  DNSB_LAUNCH(launch_col_pass(zf, 3, p->NKX, st));
+  return 0;
+}
+
+extern "C" int dnsb_couette_imm(dnsb_couette* p, const void* vel_n,
+                                const void* vel_j, const void* nl_n,
+                                const void* nl_j, void* vel_new,
+                                void* corr_out, double* err_dev,
+                                void* stream) {
+  if (!p || !vel_n || !vel_j || !nl_n || !nl_j || !vel_new)
+    return fail(DNSB_ERR_ARG, "null argument");
+  if (!p->bound) return fail(DNSB_ERR_ARG, "IMM operators not bound");
+  if (vel_new == vel_n)
+    return fail(DNSB_ERR_ARG, "vel_new must not alias vel_n");
+  cudaStream_t st = as_stream(stream);
+  DNSB_LAUNCH(launch_imm(p->imm(), (const double2*)vel_n, (const double2*)vel_j,
+                         (const double2*)nl_n, (const double2*)nl_j,
+                         (double2*)vel_new, (double2*)corr_out,
+                         err_dev ? p->partials : nullptr, st));
+  if (err_dev)
+    DNSB_LAUNCH(launch_finalize(p->partials, p->NM, err_dev, 1.0 / p->ly, 1, st));
+  return 0;
+}
+
+static int couette_norm_impl(dnsb_couette* p, const void* v, double* out_dev,
+                             int do_sqrt, void* stream) {
+  if (!p || !v || !out_dev) return fail(DNSB_ERR_ARG, "null argument");
+  cudaStream_t st = as_stream(stream);
+  DNSB_LAUNCH(launch_couette_norm2(p->imm(), (const double2*)v, p->partials, st));
+  DNSB_LAUNCH(launch_finalize(p->partials, kRedBlocks, out_dev, 1.0 / p->ly,
+                              do_sqrt, st));
+  return 0;
+}
+
+extern "C" int dnsb_couette_norm(dnsb_couette* p, const void* v,
+                                 double* out_dev, void* stream) {
+  return couette_norm_impl(p, v, out_dev, 1, stream);
+}
+
+extern "C" int dnsb_couette_norm2(dnsb_couette* p, const void* v,
+                                  double* out_dev, void* stream) {
+  return couette_norm_impl(p, v, out_dev, 0, stream);
+}
+
+extern "C" int dnsb_couette_spec_to_phys(dnsb_couette* p, const void* spec,
+                                         double* phys, void* stream) {
+  if (!p || !spec || !phys) return fail(DNSB_ERR_ARG, "null argument");
+  cudaStream_t st = as_stream(stream);
+  ZInvCurlArgs zi{};
+  zi.u = (const double2*)spec;
+  zi.out = p->B;
+  zi.NZ1 = p->NZ1;
+  zi.NKX = p->NKX;
+  zi.Ny = p->Ny;
+  zi.curl = 0;
+  zi.s1 = p->s1;
+  zi.d1_j0 = p->d1j0;
+  zi.d1_w = p->d1w;
+  zi.kx = p->kx;
+  zi.kz = p->kz;
+  zi.plan = p->pz;
+  zi.tw = p->twz;
+  DNSB_LAUNCH(launch_zinv_curl(zi, p->span_max, st));
+  XPhysArgs xa{};
+  xa.in = p->B;
+  xa.out = phys;
+  xa.in_fs = (long long)p->Mz * p->NKX * p->Ny;
+  xa.out_fs = (long long)p->Ny * p->Mz * p->Mx;
+  xa.nrows = p->Mz * p->Ny;
+  xa.inner_n = p->Ny;
+  xa.so = (long long)p->NKX * p->Ny;
+  xa.si = 1;
+  xa.ks = p->Ny;
+  xa.pso = p->Mx;
+  xa.psi = (long long)p->Mz * p->Mx;
+  xa.nkx = p->NKX;
+  xa.rows_fast = 1;
+  xa.plan = p->px;
+  xa.tw = p->twx;
+  DNSB_LAUNCH(launch_x_phys(xa, st));
+  return 0;
+}
+
+extern "C" int dnsb_couette_phys_to_spec(dnsb_couette* p, const double* phys,
+                                         void* spec, void* stream) {
+  if (!p || !spec || !phys) return fail(DNSB_ERR_ARG, "null argument");
+  cudaStream_t st = as_stream(stream);
+  XPhysArgs xa{};
+  xa.in_fs = (long long)p->Mz * p->NKX * p->Ny;
+  xa.out_fs = (long long)p->Ny * p->Mz * p->Mx;
+  xa.nrows = p->Mz * p->Ny;
+  xa.inner_n = p->Ny;
+  xa.so = (long long)p->NKX * p->Ny;
+  xa.si = 1;
+  xa.ks = p->Ny;
+  xa.pso = p->Mx;
+  xa.psi = (long long)p->Mz * p->Mx;
+  xa.nkx = p->NKX;
+  xa.rows_fast = 1;
+  xa.plan = p->px;
+  xa.tw = p->twx;
+  DNSB_LAUNCH(launch_x_fwd(xa, phys, p->B, st));
+  ColPassArgs zf{};
+  zf.in = p->B;
+  zf.out = (double2*)spec;
+  zf.in_fs = (long long)p->Mz * p->NKX * p->Ny;
+  zf.out_fs = (long long)p->NZ1 * p->NKX * p->Ny;
+  zf.in_os = p->Ny;
+  zf.out_os = p->Ny;
+  zf.in_ts = (long long)p->NKX * p->Ny;
+  zf.out_ts = (long long)p->NKX * p->Ny;
+  zf.nI = p->Ny;
+  zf.nstored = p->NZ1;
+  zf.inverse = 0;
+  zf.plan = p->pz;
+  zf.tw = p->twz;
+  DNSB_LAUNCH(launch_col_pass(zf, 3, p->NKX, st));
+  return 0;
+}
+
+extern "C" int dnsb_couette_check(dnsb_couette* p, void* stream) {
+  if (!p) return fail(DNSB_ERR_ARG, "null argument");
+  int h = 0;
+  DNSB_CUDA(cudaMemcpyAsync(&h, p->status, sizeof(int), cudaMemcpyDeviceToHost,
+                            as_stream(stream)));
+  DNSB_CUDA(cudaStreamSynchronize(as_stream(stream)));
+  if (h) return fail(DNSB_ERR_PIVOT, "pivot index outside [j, j+kl]");
+  return 0;
+}
+
+// ===========================================================================
+// Standalone banded solve
+// ===========================================================================
+extern "C" int dnsb_banded_solve(const double* ab, const int* ipiv, double* b,
+                                 int nmodes, int ny, int kl, int ku, int ncols,
+                                 int* status_dev, void* stream) {
+  if (!ab || !ipiv || !b) return fail(DNSB_ERR_ARG, "null argument");
+  if (nmodes < 0 || ny < 1 || kl < 0 || ku < 0 || ncols < 1)
+    return fail(DNSB_ERR_ARG, "invalid sizes");
+  if (nmodes == 0) return 0;
+  DNSB_LAUNCH(launch_banded_solve(ab, ipiv, b, nmodes, ny, kl, ku, ncols,
+                                  status_dev, as_stream(stream)));
+  return 0;
+}

@@ -1,0 +1,184 @@
+// Shared device code for libdnsb: complex helpers, the shared-memory
+// Stockham FFT used by every axis pass, and launch/error plumbing.
+//
+// FFT conventions follow the reference solver (src/dnsjax/fft.py):
+// norm="forward" -- the forward transform divides by the length, the
+// inverse applies no factor -- and stored spectral axes omit the Nyquist
+// mode.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#define DNSB_MAX_RADIX 8
+#define DNSB_MAX_STAGES 12
+
+namespace dnsb {
+
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) {
+  return make_double2(a.x - b.x, a.y - b.y);
+}
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cscale(double2 a, double s) {
+  return make_double2(a.x * s, a.y * s);
+}
+__host__ __device__ __forceinline__ double2 cconj(double2 a) {
+  return make_double2(a.x, -a.y);
+}
+// i * k * z for real k, evaluated as numpy evaluates 1j * k * z:
+// (0 + k i)(a + b i) = (-k b) + (k a) i.
+__host__ __device__ __forceinline__ double2 cik(double k, double2 z) {
+  return make_double2(-(k * z.y), k * z.x);
+}
+// i * z
+__host__ __device__ __forceinline__ double2 ci(double2 z) {
+  return make_double2(-z.y, z.x);
+}
+
+// An FFT length L = product of radices (each 2, 3, 4 or 8), applied as
+// Stockham auto-sort stages so the output is in natural order.
+struct FFTPlan {
+  int L;
+  int nst;
+  int radix[DNSB_MAX_STAGES];
+};
+
+// ---- small DFTs in registers; sign = -1 forward, +1 inverse ------------
+__device__ __forceinline__ void dft2(double2* v) {
+  double2 a = v[0], b = v[1];
+  v[0] = cadd(a, b);
+  v[1] = csub(a, b);
+}
+
+__device__ __forceinline__ void dft3(double2* v, int sign) {
+  const double s3 = 0.86602540378443864676;  // sin(2 pi / 3)
+  double2 t1 = cadd(v[1], v[2]);
+  double2 t2 = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
+  double2 d = csub(v[1], v[2]);
+  // i * sign * s3 * d
+  double2 t3 = make_double2(-sign * s3 * d.y, sign * s3 * d.x);
+  v[0] = cadd(v[0], t1);
+  v[1] = cadd(t2, t3);
+  v[2] = csub(t2, t3);
+}
+
+__device__ __forceinline__ void dft4(double2* v, int sign) {
+  double2 a = cadd(v[0], v[2]);
+  double2 b = csub(v[0], v[2]);
+  double2 c = cadd(v[1], v[3]);
+  double2 d = csub(v[1], v[3]);
+  // i * sign * d
+  double2 isd = make_double2(-sign * d.y, sign * d.x);
+  v[0] = cadd(a, c);
+  v[2] = csub(a, c);
+  v[1] = cadd(b, isd);
+  v[3] = csub(b, isd);
+}
+
+__device__ __forceinline__ void dft8(double2* v, int sign) {
+  const double h = 0.70710678118654752440;  // sqrt(2)/2
+  double2 e[4] = {v[0], v[2], v[4], v[6]};
+  double2 o[4] = {v[1], v[3], v[5], v[7]};
+  dft4(e, sign);
+  dft4(o, sign);
+  // twiddles w8^q = exp(sign * 2 pi i q / 8), q = 0..3
+  double2 t1 = make_double2(h * (o[1].x - sign * o[1].y),
+                            h * (o[1].y + sign * o[1].x));
+  double2 t2 = make_double2(-sign * o[2].y, sign * o[2].x);
+  double2 t3 = make_double2(h * (-o[3].x - sign * o[3].y),
+                            h * (-o[3].y + sign * o[3].x));
+  v[0] = cadd(e[0], o[0]);
+  v[4] = csub(e[0], o[0]);
+  v[1] = cadd(e[1], t1);
+  v[5] = csub(e[1], t1);
+  v[2] = cadd(e[2], t2);
+  v[6] = csub(e[2], t2);
+  v[3] = cadd(e[3], t3);
+  v[7] = csub(e[3], t3);
+}
+
+// One Stockham radix-R stage over C columns stored as buf[t * C + c].
+template <int R>
+__device__ __forceinline__ void fft_stage(const double2* __restrict__ in,
+                                          double2* __restrict__ out, int L,
+                                          int C, int Ns, int sign,
+                                          const double2* __restrict__ tw) {
+  const int nb = L / R;
+  const int step = L / (Ns * R);
+  const int total = nb * C;
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    const int c = idx % C;
+    const int j = idx / C;
+    const int k = j % Ns;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = in[(j + r * nb) * C + c];
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      double2 w = tw[r * k * step];
+      if (sign > 0) w.y = -w.y;
+      v[r] = cmul(v[r], w);
+    }
+    if (R == 2) dft2(v);
+    if (R == 3) dft3(v, sign);
+    if (R == 4) dft4(v, sign);
+    if (R == 8) dft8(v, sign);
+    const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) out[(base + r * Ns) * C + c] = v[r];
+  }
+}
+
+// Transform C columns of length P.L held in a[t * C + c]; b is scratch of
+// the same size.  tw[m] = exp(-2 pi i m / L).  Returns the buffer that
+// holds the result.  Ends with __syncthreads().
+__device__ inline double2* fft_columns(double2* a, double2* b,
+                                       const FFTPlan& P, int C, int sign,
+                                       const double2* tw) {
+  int Ns = 1;
+  double2* in = a;
+  double2* out = b;
+  for (int s = 0; s < P.nst; ++s) {
+    const int R = P.radix[s];
+    switch (R) {
+      case 2: fft_stage<2>(in, out, P.L, C, Ns, sign, tw); break;
+      case 3: fft_stage<3>(in, out, P.L, C, Ns, sign, tw); break;
+      case 4: fft_stage<4>(in, out, P.L, C, Ns, sign, tw); break;
+      default: fft_stage<8>(in, out, P.L, C, Ns, sign, tw); break;
+    }
+    __syncthreads();
+    double2* t = in;
+    in = out;
+    out = t;
+    Ns *= R;
+  }
+  return in;
+}
+
+// Stored index -> padded FFT position for a Nyquist-free complex axis of
+// n-1 stored modes placed in a length-M transform (zeropad_fft /
+// truncate_fft index maps, src/dnsjax/fft.py:41-137).
+__device__ __forceinline__ int stored_to_pos(int s, int nstored, int M) {
+  const int n = nstored + 1;
+  return (s < n / 2) ? s : s + M - n + 1;
+}
+// Padded position -> stored index, or -1 where the padded array is zero.
+__device__ __forceinline__ int pos_to_stored(int t, int nstored, int M) {
+  const int n = nstored + 1;
+  if (t < n / 2) return t;
+  if (t >= M - n / 2 + 1) return t - M + n - 1;
+  return -1;
+}
+
+// Copy a global twiddle table of length L into shared memory.
+__device__ __forceinline__ void load_twiddles(double2* s, const double2* g,
+                                              int L) {
+  for (int i = threadIdx.x; i < L; i += blockDim.x) s[i] = g[i];
+}
+
+}  // namespace dnsb

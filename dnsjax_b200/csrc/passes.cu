@@ -1,0 +1,655 @@
+// Axis-pass kernels of the 3/2-dealiased transforms.
+//
+// Index maps follow the reference's pad/truncate helpers
+// (src/dnsjax/fft.py:41-190) and transform order (fft.py:193-408); the
+// fused products follow src/dnsjax/rhs.py:77-90 (rotational form),
+// src/dnsjax/geometries/triply_periodic.py:122-132 (curl),
+// src/dnsjax/flows/plane_couette.py:251-271 (FD curl) and
+// src/dnsjax/flows/monochromatic.py:366-386 (projection).
+#include "passes.cuh"
+
+namespace dnsb {
+
+FFTPlan make_plan(int L) {
+  FFTPlan P{};
+  P.L = L;
+  P.nst = 0;
+  int n = L;
+  if (L < 1) return P;
+  while (n % 8 == 0 && n != 8 && P.nst < DNSB_MAX_STAGES) {
+    P.radix[P.nst++] = 8;
+    n /= 8;
+  }
+  while (n % 4 == 0 && n > 1 && P.nst < DNSB_MAX_STAGES) {
+    P.radix[P.nst++] = 4;
+    n /= 4;
+  }
+  while (n % 2 == 0 && n > 1 && P.nst < DNSB_MAX_STAGES) {
+    P.radix[P.nst++] = 2;
+    n /= 2;
+  }
+  while (n % 3 == 0 && n > 1 && P.nst < DNSB_MAX_STAGES) {
+    P.radix[P.nst++] = 3;
+    n /= 3;
+  }
+  if (n == 8 && P.nst < DNSB_MAX_STAGES) {
+    P.radix[P.nst++] = 8;
+    n = 1;
+  }
+  if (n != 1) P.nst = 0;
+  return P;
+}
+
+// ---------------------------------------------------------------------------
+// Generic strided column pass.
+// ---------------------------------------------------------------------------
+size_t col_pass_smem(int M) {
+  return sizeof(double2) * (size_t)(2 * M * kTile + M);
+}
+
+__global__ void __launch_bounds__(kPassThreads)
+col_pass_kernel(ColPassArgs a) {
+  extern __shared__ double2 sm[];
+  const int M = a.plan.L;
+  const int C = kTile;
+  double2* bufA = sm;
+  double2* bufB = sm + M * C;
+  double2* tw = sm + 2 * M * C;
+  const int i0 = blockIdx.x * C;
+  const long long o = blockIdx.y;
+  const long long f = blockIdx.z;
+  const double2* in = a.in + f * a.in_fs + o * a.in_os + i0;
+  double2* out = a.out + f * a.out_fs + o * a.out_os + i0;
+  const int ni = min(C, a.nI - i0);
+  load_twiddles(tw, a.tw, M);
+  if (a.inverse) {
+    for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
+      const int c = idx % C, t = idx / C;
+      const int s = pos_to_stored(t, a.nstored, M);
+      double2 v = make_double2(0.0, 0.0);
+      if (s >= 0 && c < ni) v = in[s * a.in_ts + c];
+      bufA[idx] = v;
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
+      const int c = idx % C, t = idx / C;
+      double2 v = make_double2(0.0, 0.0);
+      if (c < ni) v = in[t * a.in_ts + c];
+      bufA[idx] = v;
+    }
+  }
+  __syncthreads();
+  const double2* res = fft_columns(bufA, bufB, a.plan, C, a.inverse ? 1 : -1, tw);
+  if (a.inverse) {
+    for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
+      const int c = idx % C, t = idx / C;
+      if (c < ni) out[t * a.out_ts + c] = res[idx];
+    }
+  } else {
+    const double sc = 1.0 / M;
+    for (int idx = threadIdx.x; idx < a.nstored * C; idx += blockDim.x) {
+      const int c = idx % C, s = idx / C;
+      const int t = stored_to_pos(s, a.nstored, M);
+      if (c < ni) out[s * a.out_ts + c] = cscale(res[t * C + c], sc);
+    }
+  }
+}
+
+cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
+                            cudaStream_t st) {
+  dim3 grid((a.nI + kTile - 1) / kTile, nO, nfields);
+  size_t sm = col_pass_smem(a.plan.L);
+  col_pass_kernel<<<grid, kPassThreads, sm, st>>>(a);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// x pass: two real fields per complex transform (z = a + i b).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ long long row_offset(int r, int inner_n,
+                                                long long so, long long si) {
+  return (long long)(r / inner_n) * so + (long long)(r % inner_n) * si;
+}
+
+size_t x_pass_smem(int Mx) {
+  return sizeof(double2) * (size_t)(2 * Mx * 3 * kXRows + Mx);
+}
+
+__global__ void __launch_bounds__(kPassThreads)
+x_pass_kernel(XPassArgs a) {
+  extern __shared__ double2 sm[];
+  const int M = a.plan.L;
+  const int R = kXRows;
+  const int CI = 3 * R;  // inverse columns
+  const int CF = 2 * R;  // forward columns
+  double2* bufA = sm;
+  double2* bufB = sm + M * CI;
+  double2* tw = sm + 2 * M * CI;
+  const int r0 = blockIdx.x * R;
+  const int nr = min(R, a.nrows - r0);
+  const int nkx = a.nkx;
+  load_twiddles(tw, a.tw, M);
+  // Stage the 6 half spectra: stage[(f * nkx + k) * R + r] in bufB.
+  double2* stage = bufB;
+  const int nload = 6 * nkx * R;
+  for (int idx = threadIdx.x; idx < nload; idx += blockDim.x) {
+    int r, k, f;
+    if (a.rows_fast) {
+      r = idx % R;
+      k = (idx / R) % nkx;
+      f = idx / (R * nkx);
+    } else {
+      k = idx % nkx;
+      r = (idx / nkx) % R;
+      f = idx / (R * nkx);
+    }
+    double2 v = make_double2(0.0, 0.0);
+    if (r < nr) {
+      const long long off = row_offset(r0 + r, a.inner_n, a.so, a.si);
+      v = a.in[f * a.in_fs + off + k * a.ks];
+    }
+    stage[(f * nkx + k) * R + r] = v;
+  }
+  __syncthreads();
+  // Build the 3 complex inputs per row: (u_x,u_y), (u_z,w_x), (w_y,w_z).
+  for (int idx = threadIdx.x; idx < M * CI; idx += blockDim.x) {
+    const int q = idx % CI, t = idx / CI;
+    const int r = q / 3, pr = q % 3;
+    const int fa = 2 * pr, fb = 2 * pr + 1;
+    double2 z = make_double2(0.0, 0.0);
+    if (t == 0) {
+      z = make_double2(stage[(fa * nkx) * R + r].x, stage[(fb * nkx) * R + r].x);
+    } else if (t < nkx) {
+      const double2 A = stage[(fa * nkx + t) * R + r];
+      const double2 B = stage[(fb * nkx + t) * R + r];
+      z = make_double2(A.x - B.y, A.y + B.x);
+    } else if (M - t < nkx) {
+      const int k = M - t;
+      const double2 A = stage[(fa * nkx + k) * R + r];
+      const double2 B = stage[(fb * nkx + k) * R + r];
+      z = make_double2(A.x + B.y, -A.y + B.x);
+    }
+    bufA[idx] = z;
+  }
+  __syncthreads();
+  double2* res = fft_columns(bufA, bufB, a.plan, CI, 1, tw);
+  double2* nl = (res == bufA) ? bufB : bufA;
+  // Rotational nonlinear product at every physical point of the rows.
+  for (int idx = threadIdx.x; idx < M * R; idx += blockDim.x) {
+    const int r = idx % R, t = idx / R;
+    const int row = r0 + r;
+    double2 o0 = make_double2(0.0, 0.0), o1 = make_double2(0.0, 0.0);
+    if (r < nr) {
+      const double2 z0 = res[t * CI + 3 * r + 0];
+      const double2 z1 = res[t * CI + 3 * r + 1];
+      const double2 z2 = res[t * CI + 3 * r + 2];
+      const double u0 = z0.x, u1 = z0.y, u2 = z1.x;
+      const double w0 = z1.y, w1 = z2.x, w2 = z2.y;
+      const int y = a.y_outer ? row / a.inner_n : row % a.inner_n;
+      const int ny = a.ny_grid;
+      const double U0 = a.U[y], U1 = a.U[ny + y], U2 = a.U[2 * ny + y];
+      const double C0 = a.cU[y], C1 = a.cU[ny + y], C2 = a.cU[2 * ny + y];
+      const double N0 = a.nU[y], N1 = a.nU[ny + y], N2 = a.nU[2 * ny + y];
+      // u x w
+      const double n0 = u1 * w2 - u2 * w1;
+      const double n1 = u2 * w0 - u0 * w2;
+      const double n2 = u0 * w1 - u1 * w0;
+      // u x curl U + U x w + U x curl U
+      const double b0 = (u1 * C2 - u2 * C1) + (U1 * w2 - U2 * w1) + N0;
+      const double b1 = (u2 * C0 - u0 * C2) + (U2 * w0 - U0 * w2) + N1;
+      const double b2 = (u0 * C1 - u1 * C0) + (U0 * w1 - U1 * w0) + N2;
+      o0 = make_double2(n0 + b0, n1 + b1);
+      o1 = make_double2(n2 + b2, 0.0);
+    }
+    nl[t * CF + 2 * r + 0] = o0;
+    nl[t * CF + 2 * r + 1] = o1;
+  }
+  __syncthreads();
+  double2* other = (nl == bufA) ? bufB : bufA;
+  double2* fres = fft_columns(nl, other, a.plan, CF, -1, tw);
+  // Unpack the real-field spectra, truncate to nkx, scale 1/M, store.
+  const double h = 0.5 / M;
+  const int nst = 3 * nkx * R;
+  for (int idx = threadIdx.x; idx < nst; idx += blockDim.x) {
+    int r, k, f;
+    if (a.rows_fast) {
+      r = idx % R;
+      k = (idx / R) % nkx;
+      f = idx / (R * nkx);
+    } else {
+      k = idx % nkx;
+      r = (idx / nkx) % R;
+      f = idx / (R * nkx);
+    }
+    if (r >= nr) continue;
+    const int col = 2 * r + (f == 2 ? 1 : 0);
+    const double2 Z = fres[k * CF + col];
+    const double2 Zm = fres[((M - k) % M) * CF + col];
+    double2 v;
+    if (f == 1) {
+      v = make_double2((Z.y + Zm.y) * h, (Zm.x - Z.x) * h);
+    } else {
+      v = make_double2((Z.x + Zm.x) * h, (Z.y - Zm.y) * h);
+    }
+    const long long off = row_offset(r0 + r, a.inner_n, a.so, a.si);
+    a.out[f * a.out_fs + off + k * a.ks] = v;
+  }
+}
+
+cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
+  dim3 grid((a.nrows + kXRows - 1) / kXRows);
+  x_pass_kernel<<<grid, kPassThreads, x_pass_smem(a.plan.L), st>>>(a);
+  return cudaGetLastError();
+}
+
+// x pass to physical values only (spec_to_phys of 3 fields).
+size_t x_phys_smem(int Mx) {
+  return sizeof(double2) * (size_t)(2 * Mx * 2 * kXRows + Mx);
+}
+
+__global__ void __launch_bounds__(kPassThreads)
+x_phys_kernel(XPhysArgs a) {
+  extern __shared__ double2 sm[];
+  const int M = a.plan.L;
+  const int R = kXRows;
+  const int CI = 2 * R;
+  double2* bufA = sm;
+  double2* bufB = sm + M * CI;
+  double2* tw = sm + 2 * M * CI;
+  const int r0 = blockIdx.x * R;
+  const int nr = min(R, a.nrows - r0);
+  const int nkx = a.nkx;
+  load_twiddles(tw, a.tw, M);
+  double2* stage = bufB;
+  for (int idx = threadIdx.x; idx < 3 * nkx * R; idx += blockDim.x) {
+    int r, k, f;
+    if (a.rows_fast) {
+      r = idx % R;
+      k = (idx / R) % nkx;
+      f = idx / (R * nkx);
+    } else {
+      k = idx % nkx;
+      r = (idx / nkx) % R;
+      f = idx / (R * nkx);
+    }
+    double2 v = make_double2(0.0, 0.0);
+    if (r < nr) {
+      const long long off = row_offset(r0 + r, a.inner_n, a.so, a.si);
+      v = a.in[f * a.in_fs + off + k * a.ks];
+    }
+    stage[(f * nkx + k) * R + r] = v;
+  }
+  // Zero partner of the third field lives past the staged block.
+  double2* zeros = stage + 3 * nkx * R;
+  for (int idx = threadIdx.x; idx < nkx * R; idx += blockDim.x)
+    zeros[idx] = make_double2(0.0, 0.0);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < M * CI; idx += blockDim.x) {
+    const int q = idx % CI, t = idx / CI;
+    const int r = q / 2, pr = q % 2;
+    const double2* A = stage + ((2 * pr) * nkx) * R + r;
+    const double2* B = (pr == 0) ? stage + (1 * nkx) * R + r : zeros + r;
+    double2 z = make_double2(0.0, 0.0);
+    if (t == 0) {
+      z = make_double2(A[0].x, B[0].x);
+    } else if (t < nkx) {
+      const double2 Av = A[t * R], Bv = B[t * R];
+      z = make_double2(Av.x - Bv.y, Av.y + Bv.x);
+    } else if (M - t < nkx) {
+      const int k = M - t;
+      const double2 Av = A[k * R], Bv = B[k * R];
+      z = make_double2(Av.x + Bv.y, -Av.y + Bv.x);
+    }
+    bufA[idx] = z;
+  }
+  __syncthreads();
+  const double2* res = fft_columns(bufA, bufB, a.plan, CI, 1, tw);
+  for (int idx = threadIdx.x; idx < M * R * 3; idx += blockDim.x) {
+    const int t = idx % M;
+    const int r = (idx / M) % R;
+    const int f = idx / (M * R);
+    if (r >= nr) continue;
+    const double2 z = res[t * CI + 2 * r + (f == 2 ? 1 : 0)];
+    const double v = (f == 1) ? z.y : z.x;
+    const long long off = row_offset(r0 + r, a.inner_n, a.pso, a.psi);
+    a.out[f * a.out_fs + off + t] = v;
+  }
+}
+
+cudaError_t launch_x_phys(const XPhysArgs& a, cudaStream_t st) {
+  dim3 grid((a.nrows + kXRows - 1) / kXRows);
+  x_phys_kernel<<<grid, kPassThreads, x_phys_smem(a.plan.L), st>>>(a);
+  return cudaGetLastError();
+}
+
+// Forward x pass from physical values (phys_to_spec of 3 fields): rows of
+// real samples at outer*pso + inner*psi -> x half spectra at outer*so +
+// inner*si, kx modes ks apart, truncated to nkx, scaled 1/Mx.
+__global__ void __launch_bounds__(kPassThreads)
+x_fwd_kernel(XPhysArgs a, const double* phys, double2* spec) {
+  extern __shared__ double2 sm[];
+  const int M = a.plan.L;
+  const int R = kXRows;
+  const int CF = 2 * R;
+  double2* bufA = sm;
+  double2* bufB = sm + M * CF;
+  double2* tw = sm + 2 * M * CF;
+  const int r0 = blockIdx.x * R;
+  const int nr = min(R, a.nrows - r0);
+  const int nkx = a.nkx;
+  load_twiddles(tw, a.tw, M);
+  for (int idx = threadIdx.x; idx < M * CF; idx += blockDim.x) {
+    const int t = idx % M;
+    const int q = idx / M;
+    const int r = q / 2, pr = q % 2;
+    double re = 0.0, im = 0.0;
+    if (r < nr) {
+      const long long off = row_offset(r0 + r, a.inner_n, a.pso, a.psi);
+      if (pr == 0) {
+        re = phys[0 * a.out_fs + off + t];
+        im = phys[1 * a.out_fs + off + t];
+      } else {
+        re = phys[2 * a.out_fs + off + t];
+      }
+    }
+    bufA[t * CF + q] = make_double2(re, im);
+  }
+  __syncthreads();
+  const double2* fres = fft_columns(bufA, bufB, a.plan, CF, -1, tw);
+  const double h = 0.5 / M;
+  for (int idx = threadIdx.x; idx < 3 * nkx * R; idx += blockDim.x) {
+    int r, k, f;
+    if (a.rows_fast) {
+      r = idx % R;
+      k = (idx / R) % nkx;
+      f = idx / (R * nkx);
+    } else {
+      k = idx % nkx;
+      r = (idx / nkx) % R;
+      f = idx / (R * nkx);
+    }
+    if (r >= nr) continue;
+    const int col = 2 * r + (f == 2 ? 1 : 0);
+    const double2 Z = fres[k * CF + col];
+    const double2 Zm = fres[((M - k) % M) * CF + col];
+    double2 v;
+    if (f == 1) {
+      v = make_double2((Z.y + Zm.y) * h, (Zm.x - Z.x) * h);
+    } else {
+      v = make_double2((Z.x + Zm.x) * h, (Z.y - Zm.y) * h);
+    }
+    const long long off = row_offset(r0 + r, a.inner_n, a.so, a.si);
+    spec[f * a.in_fs + off + k * a.ks] = v;
+  }
+}
+
+size_t x_fwd_smem(int Mx) {
+  return sizeof(double2) * (size_t)(2 * Mx * 2 * kXRows + Mx);
+}
+
+cudaError_t launch_x_fwd(const XPhysArgs& a, const double* phys, double2* spec,
+                         cudaStream_t st) {
+  dim3 grid((a.nrows + kXRows - 1) / kXRows);
+  x_fwd_kernel<<<grid, kPassThreads, x_fwd_smem(a.plan.L), st>>>(a, phys, spec);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Periodic first inverse pass (y) with the spectral curl fused.
+// ---------------------------------------------------------------------------
+size_t yinv_smem(int My, int NY1) {
+  return sizeof(double2) * (size_t)(3 * NY1 * kTile + 2 * My * kTile + My);
+}
+
+__global__ void __launch_bounds__(kPassThreads)
+yinv_kernel(YInvArgs a) {
+  extern __shared__ double2 sm[];
+  const int M = a.plan.L;
+  const int C = kTile;
+  const int NY1 = a.NY1, NZ1 = a.NZ1, NKX = a.NKX;
+  double2* su = sm;                       // [3][NY1][C]
+  double2* bufA = su + 3 * NY1 * C;
+  double2* bufB = bufA + M * C;
+  double2* tw = bufB + M * C;
+  const int i0 = blockIdx.x * C;
+  const int iz = blockIdx.y;
+  const int ni = min(C, NKX - i0);
+  const long long cs = (long long)NY1 * NZ1 * NKX;
+  load_twiddles(tw, a.tw, M);
+  for (int idx = threadIdx.x; idx < 3 * NY1 * C; idx += blockDim.x) {
+    const int c = idx % C, s = (idx / C) % NY1, comp = idx / (C * NY1);
+    double2 v = make_double2(0.0, 0.0);
+    if (c < ni) v = a.u[comp * cs + ((long long)s * NZ1 + iz) * NKX + i0 + c];
+    su[idx] = v;
+  }
+  __syncthreads();
+  const double kz = a.kz[iz];
+  const int nf = a.curl ? 6 : 3;
+  const long long fs = (long long)M * NZ1 * NKX;
+  for (int f = 0; f < nf; ++f) {
+    for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
+      const int c = idx % C, t = idx / C;
+      const int s = pos_to_stored(t, NY1, M);
+      double2 v = make_double2(0.0, 0.0);
+      if (s >= 0 && c < ni) {
+        const double2 u = su[(0 * NY1 + s) * C + c];
+        const double2 vv = su[(1 * NY1 + s) * C + c];
+        const double2 w = su[(2 * NY1 + s) * C + c];
+        const double kx = a.kx[i0 + c], ky = a.ky[s];
+        switch (f) {
+          case 0: v = u; break;
+          case 1: v = vv; break;
+          case 2: v = w; break;
+          // curl = 1j * (k x u), triply_periodic.py:122-132
+          case 3: v = ci(make_double2(ky * w.x - kz * vv.x, ky * w.y - kz * vv.y)); break;
+          case 4: v = ci(make_double2(kz * u.x - kx * w.x, kz * u.y - kx * w.y)); break;
+          default: v = ci(make_double2(kx * vv.x - ky * u.x, kx * vv.y - ky * u.y)); break;
+        }
+      }
+      bufA[idx] = v;
+    }
+    __syncthreads();
+    const double2* res = fft_columns(bufA, bufB, a.plan, C, 1, tw);
+    double2* out = a.out + f * fs + (long long)iz * NKX + i0;
+    for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
+      const int c = idx % C, t = idx / C;
+      if (c < ni) out[(long long)t * NZ1 * NKX + c] = res[idx];
+    }
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_yinv(const YInvArgs& a, cudaStream_t st) {
+  dim3 grid((a.NKX + kTile - 1) / kTile, a.NZ1);
+  yinv_kernel<<<grid, kPassThreads, yinv_smem(a.plan.L, a.NY1), st>>>(a);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Periodic last forward pass (y) with the pressure projection fused.
+// ---------------------------------------------------------------------------
+size_t yfwd_smem(int My, int NY1) {
+  return sizeof(double2) * (size_t)(3 * NY1 * kTile + 2 * My * kTile + My);
+}
+
+__global__ void __launch_bounds__(kPassThreads)
+yfwd_kernel(YFwdArgs a) {
+  extern __shared__ double2 sm[];
+  const int M = a.plan.L;
+  const int C = kTile;
+  const int NY1 = a.NY1, NZ1 = a.NZ1, NKX = a.NKX;
+  double2* snl = sm;  // [3][NY1][C]
+  double2* bufA = snl + 3 * NY1 * C;
+  double2* bufB = bufA + M * C;
+  double2* tw = bufB + M * C;
+  const int i0 = blockIdx.x * C;
+  const int iz = blockIdx.y;
+  const int ni = min(C, NKX - i0);
+  load_twiddles(tw, a.tw, M);
+  const long long fs = (long long)M * NZ1 * NKX;
+  const double sc = 1.0 / M;
+  for (int f = 0; f < 3; ++f) {
+    const double2* in = a.in + f * fs + (long long)iz * NKX + i0;
+    for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
+      const int c = idx % C, t = idx / C;
+      double2 v = make_double2(0.0, 0.0);
+      if (c < ni) v = in[(long long)t * NZ1 * NKX + c];
+      bufA[idx] = v;
+    }
+    __syncthreads();
+    const double2* res = fft_columns(bufA, bufB, a.plan, C, -1, tw);
+    for (int idx = threadIdx.x; idx < NY1 * C; idx += blockDim.x) {
+      const int c = idx % C, s = idx / C;
+      const int t = stored_to_pos(s, NY1, M);
+      snl[(f * NY1 + s) * C + c] = cscale(res[t * C + c], sc);
+    }
+    __syncthreads();
+  }
+  const long long cs = (long long)NY1 * NZ1 * NKX;
+  const double kz = a.kz[iz];
+  for (int idx = threadIdx.x; idx < NY1 * C; idx += blockDim.x) {
+    const int c = idx % C, s = idx / C;
+    if (c >= ni) continue;
+    const double2 n0 = snl[(0 * NY1 + s) * C + c];
+    const double2 n1 = snl[(1 * NY1 + s) * C + c];
+    const double2 n2 = snl[(2 * NY1 + s) * C + c];
+    const long long off = ((long long)s * NZ1 + iz) * NKX + i0 + c;
+    double2 r0 = n0, r1 = n1, r2 = n2;
+    if (a.project) {
+      const double kx = a.kx[i0 + c], ky = a.ky[s];
+      // NL - grad(inv_lapl * div NL), monochromatic.py:377-385
+      const double2 div = cadd(cadd(cik(kx, n0), cik(ky, n1)), cik(kz, n2));
+      const double il = a.inv_lapl[off];
+      const double2 p = cscale(div, il);
+      r0 = csub(n0, cik(kx, p));
+      r1 = csub(n1, cik(ky, p));
+      r2 = csub(n2, cik(kz, p));
+    }
+    a.out[off] = r0;
+    a.out[cs + off] = r1;
+    a.out[2 * cs + off] = r2;
+  }
+}
+
+cudaError_t launch_yfwd(const YFwdArgs& a, cudaStream_t st) {
+  dim3 grid((a.NKX + kTile - 1) / kTile, a.NZ1);
+  yfwd_kernel<<<grid, kPassThreads, yfwd_smem(a.plan.L, a.NY1), st>>>(a);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Couette first inverse pass (z) with the FD curl fused.
+// ---------------------------------------------------------------------------
+size_t zinv_curl_smem(int Mz, int NZ1, int span_max) {
+  return sizeof(double2) *
+         (size_t)(3 * NZ1 * span_max + 2 * Mz * kZTile + Mz);
+}
+
+__global__ void __launch_bounds__(kPassThreads)
+zinv_curl_kernel(ZInvCurlArgs a, int span_max) {
+  extern __shared__ double2 sm[];
+  const int M = a.plan.L;
+  const int C = kZTile;
+  const int NZ1 = a.NZ1, NKX = a.NKX, Ny = a.Ny;
+  double2* tile = sm;  // [3][NZ1][span_max]
+  double2* bufA = tile + 3 * NZ1 * span_max;
+  double2* bufB = bufA + M * C;
+  double2* tw = bufB + M * C;
+  const int y0 = blockIdx.x * C;
+  const int ix = blockIdx.y;
+  const int y1 = min(y0 + C, Ny);
+  int ylo = y0, yhi = y1;
+  if (a.curl) {
+    ylo = min(ylo, a.d1_j0[y0]);
+    yhi = max(yhi, a.d1_j0[y1 - 1] + a.s1);
+  }
+  const int span = yhi - ylo;  // <= span_max by construction on the host
+  const long long cs = (long long)NZ1 * NKX * Ny;
+  load_twiddles(tw, a.tw, M);
+  for (int idx = threadIdx.x; idx < 3 * NZ1 * span; idx += blockDim.x) {
+    const int yy = idx % span, s = (idx / span) % NZ1, comp = idx / (span * NZ1);
+    tile[(comp * NZ1 + s) * span_max + yy] =
+        a.u[comp * cs + ((long long)s * NKX + ix) * Ny + ylo + yy];
+  }
+  __syncthreads();
+  const double kx = a.kx[ix];
+  const int nf = a.curl ? 6 : 3;
+  const long long fs = (long long)M * NKX * Ny;
+  for (int f = 0; f < nf; ++f) {
+    for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
+      const int c = idx % C, t = idx / C;
+      const int s = pos_to_stored(t, NZ1, M);
+      const int y = y0 + c;
+      double2 v = make_double2(0.0, 0.0);
+      if (s >= 0 && y < y1) {
+        // Rows of the staged tile; index with (y - ylo).
+        const double2* tu = tile + (0 * NZ1 + s) * span_max;
+        const double2* tv = tile + (1 * NZ1 + s) * span_max;
+        const double2* tw_ = tile + (2 * NZ1 + s) * span_max;
+        const int yl = y - ylo;
+        const double kz = a.kz[s];
+        switch (f) {
+          case 0: v = tu[yl]; break;
+          case 1: v = tv[yl]; break;
+          case 2: v = tw_[yl]; break;
+          case 3: {  // dy_w - dz_v
+            const int j0 = a.d1_j0[y];
+            const double* w = a.d1_w + (long long)y * a.s1;
+            double2 d = make_double2(0.0, 0.0);
+            for (int m = 0; m < a.s1; ++m) {
+              d.x += w[m] * tw_[j0 - ylo + m].x;
+              d.y += w[m] * tw_[j0 - ylo + m].y;
+            }
+            v = csub(d, cik(kz, tv[yl]));
+          } break;
+          case 4:  // dz_u - dx_w
+            v = csub(cik(kz, tu[yl]), cik(kx, tw_[yl]));
+            break;
+          default: {  // dx_v - dy_u
+            const int j0 = a.d1_j0[y];
+            const double* w = a.d1_w + (long long)y * a.s1;
+            double2 d = make_double2(0.0, 0.0);
+            for (int m = 0; m < a.s1; ++m) {
+              d.x += w[m] * tu[j0 - ylo + m].x;
+              d.y += w[m] * tu[j0 - ylo + m].y;
+            }
+            v = csub(cik(kx, tv[yl]), d);
+          } break;
+        }
+      }
+      bufA[idx] = v;
+    }
+    __syncthreads();
+    const double2* res = fft_columns(bufA, bufB, a.plan, C, 1, tw);
+    double2* out = a.out + f * fs + (long long)ix * Ny + y0;
+    for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
+      const int c = idx % C, t = idx / C;
+      if (y0 + c < y1) out[(long long)t * NKX * Ny + c] = res[idx];
+    }
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_zinv_curl(const ZInvCurlArgs& a, int span_max,
+                             cudaStream_t st) {
+  dim3 grid((a.Ny + kZTile - 1) / kZTile, a.NKX);
+  zinv_curl_kernel<<<grid, kPassThreads, zinv_curl_smem(a.plan.L, a.NZ1, span_max),
+                     st>>>(a, span_max);
+  return cudaGetLastError();
+}
+
+cudaError_t set_pass_attributes(int max_smem) {
+  cudaError_t e = cudaSuccess;
+  const void* fns[] = {(const void*)col_pass_kernel, (const void*)x_pass_kernel,
+                       (const void*)x_phys_kernel, (const void*)x_fwd_kernel,
+                       (const void*)yinv_kernel, (const void*)yfwd_kernel,
+                       (const void*)zinv_curl_kernel};
+  for (const void* f : fns) {
+    cudaError_t r = cudaFuncSetAttribute(
+        f, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+    if (r != cudaSuccess) e = r;
+  }
+  return e;
+}
+
+}  // namespace dnsb

@@ -1,0 +1,136 @@
+// Axis-pass kernels of the dealiased transforms (declarations + arg blocks).
+//
+// A 3/2-dealiased transform is a sequence of axis passes; each pass reads
+// one layout from HBM, transforms a tile of columns in shared memory and
+// writes the next layout.  Zero-padding (inverse) and truncation (forward)
+// happen on load/store, and the curl, the rotational nonlinear product and
+// the pressure projection are fused into the passes that already hold the
+// data they need.
+#pragma once
+
+#include "common.cuh"
+
+namespace dnsb {
+
+constexpr int kTile = 8;     // columns per CTA in the column passes
+constexpr int kXRows = 4;    // physical rows per CTA in the x pass
+constexpr int kPassThreads = 256;
+
+// Generic strided column pass: element (f, o, t, i) at
+// base + f*fs + o*os + t*ts + i, with i the contiguous inner index.
+struct ColPassArgs {
+  const double2* in;
+  double2* out;
+  long long in_fs, out_fs, in_os, out_os, in_ts, out_ts;
+  int nI;        // inner extent
+  int nstored;   // stored (Nyquist-free) modes on the spectral side
+  int inverse;   // 1: spectral -> padded, inverse FFT; 0: forward, truncate
+  FFTPlan plan;  // transform length M = plan.L
+  const double2* tw;
+};
+
+// x pass.  Rows are (outer, inner) pairs; row r = outer * inner_n + inner
+// starts at outer*so + inner*si and its kx modes are ks apart.
+struct XPassArgs {
+  const double2* in;   // 6 fields (u, omega) of x-half-spectra
+  double2* out;        // 3 fields of the forward x-transformed product
+  long long in_fs, out_fs;
+  int nrows, inner_n;
+  long long so, si, ks;
+  int nkx;             // stored kx modes (nx/2)
+  int y_outer;         // y index = outer (1) or inner (0)
+  int rows_fast;       // load mapping: rows contiguous (1) or kx (0)
+  const double* U;     // base flow [3][ny_grid]
+  const double* cU;    // curl of base flow
+  const double* nU;    // U x curl U
+  int ny_grid;
+  FFTPlan plan;        // Mx
+  const double2* tw;
+};
+
+// x pass to physical space only (3 fields -> real [c] at row offsets
+// outer*pso + inner*psi, x contiguous).
+struct XPhysArgs {
+  const double2* in;
+  double* out;
+  long long in_fs, out_fs;
+  int nrows, inner_n;
+  long long so, si, ks, pso, psi;
+  int nkx;
+  int rows_fast;
+  FFTPlan plan;
+  const double2* tw;
+};
+
+// Periodic first inverse pass (y), curl fused: spectral u [3][NY1][NZ1][NKX]
+// -> 6 (or 3) fields [f][My][NZ1][NKX].
+struct YInvArgs {
+  const double2* u;
+  double2* out;
+  int NY1, NZ1, NKX;
+  int curl;
+  const double* kx;
+  const double* ky;
+  const double* kz;
+  FFTPlan plan;
+  const double2* tw;
+};
+
+// Periodic last forward pass (y), projection fused: [3][My][NZ1][NKX] ->
+// spectral [3][NY1][NZ1][NKX].
+struct YFwdArgs {
+  const double2* in;
+  double2* out;
+  int NY1, NZ1, NKX;
+  int project;
+  const double* kx;
+  const double* ky;
+  const double* kz;
+  const double* inv_lapl;  // [NY1][NZ1][NKX]
+  FFTPlan plan;
+  const double2* tw;
+};
+
+// Couette first inverse pass (z), FD curl fused: spectral
+// [3][NZ1][NKX][Ny] -> 6 (or 3) fields [f][Mz][NKX][Ny].
+struct ZInvCurlArgs {
+  const double2* u;
+  double2* out;
+  int NZ1, NKX, Ny;
+  int curl;
+  int s1;              // D1 stencil width (p + 1)
+  const int* d1_j0;    // [Ny]
+  const double* d1_w;  // [Ny][s1]
+  const double* kx;
+  const double* kz;
+  FFTPlan plan;
+  const double2* tw;
+};
+
+constexpr int kZTile = 8;  // y values per CTA in the Couette z passes
+
+size_t col_pass_smem(int M);
+size_t x_pass_smem(int Mx);
+size_t x_phys_smem(int Mx);
+size_t yinv_smem(int My, int NY1);
+size_t yfwd_smem(int My, int NY1);
+size_t zinv_curl_smem(int Mz, int NZ1, int span_max);
+
+cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
+                            cudaStream_t st);
+cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st);
+cudaError_t launch_x_phys(const XPhysArgs& a, cudaStream_t st);
+// Forward x pass from physical rows (uses XPhysArgs with in_fs = spectral
+// field stride, out_fs = physical field stride).
+cudaError_t launch_x_fwd(const XPhysArgs& a, const double* phys, double2* spec,
+                         cudaStream_t st);
+size_t x_fwd_smem(int Mx);
+cudaError_t set_pass_attributes(int max_smem);
+cudaError_t launch_yinv(const YInvArgs& a, cudaStream_t st);
+cudaError_t launch_yfwd(const YFwdArgs& a, cudaStream_t st);
+cudaError_t launch_zinv_curl(const ZInvCurlArgs& a, int span_max,
+                             cudaStream_t st);
+
+FFTPlan make_plan(int L);  // host; L.nst == 0 when L is not 2^a 3^b
+
+}  // namespace dnsb

@@ -1,0 +1,98 @@
+// Per-mode solves and pointwise kernels of the time step.
+#pragma once
+
+#include "common.cuh"
+
+namespace dnsb {
+
+// ---- deterministic reductions --------------------------------------------
+constexpr int kRedThreads = 256;
+constexpr int kRedBlocks = 592;  // 4 x 148 SMs; fixed so sums are reproducible
+
+// out[0] = scale * sum(partials[0..n)), sqrt'ed if do_sqrt.
+cudaError_t launch_finalize(const double* partials, int n, double* out,
+                            double scale, int do_sqrt, cudaStream_t st);
+
+// ---- periodic pointwise ----------------------------------------------------
+struct PeriodicPointArgs {
+  int S;  // scalar spectral size (ny-1)(nz-1)(nx/2)
+  int NY1, NZ1, NKX;
+  const double* ldt_1;
+  const double* ildt_2;
+  const double* kx;
+  const double* ky;
+  const double* kz;
+  const double* inv_lapl;
+  const double* lapl;
+  double c;
+};
+
+cudaError_t launch_periodic_predict(const PeriodicPointArgs& a,
+                                    const double2* state, const double2* rhs,
+                                    double2* out, cudaStream_t st);
+// pred_out = pred + c (next - prev) ildt_2; partials of k_metric |corr|^2.
+cudaError_t launch_periodic_correct(const PeriodicPointArgs& a,
+                                    const double2* pred,
+                                    const double2* rhs_prev,
+                                    const double2* rhs_next, double2* pred_out,
+                                    double2* corr_out, double* partials,
+                                    cudaStream_t st);
+cudaError_t launch_periodic_norm2(const PeriodicPointArgs& a,
+                                  const double2* v, double* partials,
+                                  cudaStream_t st);
+cudaError_t launch_periodic_correct_velocity(const PeriodicPointArgs& a,
+                                             const double2* in, double2* out,
+                                             int divergence, cudaStream_t st);
+// partials[0..kRedBlocks) of k_metric|u|^2, partials[kRedBlocks..2 kRedBlocks)
+// of -lapl |u|^2.
+cudaError_t launch_periodic_stats(const PeriodicPointArgs& a,
+                                  const double2* v, double* partials,
+                                  cudaStream_t st);
+
+// ---- plane Couette ---------------------------------------------------------
+struct ImmArgs {
+  int NZ1, NKX, Ny, kl, ku;
+  int s1, s2;             // D1 / D2 stencil widths (p+1, p+2)
+  const int* d1_j0;       // [Ny]
+  const double* d1_w;     // [Ny][s1]
+  const int* d2_j0;       // [Ny]
+  const double* d2_w;     // [Ny][s2]
+  const double* kx;       // [NKX]
+  const double* kz;       // [NZ1]
+  const double* simpson;  // [Ny] Simpson weights (norm)
+  double dt, c, nu;
+  // IMM operators, reference layouts (cartesian.py:575-801)
+  const double* Lk_ab;    // [NZ1][NKX][2kl+ku+1][Ny]
+  const int* Lk_piv;      // [NZ1][NKX][Ny]
+  const double* Hk_ab;
+  const int* Hk_piv;
+  const double* v1;       // [NZ1][NKX][Ny]
+  const double* v2;
+  const double* q1;
+  const double* q2;
+  const double* M_inv;    // [NZ1][NKX][2][2]
+  int* status;            // set nonzero on a pivot index out of range
+};
+
+constexpr int kImmWarps = 4;  // modes per CTA (one warp each)
+
+// vel_new = IMM(vel_n, vel_j, nl_n, nl_j); partials[mode] gets the
+// Simpson-weighted k_metric |vel_new - vel_j|^2 of the mode when partials
+// is non-null; corr_out (nullable) receives vel_new - vel_j.
+cudaError_t launch_imm(const ImmArgs& a, const double2* vel_n,
+                       const double2* vel_j, const double2* nl_n,
+                       const double2* nl_j, double2* vel_new,
+                       double2* corr_out, double* partials, cudaStream_t st);
+size_t imm_smem(int Ny);
+cudaError_t set_solver_attributes(int max_smem);
+
+// Simpson-weighted k_metric |v|^2 per block (Couette norm).
+cudaError_t launch_couette_norm2(const ImmArgs& a, const double2* v,
+                                 double* partials, cudaStream_t st);
+
+// ---- standalone per-mode banded solve (PerModeBandedOperator.solve) -------
+cudaError_t launch_banded_solve(const double* ab, const int* ipiv, double* b,
+                                int nmodes, int ny, int kl, int ku,
+                                int ncols, int* status, cudaStream_t st);
+
+}  // namespace dnsb

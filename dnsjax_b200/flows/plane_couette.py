@@ -1,0 +1,246 @@
+"""Plane Couette flow on the GPU: the reference's flow interface over libdnsb.
+
+Mirrors src/dnsjax/flows/plane_couette.py.  ``PlaneCouetteFlow`` holds the
+host-side setup (CGL grid, base flow ``U = y``, FD stencils, IMM operators)
+and a ``dnsb_couette`` context; its methods are the four stepper callables
+(``get_rhs``, ``predict``, ``correct``, ``norm``), ``correct_velocity``
+(the identity, plane_couette.py:575-582), ``get_stats`` (E', :591-613),
+``init_state`` and the 2D transforms.  All arithmetic on the state runs in
+the CUDA kernels; tensors are complex128 in the ``(3, nz-1, nx//2, ny)``
+``[kz, kx, y]`` layout.
+
+Module-level ``predict_and_correct`` / ``iterate_correction`` /
+``correct_velocity`` / ``get_stats`` / ``init_state`` act on a flow built
+from the global ``params`` on first use, like the reference's import-time
+singletons.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from .. import _lib
+from ..fd import build_diff_matrices, cgl_grid, diff_bands
+from ..geometries.cartesian import Fourier, precompute_imm, simpson_weights
+from ..parameters import Parameters, derive, padded_sizes
+from ..timestep import make_fused_stepper, make_stepper
+
+
+class PlaneCouetteFlow:
+    def __init__(self, p: Parameters, imm: dict | None = None, ly: float | None = None):
+        import torch
+
+        L = _lib.lib()
+        self.params = p
+        d = derive(p)
+        self.ly = float(d.ly if ly is None else ly)
+        r = p.res
+        if p.res.double_precision is False:
+            raise NotImplementedError("the plain form computes in FP64")
+        self.nx, self.ny, self.nz = r.nx, r.ny, r.nz
+        self.nx_p, _, self.nz_p = padded_sizes(p)
+        self.p = r.fd_order
+        self.dt = p.step.dt
+        self.c = p.step.implicitness
+        self.nu = 1.0 / p.phys.re
+        self.fourier = Fourier.build(r.nx, r.nz, p.geo.lx, p.geo.lz)
+        self.ys = cgl_grid(r.ny)
+        self.D1, self.D2 = build_diff_matrices(self.ys, self.p)
+        j01, w1, j02, w2 = diff_bands(self.ys, self.p)
+        ny = r.ny
+        U = np.zeros((3, ny))
+        U[0] = self.ys
+        cU = np.zeros((3, ny))
+        cU[2] = -1.0
+        nU = np.zeros((3, ny))
+        nU[1] = self.ys * 1.0
+        self.base_flow, self.curl_base_flow, self.nonlin_base_flow = U, cU, nU
+        self.spec_shape = (3, r.nz - 1, r.nx // 2, ny)
+        self.phys_shape = (3, ny, self.nz_p, self.nx_p)
+        self.simpson = simpson_weights(self.ys)
+
+        f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+        i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)  # noqa: E731
+        # host arrays stay referenced by `hold` until create() has copied them
+        hold = dict(kx=f64(self.fourier.kx_global), kz=f64(self.fourier.kz_global),
+                    ys=f64(self.ys), j01=i32(j01), w1=f64(w1), j02=i32(j02),
+                    w2=f64(w2), U=f64(U), cU=f64(cU), nU=f64(nU))
+        c_d = _lib.as_c
+        desc = _lib.CouetteDesc(
+            r.nx, ny, r.nz, self.nx_p, self.nz_p, self.p,
+            self.dt, self.c, self.nu, self.ly,
+            c_d(hold["kx"]), c_d(hold["kz"]), c_d(hold["ys"]),
+            c_d(hold["j01"], _lib.C.c_int), c_d(hold["w1"]),
+            c_d(hold["j02"], _lib.C.c_int), c_d(hold["w2"]),
+            c_d(hold["U"]), c_d(hold["cU"]), c_d(hold["nU"]))
+        h = _lib.C.c_void_p()
+        _lib.check(L.dnsb_couette_create(_lib.C.byref(desc), _lib.C.byref(h)))
+        self._ctx = h
+        self._L = L
+
+        if imm is None:
+            imm = precompute_imm(self.ys, self.fourier.kx_global,
+                                 self.fourier.kz_global, self.p, self.dt,
+                                 self.c, self.nu, self.D1, self.D2)
+        dev = {}
+        for k in ("Lk_ab", "Hk_ab", "v1", "v2", "q1", "q2", "M_inv", "p1", "p2"):
+            dev[k] = torch.as_tensor(np.ascontiguousarray(imm[k], np.float64),
+                                     device="cuda")
+        for k in ("Lk_piv", "Hk_piv"):
+            dev[k] = torch.as_tensor(np.ascontiguousarray(imm[k], np.int32),
+                                     device="cuda")
+        self.imm = dev
+        ops = _lib.ImmOps(*[_lib.ptr(dev[k]) for k in (
+            "Lk_ab", "Lk_piv", "Hk_ab", "Hk_piv", "v1", "v2", "q1", "q2", "M_inv")])
+        _lib.check(L.dnsb_couette_bind_imm(self._ctx, _lib.C.byref(ops)))
+        self._scratch = torch.empty(2, dtype=torch.float64, device="cuda")
+
+    def __del__(self):
+        ctx = getattr(self, "_ctx", None)
+        if ctx is not None and ctx.value:
+            self._L.dnsb_couette_destroy(ctx)
+            self._ctx = None
+
+    # -- helpers ------------------------------------------------------------
+    def _new(self):
+        import torch
+
+        return torch.empty(self.spec_shape, dtype=torch.complex128, device="cuda")
+
+    def _check(self, t):
+        if tuple(t.shape) != self.spec_shape:
+            raise ValueError(f"expected shape {self.spec_shape}, got {tuple(t.shape)}")
+        if str(t.dtype) != "torch.complex128":
+            raise ValueError("expected complex128")
+        return _lib.ptr(t)
+
+    # -- stepper callables (plane_couette.py:274-549) -------------------------
+    def get_rhs(self, state, out=None):
+        out = self._new() if out is None else out
+        _lib.check(self._L.dnsb_couette_rhs(
+            self._ctx, self._check(state), self._check(out), _lib.stream_handle()))
+        return out
+
+    def imm_iteration(self, vel_n, vel_j, nl_n, nl_j, out=None, corr=None,
+                      err=None):
+        out = self._new() if out is None else out
+        _lib.check(self._L.dnsb_couette_imm(
+            self._ctx, self._check(vel_n), self._check(vel_j), self._check(nl_n),
+            self._check(nl_j), self._check(out),
+            None if corr is None else self._check(corr),
+            None if err is None else _lib.ptr(err), _lib.stream_handle()))
+        return out
+
+    def predict(self, state, rhs):
+        """plane_couette.py:507-519: IMM with (u^n, u^n, N^n, N^n)."""
+        return self.imm_iteration(state, state, rhs, rhs)
+
+    def correct(self, state_prev, prediction, rhs_prev, rhs_next):
+        """plane_couette.py:522-540 -> (prediction_new, correction)."""
+        corr = self._new()
+        new = self.imm_iteration(state_prev, prediction, rhs_prev, rhs_next,
+                                 corr=corr)
+        return new, corr
+
+    def correct_fused(self, state_prev, prediction, rhs_prev, rhs_next, err,
+                      out=None):
+        """``correct`` + ``norm`` in one kernel; the correction itself is not
+        stored.  ``out`` may be ``prediction`` (it is donated)."""
+        return self.imm_iteration(state_prev, prediction, rhs_prev, rhs_next,
+                                  out=out, err=err)
+
+    def norm(self, v, out=None):
+        """plane_couette.py:543-549 (Simpson in y, / ly), device scalar."""
+        import torch
+
+        out = torch.empty(1, dtype=torch.float64, device="cuda") if out is None else out
+        _lib.check(self._L.dnsb_couette_norm(self._ctx, self._check(v),
+                                             _lib.ptr(out), _lib.stream_handle()))
+        return out
+
+    def correct_velocity(self, state):
+        """plane_couette.py:575-582: pass-through."""
+        return state, None
+
+    def get_stats(self, state) -> dict:
+        """plane_couette.py:591-613: E' = ||u||^2 / 2."""
+        _lib.check(self._L.dnsb_couette_norm2(
+            self._ctx, self._check(state), _lib.ptr(self._scratch),
+            _lib.stream_handle()))
+        return {"E'": float(self._scratch[0].item()) / 2}
+
+    def check_status(self):
+        _lib.check(self._L.dnsb_couette_check(self._ctx, _lib.stream_handle()))
+
+    # -- transforms (operators.py:104-146) -------------------------------------
+    def spec_to_phys(self, spec):
+        import torch
+
+        out = torch.empty(self.phys_shape, dtype=torch.float64, device="cuda")
+        _lib.check(self._L.dnsb_couette_spec_to_phys(
+            self._ctx, self._check(spec), _lib.ptr(out), _lib.stream_handle()))
+        return out
+
+    def phys_to_spec(self, phys):
+        out = self._new()
+        _lib.check(self._L.dnsb_couette_phys_to_spec(
+            self._ctx, _lib.ptr(phys.contiguous()), self._check(out),
+            _lib.stream_handle()))
+        return out
+
+    def init_state(self, snapshot=None):
+        """plane_couette.py:225-248: laminar (zeros) or an npz snapshot's
+        ``velocity_phys_nonexpanded``."""
+        import torch
+
+        if self.params.init.start_from_laminar or snapshot is None:
+            return torch.zeros(self.spec_shape, dtype=torch.complex128, device="cuda")
+        arr = np.load(snapshot)["velocity_phys_nonexpanded"].astype(np.float64)
+        return self.phys_to_spec(torch.as_tensor(arr, device="cuda"))
+
+    # -- stepper ---------------------------------------------------------------
+    def make_stepper(self, fused: bool = True):
+        if fused:
+            return make_fused_stepper(self)
+        return make_stepper(
+            lambda s: self.get_rhs(s),
+            lambda s, r: self.predict(s, r),
+            lambda sp, pr, rp, rn: self.correct(sp, pr, rp, rn),
+            lambda cr: self.norm(cr))
+
+
+# -- module-level interface bound to the global params -------------------------
+flow: PlaneCouetteFlow | None = None
+_steppers = None
+
+
+def _flow() -> PlaneCouetteFlow:
+    global flow, _steppers
+    if flow is None:
+        from ..parameters import params
+
+        flow = PlaneCouetteFlow(params)
+        _steppers = flow.make_stepper(fused=True)
+    return flow
+
+
+def predict_and_correct(state):
+    _flow()
+    return _steppers[0](state)
+
+
+def iterate_correction(state_prev, prediction, rhs_prev):
+    _flow()
+    return _steppers[1](state_prev, prediction, rhs_prev)
+
+
+def correct_velocity(state):
+    return _flow().correct_velocity(state)
+
+
+def get_stats(state) -> dict:
+    return _flow().get_stats(state)
+
+
+def init_state(snapshot=None):
+    return _flow().init_state(snapshot)

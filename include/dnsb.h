@@ -1,0 +1,195 @@
+/*
+ * dnsb.h -- C ABI of libdnsb.so, the B200 (sm_100a) time-step kernels for
+ * dnsjax (gokhanyalniz/dnsjax).
+ *
+ * Conventions
+ *   - Every function returns 0 on success and a nonzero dnsb_status code
+ *     otherwise; dnsb_last_error() gives a message for the calling thread.
+ *   - Arrays are plain device pointers (complex128 = interleaved double
+ *     pairs) in the reference's layouts; the caller owns them.  Contexts own
+ *     only their coefficient copies and workspace (allocated once, at
+ *     creation, with cudaMalloc) and are not thread-safe.
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).  Calls only
+ *     enqueue work: no host synchronisation happens inside, except where a
+ *     function's comment says it returns a host value.
+ *   - Scalars such as the corrector error are written to device memory
+ *     (`double* out_dev`) so a whole step can be enqueued without a sync.
+ *
+ * Reference interfaces replaced (paths within the reference project):
+ *   triply-periodic   src/dnsjax/flows/monochromatic.py:366-410 (_get_rhs,
+ *                     _predict, _correct, _norm handed to make_stepper at
+ *                     :413-415), :516-565 (correct_velocity), :433-510 (stats)
+ *   plane Couette     src/dnsjax/flows/plane_couette.py:274-289 (_get_rhs),
+ *                     :376-549 (_imm_iteration, _predict, _correct, _norm),
+ *                     :591-613 (stats)
+ *   banded solve      src/dnsjax/geometries/cartesian.py:360-488
+ *                     (_banded_solve_device, PerModeBandedOperator.solve)
+ *   transforms        src/dnsjax/operators.py:59-146 (spec_to_phys,
+ *                     spec_to_phys_2d, phys_to_spec[_2d]) over
+ *                     src/dnsjax/fft.py:193-408
+ */
+#ifndef DNSB_H_
+#define DNSB_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum dnsb_status {
+  DNSB_OK = 0,
+  DNSB_ERR_ARG = 1,      /* invalid argument / unsupported size */
+  DNSB_ERR_CUDA = 2,     /* a CUDA runtime call failed */
+  DNSB_ERR_PIVOT = 3     /* a pivot index outside [j, j+kl] was met */
+};
+
+int dnsb_version(void);
+const char* dnsb_last_error(void);
+/* Number of kernel launches this library has enqueued in this process. */
+long long dnsb_launch_count(void);
+
+/* ------------------------------------------------------------------ */
+/* Triply periodic flows (Kolmogorov, Waleffe, decaying box).          */
+/* Spectral layout (3, ny-1, nz-1, nx/2) complex128, [ky][kz][kx].     */
+/* Physical layout (3, ny_p, nz_p, nx_p) float64, [y][z][x].           */
+/* ------------------------------------------------------------------ */
+typedef struct dnsb_periodic dnsb_periodic;
+
+typedef struct {
+  int nx, ny, nz;         /* Fourier modes before the 3/2 rule (even) */
+  int nx_p, ny_p, nz_p;   /* padded physical sizes, each 2^a 3^b */
+  double dt, implicitness;
+  /* host arrays, copied at creation */
+  const double* kx;       /* nx/2, 2 pi/lx * [0 .. nx/2-1] */
+  const double* ky;       /* ny-1, FFT order, Nyquist omitted */
+  const double* kz;       /* nz-1 */
+  const double* base_flow;        /* [3][ny_p] U(y) */
+  const double* curl_base_flow;   /* [3][ny_p] curl U */
+  const double* nonlin_base_flow; /* [3][ny_p] U x curl U */
+  const double* ldt_1;    /* (ny-1)(nz-1)(nx/2), mean mode 0 */
+  const double* ildt_2;   /* (ny-1)(nz-1)(nx/2), mean mode 0 */
+} dnsb_periodic_desc;
+
+int dnsb_periodic_create(const dnsb_periodic_desc* desc, dnsb_periodic** out);
+int dnsb_periodic_destroy(dnsb_periodic* ctx);
+/* Bytes of device workspace the context holds. */
+size_t dnsb_periodic_workspace_bytes(const dnsb_periodic* ctx);
+
+/* rhs = NL(u) - grad lapl^-1 div NL(u)   (monochromatic.py:366-386) */
+int dnsb_periodic_rhs(dnsb_periodic* ctx, const void* state, void* rhs,
+                      void* stream);
+/* out = (state ldt_1 + rhs) ildt_2       (monochromatic.py:320-333) */
+int dnsb_periodic_predict(dnsb_periodic* ctx, const void* state,
+                          const void* rhs, void* out, void* stream);
+/* corr = c (rhs_next - rhs_prev) ildt_2; pred_out = pred + corr;
+ * err_dev[0] = sqrt(sum conj(corr) k_metric corr)  (monochromatic.py:336-355,
+ * 408-410).  pred_out may alias pred; corr_out and err_dev may be NULL. */
+int dnsb_periodic_correct(dnsb_periodic* ctx, const void* pred,
+                          const void* rhs_prev, const void* rhs_next,
+                          void* pred_out, void* corr_out, double* err_dev,
+                          void* stream);
+/* out_dev[0] = sqrt(sum conj(v) k_metric v)  (triply_periodic.py:81-101) */
+int dnsb_periodic_norm(dnsb_periodic* ctx, const void* v, double* out_dev,
+                       void* stream);
+/* out = v - grad lapl^-1 div v (if divergence), mean mode zeroed
+ * (monochromatic.py:516-565).  out may alias v. */
+int dnsb_periodic_correct_velocity(dnsb_periodic* ctx, const void* v,
+                                   void* out, int divergence, void* stream);
+/* out_dev[0] = sum k_metric |v|^2, out_dev[1] = sum -lapl |v|^2 (the two
+ * reductions of monochromatic.py:433-466). */
+int dnsb_periodic_energy_sums(dnsb_periodic* ctx, const void* v,
+                              double* out_dev, void* stream);
+/* Inverse / forward dealiased 3D transforms of 3 components
+ * (operators.py:59-101). */
+int dnsb_periodic_spec_to_phys(dnsb_periodic* ctx, const void* spec,
+                               double* phys, void* stream);
+int dnsb_periodic_phys_to_spec(dnsb_periodic* ctx, const double* phys,
+                               void* spec, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Plane Couette.                                                      */
+/* Spectral layout (3, nz-1, nx/2, ny) complex128, [kz][kx][y].        */
+/* Physical layout (3, ny, nz_p, nx_p) float64, [y][z][x].             */
+/* ------------------------------------------------------------------ */
+typedef struct dnsb_couette dnsb_couette;
+
+typedef struct {
+  int nx, ny, nz;         /* Fourier modes in x, z; CGL points in y (odd) */
+  int nx_p, nz_p;         /* padded sizes, 2^a 3^b */
+  int fd_order;           /* p: D1 on p+1 points, D2 on p+2, kl = ku = p */
+  double dt, implicitness, nu, ly;
+  /* host arrays, copied at creation */
+  const double* kx;       /* nx/2 */
+  const double* kz;       /* nz-1 */
+  const double* ys;       /* ny CGL points */
+  const int* d1_j0;       /* [ny] first column of the D1 stencil of row i */
+  const double* d1_w;     /* [ny][p+1] */
+  const int* d2_j0;       /* [ny] */
+  const double* d2_w;     /* [ny][p+2] */
+  const double* base_flow;        /* [3][ny] */
+  const double* curl_base_flow;   /* [3][ny] */
+  const double* nonlin_base_flow; /* [3][ny] */
+} dnsb_couette_desc;
+
+/* IMM operators in the reference's layouts (cartesian.py:575-801): device
+ * pointers owned by the caller, kept alive while bound. */
+typedef struct {
+  const double* Lk_ab;  /* (nz-1, nx/2, 3p+1, ny), LAPACK gbtrf factors */
+  const int* Lk_piv;    /* (nz-1, nx/2, ny), 0-based */
+  const double* Hk_ab;
+  const int* Hk_piv;
+  const double* v1;     /* (nz-1, nx/2, ny) */
+  const double* v2;
+  const double* q1;
+  const double* q2;
+  const double* M_inv;  /* (nz-1, nx/2, 2, 2) */
+} dnsb_imm_ops;
+
+int dnsb_couette_create(const dnsb_couette_desc* desc, dnsb_couette** out);
+int dnsb_couette_destroy(dnsb_couette* ctx);
+size_t dnsb_couette_workspace_bytes(const dnsb_couette* ctx);
+int dnsb_couette_bind_imm(dnsb_couette* ctx, const dnsb_imm_ops* ops);
+
+/* rhs = NL(u) on the padded grid (plane_couette.py:274-289) */
+int dnsb_couette_rhs(dnsb_couette* ctx, const void* state, void* rhs,
+                     void* stream);
+/* One influence-matrix iteration (plane_couette.py:376-504):
+ * vel_new = IMM(vel_n, vel_j, nl_n, nl_j); corr_out = vel_new - vel_j
+ * (nullable); err_dev[0] = Simpson norm of the correction (nullable).
+ * vel_new may alias vel_j when vel_j != vel_n; it must not alias vel_n. */
+int dnsb_couette_imm(dnsb_couette* ctx, const void* vel_n, const void* vel_j,
+                     const void* nl_n, const void* nl_j, void* vel_new,
+                     void* corr_out, double* err_dev, void* stream);
+/* out_dev[0] = sqrt(Simpson_y(sum conj(v) k_metric v) / ly)
+ * (cartesian.py:72-103). */
+int dnsb_couette_norm(dnsb_couette* ctx, const void* v, double* out_dev,
+                      void* stream);
+/* out_dev[0] = Simpson_y(sum conj(v) k_metric v) / ly (no square root). */
+int dnsb_couette_norm2(dnsb_couette* ctx, const void* v, double* out_dev,
+                       void* stream);
+int dnsb_couette_spec_to_phys(dnsb_couette* ctx, const void* spec,
+                              double* phys, void* stream);
+int dnsb_couette_phys_to_spec(dnsb_couette* ctx, const double* phys,
+                              void* spec, void* stream);
+/* Device status word of the context (nonzero after a bad pivot). */
+int dnsb_couette_check(dnsb_couette* ctx, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Per-mode banded LU substitution (PerModeBandedOperator.solve,       */
+/* cartesian.py:444-488; dgbtrs 'N').                                  */
+/*   ab   : (nmodes, 2kl+ku+1, ny) float64, LAPACK ab packing          */
+/*   ipiv : (nmodes, ny) int32, 0-based (SciPy gbtrf convention)       */
+/*   b    : (nmodes, ny, ncols) float64, solved in place; a complex    */
+/*          right-hand side is ncols = 2 (real, imaginary interleaved) */
+/*   status_dev: optional device int, OR'ed with 1 on a bad pivot      */
+/* ------------------------------------------------------------------ */
+int dnsb_banded_solve(const double* ab, const int* ipiv, double* b,
+                      int nmodes, int ny, int kl, int ku, int ncols,
+                      int* status_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DNSB_H_ */
