@@ -233,7 +233,9 @@ def run_ours(a, w, rank, world):
         from dnsjax_b200.flows.monochromatic import TriplyPeriodicFlow
 
         flow = TriplyPeriodicFlow(p, ly=w["ly"])
-    u0 = initial_state(w, w["seed"] + rank)
+    from dnsjax_b200.replicas import max_over_ranks, replica_seed, total_steps
+
+    u0 = initial_state(w, replica_seed(w["seed"], rank))
     tf = Timed(flow)
     steppers = tf.make_stepper()
     tol, mi = w["tol"], w["max_iter"]
@@ -263,11 +265,7 @@ def run_ours(a, w, rank, world):
         barrier()
     launches = _lib.launch_count() - n0
     tf.on = False
-    ms = t0.elapsed_time(t1)
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(t0.elapsed_time(t1), dist, "cuda")
 
     # End to end through the public API: pinned host state in, new state out.
     host_in = torch.empty(state.shape, dtype=state.dtype, pin_memory=True)
@@ -284,11 +282,7 @@ def run_ours(a, w, rank, world):
         host_in, host_out = host_out, host_in
     e1.record()
     barrier()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     state_bytes = state.numel() * state.element_size()
 
     # Roofline of the dominant op (events inside the timed region).
@@ -303,7 +297,7 @@ def run_ours(a, w, rank, world):
     peaks = measured_peaks()
     peak = peaks["hbm_gbs"] if peaks else 6650.0
     achieved = bytes_ / (dur * 1e-3) / 1e9
-    nsteps = a.steps * world
+    nsteps = total_steps(a.steps, world)
     value = nsteps / (ms * 1e-3)
     out = {
         "metric": METRIC,

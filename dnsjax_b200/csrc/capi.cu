@@ -456,6 +456,7 @@ struct dnsb_couette {
   int* status = nullptr;
   dnsb_imm_ops ops{};
   bool bound = false;
+  int ab_row0 = 0;
   size_t ws_bytes = 0;
 
   ImmArgs imm() const {
@@ -486,6 +487,7 @@ struct dnsb_couette {
     a.q2 = ops.q2;
     a.M_inv = ops.M_inv;
     a.status = status;
+    a.ab_row0 = ab_row0;
     return a;
   }
 };
@@ -559,7 +561,8 @@ extern "C" int dnsb_couette_create(const dnsb_couette_desc* d,
   const size_t need[] = {col_pass_smem(p->Mz), x_pass_smem(p->Mx),
                          x_phys_smem(p->Mx), x_fwd_smem(p->Mx),
                          zinv_curl_smem(p->Mz, p->NZ1, p->span_max),
-                         imm_smem(p->Ny)};
+                         imm_smem(p->Ny),
+                         imm_v2_supported(p->p) ? imm_v2_smem(p->Ny, p->p, 0) : 0};
   for (size_t n : need)
     if ((int)n > smax) {
       couette_free(p);
@@ -600,6 +603,7 @@ extern "C" int dnsb_couette_create(const dnsb_couette_desc* d,
   if (!rc) {
     cudaError_t e = set_pass_attributes(smax);
     if (e == cudaSuccess) e = set_solver_attributes(smax);
+    if (e == cudaSuccess) e = set_imm_v2_attributes(smax);
     if (e != cudaSuccess)
       rc = fail(DNSB_ERR_CUDA, std::string("cudaFuncSetAttribute: ") +
                                    cudaGetErrorString(e));
@@ -628,6 +632,26 @@ extern "C" int dnsb_couette_bind_imm(dnsb_couette* p, const dnsb_imm_ops* ops) {
       !ops->v2 || !ops->q1 || !ops->q2 || !ops->M_inv)
     return fail(DNSB_ERR_ARG, "null IMM operator");
   p->ops = *ops;
+  // Rows of the LU factors above the first nonzero one (over all modes, both
+  // operators) are skipped by the register-window kernel.
+  const int kuu = 2 * p->p, rows = 3 * p->p + 1;
+  int* d_row = nullptr;
+  DNSB_CUDA(cudaMalloc(&d_row, sizeof(int)));
+  int h_row = kuu;
+  int rc = 0;
+  if (cudaMemcpy(d_row, &h_row, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = fail(DNSB_ERR_CUDA, "cudaMemcpy failed");
+  const double* abs_[2] = {ops->Lk_ab, ops->Hk_ab};
+  for (int k = 0; k < 2 && !rc; ++k) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (launch_ab_first_row(abs_[k], p->NM, rows, p->Ny, kuu, d_row, 0) != cudaSuccess)
+      rc = fail(DNSB_ERR_CUDA, "ab scan launch failed");
+  }
+  if (!rc && cudaMemcpy(&h_row, d_row, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = fail(DNSB_ERR_CUDA, "ab scan failed");
+  cudaFree(d_row);
+  if (rc) return rc;
+  p->ab_row0 = h_row;
   p->bound = true;
   return 0;
 }
@@ -699,10 +723,17 @@ extern "C" int dnsb_couette_imm(dnsb_couette* p, const void* vel_n,
   if (vel_new == vel_n)
     return fail(DNSB_ERR_ARG, "vel_new must not alias vel_n");
   cudaStream_t st = as_stream(stream);
-  DNSB_LAUNCH(launch_imm(p->imm(), (const double2*)vel_n, (const double2*)vel_j,
-                         (const double2*)nl_n, (const double2*)nl_j,
-                         (double2*)vel_new, (double2*)corr_out,
-                         err_dev ? p->partials : nullptr, st));
+  if (imm_v2_supported(p->p)) {
+    DNSB_LAUNCH(launch_imm_v2(p->imm(), (const double2*)vel_n, (const double2*)vel_j,
+                              (const double2*)nl_n, (const double2*)nl_j,
+                              (double2*)vel_new, (double2*)corr_out,
+                              err_dev ? p->partials : nullptr, st));
+  } else {
+    DNSB_LAUNCH(launch_imm(p->imm(), (const double2*)vel_n, (const double2*)vel_j,
+                           (const double2*)nl_n, (const double2*)nl_j,
+                           (double2*)vel_new, (double2*)corr_out,
+                           err_dev ? p->partials : nullptr, st));
+  }
   if (err_dev)
     DNSB_LAUNCH(launch_finalize(p->partials, p->NM, err_dev, 1.0 / p->ly, 1, st));
   return 0;

@@ -160,6 +160,92 @@ __device__ inline double2* fft_columns(double2* a, double2* b,
   return in;
 }
 
+// ---- compile-time plans -----------------------------------------------
+// Same factorisation rule as make_plan (8s first unless the rest is 8, then
+// 4s, 2s, 3s), evaluated at compile time so every stage's stride, twiddle
+// step and trip count are constants.
+__host__ __device__ constexpr int cplan_radix(int L, int s) {
+  int n = L, k = 0;
+  while (n % 8 == 0 && n != 8) { if (k == s) return 8; ++k; n /= 8; }
+  while (n % 4 == 0 && n > 1) { if (k == s) return 4; ++k; n /= 4; }
+  while (n % 2 == 0 && n > 1) { if (k == s) return 2; ++k; n /= 2; }
+  while (n % 3 == 0 && n > 1) { if (k == s) return 3; ++k; n /= 3; }
+  if (n == 8) { if (k == s) return 8; ++k; }
+  return 0;
+}
+__host__ __device__ constexpr int cplan_nst(int L) {
+  int s = 0;
+  while (cplan_radix(L, s) != 0) ++s;
+  return s;
+}
+
+template <int L, int R, int C, int NS, int SIGN, int NT>
+__device__ __forceinline__ void fft_stage_t(const double2* __restrict__ in,
+                                            double2* __restrict__ out,
+                                            const double2* __restrict__ tw) {
+  constexpr int NB = L / R;
+  constexpr int STEP = L / (NS * R);
+  constexpr int TOTAL = NB * C;
+#pragma unroll 2
+  for (int idx = threadIdx.x; idx < TOTAL; idx += NT) {
+    const int c = idx % C;
+    const int j = idx / C;
+    const int k = j % NS;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = in[(j + r * NB) * C + c];
+    if (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        double2 w = tw[r * k * STEP];
+        if (SIGN > 0) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    if (R == 2) dft2(v);
+    if (R == 3) dft3(v, SIGN);
+    if (R == 4) dft4(v, SIGN);
+    if (R == 8) dft8(v, SIGN);
+    const int base = (j / NS) * NS * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) out[(base + r * NS) * C + c] = v[r];
+  }
+}
+
+template <int L, int C, int SIGN, int NT, int S = 0, int NS = 1>
+__device__ __forceinline__ double2* fft_stages_t(double2* a, double2* b,
+                                                 const double2* tw) {
+  if constexpr (S >= cplan_nst(L)) {
+    return a;
+  } else {
+    constexpr int R = cplan_radix(L, S);
+    fft_stage_t<L, R, C, NS, SIGN, NT>(a, b, tw);
+    __syncthreads();
+    return fft_stages_t<L, C, SIGN, NT, S + 1, NS * R>(b, a, tw);
+  }
+}
+
+// Compile-time-planned version of fft_columns (blockDim.x must equal NT).
+template <int L, int C, int SIGN, int NT>
+__device__ __forceinline__ double2* fft_columns_t(double2* a, double2* b,
+                                                  const double2* tw) {
+  return fft_stages_t<L, C, SIGN, NT>(a, b, tw);
+}
+
+// Dispatch: ML > 0 uses the compile-time plan for length ML, ML == 0 the
+// runtime plan.
+template <int ML, int C, int NT>
+__device__ __forceinline__ double2* fft_cols(double2* a, double2* b,
+                                             const FFTPlan& P, int sign,
+                                             const double2* tw) {
+  if constexpr (ML > 0) {
+    if (sign > 0) return fft_columns_t<ML, C, 1, NT>(a, b, tw);
+    return fft_columns_t<ML, C, -1, NT>(a, b, tw);
+  } else {
+    return fft_columns(a, b, P, C, sign, tw);
+  }
+}
+
 // Stored index -> padded FFT position for a Nyquist-free complex axis of
 // n-1 stored modes placed in a length-M transform (zeropad_fft /
 // truncate_fft index maps, src/dnsjax/fft.py:41-137).

