@@ -261,6 +261,17 @@ __device__ __forceinline__ int pos_to_stored(int t, int nstored, int M) {
   return -1;
 }
 
+// Raise a kernel's dynamic shared-memory limit to what is left of max_smem
+// after its static shared memory.
+inline cudaError_t allow_dynamic_smem(const void* fn, int max_smem) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+  if (e != cudaSuccess) return e;
+  const int dyn = max_smem - (int)fa.sharedSizeBytes;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              dyn > 0 ? dyn : 0);
+}
+
 // Copy a global twiddle table of length L into shared memory.
 __device__ __forceinline__ void load_twiddles(double2* s, const double2* g,
                                               int L) {

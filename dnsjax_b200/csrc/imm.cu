@@ -453,8 +453,7 @@ cudaError_t set_imm_v2_attributes(int max_smem) {
       (const void*)imm_mode_kernel<6, 7>,  (const void*)imm_mode_kernel<6, 12>,
       (const void*)imm_mode_kernel<8, 9>,  (const void*)imm_mode_kernel<8, 16>};
   for (const void* f : fns) {
-    cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         max_smem);
+    cudaError_t r = allow_dynamic_smem(f, max_smem);
     if (r != cudaSuccess) e = r;
   }
   return e;

@@ -667,8 +667,7 @@ cudaError_t set_pass_attributes(int max_smem) {
                        DNSB_ALL_SIZES(yinv_kernel), DNSB_ALL_SIZES(yfwd_kernel),
                        DNSB_ALL_SIZES(zinv_curl_kernel)};
   for (const void* f : fns) {
-    cudaError_t r = cudaFuncSetAttribute(
-        f, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+    cudaError_t r = allow_dynamic_smem(f, max_smem);
     if (r != cudaSuccess) e = r;
   }
   return e;

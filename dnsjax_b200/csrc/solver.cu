@@ -437,9 +437,7 @@ cudaError_t launch_couette_norm2(const ImmArgs& a, const double2* v,
 }
 
 cudaError_t set_solver_attributes(int max_smem) {
-  return cudaFuncSetAttribute((const void*)imm_kernel,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              max_smem);
+  return allow_dynamic_smem((const void*)imm_kernel, max_smem);
 }
 
 }  // namespace dnsb
