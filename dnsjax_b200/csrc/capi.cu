@@ -73,6 +73,11 @@ cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 }  // namespace
 
+namespace dnsb {
+int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
+void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+}  // namespace dnsb
+
 // ===========================================================================
 // Triply periodic
 // ===========================================================================

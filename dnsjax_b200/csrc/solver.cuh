@@ -1,6 +1,8 @@
 // Per-mode solves and pointwise kernels of the time step.
 #pragma once
 
+#include <string>
+
 #include "common.cuh"
 
 namespace dnsb {
@@ -101,6 +103,10 @@ cudaError_t launch_ab_first_row(const double* ab, long long nmodes, int rows,
 // Simpson-weighted k_metric |v|^2 per block (Couette norm).
 cudaError_t launch_couette_norm2(const ImmArgs& a, const double2* v,
                                  double* partials, cudaStream_t st);
+
+// ---- library-wide error / launch bookkeeping (capi.cu) ----------------------
+int set_last_error(int code, const std::string& msg);
+void count_launches(int n);
 
 // ---- standalone per-mode banded solve (PerModeBandedOperator.solve) -------
 cudaError_t launch_banded_solve(const double* ab, const int* ipiv, double* b,

@@ -175,6 +175,23 @@ int dnsb_couette_phys_to_spec(dnsb_couette* ctx, const double* phys,
 /* Device status word of the context (nonzero after a bad pivot). */
 int dnsb_couette_check(dnsb_couette* ctx, void* stream);
 
+/* Allocation-free Couette norm (no counterpart in the reference; it exists
+ * for callers that cannot allocate device memory, such as an XLA FFI handler
+ * working inside memory its framework owns, or code recorded by CUDA stream
+ * capture).  Computes what dnsb_couette_norm computes, from the field alone
+ * (the CGL grid and its Simpson weights are generated in the kernel), with
+ * the per-mode partial sums kept in a file-scope device array instead of
+ * context workspace:
+ *   out_dev[0] = sqrt(Simpson_y(sum conj(v) k_metric v) / ly)
+ *   v: (3, nz-1, nx/2, ny) complex128.  At most 32768 (kz, kx) modes;
+ *   larger fields return DNSB_ERR_ARG.  The array (256 KiB) stays on every
+ *   device that loads the library until exit; every call shares it, so calls
+ *   that may overlap on the GPU race and must be ordered by the caller.  The
+ *   first call on a device looks up the array's device address (with that
+ *   device current); make it before any stream capture. */
+int dnsb_couette_norm_noalloc(const void* v, int nx, int ny, int nz, double ly,
+                              double* out_dev, void* stream);
+
 /* ------------------------------------------------------------------ */
 /* Per-mode banded LU substitution (PerModeBandedOperator.solve,       */
 /* cartesian.py:444-488; dgbtrs 'N').                                  */
