@@ -4,6 +4,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -462,6 +463,7 @@ struct dnsb_couette {
   dnsb_imm_ops ops{};
   bool bound = false;
   int ab_row0 = 0;
+  int pair_modes = 0;
   size_t ws_bytes = 0;
 
   ImmArgs imm() const {
@@ -493,6 +495,7 @@ struct dnsb_couette {
     a.M_inv = ops.M_inv;
     a.status = status;
     a.ab_row0 = ab_row0;
+    a.pair_modes = pair_modes;
     return a;
   }
 };
@@ -567,7 +570,7 @@ extern "C" int dnsb_couette_create(const dnsb_couette_desc* d,
                          x_phys_smem(p->Mx), x_fwd_smem(p->Mx),
                          zinv_curl_smem(p->Mz, p->NZ1, p->span_max),
                          imm_smem(p->Ny),
-                         imm_v2_supported(p->p) ? imm_v2_smem(p->Ny, p->p, 0) : 0};
+                         imm_v2_supported(p->p, p->Ny) ? imm_v2_smem(p->Ny, p->p, 0) : 0};
   for (size_t n : need)
     if ((int)n > smax) {
       couette_free(p);
@@ -654,8 +657,25 @@ extern "C" int dnsb_couette_bind_imm(dnsb_couette* p, const dnsb_imm_ops* ops) {
   }
   if (!rc && cudaMemcpy(&h_row, d_row, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
     rc = fail(DNSB_ERR_CUDA, "ab scan failed");
+  // Modes (s, kx) and (nz-1-s, kx) share k^2; the kernel solves them together
+  // when their factors are bit-identical (DNSB_IMM_PAIRS=0 disables this).
+  int h_diff = 0;
+  if (!rc && cudaMemcpy(d_row, &h_diff, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = fail(DNSB_ERR_CUDA, "cudaMemcpy failed");
+  const int* pivs[2] = {ops->Lk_piv, ops->Hk_piv};
+  for (int k = 0; k < 2 && !rc; ++k) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (launch_ab_pair_check(abs_[k], pivs[k], p->NZ1, p->NKX, rows, p->Ny, d_row, 0) !=
+        cudaSuccess)
+      rc = fail(DNSB_ERR_CUDA, "ab pair check launch failed");
+  }
+  if (!rc && cudaMemcpy(&h_diff, d_row, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = fail(DNSB_ERR_CUDA, "ab pair check failed");
   cudaFree(d_row);
   if (rc) return rc;
+  const char* env = getenv("DNSB_IMM_PAIRS");
+  const bool allow = !(env && env[0] == '0');
+  p->pair_modes = (allow && h_diff == 0) ? 1 : 0;
   p->ab_row0 = h_row;
   p->bound = true;
   return 0;
@@ -728,7 +748,7 @@ extern "C" int dnsb_couette_imm(dnsb_couette* p, const void* vel_n,
   if (vel_new == vel_n)
     return fail(DNSB_ERR_ARG, "vel_new must not alias vel_n");
   cudaStream_t st = as_stream(stream);
-  if (imm_v2_supported(p->p)) {
+  if (imm_v2_supported(p->p, p->Ny)) {
     DNSB_LAUNCH(launch_imm_v2(p->imm(), (const double2*)vel_n, (const double2*)vel_j,
                               (const double2*)nl_n, (const double2*)nl_j,
                               (double2*)vel_new, (double2*)corr_out,

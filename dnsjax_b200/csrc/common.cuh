@@ -246,6 +246,45 @@ __device__ __forceinline__ double2* fft_cols(double2* a, double2* b,
   }
 }
 
+// ---- register DFTs of size N = 3P (P in {2, 3, 4, 8}) --------------------
+// tw[m * TS] = exp(-2 pi i m / N) (a length-N*TS table); SIGN -1 forward,
+// +1 inverse; natural-order output in v.
+template <int P>
+__device__ __forceinline__ void dft_small(double2* v, int sign) {
+  if constexpr (P == 2) dft2(v);
+  else if constexpr (P == 3) dft3(v, sign);
+  else if constexpr (P == 4) dft4(v, sign);
+  else dft8(v, sign);
+}
+
+template <int N, int SIGN>
+__device__ __forceinline__ void dft_3p(double2* v, const double2* __restrict__ tw,
+                                       int TS) {
+  constexpr int P = N / 3;
+  double2 a[3][P];
+#pragma unroll
+  for (int q = 0; q < 3; ++q)
+#pragma unroll
+    for (int p = 0; p < P; ++p) a[q][p] = v[3 * p + q];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) dft_small<P>(a[q], SIGN);
+#pragma unroll
+  for (int q = 1; q < 3; ++q)
+#pragma unroll
+    for (int k1 = 1; k1 < P; ++k1) {
+      double2 w = tw[(q * k1) * TS];
+      if (SIGN > 0) w.y = -w.y;
+      a[q][k1] = cmul(a[q][k1], w);
+    }
+#pragma unroll
+  for (int k1 = 0; k1 < P; ++k1) {
+    double2 b[3] = {a[0][k1], a[1][k1], a[2][k1]};
+    dft3(b, SIGN);
+#pragma unroll
+    for (int k2 = 0; k2 < 3; ++k2) v[k1 + P * k2] = b[k2];
+  }
+}
+
 // Stored index -> padded FFT position for a Nyquist-free complex axis of
 // n-1 stored modes placed in a length-M transform (zeropad_fft /
 // truncate_fft index maps, src/dnsjax/fft.py:41-137).

@@ -65,51 +65,57 @@ struct Rec {
 
 // Forward elimination (row interchange + L update, dgbtrs 'N') on one real
 // column b (stride 2) of length Ny.  dpiv[j] = ipiv[j] - j in [0, KL].
+// The window holds b[j..j+KL] in registers, slot(o, ph) = (o + ph) % W; the
+// loop is unrolled by W so slots are compile-time.  Each block of W steps
+// first loads all its multipliers, pivots and entering values into
+// registers (one exposed shared-memory latency per block), then runs the
+// recurrence from registers; the row interchange is a warp-uniform switch.
 template <int KL, int RS>
 __device__ __forceinline__ void forward_chain(const double* __restrict__ AB,
                                               const int* __restrict__ dpiv,
                                               double* __restrict__ b, int Ny) {
-  constexpr int W = KL + 1;  // window b[j .. j+KL]; slot(o, ph) = (o+ph) % W
+  constexpr int W = KL + 1;
   double w[W];
 #pragma unroll
   for (int o = 0; o < W; ++o) w[o] = (o < Ny) ? b[2 * o] : 0.0;
   const int nsteps = Ny - 1;
-  double bb[W];  // element entering the window at each step of the block
-#pragma unroll
-  for (int ph = 0; ph < W; ++ph) {
-    const int e = ph + W;
-    bb[ph] = (e < Ny) ? b[2 * e] : 0.0;
-  }
   for (int j0 = 0; j0 < nsteps; j0 += W) {
-    double bn[W];
+    double Lr[W][KL];
+    int dr[W];
+    double be[W];
 #pragma unroll
     for (int ph = 0; ph < W; ++ph) {
-      const int e = j0 + 2 * W + ph;
-      bn[ph] = (e < Ny) ? b[2 * e] : 0.0;
+      const int j = min(j0 + ph, nsteps - 1);
+#pragma unroll
+      for (int i = 0; i < KL; ++i) Lr[ph][i] = AB[j * RS + i];
+      dr[ph] = dpiv[j];
+      const int e = j0 + ph + W;
+      be[ph] = (e < Ny) ? b[2 * e] : 0.0;
     }
 #pragma unroll
     for (int ph = 0; ph < W; ++ph) {
       const int j = j0 + ph;
       if (j < nsteps) {
-        const int d = dpiv[j];
         double bpj = w[ph % W];
-        if (d != 0) {  // warp-uniform: every lane solves the same mode
-#pragma unroll
-          for (int i = 1; i <= KL; ++i)
-            if (d == i) bpj = w[(i + ph) % W];
-#pragma unroll
-          for (int i = 1; i <= KL; ++i)
-            if (d == i) w[(i + ph) % W] = w[ph % W];
+        switch (dr[ph]) {  // warp-uniform: every lane solves the same factors
+#define DNSB_PIV(I)                                  \
+  case I:                                            \
+    if (I <= KL) {                                   \
+      bpj = w[(I + ph) % W];                         \
+      w[(I + ph) % W] = w[ph % W];                   \
+    }                                                \
+    break;
+          DNSB_PIV(1) DNSB_PIV(2) DNSB_PIV(3) DNSB_PIV(4)
+          DNSB_PIV(5) DNSB_PIV(6) DNSB_PIV(7) DNSB_PIV(8)
+#undef DNSB_PIV
+          default: break;
         }
         b[2 * j] = bpj;
-        const double* L = AB + j * RS;
 #pragma unroll
-        for (int i = 1; i <= KL; ++i) w[(i + ph) % W] -= L[i - 1] * bpj;
-        w[ph % W] = bb[ph];  // offset 0 leaves; b[j+KL+1] enters at offset KL
+        for (int i = 1; i <= KL; ++i) w[(i + ph) % W] -= Lr[ph][i - 1] * bpj;
+        w[ph % W] = be[ph];  // offset 0 leaves; b[j+W] enters at offset KL
       }
     }
-#pragma unroll
-    for (int ph = 0; ph < W; ++ph) bb[ph] = bn[ph];
   }
   // b[Ny-1] sits at offset 0 after the last step: slot nsteps % W.
   const int last = nsteps % W;
@@ -120,58 +126,85 @@ __device__ __forceinline__ void forward_chain(const double* __restrict__ AB,
   b[2 * (Ny - 1)] = v;
 }
 
-// Back substitution with U (2*KL superdiagonals, the NU nearest stored).
+// One half-block of back substitution: phases PH0 <= ph < PH1 of the block
+// starting at j0.  Record slot KL holds 1/U_jj and slots KL+i hold
+// U_{j-i,j}/U_jj, so the recurrence is one FMA deep: b[j-i] -= that * b[j];
+// x_j = b[j] / U_jj is stored off the dependency chain.
+template <int KL, int NU, int RS, int PH0, int PH1>
+__device__ __forceinline__ void backward_half(const double* __restrict__ AB,
+                                              double* __restrict__ b, int j0,
+                                              double* w) {
+  constexpr int KUU = 2 * KL;
+  constexpr int W = KUU + 1;
+  constexpr int H = PH1 - PH0;
+  double Ur[H][NU + 1];
+  double be[H];
+#pragma unroll
+  for (int h = 0; h < H; ++h) {
+    const int j = max(j0 - (PH0 + h), 0);
+#pragma unroll
+    for (int i = 0; i <= NU; ++i) Ur[h][i] = AB[j * RS + KL + i];
+    const int e = j0 - (PH0 + h) - W;
+    be[h] = (e >= 0) ? b[2 * e] : 0.0;
+  }
+#pragma unroll
+  for (int h = 0; h < H; ++h) {
+    const int ph = PH0 + h;
+    const int j = j0 - ph;
+    if (j >= 0) {
+      const int st = ((KUU - ph) % W + W) % W;
+      const double bj = w[st];
+      b[2 * j] = bj * Ur[h][0];
+#pragma unroll
+      for (int i = 1; i <= NU; ++i) {
+        const int si = ((KUU - i - ph) % W + W) % W;
+        w[si] -= Ur[h][i] * bj;
+      }
+      w[st] = be[h];  // b[j-KUU-1] enters at offset 0
+    }
+  }
+}
+
+// Back substitution with U (2*KL superdiagonals, the NU nearest stored) on
+// one real column b (stride 2).  Window b[j-KUU..j], slot(o, ph) =
+// (o - ph) mod W, loop unrolled by W in two register-loaded halves.
 template <int KL, int NU, int RS>
 __device__ __forceinline__ void backward_chain(const double* __restrict__ AB,
                                                double* __restrict__ b, int Ny) {
   constexpr int KUU = 2 * KL;
-  constexpr int W = KUU + 1;  // window b[j-KUU .. j]; slot(o, ph) = (o-ph) mod W
+  constexpr int W = KUU + 1;
+  constexpr int H = (W + 1) / 2;
   double w[W];
 #pragma unroll
   for (int o = 0; o < W; ++o) {
     const int idx = Ny - 1 - KUU + o;
     w[o] = (idx >= 0) ? b[2 * idx] : 0.0;
   }
-  double bb[W];
-#pragma unroll
-  for (int ph = 0; ph < W; ++ph) {
-    const int e = Ny - 1 - ph - W;
-    bb[ph] = (e >= 0) ? b[2 * e] : 0.0;
-  }
   for (int j0 = Ny - 1; j0 >= 0; j0 -= W) {
-    double bn[W];
-#pragma unroll
-    for (int ph = 0; ph < W; ++ph) {
-      const int e = j0 - 2 * W - ph;
-      bn[ph] = (e >= 0) ? b[2 * e] : 0.0;
-    }
-#pragma unroll
-    for (int ph = 0; ph < W; ++ph) {
-      const int j = j0 - ph;
-      if (j >= 0) {
-        const double* r = AB + j * RS;
-        const int st = ((KUU - ph) % W + W) % W;
-        const double xj = w[st] * r[KL];
-        b[2 * j] = xj;
-#pragma unroll
-        for (int i = 1; i <= NU; ++i) {
-          const int si = ((KUU - i - ph) % W + W) % W;
-          w[si] -= r[KL + i] * xj;
-        }
-        w[st] = bb[ph];  // b[j-KUU-1] enters at offset 0
-      }
-    }
-#pragma unroll
-    for (int ph = 0; ph < W; ++ph) bb[ph] = bn[ph];
+    backward_half<KL, NU, RS, 0, H>(AB, b, j0, w);
+    backward_half<KL, NU, RS, H, W>(AB, b, j0, w);
   }
 }
 
-// Shared memory of one mode: T[3][Ny] staged stencil inputs, f[Ny],
-// R[3][Ny] (double2), factor records Ny x RS (double), pivot offsets Ny.
-size_t imm_mode_smem(int Ny, int kl, int nu) {
+// Shared memory of one work item (1 or 2 modes sharing factors): per mode
+// T[3][Ny] staged stencil inputs, f[Ny], R[3][Ny] (double2); factor records
+// Ny x RS (double); pivot offsets Ny.
+size_t imm_mode_smem(int Ny, int kl, int nu, int qmax) {
   const int rs = (kl + 1 + nu + 1) & ~1;
-  return sizeof(double2) * (size_t)(7 * Ny) + sizeof(double) * (size_t)(Ny * rs) +
-         sizeof(int) * (size_t)Ny;
+  return sizeof(double2) * (size_t)(7 * qmax * Ny) +
+         sizeof(double) * (size_t)(Ny * rs) + sizeof(int) * (size_t)Ny;
+}
+
+// y values per lane: y = lane + 32 k, k < kYM (Ny <= 32 kYM).
+constexpr int kYM = 5;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_1() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
 }
 
 // Stage one operator's factors of mode m into the record layout and its
@@ -202,11 +235,14 @@ __device__ __forceinline__ void stage_factors(double* AB, int* dpiv,
   cp_async_commit();
 }
 
-template <int KL>
+template <int KL, int NU>
 __device__ __forceinline__ void finish_factors(double* AB, int* dpiv, int RS,
                                                int Ny, int lane, int* status) {
   for (int j = lane; j < Ny; j += 32) {
-    AB[j * RS + KL] = 1.0 / AB[j * RS + KL];
+    const double r = 1.0 / AB[j * RS + KL];
+    AB[j * RS + KL] = r;
+#pragma unroll
+    for (int i = 1; i <= NU; ++i) AB[j * RS + KL + i] *= r;
     int d = dpiv[j] - j;
     if (d < 0 || d > KL || j + d >= Ny) {  // never follow a bad pivot
       if (status) atomicOr(status, 1);
@@ -216,170 +252,293 @@ __device__ __forceinline__ void finish_factors(double* AB, int* dpiv, int RS,
   }
 }
 
+// One work item: mode (s, kx), and, when `paired`, also its mirror
+// (nz-1-s, kx) -- the same k^2 = kx^2 + kz^2 and therefore bit-identical L_k
+// and H_k factors (checked when the operators are bound) -- so the staged
+// factors serve both and the substitution chains run on 4 / 12 lanes.
+// Stencil inputs are staged with cp.async (the stage-3 staging overlaps the
+// L_k substitution); pointwise inputs are loaded into registers for all of a
+// lane's y values before they are used.
 template <int KL, int NU>
 __global__ void __launch_bounds__(32)
 imm_mode_kernel(ImmArgs a, const double2* __restrict__ vel_n,
                 const double2* vel_j, const double2* __restrict__ nl_n,
                 const double2* __restrict__ nl_j, double2* vel_new,
-                double2* corr_out, double* __restrict__ partials) {
+                double2* corr_out, double* __restrict__ partials, int paired) {
   constexpr int ROWS = 3 * KL + 1;
   constexpr int RS = Rec<KL, NU>::kStride;
   constexpr int S1 = KL + 1, S2 = KL + 2;
+  constexpr int YM = kYM;
   extern __shared__ double2 sm[];
   const int lane = threadIdx.x;
-  const int NKX = a.NKX, Ny = a.Ny;
-  const int NM = a.NZ1 * NKX;
-  const int m = blockIdx.x;
+  const int NKX = a.NKX, Ny = a.Ny, NZ1 = a.NZ1;
+  const int NM = NZ1 * NKX;
+  const int item = blockIdx.x;
   const int row0 = a.ab_row0;
-  double2* T = sm;          // [3][Ny]
-  double2* f = T + 3 * Ny;  // f_hat -> p_P
-  double2* R = f + Ny;      // [3][Ny] R -> (u, v, w)_arb
-  double* AB = reinterpret_cast<double*>(R + 3 * Ny);
+  int nq = 1;
+  int mq[2];
+  if (paired) {
+    const int ix = item % NKX, s = item / NKX;
+    mq[0] = s * NKX + ix;
+    mq[1] = (NZ1 - s) * NKX + ix;
+    nq = (s == 0) ? 1 : 2;
+  } else {
+    mq[0] = mq[1] = item;
+  }
+  const int qmax = paired ? 2 : 1;
+  double2* T[2];
+  double2* F[2];
+  double2* Rb[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    T[q] = sm + q * 7 * Ny;
+    F[q] = T[q] + 3 * Ny;
+    Rb[q] = F[q] + Ny;
+  }
+  double* AB = reinterpret_cast<double*>(sm + 7 * qmax * Ny);
   int* dpiv = reinterpret_cast<int*>(AB + Ny * RS);
 
-  const int iz = m / NKX, ix = m % NKX;
-  const double kx = a.kx[ix], kz = a.kz[iz];
-  const double k2 = kx * kx + kz * kz;
-  const bool k2zero = (k2 == 0.0);
   const double c = a.c, dt = a.dt, nu = a.nu;
   const double omc = 1.0 - c;
   const double omc_nu = omc * nu;
+  const double idt = 1.0 / dt;
   const long long CS = (long long)NM * Ny;
-  const long long mo = (long long)m * Ny;
-  const long long abase = (long long)m * ROWS * Ny;
   const int* d1j = a.d1_j0;
   const double* d1w = a.d1_w;
   const int* d2j = a.d2_j0;
   const double* d2w = a.d2_w;
-  const double2 *un = vel_n + mo, *vn = vel_n + CS + mo, *wn = vel_n + 2 * CS + mo;
-  const double2 *Nun = nl_n + mo, *Nvn = nl_n + CS + mo, *Nwn = nl_n + 2 * CS + mo;
-  const double2 *Nuj = nl_j + mo, *Nvj = nl_j + CS + mo, *Nwj = nl_j + 2 * CS + mo;
+  const long long abase = (long long)mq[0] * ROWS * Ny;
+  const long long pbase = (long long)mq[0] * Ny;
 
-  stage_factors<KL, NU, RS>(AB, dpiv, a.Lk_ab + abase, a.Lk_piv + mo, Ny, row0, lane);
-
-  // d_hat^n = i kx u + D1 v + i kz w  -> T[2]
-  for (int y = lane; y < Ny; y += 32) T[y] = vn[y];
+  // group: stencil inputs of stages 0-1 (v^n, N^j_v, N^n_v) of each mode
+  for (int q = 0; q < nq; ++q) {
+    const long long mo = (long long)mq[q] * Ny;
+    for (int y = lane; y < Ny; y += 32) {
+      cp_async16(T[q] + y, vel_n + CS + mo + y);
+      cp_async16(T[q] + Ny + y, nl_j + CS + mo + y);
+      cp_async16(T[q] + 2 * Ny + y, nl_n + CS + mo + y);
+    }
+  }
+  cp_async_commit();
+  // group: L_k factors
+  stage_factors<KL, NU, RS>(AB, dpiv, a.Lk_ab + abase, a.Lk_piv + pbase, Ny, row0, lane);
+  cp_async_wait_1();
   __syncwarp();
-  for (int y = lane; y < Ny; y += 32)
-    T[2 * Ny + y] = cadd(cadd(cik(kx, un[y]), sband<S1>(T, d1j, d1w, y)), cik(kz, wn[y]));
+
+  for (int q = 0; q < nq; ++q) {
+    const int m = mq[q];
+    const int iz = m / NKX, ix = m % NKX;
+    const double kx = a.kx[ix], kz = a.kz[iz];
+    const long long mo = (long long)m * Ny;
+    double2 ua[YM], wa[YM];
+#pragma unroll
+    for (int k = 0; k < YM; ++k) {
+      const int y = lane + 32 * k;
+      if (y < Ny) {
+        ua[k] = vel_n[mo + y];
+        wa[k] = vel_n[2 * CS + mo + y];
+      }
+    }
+    double2* d = Rb[q];  // d_hat^n lives in R until stage 3
+#pragma unroll
+    for (int k = 0; k < YM; ++k) {
+      const int y = lane + 32 * k;
+      if (y < Ny)
+        d[y] = cadd(cadd(cik(kx, ua[k]), sband<S1>(T[q], d1j, d1w, y)), cik(kz, wa[k]));
+    }
+  }
   __syncwarp();
   // Stage 1: f_hat (wall rows zero)
-  for (int y = lane; y < Ny; y += 32) {
-    T[y] = Nvj[y];
-    T[Ny + y] = Nvn[y];
-  }
-  __syncwarp();
-  for (int y = lane; y < Ny; y += 32) {
-    double2 fy = make_double2(0.0, 0.0);
-    if (y > 0 && y < Ny - 1) {
-      const double2 divNj = cadd(cadd(cik(kx, Nuj[y]), sband<S1>(T, d1j, d1w, y)),
-                                 cik(kz, Nwj[y]));
-      const double2 divNn = cadd(cadd(cik(kx, Nun[y]), sband<S1>(T + Ny, d1j, d1w, y)),
-                                 cik(kz, Nwn[y]));
-      const double2 dy = T[2 * Ny + y];
-      const double2 Lkd = csub(sband<S2>(T + 2 * Ny, d2j, d2w, y), cscale(dy, k2));
-      const double2 dd = make_double2(dy.x / dt, dy.y / dt);
-      fy = cadd(cadd(cadd(dd, cscale(divNj, c)), cscale(divNn, omc)),
-                cscale(Lkd, omc_nu));
-    }
-    f[y] = fy;
-  }
-  cp_async_wait_all();
-  __syncwarp();
-  finish_factors<KL>(AB, dpiv, RS, Ny, lane, a.status);
-  __syncwarp();
-  // Stage 2: p_P = Lk^-1 f_hat (real / imaginary columns on lanes 0, 1)
-  if (lane < 2) {
-    double* col = reinterpret_cast<double*>(f) + lane;
-    forward_chain<KL, RS>(AB, dpiv, col, Ny);
-    backward_chain<KL, NU, RS>(AB, col, Ny);
-  }
-  __syncwarp();
-  stage_factors<KL, NU, RS>(AB, dpiv, a.Hk_ab + abase, a.Hk_piv + mo, Ny, row0, lane);
-  // Stage 3: R = Hk^- u^n - grad p_P + c N_j + (1-c) N_n (wall rows zero)
-  for (int y = lane; y < Ny; y += 32) {
-    T[y] = un[y];
-    T[Ny + y] = vn[y];
-    T[2 * Ny + y] = wn[y];
-  }
-  __syncwarp();
-  const double idt = 1.0 / dt;
-  for (int y = lane; y < Ny; y += 32) {
-    double2 ru = make_double2(0.0, 0.0), rv = ru, rw = ru;
-    if (y > 0 && y < Ny - 1) {
-      const double2 p = f[y];
-      const double2 dxp = cik(kx, p);
-      const double2 dyp = sband<S1>(f, d1j, d1w, y);
-      const double2 dzp = cik(kz, p);
-      const double2 u = T[y], v = T[Ny + y], w = T[2 * Ny + y];
-      const double2 D2u = sband<S2>(T, d2j, d2w, y);
-      const double2 D2v = sband<S2>(T + Ny, d2j, d2w, y);
-      const double2 D2w = sband<S2>(T + 2 * Ny, d2j, d2w, y);
-      const double2 hu = cadd(cscale(u, idt), cscale(csub(D2u, cscale(u, k2)), omc_nu));
-      const double2 hv = cadd(cscale(v, idt), cscale(csub(D2v, cscale(v, k2)), omc_nu));
-      const double2 hw = cadd(cscale(w, idt), cscale(csub(D2w, cscale(w, k2)), omc_nu));
-      ru = cadd(cadd(csub(hu, dxp), cscale(Nuj[y], c)), cscale(Nun[y], omc));
-      rv = cadd(cadd(csub(hv, dyp), cscale(Nvj[y], c)), cscale(Nvn[y], omc));
-      rw = cadd(cadd(csub(hw, dzp), cscale(Nwj[y], c)), cscale(Nwn[y], omc));
-    }
-    R[y] = ru;
-    R[Ny + y] = rv;
-    R[2 * Ny + y] = rw;
-  }
-  cp_async_wait_all();
-  __syncwarp();
-  finish_factors<KL>(AB, dpiv, RS, Ny, lane, a.status);
-  __syncwarp();
-  // Helmholtz solves for u_arb, v_arb, w_arb (6 real columns, lanes 0..5)
-  if (lane < 6) {
-    double* col = reinterpret_cast<double*>(R + (lane >> 1) * Ny) + (lane & 1);
-    forward_chain<KL, RS>(AB, dpiv, col, Ny);
-    backward_chain<KL, NU, RS>(AB, col, Ny);
-  }
-  __syncwarp();
-  // Stages 4-5: wall divergence and influence-matrix weights
-  const double2* va = R + Ny;
-  double2 dw0 = sband<S1>(va, d1j, d1w, 0);
-  const double2 dw1 = sband<S1>(va, d1j, d1w, Ny - 1);
-  if (k2zero) dw0 = make_double2(0.0, 0.0);
-  const double* Mi = a.M_inv + (long long)m * 4;
-  const double2 a1 = make_double2(-(Mi[0] * dw0.x + Mi[1] * dw1.x),
-                                  -(Mi[0] * dw0.y + Mi[1] * dw1.y));
-  const double2 a2 = make_double2(-(Mi[2] * dw0.x + Mi[3] * dw1.x),
-                                  -(Mi[2] * dw0.y + Mi[3] * dw1.y));
-  // Stage 6: assemble, store, correction norm
-  const double km = (ix == 0) ? 1.0 : 2.0;
-  const double* v1 = a.v1 + mo;
-  const double* v2 = a.v2 + mo;
-  const double* q1 = a.q1 + mo;
-  const double* q2 = a.q2 + mo;
-  double acc = 0.0;
-  for (int y = lane; y < Ny; y += 32) {
-    const double2 vnew = cadd(cadd(R[Ny + y], cscale(a1, v1[y])), cscale(a2, v2[y]));
-    const double2 q = cadd(cscale(a1, q1[y]), cscale(a2, q2[y]));
-    const double2 unew = csub(R[y], cik(kx, q));
-    const double2 wnew = csub(R[2 * Ny + y], cik(kz, q));
-    const double2 cu = csub(unew, vel_j[mo + y]);
-    const double2 cv = csub(vnew, vel_j[CS + mo + y]);
-    const double2 cw = csub(wnew, vel_j[2 * CS + mo + y]);
-    vel_new[mo + y] = unew;
-    vel_new[CS + mo + y] = vnew;
-    vel_new[2 * CS + mo + y] = wnew;
-    if (corr_out) {
-      corr_out[mo + y] = cu;
-      corr_out[CS + mo + y] = cv;
-      corr_out[2 * CS + mo + y] = cw;
-    }
-    acc += a.simpson[y] * km *
-           ((cu.x * cu.x + cu.y * cu.y) + (cv.x * cv.x + cv.y * cv.y) +
-            (cw.x * cw.x + cw.y * cw.y));
-  }
+  for (int q = 0; q < nq; ++q) {
+    const int m = mq[q];
+    const int iz = m / NKX, ix = m % NKX;
+    const double kx = a.kx[ix], kz = a.kz[iz];
+    const double k2 = kx * kx + kz * kz;
+    const long long mo = (long long)m * Ny;
+    double2 uj[YM], wj[YM], un_[YM], wn_[YM];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-  if (lane == 0 && partials) partials[m] = acc;
+    for (int k = 0; k < YM; ++k) {
+      const int y = lane + 32 * k;
+      if (y < Ny) {
+        uj[k] = nl_j[mo + y];
+        wj[k] = nl_j[2 * CS + mo + y];
+        un_[k] = nl_n[mo + y];
+        wn_[k] = nl_n[2 * CS + mo + y];
+      }
+    }
+    const double2* d = Rb[q];
+    double2* f = F[q];
+#pragma unroll
+    for (int k = 0; k < YM; ++k) {
+      const int y = lane + 32 * k;
+      if (y >= Ny) continue;
+      double2 fy = make_double2(0.0, 0.0);
+      if (y > 0 && y < Ny - 1) {
+        const double2 divNj = cadd(cadd(cik(kx, uj[k]), sband<S1>(T[q] + Ny, d1j, d1w, y)),
+                                   cik(kz, wj[k]));
+        const double2 divNn = cadd(cadd(cik(kx, un_[k]), sband<S1>(T[q] + 2 * Ny, d1j, d1w, y)),
+                                   cik(kz, wn_[k]));
+        const double2 dy = d[y];
+        const double2 Lkd = csub(sband<S2>(d, d2j, d2w, y), cscale(dy, k2));
+        const double2 dd = make_double2(dy.x / dt, dy.y / dt);
+        fy = cadd(cadd(cadd(dd, cscale(divNj, c)), cscale(divNn, omc)),
+                  cscale(Lkd, omc_nu));
+      }
+      f[y] = fy;
+    }
+  }
+  __syncwarp();
+  // group: stencil inputs of stage 3 (u^n, v^n, w^n); overlaps the L_k solve
+  for (int q = 0; q < nq; ++q) {
+    const long long mo = (long long)mq[q] * Ny;
+    for (int y = lane; y < Ny; y += 32) {
+      cp_async16(T[q] + y, vel_n + mo + y);
+      cp_async16(T[q] + Ny + y, vel_n + CS + mo + y);
+      cp_async16(T[q] + 2 * Ny + y, vel_n + 2 * CS + mo + y);
+    }
+  }
+  cp_async_commit();
+  cp_async_wait_1();  // L_k factors complete
+  __syncwarp();
+  finish_factors<KL, NU>(AB, dpiv, RS, Ny, lane, a.status);
+  __syncwarp();
+  // Stage 2: p_P = Lk^-1 f_hat (real / imaginary columns, lanes 0..2nq-1)
+  if (lane < 2 * nq) {
+    double* col = reinterpret_cast<double*>(F[lane >> 1]) + (lane & 1);
+    forward_chain<KL, RS>(AB, dpiv, col, Ny);
+    backward_chain<KL, NU, RS>(AB, col, Ny);
+  }
+  __syncwarp();
+  // group: H_k factors; overlaps stage 3
+  stage_factors<KL, NU, RS>(AB, dpiv, a.Hk_ab + abase, a.Hk_piv + pbase, Ny, row0, lane);
+  cp_async_wait_1();  // stage-3 stencil inputs complete
+  __syncwarp();
+  // Stage 3: R = Hk^- u^n - grad p_P + c N_j + (1-c) N_n (wall rows zero)
+  for (int q = 0; q < nq; ++q) {
+    const int m = mq[q];
+    const int iz = m / NKX, ix = m % NKX;
+    const double kx = a.kx[ix], kz = a.kz[iz];
+    const double k2 = kx * kx + kz * kz;
+    const long long mo = (long long)m * Ny;
+    double2 nj[3][YM], nn[3][YM];
+#pragma unroll
+    for (int k = 0; k < YM; ++k) {
+      const int y = lane + 32 * k;
+      if (y < Ny) {
+#pragma unroll
+        for (int cpt = 0; cpt < 3; ++cpt) {
+          nj[cpt][k] = nl_j[cpt * CS + mo + y];
+          nn[cpt][k] = nl_n[cpt * CS + mo + y];
+        }
+      }
+    }
+    const double2* f = F[q];
+    const double2* Tq = T[q];
+    double2* R = Rb[q];
+#pragma unroll
+    for (int k = 0; k < YM; ++k) {
+      const int y = lane + 32 * k;
+      if (y >= Ny) continue;
+      double2 ru = make_double2(0.0, 0.0), rv = ru, rw = ru;
+      if (y > 0 && y < Ny - 1) {
+        const double2 p = f[y];
+        const double2 dxp = cik(kx, p);
+        const double2 dyp = sband<S1>(f, d1j, d1w, y);
+        const double2 dzp = cik(kz, p);
+        const double2 u = Tq[y], v = Tq[Ny + y], w = Tq[2 * Ny + y];
+        const double2 D2u = sband<S2>(Tq, d2j, d2w, y);
+        const double2 D2v = sband<S2>(Tq + Ny, d2j, d2w, y);
+        const double2 D2w = sband<S2>(Tq + 2 * Ny, d2j, d2w, y);
+        const double2 hu = cadd(cscale(u, idt), cscale(csub(D2u, cscale(u, k2)), omc_nu));
+        const double2 hv = cadd(cscale(v, idt), cscale(csub(D2v, cscale(v, k2)), omc_nu));
+        const double2 hw = cadd(cscale(w, idt), cscale(csub(D2w, cscale(w, k2)), omc_nu));
+        ru = cadd(cadd(csub(hu, dxp), cscale(nj[0][k], c)), cscale(nn[0][k], omc));
+        rv = cadd(cadd(csub(hv, dyp), cscale(nj[1][k], c)), cscale(nn[1][k], omc));
+        rw = cadd(cadd(csub(hw, dzp), cscale(nj[2][k], c)), cscale(nn[2][k], omc));
+      }
+      R[y] = ru;
+      R[Ny + y] = rv;
+      R[2 * Ny + y] = rw;
+    }
+  }
+  cp_async_wait_all();  // H_k factors complete
+  __syncwarp();
+  finish_factors<KL, NU>(AB, dpiv, RS, Ny, lane, a.status);
+  __syncwarp();
+  // Helmholtz solves for u_arb, v_arb, w_arb (6 real columns per mode)
+  if (lane < 6 * nq) {
+    const int q = lane / 6, col = lane % 6;
+    double* b = reinterpret_cast<double*>(Rb[q] + (col >> 1) * Ny) + (col & 1);
+    forward_chain<KL, RS>(AB, dpiv, b, Ny);
+    backward_chain<KL, NU, RS>(AB, b, Ny);
+  }
+  __syncwarp();
+  for (int q = 0; q < nq; ++q) {
+    const int m = mq[q];
+    const int iz = m / NKX, ix = m % NKX;
+    const double kx = a.kx[ix], kz = a.kz[iz];
+    const double k2 = kx * kx + kz * kz;
+    const long long mo = (long long)m * Ny;
+    double2 vj[3][YM];
+    double c1[YM], c2[YM], e1[YM], e2[YM];
+#pragma unroll
+    for (int k = 0; k < YM; ++k) {
+      const int y = lane + 32 * k;
+      if (y < Ny) {
+#pragma unroll
+        for (int cpt = 0; cpt < 3; ++cpt) vj[cpt][k] = vel_j[cpt * CS + mo + y];
+        c1[k] = a.v1[mo + y];
+        c2[k] = a.v2[mo + y];
+        e1[k] = a.q1[mo + y];
+        e2[k] = a.q2[mo + y];
+      }
+    }
+    const double2* R = Rb[q];
+    // Stages 4-5: wall divergence and influence-matrix weights
+    const double2* va = R + Ny;
+    double2 dw0 = sband<S1>(va, d1j, d1w, 0);
+    const double2 dw1 = sband<S1>(va, d1j, d1w, Ny - 1);
+    if (k2 == 0.0) dw0 = make_double2(0.0, 0.0);
+    const double* Mi = a.M_inv + (long long)m * 4;
+    const double2 a1 = make_double2(-(Mi[0] * dw0.x + Mi[1] * dw1.x),
+                                    -(Mi[0] * dw0.y + Mi[1] * dw1.y));
+    const double2 a2 = make_double2(-(Mi[2] * dw0.x + Mi[3] * dw1.x),
+                                    -(Mi[2] * dw0.y + Mi[3] * dw1.y));
+    // Stage 6: assemble, store, correction norm
+    const double km = (ix == 0) ? 1.0 : 2.0;
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < YM; ++k) {
+      const int y = lane + 32 * k;
+      if (y >= Ny) continue;
+      const double2 vnew = cadd(cadd(R[Ny + y], cscale(a1, c1[k])), cscale(a2, c2[k]));
+      const double2 qq = cadd(cscale(a1, e1[k]), cscale(a2, e2[k]));
+      const double2 unew = csub(R[y], cik(kx, qq));
+      const double2 wnew = csub(R[2 * Ny + y], cik(kz, qq));
+      const double2 cu = csub(unew, vj[0][k]);
+      const double2 cv = csub(vnew, vj[1][k]);
+      const double2 cw = csub(wnew, vj[2][k]);
+      vel_new[mo + y] = unew;
+      vel_new[CS + mo + y] = vnew;
+      vel_new[2 * CS + mo + y] = wnew;
+      if (corr_out) {
+        corr_out[mo + y] = cu;
+        corr_out[CS + mo + y] = cv;
+        corr_out[2 * CS + mo + y] = cw;
+      }
+      acc += a.simpson[y] * km *
+             ((cu.x * cu.x + cu.y * cu.y) + (cv.x * cv.x + cv.y * cv.y) +
+              (cw.x * cw.x + cw.y * cw.y));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0 && partials) partials[m] = acc;
+  }
 }
 
-bool imm_v2_supported(int kl) { return kl == 2 || kl == 4 || kl == 6 || kl == 8; }
+bool imm_v2_supported(int kl, int ny) {
+  return (kl == 2 || kl == 4 || kl == 6 || kl == 8) && ny <= 32 * kYM;
+}
 
 // Stored U rows: the nearest NU superdiagonals; NU = kl+1 when the rows
 // above ab_row0 leave at most that many, else all 2 kl.
@@ -389,19 +548,17 @@ static int imm_nu(int kl, int row0) {
 }
 
 size_t imm_v2_smem(int Ny, int kl, int row0) {
-  return imm_mode_smem(Ny, kl, imm_nu(kl, row0));
+  return imm_mode_smem(Ny, kl, imm_nu(kl, row0), 2);
 }
 
 #define DNSB_IMM_CASE(KL_)                                                      \
   case KL_:                                                                     \
     if (nuv == KL_ + 1)                                                         \
-      imm_mode_kernel<KL_, KL_ + 1><<<NM, 32, sm, st>>>(a, vel_n, vel_j, nl_n,  \
-                                                        nl_j, vel_new, corr_out, \
-                                                        partials);              \
+      imm_mode_kernel<KL_, KL_ + 1><<<items, 32, sm, st>>>(                     \
+          a, vel_n, vel_j, nl_n, nl_j, vel_new, corr_out, partials, paired);    \
     else                                                                        \
-      imm_mode_kernel<KL_, 2 * KL_><<<NM, 32, sm, st>>>(a, vel_n, vel_j, nl_n,  \
-                                                        nl_j, vel_new, corr_out, \
-                                                        partials);              \
+      imm_mode_kernel<KL_, 2 * KL_><<<items, 32, sm, st>>>(                     \
+          a, vel_n, vel_j, nl_n, nl_j, vel_new, corr_out, partials, paired);    \
     break;
 
 cudaError_t launch_imm_v2(const ImmArgs& a, const double2* vel_n,
@@ -409,8 +566,11 @@ cudaError_t launch_imm_v2(const ImmArgs& a, const double2* vel_n,
                           const double2* nl_j, double2* vel_new,
                           double2* corr_out, double* partials, cudaStream_t st) {
   const int NM = a.NZ1 * a.NKX;
+  const int paired = a.pair_modes ? 1 : 0;
+  // paired: items (s, kx) with s in [0, (nz-1+1)/2); s = 0 is alone
+  const int items = paired ? ((a.NZ1 + 1) / 2) * a.NKX : NM;
   const int nuv = imm_nu(a.kl, a.ab_row0);
-  const size_t sm = imm_mode_smem(a.Ny, a.kl, nuv);
+  const size_t sm = imm_mode_smem(a.Ny, a.kl, nuv, paired ? 2 : 1);
   switch (a.kl) {
     DNSB_IMM_CASE(2)
     DNSB_IMM_CASE(4)
@@ -419,6 +579,41 @@ cudaError_t launch_imm_v2(const ImmArgs& a, const double2* vel_n,
     default:
       return cudaErrorInvalidValue;
   }
+  return cudaGetLastError();
+}
+
+// Whether mode (s, kx) and its mirror (nz-1-s, kx) have bit-identical LU
+// factors and pivots for every s in [1, (nz-1)/2] and kx: out[0] |= 1 on
+// any difference.
+__global__ void ab_pair_check_kernel(const double* __restrict__ ab,
+                                     const int* __restrict__ piv, int nz1,
+                                     int nkx, int rows, int ny, int* out) {
+  const int npos = (nz1 - 1) / 2;  // s = 1 .. npos
+  const long long per = (long long)(rows + 1) * ny;
+  const long long n = (long long)npos * nkx * per;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long item = i / per;
+    const long long e = i % per;
+    const int s = 1 + (int)(item / nkx), ix = (int)(item % nkx);
+    const long long ma = (long long)s * nkx + ix;
+    const long long mb = (long long)(nz1 - s) * nkx + ix;
+    bool same;
+    if (e < (long long)rows * ny) {
+      same = __double_as_longlong(ab[ma * rows * ny + e]) ==
+             __double_as_longlong(ab[mb * rows * ny + e]);
+    } else {
+      const long long j = e - (long long)rows * ny;
+      same = piv[ma * ny + j] == piv[mb * ny + j];
+    }
+    if (!same) atomicOr(out, 1);
+  }
+}
+
+cudaError_t launch_ab_pair_check(const double* ab, const int* piv, int nz1,
+                                 int nkx, int rows, int ny, int* out,
+                                 cudaStream_t st) {
+  ab_pair_check_kernel<<<592, 256, 0, st>>>(ab, piv, nz1, nkx, rows, ny, out);
   return cudaGetLastError();
 }
 

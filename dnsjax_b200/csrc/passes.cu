@@ -110,8 +110,100 @@ col_pass_kernel(ColPassArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Column pass, two register stages (M = 8 R1): stage 1 (radix R1, Ns = 1)
+// loads its inputs from global memory (zero-padding applied on load),
+// stage 2 (radix 8, Ns = R1) stores its outputs to global memory
+// (truncation applied on store); one shared buffer in between.
+// ---------------------------------------------------------------------------
+constexpr int kC2Cols = 16;
+constexpr int kC2Threads = 128;
+
+size_t col_pass2_smem(int M) {
+  return sizeof(double2) * (size_t)(M * kC2Cols + M);
+}
+
+template <int ML, int SIGN>
+__global__ void __launch_bounds__(kC2Threads)
+col_pass2_kernel(ColPassArgs a) {
+  constexpr int M = ML, R1 = M / 8, C = kC2Cols;
+  extern __shared__ double2 sm[];
+  double2* X = sm;  // [t][C]
+  double2* tw = X + M * C;
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.x * C;
+  const long long o = blockIdx.y;
+  const long long f = blockIdx.z;
+  const double2* in = a.in + f * a.in_fs + o * a.in_os + i0;
+  double2* out = a.out + f * a.out_fs + o * a.out_os + i0;
+  const int ni = min(C, a.nI - i0);
+  load_twiddles(tw, a.tw, M);
+  __syncthreads();
+  for (int it = tid; it < 8 * C; it += kC2Threads) {
+    const int c = it % C, j = it / C;
+    double2 v[R1];
+#pragma unroll
+    for (int i = 0; i < R1; ++i) {
+      const int t = j + 8 * i;
+      double2 z = make_double2(0.0, 0.0);
+      if (c < ni) {
+        if (SIGN > 0) {
+          const int sidx = pos_to_stored(t, a.nstored, M);
+          if (sidx >= 0) z = in[sidx * a.in_ts + c];
+        } else {
+          z = in[t * a.in_ts + c];
+        }
+      }
+      v[i] = z;
+    }
+    dft_3p<R1, SIGN>(v, tw, 8);
+#pragma unroll
+    for (int i = 0; i < R1; ++i) X[(j * R1 + i) * C + c] = v[i];
+  }
+  __syncthreads();
+  const double sc = 1.0 / M;
+  for (int it = tid; it < R1 * C; it += kC2Threads) {
+    const int c = it % C, k = it / C;
+    double2 z[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) z[i] = X[(k + R1 * i) * C + c];
+#pragma unroll
+    for (int i = 1; i < 8; ++i) {
+      double2 w = tw[i * k];
+      if (SIGN > 0) w.y = -w.y;
+      z[i] = cmul(z[i], w);
+    }
+    dft8(z, SIGN);
+    if (c < ni) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int t = k + R1 * i;
+        if (SIGN > 0) {
+          out[t * a.out_ts + c] = z[i];
+        } else {
+          const int sidx = pos_to_stored(t, a.nstored, M);
+          if (sidx >= 0) out[sidx * a.out_ts + c] = cscale(z[i], sc);
+        }
+      }
+    }
+  }
+}
+
 cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
                             cudaStream_t st) {
+  const int L = a.plan.L;
+  if (L == 48 || L == 72 || L == 96 || L == 192) {
+    dim3 g2((a.nI + kC2Cols - 1) / kC2Cols, nO, nfields);
+    const size_t sm2 = col_pass2_smem(L);
+#define DNSB_C2(LL)                                                           \
+  case LL:                                                                    \
+    if (a.inverse) col_pass2_kernel<LL, 1><<<g2, kC2Threads, sm2, st>>>(a);   \
+    else col_pass2_kernel<LL, -1><<<g2, kC2Threads, sm2, st>>>(a);            \
+    break;
+    switch (L) { DNSB_C2(48) DNSB_C2(72) DNSB_C2(96) DNSB_C2(192) }
+#undef DNSB_C2
+    return cudaGetLastError();
+  }
   dim3 grid((a.nI + kTile - 1) / kTile, nO, nfields);
   size_t sm = col_pass_smem(a.plan.L);
   DNSB_DISPATCH(a.plan.L, col_pass_kernel, grid, sm, st, a);
@@ -256,12 +348,196 @@ x_pass_kernel(XPassArgs a) {
   }
 }
 
+template <int ML>
+__global__ void __launch_bounds__(kX2Threads) x_pass2_kernel(XPassArgs a);
+
 cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
   dim3 grid((a.nrows + kXRows - 1) / kXRows);
   // The compile-time variants assume nx/2 = M/3 (3/2 oversampling).
   const int L = (a.nkx * 3 == a.plan.L) ? a.plan.L : -1;
+  if (L == 48 || L == 72 || L == 96 || L == 192) {
+    dim3 g2((a.nrows + kX2Rows - 1) / kX2Rows);
+    const size_t sm2 = x_pass2_smem(L, a.nkx);
+    switch (L) {
+      case 48: x_pass2_kernel<48><<<g2, kX2Threads, sm2, st>>>(a); break;
+      case 72: x_pass2_kernel<72><<<g2, kX2Threads, sm2, st>>>(a); break;
+      case 96: x_pass2_kernel<96><<<g2, kX2Threads, sm2, st>>>(a); break;
+      default: x_pass2_kernel<192><<<g2, kX2Threads, sm2, st>>>(a); break;
+    }
+    return cudaGetLastError();
+  }
   DNSB_DISPATCH(L, x_pass_kernel, grid, x_pass_smem(a.plan.L), st, a);
   return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// x pass, two register stages (M = 8 R1, R1 = M/8 = 3P): inverse radix-R1
+// stage straight from the staged half spectra; inverse radix-8 stage, the
+// rotational product and the first forward radix-8 stage fused in one
+// thread (the 8 positions k + R1 i a radix-8 output holds are the inputs of
+// the forward radix-8 stage); forward radix-R1 stage; unpack and store.
+// ---------------------------------------------------------------------------
+size_t x_pass2_smem(int M, int nkx) {
+  const size_t S = (size_t)6 * nkx * kX2Rows, Y = (size_t)M * 2 * kX2Rows;
+  const size_t X = (size_t)M * 3 * kX2Rows;
+  return sizeof(double2) * ((S > Y ? S : Y) + X + M);
+}
+
+template <int ML>
+__global__ void __launch_bounds__(kX2Threads)
+x_pass2_kernel(XPassArgs a) {
+  constexpr int M = ML, R1 = M / 8, R = kX2Rows, NKX = ML / 3;
+  constexpr int CI = 3 * R, CF = 2 * R;
+  constexpr int SZ_S = 6 * NKX * R, SZ_Y = M * CF;
+  constexpr int SZ_SY = SZ_S > SZ_Y ? SZ_S : SZ_Y;
+  extern __shared__ double2 sm[];
+  double2* S = sm;            // staged half spectra, S[(f*NKX + k)*R + r]
+  double2* Y = sm;            // forward stage-1 output [t][CF] (after S dies)
+  double2* X = sm + SZ_SY;    // inverse stage-A output [t][CI]; later [t][CF]
+  double2* tw = X + M * CI;
+  const int tid = threadIdx.x;
+  const int r0 = blockIdx.x * R;
+  const int nr = min(R, a.nrows - r0);
+  __shared__ long long s_off[kX2Rows];
+  __shared__ int s_y[kX2Rows];
+  if (tid < R) {
+    const int row = r0 + tid;
+    const int outer = row / a.inner_n, inner = row % a.inner_n;
+    s_off[tid] = (long long)outer * a.so + (long long)inner * a.si;
+    s_y[tid] = a.y_outer ? outer : inner;
+  }
+  load_twiddles(tw, a.tw, M);
+  __syncthreads();
+  for (int idx = tid; idx < 6 * NKX * R; idx += kX2Threads) {
+    int r, k, f;
+    if (a.rows_fast) {
+      r = idx % R;
+      k = (idx / R) % NKX;
+      f = idx / (R * NKX);
+    } else {
+      k = idx % NKX;
+      r = (idx / NKX) % R;
+      f = idx / (R * NKX);
+    }
+    double2 v = make_double2(0.0, 0.0);
+    if (r < nr) v = a.in[f * a.in_fs + s_off[r] + k * a.ks];
+    S[(f * NKX + k) * R + r] = v;
+  }
+  __syncthreads();
+  // Stage A: inverse radix R1 (Ns = 1) on Z = A + iB, built on the fly.
+  for (int it = tid; it < 8 * CI; it += kX2Threads) {
+    const int col = it % CI, j = it / CI;
+    const int r = col / 3, pr = col % 3;
+    const double2* A = S + (2 * pr) * NKX * R + r;
+    const double2* B = S + (2 * pr + 1) * NKX * R + r;
+    double2 v[R1];
+#pragma unroll
+    for (int i = 0; i < R1; ++i) {
+      const int t = j + 8 * i;
+      double2 z = make_double2(0.0, 0.0);
+      if (t == 0) {
+        z = make_double2(A[0].x, B[0].x);
+      } else if (t < NKX) {
+        const double2 av = A[t * R], bv = B[t * R];
+        z = make_double2(av.x - bv.y, av.y + bv.x);
+      } else if (M - t < NKX) {
+        const double2 av = A[(M - t) * R], bv = B[(M - t) * R];
+        z = make_double2(av.x + bv.y, -av.y + bv.x);
+      }
+      v[i] = z;
+    }
+    dft_3p<R1, 1>(v, tw, 8);
+#pragma unroll
+    for (int i = 0; i < R1; ++i) X[(j * R1 + i) * CI + col] = v[i];
+  }
+  __syncthreads();
+  // Stage B: inverse radix 8 (Ns = R1) -> physical values at t = k + R1 i;
+  // rotational product there; forward radix-8 stage (Ns = 1) on the same t.
+  for (int it = tid; it < R1 * R; it += kX2Threads) {
+    const int r = it % R, k = it / R;
+    double2 z[3][8];
+#pragma unroll
+    for (int pr = 0; pr < 3; ++pr) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) z[pr][i] = X[(k + R1 * i) * CI + 3 * r + pr];
+#pragma unroll
+      for (int i = 1; i < 8; ++i) {
+        double2 w = tw[i * k];
+        w.y = -w.y;
+        z[pr][i] = cmul(z[pr][i], w);
+      }
+      dft8(z[pr], 1);
+    }
+    double2 F0[8], F1[8];
+    const bool live = r < nr;
+    const int y = s_y[r];
+    const int ny = a.ny_grid;
+    const double U0 = live ? a.U[y] : 0.0, U1 = live ? a.U[ny + y] : 0.0,
+                 U2 = live ? a.U[2 * ny + y] : 0.0;
+    const double C0 = live ? a.cU[y] : 0.0, C1 = live ? a.cU[ny + y] : 0.0,
+                 C2 = live ? a.cU[2 * ny + y] : 0.0;
+    const double N0 = live ? a.nU[y] : 0.0, N1 = live ? a.nU[ny + y] : 0.0,
+                 N2 = live ? a.nU[2 * ny + y] : 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const double u0 = z[0][i].x, u1 = z[0][i].y, u2 = z[1][i].x;
+      const double w0 = z[1][i].y, w1 = z[2][i].x, w2 = z[2][i].y;
+      const double n0 = u1 * w2 - u2 * w1;
+      const double n1 = u2 * w0 - u0 * w2;
+      const double n2 = u0 * w1 - u1 * w0;
+      const double b0 = (u1 * C2 - u2 * C1) + (U1 * w2 - U2 * w1) + N0;
+      const double b1 = (u2 * C0 - u0 * C2) + (U2 * w0 - U0 * w2) + N1;
+      const double b2 = (u0 * C1 - u1 * C0) + (U0 * w1 - U1 * w0) + N2;
+      F0[i] = live ? make_double2(n0 + b0, n1 + b1) : make_double2(0.0, 0.0);
+      F1[i] = live ? make_double2(n2 + b2, 0.0) : make_double2(0.0, 0.0);
+    }
+    dft8(F0, -1);
+    dft8(F1, -1);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      Y[(k * 8 + i) * CF + 2 * r] = F0[i];
+      Y[(k * 8 + i) * CF + 2 * r + 1] = F1[i];
+    }
+  }
+  __syncthreads();
+  // Stage C: forward radix R1 (Ns = 8), natural order into X[t][CF].
+  for (int it = tid; it < 8 * CF; it += kX2Threads) {
+    const int col = it % CF, j = it / CF;
+    double2 v[R1];
+#pragma unroll
+    for (int i = 0; i < R1; ++i) v[i] = Y[(j + 8 * i) * CF + col];
+#pragma unroll
+    for (int i = 1; i < R1; ++i) v[i] = cmul(v[i], tw[i * j]);
+    dft_3p<R1, -1>(v, tw, 8);
+#pragma unroll
+    for (int i = 0; i < R1; ++i) X[(j + 8 * i) * CF + col] = v[i];
+  }
+  __syncthreads();
+  // Unpack the real-field spectra, truncate to NKX, scale 1/M, store.
+  const double h = 0.5 / M;
+  for (int idx = tid; idx < 3 * NKX * R; idx += kX2Threads) {
+    int r, k, f;
+    if (a.rows_fast) {
+      r = idx % R;
+      k = (idx / R) % NKX;
+      f = idx / (R * NKX);
+    } else {
+      k = idx % NKX;
+      r = (idx / NKX) % R;
+      f = idx / (R * NKX);
+    }
+    if (r >= nr) continue;
+    const int col = 2 * r + (f == 2 ? 1 : 0);
+    const double2 Z = X[k * CF + col];
+    const double2 Zm = X[((M - k) % M) * CF + col];
+    double2 v;
+    if (f == 1) {
+      v = make_double2((Z.y + Zm.y) * h, (Zm.x - Z.x) * h);
+    } else {
+      v = make_double2((Z.x + Zm.x) * h, (Z.y - Zm.y) * h);
+    }
+    a.out[f * a.out_fs + s_off[r] + k * a.ks] = v;
+  }
 }
 
 // x pass to physical values only (spec_to_phys of 3 fields).
@@ -665,7 +941,13 @@ cudaError_t set_pass_attributes(int max_smem) {
   const void* fns[] = {DNSB_ALL_SIZES(col_pass_kernel), DNSB_ALL_SIZES(x_pass_kernel),
                        DNSB_ALL_SIZES(x_phys_kernel), DNSB_ALL_SIZES(x_fwd_kernel),
                        DNSB_ALL_SIZES(yinv_kernel), DNSB_ALL_SIZES(yfwd_kernel),
-                       DNSB_ALL_SIZES(zinv_curl_kernel)};
+                       DNSB_ALL_SIZES(zinv_curl_kernel),
+                       (const void*)x_pass2_kernel<48>, (const void*)x_pass2_kernel<72>,
+                       (const void*)x_pass2_kernel<96>, (const void*)x_pass2_kernel<192>,
+                       (const void*)col_pass2_kernel<48, 1>, (const void*)col_pass2_kernel<48, -1>,
+                       (const void*)col_pass2_kernel<72, 1>, (const void*)col_pass2_kernel<72, -1>,
+                       (const void*)col_pass2_kernel<96, 1>, (const void*)col_pass2_kernel<96, -1>,
+                       (const void*)col_pass2_kernel<192, 1>, (const void*)col_pass2_kernel<192, -1>};
   for (const void* f : fns) {
     cudaError_t r = allow_dynamic_smem(f, max_smem);
     if (r != cudaSuccess) e = r;

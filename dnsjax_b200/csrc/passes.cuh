@@ -15,6 +15,9 @@ namespace dnsb {
 constexpr int kTile = 8;     // columns per CTA in the column passes
 constexpr int kXRows = 4;    // physical rows per CTA in the x pass
 constexpr int kPassThreads = 256;
+constexpr int kX2Rows = 4;       // physical rows per CTA in the two-stage x pass
+constexpr int kX2Threads = 128;
+size_t x_pass2_smem(int M, int nkx);
 
 // Generic strided column pass: element (f, o, t, i) at
 // base + f*fs + o*os + t*ts + i, with i the contiguous inner index.

@@ -75,6 +75,7 @@ struct ImmArgs {
   const double* M_inv;    // [NZ1][NKX][2][2]
   int* status;            // set nonzero on a pivot index out of range
   int ab_row0;            // first ab row with a nonzero entry in any mode
+  int pair_modes;         // 1: (s, kx) and (nz-1-s, kx) share LU factors
 };
 
 constexpr int kImmWarps = 4;  // modes per CTA (one warp each)
@@ -90,7 +91,7 @@ size_t imm_smem(int Ny);
 cudaError_t set_solver_attributes(int max_smem);
 
 // Register-window IMM kernel (kl in {2, 4, 6, 8}), one warp per mode.
-bool imm_v2_supported(int kl);
+bool imm_v2_supported(int kl, int ny);
 size_t imm_v2_smem(int Ny, int kl, int row0);
 cudaError_t launch_imm_v2(const ImmArgs& a, const double2* vel_n,
                           const double2* vel_j, const double2* nl_n,
@@ -99,6 +100,9 @@ cudaError_t launch_imm_v2(const ImmArgs& a, const double2* vel_n,
 cudaError_t set_imm_v2_attributes(int max_smem);
 cudaError_t launch_ab_first_row(const double* ab, long long nmodes, int rows,
                                 int ny, int kuu, int* out, cudaStream_t st);
+cudaError_t launch_ab_pair_check(const double* ab, const int* piv, int nz1,
+                                 int nkx, int rows, int ny, int* out,
+                                 cudaStream_t st);
 
 // Simpson-weighted k_metric |v|^2 per block (Couette norm).
 cudaError_t launch_couette_norm2(const ImmArgs& a, const double2* v,

@@ -99,3 +99,15 @@ def test_trajectory(setup, fused):
     assert res.corrector_iterations == list(g["iters"])
     assert rel_l2(host(res.state), g["uN"]) < TRAJ_TOL
     np.testing.assert_allclose(res.errors, g["errors"], rtol=1e-6)
+
+
+@pytest.mark.parametrize("name", [c for c in GOLDEN_CASES if c.startswith("couette")])
+def test_couette_imm_unpaired(name, monkeypatch):
+    """The IMM kernel without the (kz, -kz) factor sharing gives the same."""
+    monkeypatch.setenv("DNSB_IMM_PAIRS", "0")
+    case, g = load_golden(name)
+    flow = make_flow(case)
+    u0, r0, p0, r1 = (dev(g[k]) for k in ("u0", "rhs0", "pred0", "rhs1"))
+    assert rel_l2(host(flow.predict(u0, r0)), g["pred0"]) < CALL_TOL
+    new, _ = flow.correct(u0, p0, r0, r1)
+    assert rel_l2(host(new), g["corr_state0"]) < CALL_TOL

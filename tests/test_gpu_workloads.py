@@ -149,3 +149,14 @@ def test_kolmogorov_128_rhs():
     assert rel_l2(host(flow.get_rhs(dev(u0))), orc.get_rhs(u0)) < 1e-12
     phys = flow.spec_to_phys(dev(u0))
     assert rel_l2(host(flow.phys_to_spec(phys)), u0) < 1e-13
+
+
+@pytest.mark.parametrize("n", [48, 64])
+def test_kolmogorov_rhs_sizes(n):
+    """Padded lengths 72 and 96 (the 48^3 / 64^3 ensemble members)."""
+    from dnsjax_b200 import initial
+
+    flow, orc = kolmogorov(n, 60.0, 0.01)
+    u0 = initial.periodic_field(n, n, n, 2 * pi, 2 * pi, 2 * pi, n,
+                                initial.kolmogorov_spectrum_cfg0, 1e-2)
+    assert rel_l2(host(flow.get_rhs(dev(u0))), orc.get_rhs(u0)) < 1e-12
