@@ -67,9 +67,77 @@ struct Rec {
 // column b (stride 2) of length Ny.  dpiv[j] = ipiv[j] - j in [0, KL].
 // The window holds b[j..j+KL] in registers, slot(o, ph) = (o + ph) % W; the
 // loop is unrolled by W so slots are compile-time.  Each block of W steps
-// first loads all its multipliers, pivots and entering values into
-// registers (one exposed shared-memory latency per block), then runs the
-// recurrence from registers; the row interchange is a warp-uniform switch.
+// first loads its multipliers (16-byte pairs), pivots and entering values
+// into registers, then runs the recurrence from registers.  The row
+// interchange is chosen once per block (warp-uniform: every lane solves
+// the same factors): no interchange, interchanges with the next row only
+// (two selects per step), or the general case (a switch per step).  Full
+// blocks carry no per-step bounds test; the last, partial block does.
+template <int KL, int MODE, bool TAIL>
+__device__ __forceinline__ void forward_steps(double* __restrict__ b, int j0, int nsteps,
+                                              double (&w)[KL + 1],
+                                              const double (&Lr)[KL + 1][KL],
+                                              const int (&dr)[KL + 1],
+                                              const double (&be)[KL + 1]) {
+  constexpr int W = KL + 1;
+#pragma unroll
+  for (int ph = 0; ph < W; ++ph) {
+    const int j = j0 + ph;
+    if (!TAIL || j < nsteps) {
+      double bpj = w[ph % W];
+      if (MODE == 1) {
+        const double x1 = w[(1 + ph) % W];
+        const bool p = dr[ph] != 0;
+        w[(1 + ph) % W] = p ? bpj : x1;
+        bpj = p ? x1 : bpj;
+      } else if (MODE == 2) {
+        switch (dr[ph]) {
+#define DNSB_PIV(I)                  \
+  case I:                            \
+    if (I <= KL) {                   \
+      bpj = w[(I + ph) % W];         \
+      w[(I + ph) % W] = w[ph % W];   \
+    }                                \
+    break;
+          DNSB_PIV(1) DNSB_PIV(2) DNSB_PIV(3) DNSB_PIV(4)
+          DNSB_PIV(5) DNSB_PIV(6) DNSB_PIV(7) DNSB_PIV(8)
+#undef DNSB_PIV
+          default: break;
+        }
+      }
+      b[2 * j] = bpj;
+#pragma unroll
+      for (int i = 1; i <= KL; ++i) w[(i + ph) % W] -= Lr[ph][i - 1] * bpj;
+      w[ph % W] = be[ph];  // offset 0 leaves; b[j+W] enters at offset KL
+    }
+  }
+}
+
+template <int KL, int RS, bool TAIL>
+__device__ __forceinline__ void forward_load(const double* __restrict__ AB,
+                                             const int* __restrict__ dpiv,
+                                             const double* __restrict__ b, int j0,
+                                             int nsteps, int Ny,
+                                             double (&Lr)[KL + 1][KL], int (&dr)[KL + 1],
+                                             double (&be)[KL + 1]) {
+  constexpr int W = KL + 1;
+  static_assert(KL % 2 == 0, "multipliers are loaded in pairs");
+#pragma unroll
+  for (int ph = 0; ph < W; ++ph) {
+    const int j = TAIL ? min(j0 + ph, nsteps - 1) : j0 + ph;
+    const double2* rec = reinterpret_cast<const double2*>(AB + j * RS);
+#pragma unroll
+    for (int i = 0; i < KL / 2; ++i) {
+      const double2 t = rec[i];
+      Lr[ph][2 * i] = t.x;
+      Lr[ph][2 * i + 1] = t.y;
+    }
+    dr[ph] = dpiv[j];
+    const int e = j0 + ph + W;
+    be[ph] = (e < Ny) ? b[2 * e] : 0.0;
+  }
+}
+
 template <int KL, int RS>
 __device__ __forceinline__ void forward_chain(const double* __restrict__ AB,
                                               const int* __restrict__ dpiv,
@@ -79,43 +147,25 @@ __device__ __forceinline__ void forward_chain(const double* __restrict__ AB,
 #pragma unroll
   for (int o = 0; o < W; ++o) w[o] = (o < Ny) ? b[2 * o] : 0.0;
   const int nsteps = Ny - 1;
-  for (int j0 = 0; j0 < nsteps; j0 += W) {
-    double Lr[W][KL];
-    int dr[W];
-    double be[W];
+  const int jfull = (nsteps / W) * W;
+  double Lr[W][KL];
+  int dr[W];
+  double be[W];
+  for (int j0 = 0; j0 < jfull; j0 += W) {
+    forward_load<KL, RS, false>(AB, dpiv, b, j0, nsteps, Ny, Lr, dr, be);
+    int dm = 0;
 #pragma unroll
-    for (int ph = 0; ph < W; ++ph) {
-      const int j = min(j0 + ph, nsteps - 1);
-#pragma unroll
-      for (int i = 0; i < KL; ++i) Lr[ph][i] = AB[j * RS + i];
-      dr[ph] = dpiv[j];
-      const int e = j0 + ph + W;
-      be[ph] = (e < Ny) ? b[2 * e] : 0.0;
-    }
-#pragma unroll
-    for (int ph = 0; ph < W; ++ph) {
-      const int j = j0 + ph;
-      if (j < nsteps) {
-        double bpj = w[ph % W];
-        switch (dr[ph]) {  // warp-uniform: every lane solves the same factors
-#define DNSB_PIV(I)                                  \
-  case I:                                            \
-    if (I <= KL) {                                   \
-      bpj = w[(I + ph) % W];                         \
-      w[(I + ph) % W] = w[ph % W];                   \
-    }                                                \
-    break;
-          DNSB_PIV(1) DNSB_PIV(2) DNSB_PIV(3) DNSB_PIV(4)
-          DNSB_PIV(5) DNSB_PIV(6) DNSB_PIV(7) DNSB_PIV(8)
-#undef DNSB_PIV
-          default: break;
-        }
-        b[2 * j] = bpj;
-#pragma unroll
-        for (int i = 1; i <= KL; ++i) w[(i + ph) % W] -= Lr[ph][i - 1] * bpj;
-        w[ph % W] = be[ph];  // offset 0 leaves; b[j+W] enters at offset KL
-      }
-    }
+    for (int ph = 0; ph < W; ++ph) dm = max(dm, dr[ph]);
+    if (dm == 0)
+      forward_steps<KL, 0, false>(b, j0, nsteps, w, Lr, dr, be);
+    else if (dm == 1)
+      forward_steps<KL, 1, false>(b, j0, nsteps, w, Lr, dr, be);
+    else
+      forward_steps<KL, 2, false>(b, j0, nsteps, w, Lr, dr, be);
+  }
+  if (jfull < nsteps) {
+    forward_load<KL, RS, true>(AB, dpiv, b, jfull, nsteps, Ny, Lr, dr, be);
+    forward_steps<KL, 2, true>(b, jfull, nsteps, w, Lr, dr, be);
   }
   // b[Ny-1] sits at offset 0 after the last step: slot nsteps % W.
   const int last = nsteps % W;
@@ -126,24 +176,32 @@ __device__ __forceinline__ void forward_chain(const double* __restrict__ AB,
   b[2 * (Ny - 1)] = v;
 }
 
-// One half-block of back substitution: phases PH0 <= ph < PH1 of the block
-// starting at j0.  Record slot KL holds 1/U_jj and slots KL+i hold
-// U_{j-i,j}/U_jj, so the recurrence is one FMA deep: b[j-i] -= that * b[j];
-// x_j = b[j] / U_jj is stored off the dependency chain.
-template <int KL, int NU, int RS, int PH0, int PH1>
-__device__ __forceinline__ void backward_half(const double* __restrict__ AB,
+// Phases PH0 <= ph < PH1 of a back-substitution block starting at row j0
+// (row j = j0 - ph).  Record slot KL holds 1/U_jj and slots KL+i hold
+// U_{j-i,j}/U_jj (i = 1..NU), so the recurrence is one FMA deep:
+// b[j-i] -= that * b[j]; x_j = b[j] / U_jj is stored off the dependency
+// chain.  The window holds b[j-NU..j], slot(o, ph) = (o - ph) mod W with
+// W = NU + 1: superdiagonals beyond NU are zero and never applied.
+template <int KL, int NU, int RS, int PH0, int PH1, bool TAIL>
+__device__ __forceinline__ void backward_part(const double* __restrict__ AB,
                                               double* __restrict__ b, int j0,
-                                              double* w) {
-  constexpr int KUU = 2 * KL;
-  constexpr int W = KUU + 1;
+                                              double (&w)[NU + 1]) {
+  constexpr int W = NU + 1;
   constexpr int H = PH1 - PH0;
-  double Ur[H][NU + 1];
+  constexpr int NP = (NU + 2) / 2;  // 16-byte pairs covering slots KL..KL+NU
+  static_assert(KL % 2 == 0, "U records are loaded in pairs");
+  double Ur[H][2 * NP];
   double be[H];
 #pragma unroll
   for (int h = 0; h < H; ++h) {
-    const int j = max(j0 - (PH0 + h), 0);
+    const int j = TAIL ? max(j0 - (PH0 + h), 0) : j0 - (PH0 + h);
+    const double2* rec = reinterpret_cast<const double2*>(AB + j * RS + KL);
 #pragma unroll
-    for (int i = 0; i <= NU; ++i) Ur[h][i] = AB[j * RS + KL + i];
+    for (int i = 0; i < NP; ++i) {
+      const double2 t = rec[i];
+      Ur[h][2 * i] = t.x;
+      Ur[h][2 * i + 1] = t.y;
+    }
     const int e = j0 - (PH0 + h) - W;
     be[h] = (e >= 0) ? b[2 * e] : 0.0;
   }
@@ -151,38 +209,43 @@ __device__ __forceinline__ void backward_half(const double* __restrict__ AB,
   for (int h = 0; h < H; ++h) {
     const int ph = PH0 + h;
     const int j = j0 - ph;
-    if (j >= 0) {
-      const int st = ((KUU - ph) % W + W) % W;
+    if (!TAIL || j >= 0) {
+      const int st = ((NU - ph) % W + W) % W;
       const double bj = w[st];
       b[2 * j] = bj * Ur[h][0];
 #pragma unroll
       for (int i = 1; i <= NU; ++i) {
-        const int si = ((KUU - i - ph) % W + W) % W;
+        const int si = ((NU - i - ph) % W + W) % W;
         w[si] -= Ur[h][i] * bj;
       }
-      w[st] = be[h];  // b[j-KUU-1] enters at offset 0
+      w[st] = be[h];  // b[j-NU-1] enters at offset 0
     }
   }
 }
 
-// Back substitution with U (2*KL superdiagonals, the NU nearest stored) on
-// one real column b (stride 2).  Window b[j-KUU..j], slot(o, ph) =
-// (o - ph) mod W, loop unrolled by W in two register-loaded halves.
+// Back substitution with U (its NU nearest superdiagonals) on one real
+// column b (stride 2), in blocks of W = NU + 1 rows, each loaded in two
+// register halves.
 template <int KL, int NU, int RS>
 __device__ __forceinline__ void backward_chain(const double* __restrict__ AB,
                                                double* __restrict__ b, int Ny) {
-  constexpr int KUU = 2 * KL;
-  constexpr int W = KUU + 1;
+  constexpr int W = NU + 1;
   constexpr int H = (W + 1) / 2;
   double w[W];
 #pragma unroll
   for (int o = 0; o < W; ++o) {
-    const int idx = Ny - 1 - KUU + o;
+    const int idx = Ny - 1 - NU + o;
     w[o] = (idx >= 0) ? b[2 * idx] : 0.0;
   }
-  for (int j0 = Ny - 1; j0 >= 0; j0 -= W) {
-    backward_half<KL, NU, RS, 0, H>(AB, b, j0, w);
-    backward_half<KL, NU, RS, H, W>(AB, b, j0, w);
+  const int nfull = Ny / W;
+  int j0 = Ny - 1;
+  for (int blk = 0; blk < nfull; ++blk, j0 -= W) {
+    backward_part<KL, NU, RS, 0, H, false>(AB, b, j0, w);
+    backward_part<KL, NU, RS, H, W, false>(AB, b, j0, w);
+  }
+  if (j0 >= 0) {
+    backward_part<KL, NU, RS, 0, H, true>(AB, b, j0, w);
+    backward_part<KL, NU, RS, H, W, true>(AB, b, j0, w);
   }
 }
 
