@@ -271,37 +271,40 @@ __device__ __forceinline__ void cp_async_wait_1() {
 }
 
 // Stage one operator's factors of mode m into the record layout and its
-// validated pivot offsets; flags a pivot outside [j, j+KL].
+// pivots (threads tid = 0..nthr-1 of the CTA share the copies).
 template <int KL, int NU, int RS>
 __device__ __forceinline__ void stage_factors(double* AB, int* dpiv,
                                               const double* __restrict__ ab,
                                               const int* __restrict__ piv,
-                                              int Ny, int row0, int lane) {
+                                              int Ny, int row0, int tid, int nthr) {
   constexpr int KUU = 2 * KL;
   // L multipliers: rows KUU+1 .. KUU+KL -> record slots 0..KL-1
 #pragma unroll
   for (int i = 1; i <= KL; ++i)
-    for (int j = lane; j < Ny; j += 32)
+    for (int j = tid; j < Ny; j += nthr)
       cp_async8(AB + j * RS + (i - 1), ab + (KUU + i) * Ny + j);
   // diagonal -> slot KL (inverted after arrival)
-  for (int j = lane; j < Ny; j += 32) cp_async8(AB + j * RS + KL, ab + KUU * Ny + j);
+  for (int j = tid; j < Ny; j += nthr) cp_async8(AB + j * RS + KL, ab + KUU * Ny + j);
   // U rows KUU-i for i = 1..NU -> slots KL+i; rows above row0 are zero
 #pragma unroll
   for (int i = 1; i <= NU; ++i) {
     const int r = KUU - i;
-    for (int j = lane; j < Ny; j += 32) {
+    for (int j = tid; j < Ny; j += nthr) {
       if (r >= row0) cp_async8(AB + j * RS + KL + i, ab + r * Ny + j);
       else AB[j * RS + KL + i] = 0.0;
     }
   }
-  for (int j = lane; j < Ny; j += 32) cp_async4(dpiv + j, piv + j);
+  for (int j = tid; j < Ny; j += nthr) cp_async4(dpiv + j, piv + j);
   cp_async_commit();
 }
 
+// After the staged factors arrived: slot KL <- 1/U_jj, U slots scaled by it,
+// pivots turned into validated offsets (a pivot outside [j, j+KL] is flagged
+// and not followed).
 template <int KL, int NU>
 __device__ __forceinline__ void finish_factors(double* AB, int* dpiv, int RS,
-                                               int Ny, int lane, int* status) {
-  for (int j = lane; j < Ny; j += 32) {
+                                               int Ny, int tid, int nthr, int* status) {
+  for (int j = tid; j < Ny; j += nthr) {
     const double r = 1.0 / AB[j * RS + KL];
     AB[j * RS + KL] = r;
 #pragma unroll
@@ -317,13 +320,14 @@ __device__ __forceinline__ void finish_factors(double* AB, int* dpiv, int RS,
 
 // One work item: mode (s, kx), and, when `paired`, also its mirror
 // (nz-1-s, kx) -- the same k^2 = kx^2 + kz^2 and therefore bit-identical L_k
-// and H_k factors (checked when the operators are bound) -- so the staged
-// factors serve both and the substitution chains run on 4 / 12 lanes.
-// Stencil inputs are staged with cp.async (the stage-3 staging overlaps the
-// L_k substitution); pointwise inputs are loaded into registers for all of a
-// lane's y values before they are used.
+// and H_k factors (checked when the operators are bound).  The CTA has one
+// warp per mode of the item: all its threads stage each operator's factors
+// once, then every warp runs its own mode's stages and substitution chains
+// (2 / 6 lanes).  Stencil inputs are staged with cp.async (the stage-3
+// staging overlaps the L_k substitution); pointwise inputs are loaded into
+// registers for all of a lane's y values before they are used.
 template <int KL, int NU>
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(64)
 imm_mode_kernel(ImmArgs a, const double2* __restrict__ vel_n,
                 const double2* vel_j, const double2* __restrict__ nl_n,
                 const double2* __restrict__ nl_j, double2* vel_new,
@@ -333,31 +337,25 @@ imm_mode_kernel(ImmArgs a, const double2* __restrict__ vel_n,
   constexpr int S1 = KL + 1, S2 = KL + 2;
   constexpr int YM = kYM;
   extern __shared__ double2 sm[];
-  const int lane = threadIdx.x;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int q = tid >> 5;  // this warp's mode of the item
+  const int lane = tid & 31;
   const int NKX = a.NKX, Ny = a.Ny, NZ1 = a.NZ1;
   const int NM = NZ1 * NKX;
   const int item = blockIdx.x;
   const int row0 = a.ab_row0;
-  int nq = 1;
-  int mq[2];
+  int m0 = item, m = item;
+  bool mine = true;  // warp-uniform: the (s = 0, kx) items have one mode
   if (paired) {
-    const int ix = item % NKX, s = item / NKX;
-    mq[0] = s * NKX + ix;
-    mq[1] = (NZ1 - s) * NKX + ix;
-    nq = (s == 0) ? 1 : 2;
-  } else {
-    mq[0] = mq[1] = item;
+    const int ixp = item % NKX, s = item / NKX;
+    m0 = s * NKX + ixp;
+    m = (q == 0) ? m0 : (NZ1 - s) * NKX + ixp;
+    mine = (q == 0) || (s != 0);
   }
-  const int qmax = paired ? 2 : 1;
-  double2* T[2];
-  double2* F[2];
-  double2* Rb[2];
-#pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    T[q] = sm + q * 7 * Ny;
-    F[q] = T[q] + 3 * Ny;
-    Rb[q] = F[q] + Ny;
-  }
+  const int qmax = nthr >> 5;
+  double2* T = sm + q * 7 * Ny;  // staged stencil inputs [3][Ny]
+  double2* F = T + 3 * Ny;       // f_hat, then p_P
+  double2* R = F + Ny;           // d_hat^n, then R / (u, v, w)_arb
   double* AB = reinterpret_cast<double*>(sm + 7 * qmax * Ny);
   int* dpiv = reinterpret_cast<int*>(AB + Ny * RS);
 
@@ -370,54 +368,48 @@ imm_mode_kernel(ImmArgs a, const double2* __restrict__ vel_n,
   const double* d1w = a.d1_w;
   const int* d2j = a.d2_j0;
   const double* d2w = a.d2_w;
-  const long long abase = (long long)mq[0] * ROWS * Ny;
-  const long long pbase = (long long)mq[0] * Ny;
+  const long long abase = (long long)m0 * ROWS * Ny;
+  const long long pbase = (long long)m0 * Ny;
+  const int iz = m / NKX, ix = m % NKX;
+  const double kx = a.kx[ix], kz = a.kz[iz];
+  const double k2 = kx * kx + kz * kz;
+  const long long mo = (long long)m * Ny;
 
-  // group: stencil inputs of stages 0-1 (v^n, N^j_v, N^n_v) of each mode
-  for (int q = 0; q < nq; ++q) {
-    const long long mo = (long long)mq[q] * Ny;
+  // group: stencil inputs of stages 0-1 (v^n, N^j_v, N^n_v)
+  if (mine) {
     for (int y = lane; y < Ny; y += 32) {
-      cp_async16(T[q] + y, vel_n + CS + mo + y);
-      cp_async16(T[q] + Ny + y, nl_j + CS + mo + y);
-      cp_async16(T[q] + 2 * Ny + y, nl_n + CS + mo + y);
+      cp_async16(T + y, vel_n + CS + mo + y);
+      cp_async16(T + Ny + y, nl_j + CS + mo + y);
+      cp_async16(T + 2 * Ny + y, nl_n + CS + mo + y);
     }
   }
   cp_async_commit();
   // group: L_k factors
-  stage_factors<KL, NU, RS>(AB, dpiv, a.Lk_ab + abase, a.Lk_piv + pbase, Ny, row0, lane);
+  stage_factors<KL, NU, RS>(AB, dpiv, a.Lk_ab + abase, a.Lk_piv + pbase, Ny, row0, tid, nthr);
   cp_async_wait_1();
   __syncwarp();
 
-  for (int q = 0; q < nq; ++q) {
-    const int m = mq[q];
-    const int iz = m / NKX, ix = m % NKX;
-    const double kx = a.kx[ix], kz = a.kz[iz];
-    const long long mo = (long long)m * Ny;
-    double2 ua[YM], wa[YM];
+  if (mine) {
+    // Stage 0: d_hat^n = div u^n (kept in R until stage 3)
+    {
+      double2 ua[YM], wa[YM];
 #pragma unroll
-    for (int k = 0; k < YM; ++k) {
-      const int y = lane + 32 * k;
-      if (y < Ny) {
-        ua[k] = vel_n[mo + y];
-        wa[k] = vel_n[2 * CS + mo + y];
+      for (int k = 0; k < YM; ++k) {
+        const int y = lane + 32 * k;
+        if (y < Ny) {
+          ua[k] = vel_n[mo + y];
+          wa[k] = vel_n[2 * CS + mo + y];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < YM; ++k) {
+        const int y = lane + 32 * k;
+        if (y < Ny)
+          R[y] = cadd(cadd(cik(kx, ua[k]), sband<S1>(T, d1j, d1w, y)), cik(kz, wa[k]));
       }
     }
-    double2* d = Rb[q];  // d_hat^n lives in R until stage 3
-#pragma unroll
-    for (int k = 0; k < YM; ++k) {
-      const int y = lane + 32 * k;
-      if (y < Ny)
-        d[y] = cadd(cadd(cik(kx, ua[k]), sband<S1>(T[q], d1j, d1w, y)), cik(kz, wa[k]));
-    }
-  }
-  __syncwarp();
-  // Stage 1: f_hat (wall rows zero)
-  for (int q = 0; q < nq; ++q) {
-    const int m = mq[q];
-    const int iz = m / NKX, ix = m % NKX;
-    const double kx = a.kx[ix], kz = a.kz[iz];
-    const double k2 = kx * kx + kz * kz;
-    const long long mo = (long long)m * Ny;
+    __syncwarp();
+    // Stage 1: f_hat (wall rows zero)
     double2 uj[YM], wj[YM], un_[YM], wn_[YM];
 #pragma unroll
     for (int k = 0; k < YM; ++k) {
@@ -429,60 +421,52 @@ imm_mode_kernel(ImmArgs a, const double2* __restrict__ vel_n,
         wn_[k] = nl_n[2 * CS + mo + y];
       }
     }
-    const double2* d = Rb[q];
-    double2* f = F[q];
 #pragma unroll
     for (int k = 0; k < YM; ++k) {
       const int y = lane + 32 * k;
       if (y >= Ny) continue;
       double2 fy = make_double2(0.0, 0.0);
       if (y > 0 && y < Ny - 1) {
-        const double2 divNj = cadd(cadd(cik(kx, uj[k]), sband<S1>(T[q] + Ny, d1j, d1w, y)),
+        const double2 divNj = cadd(cadd(cik(kx, uj[k]), sband<S1>(T + Ny, d1j, d1w, y)),
                                    cik(kz, wj[k]));
-        const double2 divNn = cadd(cadd(cik(kx, un_[k]), sband<S1>(T[q] + 2 * Ny, d1j, d1w, y)),
+        const double2 divNn = cadd(cadd(cik(kx, un_[k]), sband<S1>(T + 2 * Ny, d1j, d1w, y)),
                                    cik(kz, wn_[k]));
-        const double2 dy = d[y];
-        const double2 Lkd = csub(sband<S2>(d, d2j, d2w, y), cscale(dy, k2));
+        const double2 dy = R[y];
+        const double2 Lkd = csub(sband<S2>(R, d2j, d2w, y), cscale(dy, k2));
         const double2 dd = make_double2(dy.x / dt, dy.y / dt);
         fy = cadd(cadd(cadd(dd, cscale(divNj, c)), cscale(divNn, omc)),
                   cscale(Lkd, omc_nu));
       }
-      f[y] = fy;
+      F[y] = fy;
     }
   }
   __syncwarp();
   // group: stencil inputs of stage 3 (u^n, v^n, w^n); overlaps the L_k solve
-  for (int q = 0; q < nq; ++q) {
-    const long long mo = (long long)mq[q] * Ny;
+  if (mine) {
     for (int y = lane; y < Ny; y += 32) {
-      cp_async16(T[q] + y, vel_n + mo + y);
-      cp_async16(T[q] + Ny + y, vel_n + CS + mo + y);
-      cp_async16(T[q] + 2 * Ny + y, vel_n + 2 * CS + mo + y);
+      cp_async16(T + y, vel_n + mo + y);
+      cp_async16(T + Ny + y, vel_n + CS + mo + y);
+      cp_async16(T + 2 * Ny + y, vel_n + 2 * CS + mo + y);
     }
   }
   cp_async_commit();
   cp_async_wait_1();  // L_k factors complete
-  __syncwarp();
-  finish_factors<KL, NU>(AB, dpiv, RS, Ny, lane, a.status);
-  __syncwarp();
-  // Stage 2: p_P = Lk^-1 f_hat (real / imaginary columns, lanes 0..2nq-1)
-  if (lane < 2 * nq) {
-    double* col = reinterpret_cast<double*>(F[lane >> 1]) + (lane & 1);
+  __syncthreads();
+  finish_factors<KL, NU>(AB, dpiv, RS, Ny, tid, nthr, a.status);
+  __syncthreads();
+  // Stage 2: p_P = Lk^-1 f_hat (real / imaginary columns)
+  if (mine && lane < 2) {
+    double* col = reinterpret_cast<double*>(F) + lane;
     forward_chain<KL, RS>(AB, dpiv, col, Ny);
     backward_chain<KL, NU, RS>(AB, col, Ny);
   }
-  __syncwarp();
+  __syncthreads();  // every warp is done with the L_k factors
   // group: H_k factors; overlaps stage 3
-  stage_factors<KL, NU, RS>(AB, dpiv, a.Hk_ab + abase, a.Hk_piv + pbase, Ny, row0, lane);
+  stage_factors<KL, NU, RS>(AB, dpiv, a.Hk_ab + abase, a.Hk_piv + pbase, Ny, row0, tid, nthr);
   cp_async_wait_1();  // stage-3 stencil inputs complete
   __syncwarp();
-  // Stage 3: R = Hk^- u^n - grad p_P + c N_j + (1-c) N_n (wall rows zero)
-  for (int q = 0; q < nq; ++q) {
-    const int m = mq[q];
-    const int iz = m / NKX, ix = m % NKX;
-    const double kx = a.kx[ix], kz = a.kz[iz];
-    const double k2 = kx * kx + kz * kz;
-    const long long mo = (long long)m * Ny;
+  if (mine) {
+    // Stage 3: R = Hk^- u^n - grad p_P + c N_j + (1-c) N_n (wall rows zero)
     double2 nj[3][YM], nn[3][YM];
 #pragma unroll
     for (int k = 0; k < YM; ++k) {
@@ -495,23 +479,20 @@ imm_mode_kernel(ImmArgs a, const double2* __restrict__ vel_n,
         }
       }
     }
-    const double2* f = F[q];
-    const double2* Tq = T[q];
-    double2* R = Rb[q];
 #pragma unroll
     for (int k = 0; k < YM; ++k) {
       const int y = lane + 32 * k;
       if (y >= Ny) continue;
       double2 ru = make_double2(0.0, 0.0), rv = ru, rw = ru;
       if (y > 0 && y < Ny - 1) {
-        const double2 p = f[y];
+        const double2 p = F[y];
         const double2 dxp = cik(kx, p);
-        const double2 dyp = sband<S1>(f, d1j, d1w, y);
+        const double2 dyp = sband<S1>(F, d1j, d1w, y);
         const double2 dzp = cik(kz, p);
-        const double2 u = Tq[y], v = Tq[Ny + y], w = Tq[2 * Ny + y];
-        const double2 D2u = sband<S2>(Tq, d2j, d2w, y);
-        const double2 D2v = sband<S2>(Tq + Ny, d2j, d2w, y);
-        const double2 D2w = sband<S2>(Tq + 2 * Ny, d2j, d2w, y);
+        const double2 u = T[y], v = T[Ny + y], w = T[2 * Ny + y];
+        const double2 D2u = sband<S2>(T, d2j, d2w, y);
+        const double2 D2v = sband<S2>(T + Ny, d2j, d2w, y);
+        const double2 D2w = sband<S2>(T + 2 * Ny, d2j, d2w, y);
         const double2 hu = cadd(cscale(u, idt), cscale(csub(D2u, cscale(u, k2)), omc_nu));
         const double2 hv = cadd(cscale(v, idt), cscale(csub(D2v, cscale(v, k2)), omc_nu));
         const double2 hw = cadd(cscale(w, idt), cscale(csub(D2w, cscale(w, k2)), omc_nu));
@@ -525,78 +506,70 @@ imm_mode_kernel(ImmArgs a, const double2* __restrict__ vel_n,
     }
   }
   cp_async_wait_all();  // H_k factors complete
-  __syncwarp();
-  finish_factors<KL, NU>(AB, dpiv, RS, Ny, lane, a.status);
-  __syncwarp();
-  // Helmholtz solves for u_arb, v_arb, w_arb (6 real columns per mode)
-  if (lane < 6 * nq) {
-    const int q = lane / 6, col = lane % 6;
-    double* b = reinterpret_cast<double*>(Rb[q] + (col >> 1) * Ny) + (col & 1);
+  __syncthreads();
+  finish_factors<KL, NU>(AB, dpiv, RS, Ny, tid, nthr, a.status);
+  __syncthreads();
+  // Helmholtz solves for u_arb, v_arb, w_arb (6 real columns)
+  if (mine && lane < 6) {
+    double* b = reinterpret_cast<double*>(R + (lane >> 1) * Ny) + (lane & 1);
     forward_chain<KL, RS>(AB, dpiv, b, Ny);
     backward_chain<KL, NU, RS>(AB, b, Ny);
   }
   __syncwarp();
-  for (int q = 0; q < nq; ++q) {
-    const int m = mq[q];
-    const int iz = m / NKX, ix = m % NKX;
-    const double kx = a.kx[ix], kz = a.kz[iz];
-    const double k2 = kx * kx + kz * kz;
-    const long long mo = (long long)m * Ny;
-    double2 vj[3][YM];
-    double c1[YM], c2[YM], e1[YM], e2[YM];
+  if (!mine) return;
+  double2 vj[3][YM];
+  double c1[YM], c2[YM], e1[YM], e2[YM];
 #pragma unroll
-    for (int k = 0; k < YM; ++k) {
-      const int y = lane + 32 * k;
-      if (y < Ny) {
+  for (int k = 0; k < YM; ++k) {
+    const int y = lane + 32 * k;
+    if (y < Ny) {
 #pragma unroll
-        for (int cpt = 0; cpt < 3; ++cpt) vj[cpt][k] = vel_j[cpt * CS + mo + y];
-        c1[k] = a.v1[mo + y];
-        c2[k] = a.v2[mo + y];
-        e1[k] = a.q1[mo + y];
-        e2[k] = a.q2[mo + y];
-      }
+      for (int cpt = 0; cpt < 3; ++cpt) vj[cpt][k] = vel_j[cpt * CS + mo + y];
+      c1[k] = a.v1[mo + y];
+      c2[k] = a.v2[mo + y];
+      e1[k] = a.q1[mo + y];
+      e2[k] = a.q2[mo + y];
     }
-    const double2* R = Rb[q];
-    // Stages 4-5: wall divergence and influence-matrix weights
-    const double2* va = R + Ny;
-    double2 dw0 = sband<S1>(va, d1j, d1w, 0);
-    const double2 dw1 = sband<S1>(va, d1j, d1w, Ny - 1);
-    if (k2 == 0.0) dw0 = make_double2(0.0, 0.0);
-    const double* Mi = a.M_inv + (long long)m * 4;
-    const double2 a1 = make_double2(-(Mi[0] * dw0.x + Mi[1] * dw1.x),
-                                    -(Mi[0] * dw0.y + Mi[1] * dw1.y));
-    const double2 a2 = make_double2(-(Mi[2] * dw0.x + Mi[3] * dw1.x),
-                                    -(Mi[2] * dw0.y + Mi[3] * dw1.y));
-    // Stage 6: assemble, store, correction norm
-    const double km = (ix == 0) ? 1.0 : 2.0;
-    double acc = 0.0;
-#pragma unroll
-    for (int k = 0; k < YM; ++k) {
-      const int y = lane + 32 * k;
-      if (y >= Ny) continue;
-      const double2 vnew = cadd(cadd(R[Ny + y], cscale(a1, c1[k])), cscale(a2, c2[k]));
-      const double2 qq = cadd(cscale(a1, e1[k]), cscale(a2, e2[k]));
-      const double2 unew = csub(R[y], cik(kx, qq));
-      const double2 wnew = csub(R[2 * Ny + y], cik(kz, qq));
-      const double2 cu = csub(unew, vj[0][k]);
-      const double2 cv = csub(vnew, vj[1][k]);
-      const double2 cw = csub(wnew, vj[2][k]);
-      vel_new[mo + y] = unew;
-      vel_new[CS + mo + y] = vnew;
-      vel_new[2 * CS + mo + y] = wnew;
-      if (corr_out) {
-        corr_out[mo + y] = cu;
-        corr_out[CS + mo + y] = cv;
-        corr_out[2 * CS + mo + y] = cw;
-      }
-      acc += a.simpson[y] * km *
-             ((cu.x * cu.x + cu.y * cu.y) + (cv.x * cv.x + cv.y * cv.y) +
-              (cw.x * cw.x + cw.y * cw.y));
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if (lane == 0 && partials) partials[m] = acc;
   }
+  // Stages 4-5: wall divergence and influence-matrix weights
+  const double2* va = R + Ny;
+  double2 dw0 = sband<S1>(va, d1j, d1w, 0);
+  const double2 dw1 = sband<S1>(va, d1j, d1w, Ny - 1);
+  if (k2 == 0.0) dw0 = make_double2(0.0, 0.0);
+  const double* Mi = a.M_inv + (long long)m * 4;
+  const double2 a1 = make_double2(-(Mi[0] * dw0.x + Mi[1] * dw1.x),
+                                  -(Mi[0] * dw0.y + Mi[1] * dw1.y));
+  const double2 a2 = make_double2(-(Mi[2] * dw0.x + Mi[3] * dw1.x),
+                                  -(Mi[2] * dw0.y + Mi[3] * dw1.y));
+  // Stage 6: assemble, store, correction norm
+  const double km = (ix == 0) ? 1.0 : 2.0;
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < YM; ++k) {
+    const int y = lane + 32 * k;
+    if (y >= Ny) continue;
+    const double2 vnew = cadd(cadd(R[Ny + y], cscale(a1, c1[k])), cscale(a2, c2[k]));
+    const double2 qq = cadd(cscale(a1, e1[k]), cscale(a2, e2[k]));
+    const double2 unew = csub(R[y], cik(kx, qq));
+    const double2 wnew = csub(R[2 * Ny + y], cik(kz, qq));
+    const double2 cu = csub(unew, vj[0][k]);
+    const double2 cv = csub(vnew, vj[1][k]);
+    const double2 cw = csub(wnew, vj[2][k]);
+    vel_new[mo + y] = unew;
+    vel_new[CS + mo + y] = vnew;
+    vel_new[2 * CS + mo + y] = wnew;
+    if (corr_out) {
+      corr_out[mo + y] = cu;
+      corr_out[CS + mo + y] = cv;
+      corr_out[2 * CS + mo + y] = cw;
+    }
+    acc += a.simpson[y] * km *
+           ((cu.x * cu.x + cu.y * cu.y) + (cv.x * cv.x + cv.y * cv.y) +
+            (cw.x * cw.x + cw.y * cw.y));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0 && partials) partials[m] = acc;
 }
 
 bool imm_v2_supported(int kl, int ny) {
@@ -617,10 +590,10 @@ size_t imm_v2_smem(int Ny, int kl, int row0) {
 #define DNSB_IMM_CASE(KL_)                                                      \
   case KL_:                                                                     \
     if (nuv == KL_ + 1)                                                         \
-      imm_mode_kernel<KL_, KL_ + 1><<<items, 32, sm, st>>>(                     \
+      imm_mode_kernel<KL_, KL_ + 1><<<items, threads, sm, st>>>(                     \
           a, vel_n, vel_j, nl_n, nl_j, vel_new, corr_out, partials, paired);    \
     else                                                                        \
-      imm_mode_kernel<KL_, 2 * KL_><<<items, 32, sm, st>>>(                     \
+      imm_mode_kernel<KL_, 2 * KL_><<<items, threads, sm, st>>>(                     \
           a, vel_n, vel_j, nl_n, nl_j, vel_new, corr_out, partials, paired);    \
     break;
 
@@ -634,6 +607,7 @@ cudaError_t launch_imm_v2(const ImmArgs& a, const double2* vel_n,
   const int items = paired ? ((a.NZ1 + 1) / 2) * a.NKX : NM;
   const int nuv = imm_nu(a.kl, a.ab_row0);
   const size_t sm = imm_mode_smem(a.Ny, a.kl, nuv, paired ? 2 : 1);
+  const int threads = paired ? 64 : 32;  // one warp per mode of an item
   switch (a.kl) {
     DNSB_IMM_CASE(2)
     DNSB_IMM_CASE(4)
