@@ -104,42 +104,75 @@ def op_bytes(w):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during a region."""
+    """nvidia-smi clocks and throttle reasons sampled during a region.
+
+    The sampler starts nvidia-smi, waits for its first sample, and only then
+    opens the region; every sample is time-stamped on arrival and the summary
+    keeps those taken inside the region (if the region is shorter than the
+    sampling period, the samples on either side of it).
+    """
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 50
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.samples = []
+        self.t0 = self.t1 = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            if ln.strip():
+                self.samples.append((time.monotonic(), ln))
 
     def __enter__(self):
+        import threading
+
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.PERIOD_MS)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+        if self.proc is not None:
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+            deadline = time.monotonic() + 5.0
+            while not self.samples and time.monotonic() < deadline:
+                time.sleep(0.01)
+        self.t0 = time.monotonic()
         return self
 
     def __exit__(self, *a):
-        self.lines = []
+        self.t1 = time.monotonic()
         if self.proc is not None:
+            time.sleep(2 * self.PERIOD_MS / 1000)  # the sample closing the region
             self.proc.terminate()
             try:
-                out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+                self.proc.wait()
+            self.thread.join(timeout=5)
+
+    def window(self):
+        inside = [ln for t, ln in self.samples if self.t0 <= t <= self.t1]
+        if inside:
+            return inside, "inside"
+        before = [ln for t, ln in self.samples if t < self.t0][-1:]
+        after = [ln for t, ln in self.samples if t > self.t1][:1]
+        return before + after, "adjacent"
 
     def summary(self):
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
                  "sw_power_cap"]
-        for ln in getattr(self, "lines", []):
+        lines, where = self.window() if self.t0 is not None else ([], "none")
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -155,7 +188,8 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
                     "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "sampled": where}
 
 
 def measured_peaks():
@@ -455,7 +489,7 @@ def run_reference(a, w, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="couette128", choices=sorted(WORKLOADS))

@@ -249,6 +249,17 @@ __device__ __forceinline__ void backward_chain(const double* __restrict__ AB,
   }
 }
 
+// Both substitutions on one real column.  Kept out of line: the L_k and
+// H_k solves share one copy of the fully unrolled recurrences, which keeps
+// the kernel's hot code within the instruction cache.
+template <int KL, int NU, int RS>
+__device__ __noinline__ void lu_solve_column(const double* __restrict__ AB,
+                                             const int* __restrict__ dpiv,
+                                             double* __restrict__ b, int Ny) {
+  forward_chain<KL, RS>(AB, dpiv, b, Ny);
+  backward_chain<KL, NU, RS>(AB, b, Ny);
+}
+
 // Shared memory of one work item (1 or 2 modes sharing factors): per mode
 // T[3][Ny] staged stencil inputs, f[Ny], R[3][Ny] (double2); factor records
 // Ny x RS (double); pivot offsets Ny.
@@ -457,8 +468,7 @@ imm_mode_kernel(ImmArgs a, const double2* __restrict__ vel_n,
   // Stage 2: p_P = Lk^-1 f_hat (real / imaginary columns)
   if (mine && lane < 2) {
     double* col = reinterpret_cast<double*>(F) + lane;
-    forward_chain<KL, RS>(AB, dpiv, col, Ny);
-    backward_chain<KL, NU, RS>(AB, col, Ny);
+    lu_solve_column<KL, NU, RS>(AB, dpiv, col, Ny);
   }
   __syncthreads();  // every warp is done with the L_k factors
   // group: H_k factors; overlaps stage 3
@@ -512,8 +522,7 @@ imm_mode_kernel(ImmArgs a, const double2* __restrict__ vel_n,
   // Helmholtz solves for u_arb, v_arb, w_arb (6 real columns)
   if (mine && lane < 6) {
     double* b = reinterpret_cast<double*>(R + (lane >> 1) * Ny) + (lane & 1);
-    forward_chain<KL, RS>(AB, dpiv, b, Ny);
-    backward_chain<KL, NU, RS>(AB, b, Ny);
+    lu_solve_column<KL, NU, RS>(AB, dpiv, b, Ny);
   }
   __syncwarp();
   if (!mine) return;
