@@ -22,23 +22,6 @@
 
 namespace dnsb {
 
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-}
-
 // Banded stencil row y applied to x (S taps from column j0[y]).
 template <int S>
 __device__ __forceinline__ double2 sband(const double2* x, const int* __restrict__ j0,
@@ -271,15 +254,6 @@ size_t imm_mode_smem(int Ny, int kl, int nu, int qmax) {
 
 // y values per lane: y = lane + 32 k, k < kYM (Ny <= 32 kYM).
 constexpr int kYM = 5;
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_1() {
-  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-}
 
 // Stage one operator's factors of mode m into the record layout and its
 // pivots (threads tid = 0..nthr-1 of the CTA share the copies).

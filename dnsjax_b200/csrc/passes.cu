@@ -406,7 +406,7 @@ x_pass2_kernel(XPassArgs a) {
     s_off[tid] = (long long)outer * a.so + (long long)inner * a.si;
     s_y[tid] = a.y_outer ? outer : inner;
   }
-  load_twiddles(tw, a.tw, M);
+  for (int i = tid; i < M; i += kX2Threads) cp_async16(tw + i, a.tw + i);
   __syncthreads();
   for (int idx = tid; idx < 6 * NKX * R; idx += kX2Threads) {
     int r, k, f;
@@ -419,10 +419,12 @@ x_pass2_kernel(XPassArgs a) {
       r = (idx / NKX) % R;
       f = idx / (R * NKX);
     }
-    double2 v = make_double2(0.0, 0.0);
-    if (r < nr) v = a.in[f * a.in_fs + s_off[r] + k * a.ks];
-    S[(f * NKX + k) * R + r] = v;
+    double2* dst = S + (f * NKX + k) * R + r;
+    if (r < nr) cp_async16(dst, a.in + f * a.in_fs + s_off[r] + k * a.ks);
+    else *dst = make_double2(0.0, 0.0);
   }
+  cp_async_commit();
+  cp_async_wait_all();
   __syncthreads();
   // Stage A: inverse radix R1 (Ns = 1) on Z = A + iB, built on the fly.
   for (int it = tid; it < 8 * CI; it += kX2Threads) {
@@ -848,6 +850,103 @@ size_t zinv_curl_smem(int Mz, int NZ1, int span_max) {
   return sizeof(double2) * (size_t)(2 * Mz * kZTile + Mz);
 }
 
+// D1 along y of column x (complex, stride 1) at row y: sum_m w[m] x[j0 + m].
+// Up to kD1Unroll taps are unrolled (predicated), so the loads of several
+// rows can be in flight together; wider stencils take the plain loop.
+constexpr int kD1Unroll = 9;
+
+__device__ __forceinline__ double2 d1_row(const double2* x, const ZInvCurlArgs& a, int y) {
+  const int j0 = a.d1_j0[y];
+  const double* w = a.d1_w + (long long)y * a.s1;
+  double2 d = make_double2(0.0, 0.0);
+  if (a.s1 <= kD1Unroll) {
+#pragma unroll
+    for (int m = 0; m < kD1Unroll; ++m) {
+      if (m < a.s1) {
+        const double2 q = x[j0 + m];
+        d.x += w[m] * q.x;
+        d.y += w[m] * q.y;
+      }
+    }
+  } else {
+    for (int m = 0; m < a.s1; ++m) {
+      const double2 q = x[j0 + m];
+      d.x += w[m] * q.x;
+      d.y += w[m] * q.y;
+    }
+  }
+  return d;
+}
+
+// Field F of the z-inverse input at stored z mode s (column base b) and row
+// y: 0 u, 1 v, 2 w, 3 dy w - dz v, 4 dz u - dx w, 5 dx v - dy u
+// (plane_couette.py:251-271).
+template <int F>
+__device__ __forceinline__ double2 zinv_field(const ZInvCurlArgs& a, const double2* U,
+                                              const double2* V, const double2* Wc,
+                                              long long b, int s, int y, double kx) {
+  if (F == 0) return U[b + y];
+  if (F == 1) return V[b + y];
+  if (F == 2) return Wc[b + y];
+  const double kz = a.kz[s];
+  if (F == 3) return csub(d1_row(Wc + b, a, y), cik(kz, V[b + y]));
+  if (F == 4) return csub(cik(kz, U[b + y]), cik(kx, Wc[b + y]));
+  return csub(cik(kx, V[b + y]), d1_row(U + b, a, y));
+}
+
+// Fill buf[t][c] with field F over the tile.  Every element of a thread is
+// computed into registers before any is stored, so the global loads of all
+// of a thread's elements are in flight together.
+template <int M, int F>
+__device__ __forceinline__ void zinv_fill(const ZInvCurlArgs& a, double2* buf,
+                                          const double2* U, const double2* V,
+                                          const double2* Wc, long long sstride,
+                                          int y0, int y1, double kx) {
+  constexpr int C = kZTile;
+  constexpr int NE = (M * C + kPassThreads - 1) / kPassThreads;
+  double2 v[NE];
+#pragma unroll
+  for (int e = 0; e < NE; ++e) {
+    const int idx = threadIdx.x + e * kPassThreads;
+    const int c = idx % C, t = idx / C;
+    const int s = (idx < M * C) ? pos_to_stored(t, a.NZ1, M) : -1;
+    const int y = y0 + c;
+    v[e] = make_double2(0.0, 0.0);
+    if (s >= 0 && y < y1) v[e] = zinv_field<F>(a, U, V, Wc, s * sstride, s, y, kx);
+  }
+#pragma unroll
+  for (int e = 0; e < NE; ++e) {
+    const int idx = threadIdx.x + e * kPassThreads;
+    if (idx < M * C) buf[idx] = v[e];
+  }
+}
+
+// Runtime-length variant of the fill (no compile-time plan).
+__device__ __forceinline__ void zinv_fill_rt(const ZInvCurlArgs& a, double2* buf, int M, int f,
+                                             const double2* U, const double2* V,
+                                             const double2* Wc, long long sstride,
+                                             int y0, int y1, double kx) {
+  const int C = kZTile;
+  for (int idx = threadIdx.x; idx < M * C; idx += kPassThreads) {
+    const int c = idx % C, t = idx / C;
+    const int s = pos_to_stored(t, a.NZ1, M);
+    const int y = y0 + c;
+    double2 v = make_double2(0.0, 0.0);
+    if (s >= 0 && y < y1) {
+      const long long b = s * sstride;
+      switch (f) {
+        case 0: v = zinv_field<0>(a, U, V, Wc, b, s, y, kx); break;
+        case 1: v = zinv_field<1>(a, U, V, Wc, b, s, y, kx); break;
+        case 2: v = zinv_field<2>(a, U, V, Wc, b, s, y, kx); break;
+        case 3: v = zinv_field<3>(a, U, V, Wc, b, s, y, kx); break;
+        case 4: v = zinv_field<4>(a, U, V, Wc, b, s, y, kx); break;
+        default: v = zinv_field<5>(a, U, V, Wc, b, s, y, kx); break;
+      }
+    }
+    buf[idx] = v;
+  }
+}
+
 // Fills read the spectral state straight from global memory (the y-stencil
 // neighbours of a tile come from L1/L2), so only the FFT buffers occupy
 // shared memory and four CTAs fit per SM.
@@ -876,46 +975,18 @@ zinv_curl_kernel(ZInvCurlArgs a, int span_max) {
   const int nf = a.curl ? 6 : 3;
   const long long fs = (long long)M * NKX * Ny;
   for (int f = 0; f < nf; ++f) {
-    for (int idx = threadIdx.x; idx < M * C; idx += kPassThreads) {
-      const int c = idx % C, t = idx / C;
-      const int s = pos_to_stored(t, NZ1, M);
-      const int y = y0 + c;
-      double2 v = make_double2(0.0, 0.0);
-      if (s >= 0 && y < y1) {
-        const long long b = s * sstride;
-        const double kz = a.kz[s];
-        switch (f) {
-          case 0: v = U[b + y]; break;
-          case 1: v = V[b + y]; break;
-          case 2: v = Wc[b + y]; break;
-          case 3: {  // dy_w - dz_v
-            const int j0 = a.d1_j0[y];
-            const double* w = a.d1_w + (long long)y * a.s1;
-            double2 d = make_double2(0.0, 0.0);
-            for (int m = 0; m < a.s1; ++m) {
-              const double2 q = Wc[b + j0 + m];
-              d.x += w[m] * q.x;
-              d.y += w[m] * q.y;
-            }
-            v = csub(d, cik(kz, V[b + y]));
-          } break;
-          case 4:  // dz_u - dx_w
-            v = csub(cik(kz, U[b + y]), cik(kx, Wc[b + y]));
-            break;
-          default: {  // dx_v - dy_u
-            const int j0 = a.d1_j0[y];
-            const double* w = a.d1_w + (long long)y * a.s1;
-            double2 d = make_double2(0.0, 0.0);
-            for (int m = 0; m < a.s1; ++m) {
-              const double2 q = U[b + j0 + m];
-              d.x += w[m] * q.x;
-              d.y += w[m] * q.y;
-            }
-            v = csub(cik(kx, V[b + y]), d);
-          } break;
-        }
+    if (ML > 0) {
+      constexpr int MC = ML > 0 ? ML : 1;
+      switch (f) {
+        case 0: zinv_fill<MC, 0>(a, bufA, U, V, Wc, sstride, y0, y1, kx); break;
+        case 1: zinv_fill<MC, 1>(a, bufA, U, V, Wc, sstride, y0, y1, kx); break;
+        case 2: zinv_fill<MC, 2>(a, bufA, U, V, Wc, sstride, y0, y1, kx); break;
+        case 3: zinv_fill<MC, 3>(a, bufA, U, V, Wc, sstride, y0, y1, kx); break;
+        case 4: zinv_fill<MC, 4>(a, bufA, U, V, Wc, sstride, y0, y1, kx); break;
+        default: zinv_fill<MC, 5>(a, bufA, U, V, Wc, sstride, y0, y1, kx); break;
       }
-      bufA[idx] = v;
+    } else {
+      zinv_fill_rt(a, bufA, M, f, U, V, Wc, sstride, y0, y1, kx);
     }
     __syncthreads();
     const double2* res = fft_cols<ML, C, kPassThreads>(bufA, bufB, a.plan, 1, tw);
