@@ -569,7 +569,7 @@ extern "C" int dnsb_couette_create(const dnsb_couette_desc* d,
   const size_t need[] = {col_pass_smem(p->Mz), x_pass_smem(p->Mx),
                          x_phys_smem(p->Mx), x_fwd_smem(p->Mx),
                          zinv_curl_smem(p->Mz, p->NZ1, p->span_max),
-                         imm_smem(p->Ny),
+                         zinv_curl2_smem(p->Mz), imm_smem(p->Ny),
                          imm_v2_supported(p->p, p->Ny) ? imm_v2_smem(p->Ny, p->p, 0) : 0};
   for (size_t n : need)
     if ((int)n > smax) {

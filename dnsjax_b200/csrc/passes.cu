@@ -999,8 +999,130 @@ zinv_curl_kernel(ZInvCurlArgs a, int span_max) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Couette z-inverse pass, two register stages (M = 8 R1): a CTA takes 16
+// consecutive (kx, y) columns -- contiguous in the (nz-1, nx/2, ny) layout --
+// fills each field's zero-padded z column into shared memory (all of a
+// thread's loads of a batch in flight together), runs the inverse radix-R1
+// stage in registers, exchanges once through shared memory, and stores the
+// inverse radix-8 stage's outputs straight to global memory.
+// ---------------------------------------------------------------------------
+constexpr int kZ2Cols = 16;
+constexpr int kZ2Threads = 8 * kZ2Cols;  // stage 1: one thread per (j, column)
+
+size_t zinv_curl2_smem(int M) {
+  return sizeof(double2) * (size_t)(M * kZ2Cols + M);
+}
+
+template <int M, int F>
+__device__ __forceinline__ void zinv2_fill(const ZInvCurlArgs& a, double2* X,
+                                           const double2* U, const double2* V,
+                                           const double2* Wc, long long sstride,
+                                           int y, double kx, bool live) {
+  constexpr int NE = M * kZ2Cols / kZ2Threads;  // elements per thread (= M / 8)
+  constexpr int B = (NE % 6 == 0) ? 6 : ((NE % 3 == 0) ? 3 : 1);
+  const int tid = threadIdx.x;
+  for (int e0 = 0; e0 < NE; e0 += B) {
+    double2 v[B];
+#pragma unroll
+    for (int e = 0; e < B; ++e) {
+      const int t = (tid + (e0 + e) * kZ2Threads) / kZ2Cols;
+      const int s = pos_to_stored(t, a.NZ1, M);
+      v[e] = make_double2(0.0, 0.0);
+      if (live && s >= 0) v[e] = zinv_field<F>(a, U, V, Wc, s * sstride, s, y, kx);
+    }
+#pragma unroll
+    for (int e = 0; e < B; ++e) X[tid + (e0 + e) * kZ2Threads] = v[e];
+  }
+}
+
+template <int ML>
+__global__ void __launch_bounds__(kZ2Threads, 4)
+zinv_curl2_kernel(ZInvCurlArgs a) {
+  constexpr int M = ML, R1 = M / 8, C = kZ2Cols;
+  extern __shared__ double2 sm[];
+  double2* X = sm;  // [t][C]
+  double2* tw = X + M * C;
+  const int tid = threadIdx.x;
+  const int NZ1 = a.NZ1, NKX = a.NKX, Ny = a.Ny;
+  const long long ncol = (long long)NKX * Ny;
+  const long long q0 = (long long)blockIdx.x * C;
+  const int nq = (int)min((long long)C, ncol - q0);
+  const long long cs = (long long)NZ1 * ncol;
+  for (int i = tid; i < M; i += kZ2Threads) cp_async16(tw + i, a.tw + i);
+  cp_async_commit();
+  // The fill column of this thread (the same for all its elements).
+  const int cf = tid % C;
+  const bool live = cf < nq;
+  const long long q = q0 + (live ? cf : 0);
+  const int ix = (int)(q / Ny), y = (int)(q % Ny);
+  const double kx = a.kx[ix];
+  const double2* U = a.u + (long long)ix * Ny;
+  const double2* V = U + cs;
+  const double2* Wc = U + 2 * cs;
+  const int nf = a.curl ? 6 : 3;
+  const long long fs = (long long)M * ncol;
+  for (int f = 0; f < nf; ++f) {
+    switch (f) {
+      case 0: zinv2_fill<M, 0>(a, X, U, V, Wc, ncol, y, kx, live); break;
+      case 1: zinv2_fill<M, 1>(a, X, U, V, Wc, ncol, y, kx, live); break;
+      case 2: zinv2_fill<M, 2>(a, X, U, V, Wc, ncol, y, kx, live); break;
+      case 3: zinv2_fill<M, 3>(a, X, U, V, Wc, ncol, y, kx, live); break;
+      case 4: zinv2_fill<M, 4>(a, X, U, V, Wc, ncol, y, kx, live); break;
+      default: zinv2_fill<M, 5>(a, X, U, V, Wc, ncol, y, kx, live); break;
+    }
+    cp_async_wait_all();  // twiddles
+    __syncthreads();
+    // Stage 1: inverse radix R1 (Ns = 1) on positions t = j + 8 i of column c.
+    {
+      const int c = tid % C, j = tid / C;
+      double2 v[R1];
+#pragma unroll
+      for (int i = 0; i < R1; ++i) v[i] = X[(j + 8 * i) * C + c];
+      dft_3p<R1, 1>(v, tw, 8);
+      __syncthreads();  // every read done before the in-place writes
+#pragma unroll
+      for (int i = 0; i < R1; ++i) X[(j * R1 + i) * C + c] = v[i];
+    }
+    __syncthreads();
+    // Stage 2: inverse radix 8 (Ns = R1) -> positions t = k + R1 i.
+    for (int it = tid; it < R1 * C; it += kZ2Threads) {
+      const int c = it % C, k = it / C;
+      double2 z[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) z[i] = X[(k + R1 * i) * C + c];
+#pragma unroll
+      for (int i = 1; i < 8; ++i) {
+        double2 w = tw[i * k];
+        w.y = -w.y;
+        z[i] = cmul(z[i], w);
+      }
+      dft8(z, 1);
+      if (c < nq) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+          a.out[f * fs + (long long)(k + R1 * i) * ncol + q0 + c] = z[i];
+      }
+    }
+    __syncthreads();  // X is refilled by the next field
+  }
+}
+
 cudaError_t launch_zinv_curl(const ZInvCurlArgs& a, int span_max,
                              cudaStream_t st) {
+  const int L = a.plan.L;
+  if (L == 48 || L == 72 || L == 96 || L == 192) {
+    const long long ncol = (long long)a.NKX * a.Ny;
+    const int grid = (int)((ncol + kZ2Cols - 1) / kZ2Cols);
+    const size_t sm = zinv_curl2_smem(L);
+    switch (L) {
+      case 48: zinv_curl2_kernel<48><<<grid, kZ2Threads, sm, st>>>(a); break;
+      case 72: zinv_curl2_kernel<72><<<grid, kZ2Threads, sm, st>>>(a); break;
+      case 96: zinv_curl2_kernel<96><<<grid, kZ2Threads, sm, st>>>(a); break;
+      default: zinv_curl2_kernel<192><<<grid, kZ2Threads, sm, st>>>(a); break;
+    }
+    return cudaGetLastError();
+  }
   dim3 grid((a.Ny + kZTile - 1) / kZTile, a.NKX);
   DNSB_DISPATCH(a.plan.L, zinv_curl_kernel, grid,
                 zinv_curl_smem(a.plan.L, a.NZ1, span_max), st, a, span_max);
@@ -1013,6 +1135,8 @@ cudaError_t set_pass_attributes(int max_smem) {
                        DNSB_ALL_SIZES(x_phys_kernel), DNSB_ALL_SIZES(x_fwd_kernel),
                        DNSB_ALL_SIZES(yinv_kernel), DNSB_ALL_SIZES(yfwd_kernel),
                        DNSB_ALL_SIZES(zinv_curl_kernel),
+                       (const void*)zinv_curl2_kernel<48>, (const void*)zinv_curl2_kernel<72>,
+                       (const void*)zinv_curl2_kernel<96>, (const void*)zinv_curl2_kernel<192>,
                        (const void*)x_pass2_kernel<48>, (const void*)x_pass2_kernel<72>,
                        (const void*)x_pass2_kernel<96>, (const void*)x_pass2_kernel<192>,
                        (const void*)col_pass2_kernel<48, 1>, (const void*)col_pass2_kernel<48, -1>,

@@ -118,6 +118,7 @@ size_t x_phys_smem(int Mx);
 size_t yinv_smem(int My, int NY1);
 size_t yfwd_smem(int My, int NY1);
 size_t zinv_curl_smem(int Mz, int NZ1, int span_max);
+size_t zinv_curl2_smem(int M);
 
 cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
                             cudaStream_t st);
