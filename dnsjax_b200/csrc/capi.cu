@@ -465,6 +465,13 @@ struct dnsb_couette {
   int ab_row0 = 0;
   int pair_modes = 0;
   size_t ws_bytes = 0;
+  // five-kernel IMM: repacked factors and stage workspace (bind time)
+  double* fac = nullptr;
+  unsigned char* dp = nullptr;
+  double2* Fw = nullptr;
+  double2* Rw = nullptr;
+  ImmBatch batch{};
+  bool batch_ready = false;
 
   ImmArgs imm() const {
     ImmArgs a{};
@@ -503,7 +510,7 @@ struct dnsb_couette {
 static void couette_free(dnsb_couette* p) {
   void* ptrs[] = {p->twz, p->twx, p->kx, p->kz, p->d1w, p->d2w, p->d1j0,
                   p->d2j0, p->U, p->cU, p->nU, p->simpson, p->B, p->partials,
-                  p->status};
+                  p->status, p->fac, p->dp, p->Fw, p->Rw};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete p;
@@ -570,7 +577,8 @@ extern "C" int dnsb_couette_create(const dnsb_couette_desc* d,
                          x_phys_smem(p->Mx), x_fwd_smem(p->Mx),
                          zinv_curl_smem(p->Mz, p->NZ1, p->span_max),
                          zinv_curl2_smem(p->Mz), imm_smem(p->Ny),
-                         imm_v2_supported(p->p, p->Ny) ? imm_v2_smem(p->Ny, p->p, 0) : 0};
+                         imm_v2_supported(p->p, p->Ny) ? imm_v2_smem(p->Ny, p->p, 0) : 0,
+                         imm_batch_supported(p->p, p->Ny) ? imm_batch_stage_smem(p->Ny) : 0};
   for (size_t n : need)
     if ((int)n > smax) {
       couette_free(p);
@@ -612,6 +620,7 @@ extern "C" int dnsb_couette_create(const dnsb_couette_desc* d,
     cudaError_t e = set_pass_attributes(smax);
     if (e == cudaSuccess) e = set_solver_attributes(smax);
     if (e == cudaSuccess) e = set_imm_v2_attributes(smax);
+    if (e == cudaSuccess) e = set_imm_batch_attributes(smax);
     if (e != cudaSuccess)
       rc = fail(DNSB_ERR_CUDA, std::string("cudaFuncSetAttribute: ") +
                                    cudaGetErrorString(e));
@@ -632,6 +641,61 @@ extern "C" int dnsb_couette_destroy(dnsb_couette* p) {
 
 extern "C" size_t dnsb_couette_workspace_bytes(const dnsb_couette* p) {
   return p ? p->ws_bytes : 0;
+}
+
+// Repack both operators' factors for the five-kernel IMM (items = modes
+// (s, kx), s <= (nz-1)/2, when mirror modes share factors; 32-item tiles)
+// and allocate its stage workspace; kept until the next bind or destroy.
+// Returns 0 with batch_ready false when the ring of the substitution
+// kernel does not fit in shared memory (the single-kernel IMM runs then).
+static int bind_batch(dnsb_couette* p) {
+  const int kl = p->p, nu = imm_nu(kl, p->ab_row0);
+  const int smax = max_smem_optin();
+  if (!imm_batch_fits(kl, nu, smax)) return 0;
+  const int NP = p->pair_modes ? ((p->NZ1 + 1) / 2) * p->NKX : p->NM;
+  const int ntiles = (NP + 31) / 32;
+  const size_t nL = (size_t)ntiles * (p->Ny + kl + 1) * kl * 32;
+  const size_t nU = (size_t)ntiles * (p->Ny + nu + 1) * ((nu + 2) & ~1) * 32;
+  const size_t nP = (size_t)ntiles * (p->Ny + kl + 1) * 32;
+  void* ptrs[] = {p->fac, p->dp, p->Fw, p->Rw};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  p->fac = nullptr;
+  p->dp = nullptr;
+  p->Fw = p->Rw = nullptr;
+  const size_t fac_bytes = 2 * (nL + nU) * sizeof(double);
+  cudaError_t e1 = cudaMalloc(&p->fac, fac_bytes);
+  cudaError_t e2 = cudaMalloc(&p->dp, 2 * nP);
+  cudaError_t e3 = cudaMalloc(&p->Fw, (size_t)p->NM * p->Ny * sizeof(double2));
+  cudaError_t e4 = cudaMalloc(&p->Rw, 3 * (size_t)p->NM * p->Ny * sizeof(double2));
+  if (e1 || e2 || e3 || e4) return fail(DNSB_ERR_CUDA, "IMM workspace allocation failed");
+  if (cudaMemset(p->fac, 0, fac_bytes) != cudaSuccess || cudaMemset(p->dp, 0, 2 * nP) != cudaSuccess)
+    return fail(DNSB_ERR_CUDA, "cudaMemset failed");
+  ImmBatch& b = p->batch;
+  const double* abs_[2] = {p->ops.Lk_ab, p->ops.Hk_ab};
+  const int* pivs[2] = {p->ops.Lk_piv, p->ops.Hk_piv};
+  for (int k = 0; k < 2; ++k) {
+    double* fL = p->fac + k * (nL + nU);
+    double* fU = fL + nL;
+    unsigned char* d = p->dp + k * nP;
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (launch_imm_repack(abs_[k], pivs[k], p->Ny, kl, nu, p->ab_row0, NP, ntiles, fL, fU, d,
+                          p->status, 0) != cudaSuccess)
+      return fail(DNSB_ERR_CUDA, "IMM repack launch failed");
+    b.facL[k] = fL;
+    b.facU[k] = fU;
+    b.dp[k] = d;
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(DNSB_ERR_CUDA, "IMM repack failed");
+  b.NP = NP;
+  b.nu = nu;
+  b.paired = p->pair_modes;
+  b.max_smem = smax;
+  b.status = p->status;
+  b.F = p->Fw;
+  b.R = p->Rw;
+  p->batch_ready = true;
+  return 0;
 }
 
 extern "C" int dnsb_couette_bind_imm(dnsb_couette* p, const dnsb_imm_ops* ops) {
@@ -678,6 +742,11 @@ extern "C" int dnsb_couette_bind_imm(dnsb_couette* p, const dnsb_imm_ops* ops) {
   p->pair_modes = (allow && h_diff == 0) ? 1 : 0;
   p->ab_row0 = h_row;
   p->bound = true;
+  p->batch_ready = false;
+  if (imm_batch_supported(p->p, p->Ny)) {
+    rc = bind_batch(p);
+    if (rc) return rc;
+  }
   return 0;
 }
 
@@ -748,7 +817,13 @@ extern "C" int dnsb_couette_imm(dnsb_couette* p, const void* vel_n,
   if (vel_new == vel_n)
     return fail(DNSB_ERR_ARG, "vel_new must not alias vel_n");
   cudaStream_t st = as_stream(stream);
-  if (imm_v2_supported(p->p, p->Ny)) {
+  if (p->batch_ready) {
+    DNSB_LAUNCH(launch_imm_batch(p->imm(), p->batch, (const double2*)vel_n,
+                                 (const double2*)vel_j, (const double2*)nl_n,
+                                 (const double2*)nl_j, (double2*)vel_new,
+                                 (double2*)corr_out, err_dev ? p->partials : nullptr, st));
+    count_launches(4);  // five kernels
+  } else if (imm_v2_supported(p->p, p->Ny)) {
     DNSB_LAUNCH(launch_imm_v2(p->imm(), (const double2*)vel_n, (const double2*)vel_j,
                               (const double2*)nl_n, (const double2*)nl_j,
                               (double2*)vel_new, (double2*)corr_out,
@@ -866,7 +941,8 @@ extern "C" int dnsb_couette_check(dnsb_couette* p, void* stream) {
   DNSB_CUDA(cudaMemcpyAsync(&h, p->status, sizeof(int), cudaMemcpyDeviceToHost,
                             as_stream(stream)));
   DNSB_CUDA(cudaStreamSynchronize(as_stream(stream)));
-  if (h) return fail(DNSB_ERR_PIVOT, "pivot index outside [j, j+kl]");
+  if (h & 1) return fail(DNSB_ERR_PIVOT, "pivot index outside [j, j+kl]");
+  if (h & 2) return fail(DNSB_ERR_CUDA, "IMM substitution: a shared-memory ring wait timed out");
   return 0;
 }
 

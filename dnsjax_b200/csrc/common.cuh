@@ -338,6 +338,9 @@ __device__ __forceinline__ void cp_async_wait_all() {
 __device__ __forceinline__ void cp_async_wait_1() {
   asm volatile("cp.async.wait_group 1;\n" ::: "memory");
 }
+__device__ __forceinline__ void cp_async_wait_2() {
+  asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+}
 
 __device__ __forceinline__ void load_twiddles(double2* s, const double2* g,
                                               int L) {

@@ -561,7 +561,7 @@ bool imm_v2_supported(int kl, int ny) {
 
 // Stored U rows: the nearest NU superdiagonals; NU = kl+1 when the rows
 // above ab_row0 leave at most that many, else all 2 kl.
-static int imm_nu(int kl, int row0) {
+int imm_nu(int kl, int row0) {
   const int nu = 2 * kl - row0;
   return nu <= kl + 1 ? kl + 1 : 2 * kl;
 }

@@ -104,6 +104,35 @@ cudaError_t launch_ab_pair_check(const double* ab, const int* piv, int nz1,
                                  int nkx, int rows, int ny, int* out,
                                  cudaStream_t st);
 
+// Five-kernel IMM iteration (csrc/imm_batch.cu) over factors repacked at
+// bind time (record-major, item index fastest; 1/U_jj and U/U_jj pre-scaled;
+// pivots as validated offsets) and workspace F [NM][Ny], R [3][NM][Ny].
+struct ImmBatch {
+  // per operator (0 = L_k, 1 = H_k), 32-item tiles (csrc/imm_batch.cu)
+  const double* facL[2];
+  const double* facU[2];
+  const unsigned char* dp[2];
+  int NP;        // items: (nz-1+1)/2 * nx/2 when paired, else all modes
+  int nu;        // stored superdiagonals (kl+1 or 2 kl)
+  int paired;    // mirror mode (nz-1-s, kx) reads item (s, kx)'s factors
+  int max_smem;  // per-CTA shared-memory limit of the device
+  int* status;   // bit 1: bad pivot, bit 2: a substitution ring wait timed out
+  double2* F;
+  double2* R;
+};
+bool imm_batch_supported(int kl, int ny);
+size_t imm_batch_stage_smem(int Ny);
+int imm_nu(int kl, int row0);
+bool imm_batch_fits(int kl, int nu, int max_smem);
+cudaError_t launch_imm_repack(const double* ab, const int* piv, int Ny, int kl, int nu,
+                              int row0, int NP, int ntiles, double* facL, double* facU,
+                              unsigned char* dp, int* status, cudaStream_t st);
+cudaError_t launch_imm_batch(const ImmArgs& a, const ImmBatch& bt, const double2* vel_n,
+                             const double2* vel_j, const double2* nl_n,
+                             const double2* nl_j, double2* vel_new, double2* corr_out,
+                             double* partials, cudaStream_t st);
+cudaError_t set_imm_batch_attributes(int max_smem);
+
 // Simpson-weighted k_metric |v|^2 per block (Couette norm).
 cudaError_t launch_couette_norm2(const ImmArgs& a, const double2* v,
                                  double* partials, cudaStream_t st);
