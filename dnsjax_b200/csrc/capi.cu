@@ -455,6 +455,7 @@ struct dnsb_couette {
   FFTPlan pz, px;
   double2 *twz = nullptr, *twx = nullptr;
   double *kx = nullptr, *kz = nullptr, *d1w = nullptr, *d2w = nullptr;
+  double *d1wT = nullptr, *d2wT = nullptr;  // [tap][Ny]: lanes over y read contiguously
   int *d1j0 = nullptr, *d2j0 = nullptr;
   double *U = nullptr, *cU = nullptr, *nU = nullptr, *simpson = nullptr;
   double2* B = nullptr;
@@ -485,6 +486,8 @@ struct dnsb_couette {
     a.d1_w = d1w;
     a.d2_j0 = d2j0;
     a.d2_w = d2w;
+    a.d1_wT = d1wT;
+    a.d2_wT = d2wT;
     a.kx = kx;
     a.kz = kz;
     a.simpson = simpson;
@@ -508,7 +511,7 @@ struct dnsb_couette {
 };
 
 static void couette_free(dnsb_couette* p) {
-  void* ptrs[] = {p->twz, p->twx, p->kx, p->kz, p->d1w, p->d2w, p->d1j0,
+  void* ptrs[] = {p->twz, p->twx, p->kx, p->kz, p->d1w, p->d2w, p->d1wT, p->d2wT, p->d1j0,
                   p->d2j0, p->U, p->cU, p->nU, p->simpson, p->B, p->partials,
                   p->status, p->fac, p->dp, p->Fw, p->Rw};
   for (void* q : ptrs)
@@ -596,6 +599,15 @@ extern "C" int dnsb_couette_create(const dnsb_couette_desc* d,
   chk(upload(&p->d2j0, d->d2_j0, p->Ny));
   chk(upload(&p->d1w, d->d1_w, (size_t)p->Ny * p->s1));
   chk(upload(&p->d2w, d->d2_w, (size_t)p->Ny * p->s2));
+  {
+    std::vector<double> t1((size_t)p->Ny * p->s1), t2((size_t)p->Ny * p->s2);
+    for (int y = 0; y < p->Ny; ++y) {
+      for (int m = 0; m < p->s1; ++m) t1[(size_t)m * p->Ny + y] = d->d1_w[(size_t)y * p->s1 + m];
+      for (int m = 0; m < p->s2; ++m) t2[(size_t)m * p->Ny + y] = d->d2_w[(size_t)y * p->s2 + m];
+    }
+    chk(upload(&p->d1wT, t1.data(), t1.size()));
+    chk(upload(&p->d2wT, t2.data(), t2.size()));
+  }
   chk(upload(&p->U, d->base_flow, 3 * (size_t)p->Ny));
   chk(upload(&p->cU, d->curl_base_flow, 3 * (size_t)p->Ny));
   chk(upload(&p->nU, d->nonlin_base_flow, 3 * (size_t)p->Ny));
@@ -764,6 +776,7 @@ extern "C" int dnsb_couette_rhs(dnsb_couette* p, const void* state, void* rhs,
   zi.s1 = p->s1;
   zi.d1_j0 = p->d1j0;
   zi.d1_w = p->d1w;
+  zi.d1_wT = p->d1wT;
   zi.kx = p->kx;
   zi.kz = p->kz;
   zi.plan = p->pz;
@@ -873,6 +886,7 @@ extern "C" int dnsb_couette_spec_to_phys(dnsb_couette* p, const void* spec,
   zi.s1 = p->s1;
   zi.d1_j0 = p->d1j0;
   zi.d1_w = p->d1w;
+  zi.d1_wT = p->d1wT;
   zi.kx = p->kx;
   zi.kz = p->kz;
   zi.plan = p->pz;

@@ -31,17 +31,20 @@ namespace {
 constexpr int kStageWarps = 4;  // modes per CTA in the stage kernels
 constexpr int kSYM = 5;         // y values per lane: y = lane + 32 k, Ny <= 160
 
+// Banded stencil row y applied to x: sum_m w[m][y] x[j0[y] + m], with the
+// weights stored tap-major ([S][Ny]) so the lanes of a warp (consecutive y)
+// read each tap's weights contiguously.
 template <int S>
 __device__ __forceinline__ double2 band_row(const double2* x, const int* __restrict__ j0,
-                                            const double* __restrict__ w, int y) {
+                                            const double* __restrict__ wT, int Ny, int y) {
   const int j = j0[y];
-  const double* wy = w + y * S;
   double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
   for (int m = 0; m < S; ++m) {
+    const double wm = wT[m * Ny + y];
     const double2 v = x[j + m];
-    acc.x += wy[m] * v.x;
-    acc.y += wy[m] * v.y;
+    acc.x += wm * v.x;
+    acc.y += wm * v.y;
   }
   return acc;
 }
@@ -153,7 +156,7 @@ imm_stage01_kernel(ImmArgs a, const double2* __restrict__ vel_n,
   for (int k = 0; k < YM; ++k) {
     const int y = lane + 32 * k;
     if (y < Ny)
-      D[y] = cadd(cadd(cik(kx, ua[k]), band_row<S1>(T, a.d1_j0, a.d1_w, y)), cik(kz, wa[k]));
+      D[y] = cadd(cadd(cik(kx, ua[k]), band_row<S1>(T, a.d1_j0, a.d1_wT, Ny, y)), cik(kz, wa[k]));
   }
   __syncwarp();
   // Stage 1: f_hat (wall rows zero)
@@ -164,11 +167,11 @@ imm_stage01_kernel(ImmArgs a, const double2* __restrict__ vel_n,
     double2 fy = make_double2(0.0, 0.0);
     if (y > 0 && y < Ny - 1) {
       const double2 divNj =
-          cadd(cadd(cik(kx, uj[k]), band_row<S1>(T + Ny, a.d1_j0, a.d1_w, y)), cik(kz, wj[k]));
+          cadd(cadd(cik(kx, uj[k]), band_row<S1>(T + Ny, a.d1_j0, a.d1_wT, Ny, y)), cik(kz, wj[k]));
       const double2 divNn =
-          cadd(cadd(cik(kx, un[k]), band_row<S1>(T + 2 * Ny, a.d1_j0, a.d1_w, y)), cik(kz, wn[k]));
+          cadd(cadd(cik(kx, un[k]), band_row<S1>(T + 2 * Ny, a.d1_j0, a.d1_wT, Ny, y)), cik(kz, wn[k]));
       const double2 dy = D[y];
-      const double2 Lkd = csub(band_row<S2>(D, a.d2_j0, a.d2_w, y), cscale(dy, k2));
+      const double2 Lkd = csub(band_row<S2>(D, a.d2_j0, a.d2_wT, Ny, y), cscale(dy, k2));
       const double2 dd = make_double2(dy.x / dt, dy.y / dt);
       fy = cadd(cadd(cadd(dd, cscale(divNj, c)), cscale(divNn, omc)), cscale(Lkd, omc_nu));
     }
@@ -226,12 +229,12 @@ imm_stage3_kernel(ImmArgs a, const double2* __restrict__ vel_n,
     if (y > 0 && y < Ny - 1) {
       const double2 p = Pp[y];
       const double2 dxp = cik(kx, p);
-      const double2 dyp = band_row<S1>(Pp, a.d1_j0, a.d1_w, y);
+      const double2 dyp = band_row<S1>(Pp, a.d1_j0, a.d1_wT, Ny, y);
       const double2 dzp = cik(kz, p);
       const double2 u = T[y], v = T[Ny + y], w = T[2 * Ny + y];
-      const double2 D2u = band_row<S2>(T, a.d2_j0, a.d2_w, y);
-      const double2 D2v = band_row<S2>(T + Ny, a.d2_j0, a.d2_w, y);
-      const double2 D2w = band_row<S2>(T + 2 * Ny, a.d2_j0, a.d2_w, y);
+      const double2 D2u = band_row<S2>(T, a.d2_j0, a.d2_wT, Ny, y);
+      const double2 D2v = band_row<S2>(T + Ny, a.d2_j0, a.d2_wT, Ny, y);
+      const double2 D2w = band_row<S2>(T + 2 * Ny, a.d2_j0, a.d2_wT, Ny, y);
       const double2 hu = cadd(cscale(u, idt), cscale(csub(D2u, cscale(u, k2)), omc_nu));
       const double2 hv = cadd(cscale(v, idt), cscale(csub(D2v, cscale(v, k2)), omc_nu));
       const double2 hw = cadd(cscale(w, idt), cscale(csub(D2w, cscale(w, k2)), omc_nu));
@@ -281,8 +284,8 @@ imm_stage6_kernel(ImmArgs a, const double2* __restrict__ R, const double2* vel_j
   }
   // Stages 4-5: wall divergence and influence-matrix weights
   const double2* va = R + CS + mo;
-  double2 dw0 = band_row<S1>(va, a.d1_j0, a.d1_w, 0);
-  const double2 dw1 = band_row<S1>(va, a.d1_j0, a.d1_w, Ny - 1);
+  double2 dw0 = band_row<S1>(va, a.d1_j0, a.d1_wT, Ny, 0);
+  const double2 dw1 = band_row<S1>(va, a.d1_j0, a.d1_wT, Ny, Ny - 1);
   if (k2 == 0.0) dw0 = make_double2(0.0, 0.0);
   const double* Mi = a.M_inv + (long long)m * 4;
   const double2 a1 = make_double2(-(Mi[0] * dw0.x + Mi[1] * dw1.x),

@@ -857,22 +857,23 @@ constexpr int kD1Unroll = 9;
 
 __device__ __forceinline__ double2 d1_row(const double2* x, const ZInvCurlArgs& a, int y) {
   const int j0 = a.d1_j0[y];
-  const double* w = a.d1_w + (long long)y * a.s1;
+  const double* w = a.d1_wT + y;  // tap m at w[m * Ny]: consecutive y contiguous
+  const int Ny = a.Ny;
   double2 d = make_double2(0.0, 0.0);
   if (a.s1 <= kD1Unroll) {
 #pragma unroll
     for (int m = 0; m < kD1Unroll; ++m) {
       if (m < a.s1) {
         const double2 q = x[j0 + m];
-        d.x += w[m] * q.x;
-        d.y += w[m] * q.y;
+        d.x += w[m * Ny] * q.x;
+        d.y += w[m * Ny] * q.y;
       }
     }
   } else {
     for (int m = 0; m < a.s1; ++m) {
       const double2 q = x[j0 + m];
-      d.x += w[m] * q.x;
-      d.y += w[m] * q.y;
+      d.x += w[m * Ny] * q.x;
+      d.y += w[m * Ny] * q.y;
     }
   }
   return d;

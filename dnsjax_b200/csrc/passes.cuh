@@ -104,6 +104,7 @@ struct ZInvCurlArgs {
   int s1;              // D1 stencil width (p + 1)
   const int* d1_j0;    // [Ny]
   const double* d1_w;  // [Ny][s1]
+  const double* d1_wT; // [s1][Ny] (the same weights, tap-major)
   const double* kx;
   const double* kz;
   FFTPlan plan;

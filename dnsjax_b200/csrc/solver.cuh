@@ -59,6 +59,8 @@ struct ImmArgs {
   const double* d1_w;     // [Ny][s1]
   const int* d2_j0;       // [Ny]
   const double* d2_w;     // [Ny][s2]
+  const double* d1_wT;    // [s1][Ny] (the same weights, tap-major)
+  const double* d2_wT;    // [s2][Ny]
   const double* kx;       // [NKX]
   const double* kz;       // [NZ1]
   const double* simpson;  // [Ny] Simpson weights (norm)
