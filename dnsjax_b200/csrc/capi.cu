@@ -656,7 +656,7 @@ extern "C" size_t dnsb_couette_workspace_bytes(const dnsb_couette* p) {
 }
 
 // Repack both operators' factors for the five-kernel IMM (items = modes
-// (s, kx), s <= (nz-1)/2, when mirror modes share factors; 32-item tiles)
+// (s, kx), s <= (nz-1)/2, when mirror modes share factors; 16-item tiles)
 // and allocate its stage workspace; kept until the next bind or destroy.
 // Returns 0 with batch_ready false when the ring of the substitution
 // kernel does not fit in shared memory (the single-kernel IMM runs then).
@@ -665,10 +665,11 @@ static int bind_batch(dnsb_couette* p) {
   const int smax = max_smem_optin();
   if (!imm_batch_fits(kl, nu, smax)) return 0;
   const int NP = p->pair_modes ? ((p->NZ1 + 1) / 2) * p->NKX : p->NM;
-  const int ntiles = (NP + 31) / 32;
-  const size_t nL = (size_t)ntiles * (p->Ny + kl + 1) * kl * 32;
-  const size_t nU = (size_t)ntiles * (p->Ny + nu + 1) * ((nu + 2) & ~1) * 32;
-  const size_t nP = (size_t)ntiles * (p->Ny + kl + 1) * 32;
+  const int tile = 16;  // items per substitution tile (csrc/imm_batch.cu)
+  const int ntiles = (NP + tile - 1) / tile;
+  const size_t nL = (size_t)ntiles * (p->Ny + kl + 1) * kl * tile;
+  const size_t nU = (size_t)ntiles * (p->Ny + nu + 1) * ((nu + 2) & ~1) * tile;
+  const size_t nP = (size_t)ntiles * (p->Ny + kl + 1) * tile;
   void* ptrs[] = {p->fac, p->dp, p->Fw, p->Rw};
   for (void* q : ptrs)
     if (q) cudaFree(q);

@@ -28,6 +28,7 @@ namespace dnsb {
 
 namespace {
 
+constexpr int kTile = 16;       // items per substitution CTA (two sides per item)
 constexpr int kStageWarps = 4;  // modes per CTA in the stage kernels
 constexpr int kSYM = 5;         // y values per lane: y = lane + 32 k, Ny <= 160
 
@@ -75,28 +76,28 @@ __global__ void imm_repack_kernel(const double* __restrict__ ab, const int* __re
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
        idx += (long long)gridDim.x * blockDim.x) {
     const int p = (int)(idx % NP), j = (int)(idx / NP);
-    const int tile = p >> 5, lane = p & 31;
+    const int tile = p / kTile, it = p % kTile;
     const double* abm = ab + (long long)p * rows * Ny;
     const double r = 1.0 / abm[(long long)kuu * Ny + j];
-    // element i of row j: [tile][j][i / 2][lane][i % 2]
-    double* L = facL + (tile * NyF + j) * kl * 32 + 2 * lane;
+    // element i of row j: [tile][j][i / 2][it][i % 2]
+    double* L = facL + (tile * NyF + j) * kl * kTile + 2 * it;
     for (int i = 1; i <= kl; ++i) {
       const int e = i - 1;
-      L[(e >> 1) * 64 + (e & 1)] = abm[(long long)(kuu + i) * Ny + j];
+      L[(e >> 1) * 2 * kTile + (e & 1)] = abm[(long long)(kuu + i) * Ny + j];
     }
-    double* U = facU + (tile * NyB + j + WB) * nup * 32 + 2 * lane;
+    double* U = facU + (tile * NyB + j + WB) * nup * kTile + 2 * it;
     U[0] = r;
     for (int i = 1; i <= nu; ++i) {
       const int row = kuu - i;
       const double u = (row >= row0) ? abm[(long long)row * Ny + j] : 0.0;
-      U[(i >> 1) * 64 + (i & 1)] = u * r;
+      U[(i >> 1) * 2 * kTile + (i & 1)] = u * r;
     }
     int d = piv[(long long)p * Ny + j] - j;
     if (d < 0 || d > kl || j + d >= Ny) {  // never follow a bad pivot
       atomicOr(status, 1);
       d = 0;
     }
-    dp[(tile * NyF + j) * 32 + lane] = (unsigned char)d;
+    dp[(tile * NyF + j) * kTile + it] = (unsigned char)d;
   }
   (void)ntiles;
 }
@@ -324,30 +325,33 @@ imm_stage6_kernel(ImmArgs a, const double2* __restrict__ R, const double2* vel_j
 }
 
 // ---------------------------------------------------------------------------
-// Batched banded substitution: one CTA per (tile of 32 items, side), one
-// warp per real column (2 for L_k: re / im of p_P; 6 for H_k), one thread
-// per (item, column).  One thread streams each block of steps -- the tile's
-// factors (and pivots) for that block, one contiguous chunk each -- into a
-// ring of shared-memory slots with bulk copies that complete on the slot's
-// mbarrier, ring-1 blocks ahead of the block being computed; every thread
-// runs its column's recurrence from registers and the ring, loading the
-// right-hand-side rows that enter its window one block ahead.
+// Batched banded substitution: one warp per CTA; lane = (side, item) over
+// a tile of 16 items (lanes 0-15 the items' own modes, 16-31 their mirrors),
+// and each thread solves all real columns of its mode -- NC = 2 for L_k (re,
+// im of p_P), 6 for H_k (re, im of three components) -- as NC independent
+// recurrences sharing every factor load.  Lane 0 streams each block of
+// steps' factors (and pivots) for the tile -- one contiguous chunk each --
+// into a ring of shared-memory slots with bulk copies completing on the
+// slot's mbarrier; every thread copies the right-hand-side rows entering its
+// windows during the block into the same slot with cp.async.  Both run
+// ring-1 blocks ahead of the block being computed.
 //
-// Forward elimination (dgbtrs 'N'): window b[j..j+KL] in registers,
+// Forward elimination (dgbtrs 'N'): windows b[j..j+KL] in registers,
 // slot(o, ph) = (o + ph) % W, W = KL + 1; the row interchange is chosen per
 // block for the warp: none, with the next row only (two selects), or
-// general (switch).  Back substitution: window b[j-NU..j], slot(o, ph) =
+// general (switch).  Back substitution: windows b[j-NU..j], slot(o, ph) =
 // (o - ph) mod WB, WB = NU + 1, one FMA deep per step (U pre-scaled).
 // A ring wait that does not complete within its bound sets bit 2 of the
 // status word and the CTA stops computing.
 // ---------------------------------------------------------------------------
+
 struct SolveArgs {
   const double* facL;
   const double* facU;
   const unsigned char* dp;
   double2* X;  // [ncomp][NM][Ny]
   int* status;
-  int NP, ncomp, NM, Ny, NKX, NZ1, paired, ring, slot_bytes;
+  int NP, NM, Ny, NKX, NZ1, paired, ring, slot_bytes;
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -390,7 +394,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
   return false;
 }
 
-// Mode of item p on side q and whether its column is solved.
+// Mode of item p on side q and whether its columns are solved.
 __device__ __forceinline__ bool item_mode(const SolveArgs& a, int p, int q, int* m) {
   bool live = p < a.NP;
   int mm = min(p, a.NP - 1);
@@ -403,11 +407,39 @@ __device__ __forceinline__ bool item_mode(const SolveArgs& a, int p, int q, int*
   return live;
 }
 
-template <int KL, int MODE, bool TAIL>
-__device__ __forceinline__ void ring_fwd_steps(double* b, int j0, int nsteps, bool live,
-                                               double (&w)[KL + 1], const double2* Lp,
-                                               const int (&dr)[KL + 1],
-                                               const double (&be)[KL + 1]) {
+// Row interchange of step ph (pivot offset d) on one window.
+template <int KL, int MODE>
+__device__ __forceinline__ double pivot_take(double (&w)[KL + 1], int ph, int d) {
+  constexpr int W = KL + 1;
+  double bpj = w[ph % W];
+  if (MODE == 1) {
+    const double x1 = w[(1 + ph) % W];
+    const bool p = d != 0;
+    w[(1 + ph) % W] = p ? bpj : x1;
+    bpj = p ? x1 : bpj;
+  } else if (MODE == 2) {
+    switch (d) {
+#define DNSB_PIV(I)                  \
+  case I:                            \
+    if (I <= KL) {                   \
+      bpj = w[(I + ph) % W];         \
+      w[(I + ph) % W] = w[ph % W];   \
+    }                                \
+    break;
+      DNSB_PIV(1) DNSB_PIV(2) DNSB_PIV(3) DNSB_PIV(4)
+      DNSB_PIV(5) DNSB_PIV(6) DNSB_PIV(7) DNSB_PIV(8)
+#undef DNSB_PIV
+      default: break;
+    }
+  }
+  return bpj;
+}
+
+template <int KL, int NCP, int MW, int MODE, bool TAIL>
+__device__ __forceinline__ void tile_fwd_block(double2* const (&col)[NCP], int j0, int nsteps,
+                                               int Ny, bool live, double (&w)[2 * NCP][KL + 1],
+                                               const double2* Lp, const int (&dr)[KL + 1],
+                                               const double2* ent) {
   constexpr int W = KL + 1;
 #pragma unroll
   for (int ph = 0; ph < W; ++ph) {
@@ -416,156 +448,201 @@ __device__ __forceinline__ void ring_fwd_steps(double* b, int j0, int nsteps, bo
       double L[KL];
 #pragma unroll
       for (int i2 = 0; i2 < KL / 2; ++i2) {
-        const double2 t = Lp[(ph * (KL / 2) + i2) * 32];
+        const double2 t = Lp[(ph * (KL / 2) + i2) * kTile];
         L[2 * i2] = t.x;
         L[2 * i2 + 1] = t.y;
       }
-      double bpj = w[ph % W];
-      if (MODE == 1) {
-        const double x1 = w[(1 + ph) % W];
-        const bool p = dr[ph] != 0;
-        w[(1 + ph) % W] = p ? bpj : x1;
-        bpj = p ? x1 : bpj;
-      } else if (MODE == 2) {
-        switch (dr[ph]) {
-#define DNSB_PIV(I)                  \
-  case I:                            \
-    if (I <= KL) {                   \
-      bpj = w[(I + ph) % W];         \
-      w[(I + ph) % W] = w[ph % W];   \
-    }                                \
-    break;
-          DNSB_PIV(1) DNSB_PIV(2) DNSB_PIV(3) DNSB_PIV(4)
-          DNSB_PIV(5) DNSB_PIV(6) DNSB_PIV(7) DNSB_PIV(8)
-#undef DNSB_PIV
-          default: break;
-        }
-      }
-      if (live) b[2 * j] = bpj;
+      double bp[2 * NCP];
 #pragma unroll
-      for (int i = 1; i <= KL; ++i) w[(i + ph) % W] -= L[i - 1] * bpj;
-      w[ph % W] = be[ph];  // b[j+W] enters at offset KL
+      for (int c = 0; c < 2 * NCP; ++c) bp[c] = pivot_take<KL, MODE>(w[c], ph, dr[ph]);
+      if (live) {
+#pragma unroll
+        for (int cc = 0; cc < NCP; ++cc) col[cc][j] = make_double2(bp[2 * cc], bp[2 * cc + 1]);
+      }
+#pragma unroll
+      for (int c = 0; c < 2 * NCP; ++c) {
+#pragma unroll
+        for (int i = 1; i <= KL; ++i) w[c][(i + ph) % W] -= L[i - 1] * bp[c];
+      }
+      // b[j+W] enters at offset KL (0 past the last row)
+      const bool in = j + W < Ny;
+#pragma unroll
+      for (int cc = 0; cc < NCP; ++cc) {
+        const double2 e = in ? ent[(cc * MW + ph) * 32] : make_double2(0.0, 0.0);
+        w[2 * cc][ph % W] = e.x;
+        w[2 * cc + 1][ph % W] = e.y;
+      }
     }
   }
 }
 
-template <int NU, bool TAIL>
-__device__ __forceinline__ void ring_bwd_steps(double* b, int j0, bool live,
-                                               double (&w)[NU + 1], const double2* Up,
-                                               const double (&be)[NU + 1]) {
+template <int NU, int NCP, int MW, bool TAIL>
+__device__ __forceinline__ void tile_bwd_block(double2* const (&col)[NCP], int j0, bool live,
+                                               double (&w)[2 * NCP][NU + 1], const double2* Up,
+                                               const double2* ent) {
   constexpr int WB = NU + 1, NUP = (NU + 2) & ~1;
 #pragma unroll
   for (int ph = 0; ph < WB; ++ph) {
     const int j = j0 - ph;
     if (!TAIL || j >= 0) {
-      const double2* u = Up + (WB - 1 - ph) * (NUP / 2) * 32;
+      const double2* u = Up + (WB - 1 - ph) * (NUP / 2) * kTile;
       double U[NUP];
 #pragma unroll
       for (int i2 = 0; i2 < NUP / 2; ++i2) {
-        const double2 t = u[i2 * 32];
+        const double2 t = u[i2 * kTile];
         U[2 * i2] = t.x;
         U[2 * i2 + 1] = t.y;
       }
       const int st = ((NU - ph) % WB + WB) % WB;
-      const double bj = w[st];
-      if (live) b[2 * j] = bj * U[0];
+      double bj[2 * NCP];
+#pragma unroll
+      for (int c = 0; c < 2 * NCP; ++c) bj[c] = w[c][st];
+      if (live) {
+#pragma unroll
+        for (int cc = 0; cc < NCP; ++cc)
+          col[cc][j] = make_double2(bj[2 * cc] * U[0], bj[2 * cc + 1] * U[0]);
+      }
 #pragma unroll
       for (int i = 1; i <= NU; ++i) {
         const int si = ((NU - i - ph) % WB + WB) % WB;
-        w[si] -= U[i] * bj;
+#pragma unroll
+        for (int c = 0; c < 2 * NCP; ++c) w[c][si] -= U[i] * bj[c];
       }
-      w[st] = be[ph];  // b[j-WB] enters at offset 0
+      // b[j-WB] enters at offset 0 (0 below row 0)
+      const bool in = j - WB >= 0;
+#pragma unroll
+      for (int cc = 0; cc < NCP; ++cc) {
+        const double2 e = in ? ent[(cc * MW + ph) * 32] : make_double2(0.0, 0.0);
+        w[2 * cc][st] = e.x;
+        w[2 * cc + 1][st] = e.y;
+      }
     }
   }
 }
 
-template <int KL, int NU>
-__global__ void __launch_bounds__(192)
+template <int KL, int NU, int NCP>
+__global__ void __launch_bounds__(32)
 imm_solve_kernel(SolveArgs a) {
   constexpr int W = KL + 1, WB = NU + 1, NUP = (NU + 2) & ~1;
-  constexpr int LB = W * KL * 32 * 8, PB = W * 32, UB = WB * NUP * 32 * 8;
+  constexpr int LB = W * KL * kTile * 8, PB = W * kTile, UB = WB * NUP * kTile * 8;
+  constexpr int MW = W > WB ? W : WB;  // rows per (component, lane) in a slot
+  constexpr int EB = NCP * MW * 32 * 16;
   extern __shared__ __align__(128) unsigned char ring[];
   __shared__ __align__(8) unsigned long long bars[3];
   __shared__ int s_fail;
-  const int tid = threadIdx.x;
-  const int lane = tid & 31, c = tid >> 5;
-  const int comp = c >> 1, reim = c & 1;
-  const int tile = blockIdx.x, q = blockIdx.y;
+  const int lane = threadIdx.x;
+  const int side = lane >> 4, it = lane & (kTile - 1);
+  const int tile = blockIdx.x;
   const int Ny = a.Ny, R = a.ring, SB = a.slot_bytes;
   const long long NyF = Ny + W, NyB = Ny + WB;
   int m;
-  const bool live = item_mode(a, tile * 32 + lane, q, &m);
-  double* b = reinterpret_cast<double*>(a.X + ((long long)comp * a.NM + m) * Ny) + reim;
+  const bool live = item_mode(a, tile * kTile + it, side, &m);
+  double2* col[NCP];
+#pragma unroll
+  for (int cc = 0; cc < NCP; ++cc) col[cc] = a.X + ((long long)cc * a.NM + m) * Ny;
   const int nsteps = Ny - 1;
-  const int nbf = (nsteps + W - 1) / W;   // forward blocks
-  const int nbb = (Ny + WB - 1) / WB;     // back-substitution blocks
+  const int nbf = (nsteps + W - 1) / W;  // forward blocks
+  const int nbb = (Ny + WB - 1) / WB;    // back-substitution blocks
   const int nblk = nbf + nbb;
 
-  if (tid == 0) {
+  if (lane == 0) {
     for (int r = 0; r < R; ++r) mbar_init(&bars[r], 1);
     mbar_fence_init();
     s_fail = 0;
   }
-  __syncthreads();
-  // Producer (thread 0): block g of the combined sequence into slot g % R.
+  __syncwarp();
+  // Block g of the combined sequence into slot g % R: factors by lane 0
+  // (bulk, mbarrier), this lane's entering rows by every lane (cp.async
+  // group g).  Entering rows of component cc at ent[(cc * MW + ph) * 32 +
+  // lane]: forward row j0+W+ph, back substitution row j0-WB-ph.
+  int hi_issued = -1;
   auto issue = [&](int g) {
-    if (g >= nblk) return;
-    unsigned char* slot = ring + (g % R) * SB;
-    unsigned long long* bar = &bars[g % R];
-    if (g < nbf) {
-      const int j0 = g * W;
-      mbar_arrive_tx(bar, LB + PB);
-      bulk_g2s(slot, a.facL + (tile * NyF + j0) * KL * 32, LB, bar);
-      bulk_g2s(slot + LB, a.dp + (tile * NyF + j0) * 32, PB, bar);
-    } else {
-      const int j0 = Ny - 1 - (g - nbf) * WB;  // rows j0-WB+1 .. j0
-      mbar_arrive_tx(bar, UB);
-      bulk_g2s(slot, a.facU + (tile * NyB + j0 + 1) * NUP * 32, UB, bar);
+    if (g < nblk) {
+      hi_issued = g;
+      unsigned char* slot = ring + (g % R) * SB;
+      unsigned long long* bar = &bars[g % R];
+      double2* ent = reinterpret_cast<double2*>(slot + SB - EB) + lane;
+      if (g < nbf) {
+        const int j0 = g * W;
+        if (lane == 0) {
+          mbar_arrive_tx(bar, LB + PB);
+          bulk_g2s(slot, a.facL + (tile * NyF + j0) * KL * kTile, LB, bar);
+          bulk_g2s(slot + LB, a.dp + (tile * NyF + j0) * kTile, PB, bar);
+        }
+        if (live) {
+#pragma unroll
+          for (int ph = 0; ph < W; ++ph) {
+            const int e = j0 + W + ph;
+            if (e < Ny)
+              for (int cc = 0; cc < NCP; ++cc) cp_async16(ent + (cc * MW + ph) * 32, col[cc] + e);
+          }
+        }
+      } else {
+        const int j0 = Ny - 1 - (g - nbf) * WB;
+        if (lane == 0) {
+          mbar_arrive_tx(bar, UB);
+          bulk_g2s(slot, a.facU + (tile * NyB + j0 + 1) * NUP * kTile, UB, bar);
+        }
+        if (live) {
+#pragma unroll
+          for (int ph = 0; ph < WB; ++ph) {
+            const int e = j0 - WB - ph;
+            if (e >= 0)
+              for (int cc = 0; cc < NCP; ++cc) cp_async16(ent + (cc * MW + ph) * 32, col[cc] + e);
+          }
+        }
+      }
     }
+    cp_async_commit();
   };
-  if (tid == 0)
-    for (int g = 0; g < R - 1; ++g) issue(g);
+  auto wait_block = [&](int g) {
+    if (R == 3) cp_async_wait_2(); else cp_async_wait_1();  // this lane's rows of block g
+    if (!mbar_wait(&bars[g % R], (g / R) & 1)) s_fail = 1;
+    __syncwarp();
+  };
+  // The back substitution reads the forward results: its blocks are issued
+  // only after every forward result is stored.
+  for (int h = 0; h < R - 1; ++h) issue(h < nbf ? h : nblk);
   int g = 0;
   bool ok = true;
 
   // ---- forward elimination, steps j = 0 .. Ny-2 ----
   {
-    double w[W], be[W], bn[W];
+    double w[2 * NCP][W];
 #pragma unroll
-    for (int o = 0; o < W; ++o) w[o] = (o < Ny) ? b[2 * o] : 0.0;
+    for (int cc = 0; cc < NCP; ++cc) {
 #pragma unroll
-    for (int ph = 0; ph < W; ++ph) bn[ph] = (W + ph < Ny) ? b[2 * (W + ph)] : 0.0;
-    for (int k = 0; k < nbf; ++k, ++g) {
-      if (tid == 0) issue(g + R - 1);
-#pragma unroll
-      for (int ph = 0; ph < W; ++ph) be[ph] = bn[ph];
-      const int j0 = k * W;
-#pragma unroll
-      for (int ph = 0; ph < W; ++ph) {
-        const int e = j0 + 2 * W + ph;  // entering rows of the next block
-        bn[ph] = (e < Ny) ? b[2 * e] : 0.0;
+      for (int o = 0; o < W; ++o) {
+        const double2 v = (o < Ny) ? col[cc][o] : make_double2(0.0, 0.0);
+        w[2 * cc][o] = v.x;
+        w[2 * cc + 1][o] = v.y;
       }
-      if (!mbar_wait(&bars[g % R], (g / R) & 1)) s_fail = 1;
+    }
+    for (int k = 0; k < nbf; ++k, ++g) {
+      issue(g + R - 1 < nbf ? g + R - 1 : nblk);
+      wait_block(g);
       const unsigned char* slot = ring + (g % R) * SB;
-      const double2* Lp = reinterpret_cast<const double2*>(slot) + lane;
+      const double2* Lp = reinterpret_cast<const double2*>(slot) + it;
       const unsigned char* Ps = slot + LB;
+      const double2* ent = reinterpret_cast<const double2*>(slot + SB - EB) + lane;
       int dr[W];
       int dm = 0;
 #pragma unroll
       for (int ph = 0; ph < W; ++ph) {
-        dr[ph] = Ps[ph * 32 + lane];
+        dr[ph] = Ps[ph * kTile + it];
         dm = max(dm, dr[ph]);
       }
       dm = __reduce_max_sync(0xffffffffu, dm);
+      const int j0 = k * W;
       if (j0 + W > nsteps)
-        ring_fwd_steps<KL, 2, true>(b, j0, nsteps, live, w, Lp, dr, be);
+        tile_fwd_block<KL, NCP, MW, 2, true>(col, j0, nsteps, Ny, live, w, Lp, dr, ent);
       else if (dm == 0)
-        ring_fwd_steps<KL, 0, false>(b, j0, nsteps, live, w, Lp, dr, be);
+        tile_fwd_block<KL, NCP, MW, 0, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent);
       else if (dm == 1)
-        ring_fwd_steps<KL, 1, false>(b, j0, nsteps, live, w, Lp, dr, be);
+        tile_fwd_block<KL, NCP, MW, 1, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent);
       else
-        ring_fwd_steps<KL, 2, false>(b, j0, nsteps, live, w, Lp, dr, be);
-      __syncthreads();  // the slot is refilled by the next issue
+        tile_fwd_block<KL, NCP, MW, 2, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent);
+      __syncwarp();  // the slot is refilled by the next issue
       if (s_fail) {
         ok = false;
         break;
@@ -573,59 +650,58 @@ imm_solve_kernel(SolveArgs a) {
     }
     // b[Ny-1] sits at offset 0 after the last step: slot nsteps % W.
     const int last = nsteps % W;
-    double v = w[0];
 #pragma unroll
-    for (int s = 1; s < W; ++s)
-      if (last == s) v = w[s];
-    if (live && ok) b[2 * (Ny - 1)] = v;
+    for (int cc = 0; cc < NCP; ++cc) {
+      double v0 = w[2 * cc][0], v1 = w[2 * cc + 1][0];
+#pragma unroll
+      for (int s = 1; s < W; ++s)
+        if (last == s) {
+          v0 = w[2 * cc][s];
+          v1 = w[2 * cc + 1][s];
+        }
+      if (live && ok) col[cc][Ny - 1] = make_double2(v0, v1);
+    }
   }
 
-  // ---- back substitution, rows j = Ny-1 .. 0 (this thread's forward
+  // ---- back substitution, rows j = Ny-1 .. 0 (this lane's own forward
   // results, read back in program order) ----
   if (ok) {
-    double w[WB], be[WB], bn[WB];
+    for (int h = nbf; h < nbf + R - 1; ++h) issue(h);
+    double w[2 * NCP][WB];
 #pragma unroll
-    for (int o = 0; o < WB; ++o) {
-      const int idx = Ny - 1 - NU + o;
-      w[o] = (idx >= 0) ? b[2 * idx] : 0.0;
-    }
+    for (int cc = 0; cc < NCP; ++cc) {
 #pragma unroll
-    for (int ph = 0; ph < WB; ++ph) {
-      const int e = Ny - 1 - ph - WB;
-      bn[ph] = (e >= 0) ? b[2 * e] : 0.0;
+      for (int o = 0; o < WB; ++o) {
+        const int idx = Ny - 1 - NU + o;
+        const double2 v = (idx >= 0) ? col[cc][idx] : make_double2(0.0, 0.0);
+        w[2 * cc][o] = v.x;
+        w[2 * cc + 1][o] = v.y;
+      }
     }
     for (int k = 0; k < nbb; ++k, ++g) {
-      if (tid == 0) issue(g + R - 1);
-#pragma unroll
-      for (int ph = 0; ph < WB; ++ph) be[ph] = bn[ph];
+      issue(g + R - 1);
+      wait_block(g);
+      const unsigned char* slot = ring + (g % R) * SB;
+      const double2* Up = reinterpret_cast<const double2*>(slot) + it;
+      const double2* ent = reinterpret_cast<const double2*>(slot + SB - EB) + lane;
       const int j0 = Ny - 1 - k * WB;
-#pragma unroll
-      for (int ph = 0; ph < WB; ++ph) {
-        const int e = j0 - WB - ph - WB;  // entering rows of the next block
-        bn[ph] = (e >= 0) ? b[2 * e] : 0.0;
-      }
-      if (!mbar_wait(&bars[g % R], (g / R) & 1)) s_fail = 1;
-      const double2* Up = reinterpret_cast<const double2*>(ring + (g % R) * SB) + lane;
       if (j0 - WB + 1 < 0)
-        ring_bwd_steps<NU, true>(b, j0, live, w, Up, be);
+        tile_bwd_block<NU, NCP, MW, true>(col, j0, live, w, Up, ent);
       else
-        ring_bwd_steps<NU, false>(b, j0, live, w, Up, be);
-      __syncthreads();
+        tile_bwd_block<NU, NCP, MW, false>(col, j0, live, w, Up, ent);
+      __syncwarp();
       if (s_fail) {
         ok = false;
         break;
       }
     }
   }
-  if (!ok) {
-    // Leave no bulk copy in flight: wait (bounded) for every issued block
-    // not yet consumed, then report.
-    if (tid == 0) {
-      // blocks g .. g+R-1 were issued (block g is the one that timed out)
-      const int last = min(g + R - 1, nblk - 1);
-      for (int h = g; h <= last; ++h) mbar_wait(&bars[h % R], (h / R) & 1);
-      atomicOr(a.status, 2);
-    }
+  cp_async_wait_all();
+  if (!ok && lane == 0) {
+    // Leave no bulk copy in flight: blocks g .. hi_issued were issued
+    // (block g is the one that timed out).
+    for (int h = g; h <= hi_issued; ++h) mbar_wait(&bars[h % R], (h / R) & 1);
+    atomicOr(a.status, 2);
   }
 }
 
@@ -640,19 +716,20 @@ bool imm_batch_supported(int kl, int ny) {
   return (kl == 2 || kl == 4 || kl == 6 || kl == 8) && ny <= 32 * kSYM;
 }
 
-// Ring slot bytes of one solve launch (the larger of a forward and a back-
-// substitution block) and the ring depth that fits.
+// Ring slot bytes of one substitution launch: the larger of a forward block
+// (factors, pivots) and a back-substitution block (U records), plus the
+// entering rows of every lane; and the ring depth that fits.
 static int solve_slot_bytes(int kl, int nu, int ncomp) {
-  (void)ncomp;
   const int W = kl + 1, WB = nu + 1, nup = (nu + 2) & ~1;
-  const int f = W * kl * 32 * 8 + W * 32;
-  const int b = WB * nup * 32 * 8;
-  return ((f > b ? f : b) + 127) & ~127;
+  const int MW = W > WB ? W : WB;
+  const int f = W * kl * kTile * 8 + W * kTile;
+  const int b = WB * nup * kTile * 8;
+  return (((f > b ? f : b) + 127) & ~127) + ncomp * MW * 32 * 16;
 }
 
 static int solve_ring(int kl, int nu, int ncomp, int max_smem) {
   const int sb = solve_slot_bytes(kl, nu, ncomp);
-  if (3 * sb <= max_smem && 3 * sb <= 110 * 1024) return 3;
+  if (3 * sb <= max_smem && 3 * sb <= 100 * 1024) return 3;
   if (2 * sb <= max_smem) return 2;
   return 0;
 }
@@ -661,33 +738,38 @@ bool imm_batch_fits(int kl, int nu, int max_smem) {
   return solve_ring(kl, nu, 3, max_smem) > 0 && solve_ring(kl, nu, 1, max_smem) > 0;
 }
 
-template <int KL>
-static cudaError_t solve_launch(const ImmBatch& bt, int op, double2* X, int ncomp, int NM,
-                                int Ny, int NKX, int NZ1, cudaStream_t st) {
+template <int KL, int NCP>
+static cudaError_t solve_launch_nc(const ImmBatch& bt, int op, double2* X, int NM, int Ny,
+                                   int NKX, int NZ1, cudaStream_t st) {
   SolveArgs s{};
   s.facL = bt.facL[op];
   s.facU = bt.facU[op];
   s.dp = bt.dp[op];
   s.X = X;
+  s.status = bt.status;
   s.NP = bt.NP;
-  s.ncomp = ncomp;
   s.NM = NM;
   s.Ny = Ny;
   s.NKX = NKX;
   s.NZ1 = NZ1;
   s.paired = bt.paired;
-  s.status = bt.status;
-  s.ring = solve_ring(KL, bt.nu, ncomp, bt.max_smem);
-  s.slot_bytes = solve_slot_bytes(KL, bt.nu, ncomp);
+  s.ring = solve_ring(KL, bt.nu, NCP, bt.max_smem);
+  s.slot_bytes = solve_slot_bytes(KL, bt.nu, NCP);
   if (s.ring == 0) return cudaErrorInvalidValue;
   const size_t sm = (size_t)s.ring * s.slot_bytes;
-  dim3 grid((bt.NP + 31) / 32, bt.paired ? 2 : 1);
-  const int threads = 64 * ncomp;
+  const int grid = (bt.NP + kTile - 1) / kTile;
   if (bt.nu == KL + 1)
-    imm_solve_kernel<KL, KL + 1><<<grid, threads, sm, st>>>(s);
+    imm_solve_kernel<KL, KL + 1, NCP><<<grid, 32, sm, st>>>(s);
   else
-    imm_solve_kernel<KL, 2 * KL><<<grid, threads, sm, st>>>(s);
+    imm_solve_kernel<KL, 2 * KL, NCP><<<grid, 32, sm, st>>>(s);
   return cudaGetLastError();
+}
+
+template <int KL>
+static cudaError_t solve_launch(const ImmBatch& bt, int op, double2* X, int ncomp, int NM,
+                                int Ny, int NKX, int NZ1, cudaStream_t st) {
+  return ncomp == 1 ? solve_launch_nc<KL, 1>(bt, op, X, NM, Ny, NKX, NZ1, st)
+                    : solve_launch_nc<KL, 3>(bt, op, X, NM, Ny, NKX, NZ1, st);
 }
 
 template <int K>
@@ -732,10 +814,11 @@ cudaError_t set_imm_batch_attributes(int max_smem) {
       (const void*)imm_stage01_kernel<6>, (const void*)imm_stage01_kernel<8>,
       (const void*)imm_stage3_kernel<2>,  (const void*)imm_stage3_kernel<4>,
       (const void*)imm_stage3_kernel<6>,  (const void*)imm_stage3_kernel<8>,
-      (const void*)imm_solve_kernel<2, 3>, (const void*)imm_solve_kernel<2, 4>,
-      (const void*)imm_solve_kernel<4, 5>, (const void*)imm_solve_kernel<4, 8>,
-      (const void*)imm_solve_kernel<6, 7>, (const void*)imm_solve_kernel<6, 12>,
-      (const void*)imm_solve_kernel<8, 9>, (const void*)imm_solve_kernel<8, 16>};
+#define DNSB_SOLVE_FNS(K)                                                     \
+  (const void*)imm_solve_kernel<K, K + 1, 1>, (const void*)imm_solve_kernel<K, K + 1, 3>, \
+      (const void*)imm_solve_kernel<K, 2 * K, 1>, (const void*)imm_solve_kernel<K, 2 * K, 3>
+      DNSB_SOLVE_FNS(2), DNSB_SOLVE_FNS(4), DNSB_SOLVE_FNS(6), DNSB_SOLVE_FNS(8)};
+#undef DNSB_SOLVE_FNS
   cudaError_t e = cudaSuccess;
   for (const void* f : fns) {
     cudaError_t r = allow_dynamic_smem(f, max_smem);
