@@ -325,11 +325,11 @@ imm_stage6_kernel(ImmArgs a, const double2* __restrict__ R, const double2* vel_j
 }
 
 // ---------------------------------------------------------------------------
-// Batched banded substitution: one warp per CTA; lane = (side, item) over
-// a tile of 16 items (lanes 0-15 the items' own modes, 16-31 their mirrors),
-// and each thread solves all real columns of its mode -- NC = 2 for L_k (re,
-// im of p_P), 6 for H_k (re, im of three components) -- as NC independent
-// recurrences sharing every factor load.  Lane 0 streams each block of
+// Batched banded substitution: one CTA per tile of 16 items, one warp per
+// component (1 for L_k: p_P; 3 for H_k); lane = (side, item) (lanes 0-15 the
+// items' own modes, 16-31 their mirrors), and each thread solves both real
+// columns (re, im) of its mode's component as two recurrences sharing every
+// factor load; the warps share the tile's factor stream.  Lane 0 streams each block of
 // steps' factors (and pivots) for the tile -- one contiguous chunk each --
 // into a ring of shared-memory slots with bulk copies completing on the
 // slot's mbarrier; every thread copies the right-hand-side rows entering its
@@ -439,7 +439,7 @@ template <int KL, int NCP, int MW, int MODE, bool TAIL>
 __device__ __forceinline__ void tile_fwd_block(double2* const (&col)[NCP], int j0, int nsteps,
                                                int Ny, bool live, double (&w)[2 * NCP][KL + 1],
                                                const double2* Lp, const int (&dr)[KL + 1],
-                                               const double2* ent) {
+                                               const double2* ent, int ES) {
   constexpr int W = KL + 1;
 #pragma unroll
   for (int ph = 0; ph < W; ++ph) {
@@ -468,7 +468,7 @@ __device__ __forceinline__ void tile_fwd_block(double2* const (&col)[NCP], int j
       const bool in = j + W < Ny;
 #pragma unroll
       for (int cc = 0; cc < NCP; ++cc) {
-        const double2 e = in ? ent[(cc * MW + ph) * 32] : make_double2(0.0, 0.0);
+        const double2 e = in ? ent[(cc * MW + ph) * ES] : make_double2(0.0, 0.0);
         w[2 * cc][ph % W] = e.x;
         w[2 * cc + 1][ph % W] = e.y;
       }
@@ -479,7 +479,7 @@ __device__ __forceinline__ void tile_fwd_block(double2* const (&col)[NCP], int j
 template <int NU, int NCP, int MW, bool TAIL>
 __device__ __forceinline__ void tile_bwd_block(double2* const (&col)[NCP], int j0, bool live,
                                                double (&w)[2 * NCP][NU + 1], const double2* Up,
-                                               const double2* ent) {
+                                               const double2* ent, int ES) {
   constexpr int WB = NU + 1, NUP = (NU + 2) & ~1;
 #pragma unroll
   for (int ph = 0; ph < WB; ++ph) {
@@ -512,7 +512,7 @@ __device__ __forceinline__ void tile_bwd_block(double2* const (&col)[NCP], int j
       const bool in = j - WB >= 0;
 #pragma unroll
       for (int cc = 0; cc < NCP; ++cc) {
-        const double2 e = in ? ent[(cc * MW + ph) * 32] : make_double2(0.0, 0.0);
+        const double2 e = in ? ent[(cc * MW + ph) * ES] : make_double2(0.0, 0.0);
         w[2 * cc][st] = e.x;
         w[2 * cc + 1][st] = e.y;
       }
@@ -520,37 +520,38 @@ __device__ __forceinline__ void tile_bwd_block(double2* const (&col)[NCP], int j
   }
 }
 
-template <int KL, int NU, int NCP>
-__global__ void __launch_bounds__(32)
+template <int KL, int NU>
+__global__ void __launch_bounds__(96)
 imm_solve_kernel(SolveArgs a) {
+  constexpr int NCP = 1;  // components per thread (one warp per component)
   constexpr int W = KL + 1, WB = NU + 1, NUP = (NU + 2) & ~1;
   constexpr int LB = W * KL * kTile * 8, PB = W * kTile, UB = WB * NUP * kTile * 8;
   constexpr int MW = W > WB ? W : WB;  // rows per (component, lane) in a slot
-  constexpr int EB = NCP * MW * 32 * 16;
   extern __shared__ __align__(128) unsigned char ring[];
   __shared__ __align__(8) unsigned long long bars[3];
   __shared__ int s_fail;
-  const int lane = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, cw = tid >> 5;  // warp = component
   const int side = lane >> 4, it = lane & (kTile - 1);
   const int tile = blockIdx.x;
-  const int Ny = a.Ny, R = a.ring, SB = a.slot_bytes;
+  const int Ny = a.Ny, R = a.ring, SB = a.slot_bytes, nthr = blockDim.x;
+  const int EB = MW * nthr * 16;  // entering rows of every thread, at the slot's end
   const long long NyF = Ny + W, NyB = Ny + WB;
   int m;
   const bool live = item_mode(a, tile * kTile + it, side, &m);
   double2* col[NCP];
 #pragma unroll
-  for (int cc = 0; cc < NCP; ++cc) col[cc] = a.X + ((long long)cc * a.NM + m) * Ny;
+  for (int cc = 0; cc < NCP; ++cc) col[cc] = a.X + ((long long)(cw + cc) * a.NM + m) * Ny;
   const int nsteps = Ny - 1;
   const int nbf = (nsteps + W - 1) / W;  // forward blocks
   const int nbb = (Ny + WB - 1) / WB;    // back-substitution blocks
   const int nblk = nbf + nbb;
 
-  if (lane == 0) {
+  if (tid == 0) {
     for (int r = 0; r < R; ++r) mbar_init(&bars[r], 1);
     mbar_fence_init();
     s_fail = 0;
   }
-  __syncwarp();
+  __syncthreads();
   // Block g of the combined sequence into slot g % R: factors by lane 0
   // (bulk, mbarrier), this lane's entering rows by every lane (cp.async
   // group g).  Entering rows of component cc at ent[(cc * MW + ph) * 32 +
@@ -561,10 +562,10 @@ imm_solve_kernel(SolveArgs a) {
       hi_issued = g;
       unsigned char* slot = ring + (g % R) * SB;
       unsigned long long* bar = &bars[g % R];
-      double2* ent = reinterpret_cast<double2*>(slot + SB - EB) + lane;
+      double2* ent = reinterpret_cast<double2*>(slot + SB - EB) + tid;
       if (g < nbf) {
         const int j0 = g * W;
-        if (lane == 0) {
+        if (tid == 0) {
           mbar_arrive_tx(bar, LB + PB);
           bulk_g2s(slot, a.facL + (tile * NyF + j0) * KL * kTile, LB, bar);
           bulk_g2s(slot + LB, a.dp + (tile * NyF + j0) * kTile, PB, bar);
@@ -574,12 +575,12 @@ imm_solve_kernel(SolveArgs a) {
           for (int ph = 0; ph < W; ++ph) {
             const int e = j0 + W + ph;
             if (e < Ny)
-              for (int cc = 0; cc < NCP; ++cc) cp_async16(ent + (cc * MW + ph) * 32, col[cc] + e);
+              for (int cc = 0; cc < NCP; ++cc) cp_async16(ent + (cc * MW + ph) * nthr, col[cc] + e);
           }
         }
       } else {
         const int j0 = Ny - 1 - (g - nbf) * WB;
-        if (lane == 0) {
+        if (tid == 0) {
           mbar_arrive_tx(bar, UB);
           bulk_g2s(slot, a.facU + (tile * NyB + j0 + 1) * NUP * kTile, UB, bar);
         }
@@ -588,7 +589,7 @@ imm_solve_kernel(SolveArgs a) {
           for (int ph = 0; ph < WB; ++ph) {
             const int e = j0 - WB - ph;
             if (e >= 0)
-              for (int cc = 0; cc < NCP; ++cc) cp_async16(ent + (cc * MW + ph) * 32, col[cc] + e);
+              for (int cc = 0; cc < NCP; ++cc) cp_async16(ent + (cc * MW + ph) * nthr, col[cc] + e);
           }
         }
       }
@@ -598,7 +599,7 @@ imm_solve_kernel(SolveArgs a) {
   auto wait_block = [&](int g) {
     if (R == 3) cp_async_wait_2(); else cp_async_wait_1();  // this lane's rows of block g
     if (!mbar_wait(&bars[g % R], (g / R) & 1)) s_fail = 1;
-    __syncwarp();
+    __syncthreads();
   };
   // The back substitution reads the forward results: its blocks are issued
   // only after every forward result is stored.
@@ -624,7 +625,7 @@ imm_solve_kernel(SolveArgs a) {
       const unsigned char* slot = ring + (g % R) * SB;
       const double2* Lp = reinterpret_cast<const double2*>(slot) + it;
       const unsigned char* Ps = slot + LB;
-      const double2* ent = reinterpret_cast<const double2*>(slot + SB - EB) + lane;
+      const double2* ent = reinterpret_cast<const double2*>(slot + SB - EB) + tid;
       int dr[W];
       int dm = 0;
 #pragma unroll
@@ -635,14 +636,14 @@ imm_solve_kernel(SolveArgs a) {
       dm = __reduce_max_sync(0xffffffffu, dm);
       const int j0 = k * W;
       if (j0 + W > nsteps)
-        tile_fwd_block<KL, NCP, MW, 2, true>(col, j0, nsteps, Ny, live, w, Lp, dr, ent);
+        tile_fwd_block<KL, NCP, MW, 2, true>(col, j0, nsteps, Ny, live, w, Lp, dr, ent, nthr);
       else if (dm == 0)
-        tile_fwd_block<KL, NCP, MW, 0, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent);
+        tile_fwd_block<KL, NCP, MW, 0, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent, nthr);
       else if (dm == 1)
-        tile_fwd_block<KL, NCP, MW, 1, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent);
+        tile_fwd_block<KL, NCP, MW, 1, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent, nthr);
       else
-        tile_fwd_block<KL, NCP, MW, 2, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent);
-      __syncwarp();  // the slot is refilled by the next issue
+        tile_fwd_block<KL, NCP, MW, 2, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent, nthr);
+      __syncthreads();  // the slot is refilled by the next issue
       if (s_fail) {
         ok = false;
         break;
@@ -683,13 +684,13 @@ imm_solve_kernel(SolveArgs a) {
       wait_block(g);
       const unsigned char* slot = ring + (g % R) * SB;
       const double2* Up = reinterpret_cast<const double2*>(slot) + it;
-      const double2* ent = reinterpret_cast<const double2*>(slot + SB - EB) + lane;
+      const double2* ent = reinterpret_cast<const double2*>(slot + SB - EB) + tid;
       const int j0 = Ny - 1 - k * WB;
       if (j0 - WB + 1 < 0)
-        tile_bwd_block<NU, NCP, MW, true>(col, j0, live, w, Up, ent);
+        tile_bwd_block<NU, NCP, MW, true>(col, j0, live, w, Up, ent, nthr);
       else
-        tile_bwd_block<NU, NCP, MW, false>(col, j0, live, w, Up, ent);
-      __syncwarp();
+        tile_bwd_block<NU, NCP, MW, false>(col, j0, live, w, Up, ent, nthr);
+      __syncthreads();
       if (s_fail) {
         ok = false;
         break;
@@ -697,7 +698,7 @@ imm_solve_kernel(SolveArgs a) {
     }
   }
   cp_async_wait_all();
-  if (!ok && lane == 0) {
+  if (!ok && tid == 0) {
     // Leave no bulk copy in flight: blocks g .. hi_issued were issued
     // (block g is the one that timed out).
     for (int h = g; h <= hi_issued; ++h) mbar_wait(&bars[h % R], (h / R) & 1);
@@ -738,9 +739,9 @@ bool imm_batch_fits(int kl, int nu, int max_smem) {
   return solve_ring(kl, nu, 3, max_smem) > 0 && solve_ring(kl, nu, 1, max_smem) > 0;
 }
 
-template <int KL, int NCP>
-static cudaError_t solve_launch_nc(const ImmBatch& bt, int op, double2* X, int NM, int Ny,
-                                   int NKX, int NZ1, cudaStream_t st) {
+template <int KL>
+static cudaError_t solve_launch(const ImmBatch& bt, int op, double2* X, int ncomp, int NM,
+                                int Ny, int NKX, int NZ1, cudaStream_t st) {
   SolveArgs s{};
   s.facL = bt.facL[op];
   s.facU = bt.facU[op];
@@ -753,23 +754,16 @@ static cudaError_t solve_launch_nc(const ImmBatch& bt, int op, double2* X, int N
   s.NKX = NKX;
   s.NZ1 = NZ1;
   s.paired = bt.paired;
-  s.ring = solve_ring(KL, bt.nu, NCP, bt.max_smem);
-  s.slot_bytes = solve_slot_bytes(KL, bt.nu, NCP);
+  s.ring = solve_ring(KL, bt.nu, ncomp, bt.max_smem);
+  s.slot_bytes = solve_slot_bytes(KL, bt.nu, ncomp);
   if (s.ring == 0) return cudaErrorInvalidValue;
   const size_t sm = (size_t)s.ring * s.slot_bytes;
   const int grid = (bt.NP + kTile - 1) / kTile;
   if (bt.nu == KL + 1)
-    imm_solve_kernel<KL, KL + 1, NCP><<<grid, 32, sm, st>>>(s);
+    imm_solve_kernel<KL, KL + 1><<<grid, 32 * ncomp, sm, st>>>(s);
   else
-    imm_solve_kernel<KL, 2 * KL, NCP><<<grid, 32, sm, st>>>(s);
+    imm_solve_kernel<KL, 2 * KL><<<grid, 32 * ncomp, sm, st>>>(s);
   return cudaGetLastError();
-}
-
-template <int KL>
-static cudaError_t solve_launch(const ImmBatch& bt, int op, double2* X, int ncomp, int NM,
-                                int Ny, int NKX, int NZ1, cudaStream_t st) {
-  return ncomp == 1 ? solve_launch_nc<KL, 1>(bt, op, X, NM, Ny, NKX, NZ1, st)
-                    : solve_launch_nc<KL, 3>(bt, op, X, NM, Ny, NKX, NZ1, st);
 }
 
 template <int K>
@@ -814,9 +808,8 @@ cudaError_t set_imm_batch_attributes(int max_smem) {
       (const void*)imm_stage01_kernel<6>, (const void*)imm_stage01_kernel<8>,
       (const void*)imm_stage3_kernel<2>,  (const void*)imm_stage3_kernel<4>,
       (const void*)imm_stage3_kernel<6>,  (const void*)imm_stage3_kernel<8>,
-#define DNSB_SOLVE_FNS(K)                                                     \
-  (const void*)imm_solve_kernel<K, K + 1, 1>, (const void*)imm_solve_kernel<K, K + 1, 3>, \
-      (const void*)imm_solve_kernel<K, 2 * K, 1>, (const void*)imm_solve_kernel<K, 2 * K, 3>
+#define DNSB_SOLVE_FNS(K) \
+  (const void*)imm_solve_kernel<K, K + 1>, (const void*)imm_solve_kernel<K, 2 * K>
       DNSB_SOLVE_FNS(2), DNSB_SOLVE_FNS(4), DNSB_SOLVE_FNS(6), DNSB_SOLVE_FNS(8)};
 #undef DNSB_SOLVE_FNS
   cudaError_t e = cudaSuccess;

@@ -378,8 +378,8 @@ cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
 // the forward radix-8 stage); forward radix-R1 stage; unpack and store.
 // ---------------------------------------------------------------------------
 size_t x_pass2_smem(int M, int nkx) {
-  const size_t S = (size_t)6 * nkx * kX2Rows, Y = (size_t)M * 2 * kX2Rows;
-  const size_t X = (size_t)M * 3 * kX2Rows;
+  const size_t S = (size_t)6 * nkx * kX2Rows, Y = (size_t)M * 2 * kX2Rows + M / 8;
+  const size_t X = (size_t)M * 3 * kX2Rows + 4 * 8;  // + the stage-A skew
   return sizeof(double2) * ((S > Y ? S : Y) + X + M);
 }
 
@@ -388,13 +388,18 @@ __global__ void __launch_bounds__(kX2Threads)
 x_pass2_kernel(XPassArgs a) {
   constexpr int M = ML, R1 = M / 8, R = kX2Rows, NKX = ML / 3;
   constexpr int CI = 3 * R, CF = 2 * R;
-  constexpr int SZ_S = 6 * NKX * R, SZ_Y = M * CF;
+  // Stage outputs carry a skew of XS (X) / 1 (Y) slots per block of R1 (X)
+  // / 8 (Y) positions, so the 8 lanes of a 16-byte shared access hit 8
+  // different bank groups on both the store and the next stage's load.
+  constexpr int XS = 4;
+  static_assert(R == 4, "the stage-A lane map assumes 4 rows");
+  constexpr int SZ_S = 6 * NKX * R, SZ_Y = M * CF + R1;
   constexpr int SZ_SY = SZ_S > SZ_Y ? SZ_S : SZ_Y;
   extern __shared__ double2 sm[];
   double2* S = sm;            // staged half spectra, S[(f*NKX + k)*R + r]
   double2* Y = sm;            // forward stage-1 output [t][CF] (after S dies)
   double2* X = sm + SZ_SY;    // inverse stage-A output [t][CI]; later [t][CF]
-  double2* tw = X + M * CI;
+  double2* tw = X + M * CI + XS * 8;
   const int tid = threadIdx.x;
   const int r0 = blockIdx.x * R;
   const int nr = min(R, a.nrows - r0);
@@ -428,8 +433,10 @@ x_pass2_kernel(XPassArgs a) {
   __syncthreads();
   // Stage A: inverse radix R1 (Ns = 1) on Z = A + iB, built on the fly.
   for (int it = tid; it < 8 * CI; it += kX2Threads) {
-    const int col = it % CI, j = it / CI;
-    const int r = col / 3, pr = col % 3;
+    // lanes of a quarter warp: 4 rows x 2 parities of j, one field pair
+    const int r = it & 3, rest = it >> 3;
+    const int pr = rest % 3, j = ((it >> 2) & 1) + 2 * (rest / 3);
+    const int col = 3 * r + pr;
     const double2* A = S + (2 * pr) * NKX * R + r;
     const double2* B = S + (2 * pr + 1) * NKX * R + r;
     double2 v[R1];
@@ -450,7 +457,7 @@ x_pass2_kernel(XPassArgs a) {
     }
     dft_3p<R1, 1>(v, tw, 8);
 #pragma unroll
-    for (int i = 0; i < R1; ++i) X[(j * R1 + i) * CI + col] = v[i];
+    for (int i = 0; i < R1; ++i) X[(j * R1 + i) * CI + col + XS * j] = v[i];
   }
   __syncthreads();
   // Stage B: inverse radix 8 (Ns = R1) -> physical values at t = k + R1 i;
@@ -461,7 +468,7 @@ x_pass2_kernel(XPassArgs a) {
 #pragma unroll
     for (int pr = 0; pr < 3; ++pr) {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) z[pr][i] = X[(k + R1 * i) * CI + 3 * r + pr];
+      for (int i = 0; i < 8; ++i) z[pr][i] = X[(k + R1 * i) * CI + 3 * r + pr + XS * i];
 #pragma unroll
       for (int i = 1; i < 8; ++i) {
         double2 w = tw[i * k];
@@ -497,8 +504,8 @@ x_pass2_kernel(XPassArgs a) {
     dft8(F1, -1);
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      Y[(k * 8 + i) * CF + 2 * r] = F0[i];
-      Y[(k * 8 + i) * CF + 2 * r + 1] = F1[i];
+      Y[(k * 8 + i) * CF + 2 * r + k] = F0[i];
+      Y[(k * 8 + i) * CF + 2 * r + 1 + k] = F1[i];
     }
   }
   __syncthreads();
@@ -507,7 +514,7 @@ x_pass2_kernel(XPassArgs a) {
     const int col = it % CF, j = it / CF;
     double2 v[R1];
 #pragma unroll
-    for (int i = 0; i < R1; ++i) v[i] = Y[(j + 8 * i) * CF + col];
+    for (int i = 0; i < R1; ++i) v[i] = Y[(j + 8 * i) * CF + col + i];
 #pragma unroll
     for (int i = 1; i < R1; ++i) v[i] = cmul(v[i], tw[i * j]);
     dft_3p<R1, -1>(v, tw, 8);
