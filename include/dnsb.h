@@ -172,7 +172,11 @@ int dnsb_couette_spec_to_phys(dnsb_couette* ctx, const void* spec,
                               double* phys, void* stream);
 int dnsb_couette_phys_to_spec(dnsb_couette* ctx, const double* phys,
                               void* spec, void* stream);
-/* Device status word of the context (nonzero after a bad pivot). */
+/* Reads the context's device status word (synchronising `stream`):
+ * DNSB_ERR_PIVOT when a bound operator holds a pivot index outside
+ * [j, j+kl] (found when the operators are bound; such a pivot is not
+ * followed), DNSB_ERR_CUDA when a bounded wait inside the IMM substitution
+ * kernel gave up (its results are then invalid), else 0. */
 int dnsb_couette_check(dnsb_couette* ctx, void* stream);
 
 /* Allocation-free Couette norm (no counterpart in the reference; it exists
