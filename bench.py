@@ -103,6 +103,12 @@ def op_bytes(w):
     return {"rhs": cb * (6 * S + 18 * A1 + 18 * A2), "correct": cb * 12 * S}
 
 
+# DRAM bytes (read + write) of one call, summed over the call's kernels, from
+# one ncu capture of this workload (profiles/couette128_step_kernels_ncu.md);
+# None where no capture exists.
+MEASURED_TRAFFIC = {"couette128": {"rhs": 470.2e6, "imm": 717.4e6}}
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during a region.
 
@@ -364,13 +370,15 @@ def run_ours(a, w, rank, world):
         },
         "roofline": {
             "bound": "hbm",
-            "kernel": "imm_kernel (+1-block norm finalize)" if dom == "imm"
-                      else "rhs passes (3 kernels)",
+            "kernel": ("IMM corrector (5 kernels + 1-block norm finalize)"
+                       if w["system"] == "plane-couette" else "corrector (1 kernel)")
+                      if dom == "imm" else "rhs passes (3 kernels)"
+                      if w["system"] == "plane-couette" else "rhs passes (5 kernels)",
             "achieved": achieved,
             "peak": peak,
             "unit": "GB/s",
             "frac": achieved / peak,
-            "traffic": None,
+            "traffic": MEASURED_TRAFFIC.get(a.workload, {}).get(dom),
             "peak_source": "measured" if peaks else "fallback",
             "algorithmic_bytes_per_launch": bytes_,
             "avg_launch_ms": dur,
