@@ -57,10 +57,10 @@ PLAIN_ITERS_PER_STEP = {"couette128": 11, "couette64": 21, "kolmogorov32": 3,
                         "kolmogorov128": 3}
 
 
-def params_for(w):
+def params_for(w, fp64=True):
     from dnsjax_b200.parameters import Parameters
 
-    res = dict(nx=w["nx"], ny=w["ny"], nz=w["nz"])
+    res = dict(nx=w["nx"], ny=w["ny"], nz=w["nz"], double_precision=fp64)
     if "p" in w:
         res["fd_order"] = w["p"]
     return Parameters(phys=dict(system=w["system"], re=w["re"]),
@@ -264,7 +264,10 @@ def run_ours(a, w, rank, world):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    p = params_for(w)
+    mixed = a.form == "mixed"
+    if mixed and w["system"] != "plane-couette":
+        raise SystemExit("--form mixed is built for plane Couette")
+    p = params_for(w, fp64=not mixed)
     if w["system"] == "plane-couette":
         from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
 
@@ -278,7 +281,7 @@ def run_ours(a, w, rank, world):
     u0 = initial_state(w, replica_seed(w["seed"], rank))
     tf = Timed(flow)
     steppers = tf.make_stepper()
-    tol, mi = w["tol"], w["max_iter"]
+    tol, mi = (w["tol"] if a.tol is None else a.tol), w["max_iter"]
     state = torch.as_tensor(u0, device="cuda")
     for _ in range(a.warmup):
         state, c, e = driver.step(tf, steppers, state, tol, mi)
@@ -354,10 +357,10 @@ def run_ours(a, w, rank, world):
         "data": "synthetic (seeded divergence-free spectral field)",
         "config": {
             "workload": a.workload,
-            "form": "plain-fp64",
+            "form": "mixed: FP32 RHS passes, FP64 state/IMM/norms" if mixed else "plain-fp64",
             "grid": [w["nx"], w["ny"], w["nz"]],
             "fd_order": w.get("p"),
-            "re": w["re"], "dt": w["dt"], "tol": w["tol"],
+            "re": w["re"], "dt": w["dt"], "tol": tol,
             "max_corrector_iterations": w["max_iter"],
             "corrector_iterations_per_step": sum(iters) / len(iters),
             "last_error": errs[-1],
@@ -392,6 +395,23 @@ def run_ours(a, w, rank, world):
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
+    if mixed:
+        # Error of the mixed form after the warm-up + timed steps, against the
+        # plain FP64 form advanced the same number of steps from the same field.
+        from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
+
+        plain = PlaneCouetteFlow(params_for(w, fp64=True))
+        ps = plain.make_stepper()
+        ref = torch.as_tensor(u0, device="cuda")
+        for _ in range(a.warmup + a.steps):
+            ref, _, _ = driver.step(plain, ps, ref, w["tol"], mi)
+        ke_m = float(flow.norm(state).item()) ** 2 / 2
+        ke_p = float(plain.norm(ref).item()) ** 2 / 2
+        diff = torch.linalg.vector_norm(state - ref) / torch.linalg.vector_norm(ref)
+        out["config"]["vs_plain"] = {"steps": a.warmup + a.steps,
+                                     "ke_rel_err": abs(ke_m - ke_p) / ke_p,
+                                     "field_rel_l2": float(diff.item())}
+        out["dtype"] = "f32 (RHS passes) + f64"
     if rank == 0 and not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_sample(w, flow, u0, sum(iters) / len(iters))
     if dist is not None:
@@ -502,6 +522,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="couette128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", default="plain", choices=["plain", "mixed"],
+                    help="mixed: FP32 RHS passes (plane Couette), FP64 elsewhere")
+    ap.add_argument("--tol", type=float, default=None,
+                    help="corrector tolerance of the timed run (default: the workload's)")
     a = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

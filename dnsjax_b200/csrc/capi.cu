@@ -61,6 +61,17 @@ int make_twiddles(double2** dst, int L) {
   return upload(dst, h.data(), (size_t)L);
 }
 
+// The same table rounded to single precision (FP32 passes).
+int make_twiddles32(float2** dst, int L) {
+  std::vector<float2> h(L);
+  const long double pi = 3.14159265358979323846264338327950288L;
+  for (int m = 0; m < L; ++m) {
+    const long double a = 2.0L * pi * (long double)m / (long double)L;
+    h[m] = make_float2((float)cosl(a), (float)(-sinl(a)));
+  }
+  return upload(dst, h.data(), (size_t)L);
+}
+
 bool fft_size_ok(int L) { return L >= 1 && make_plan(L).nst > 0; }
 
 int max_smem_optin() {
@@ -454,6 +465,8 @@ struct dnsb_couette {
   double dt, c, nu, ly;
   FFTPlan pz, px;
   double2 *twz = nullptr, *twx = nullptr;
+  float2 *twz32 = nullptr, *twx32 = nullptr;
+  int rhs_fp32 = 0;  // RHS passes in FP32 (dnsb_couette_set_rhs_precision)
   double *kx = nullptr, *kz = nullptr, *d1w = nullptr, *d2w = nullptr;
   double *d1wT = nullptr, *d2wT = nullptr;  // [tap][Ny]: lanes over y read contiguously
   int *d1j0 = nullptr, *d2j0 = nullptr;
@@ -511,7 +524,7 @@ struct dnsb_couette {
 };
 
 static void couette_free(dnsb_couette* p) {
-  void* ptrs[] = {p->twz, p->twx, p->kx, p->kz, p->d1w, p->d2w, p->d1wT, p->d2wT, p->d1j0,
+  void* ptrs[] = {p->twz, p->twx, p->twz32, p->twx32, p->kx, p->kz, p->d1w, p->d2w, p->d1wT, p->d2wT, p->d1j0,
                   p->d2j0, p->U, p->cU, p->nU, p->simpson, p->B, p->partials,
                   p->status, p->fac, p->dp, p->Fw, p->Rw};
   for (void* q : ptrs)
@@ -593,6 +606,8 @@ extern "C" int dnsb_couette_create(const dnsb_couette_desc* d,
   };
   chk(make_twiddles(&p->twz, p->Mz));
   chk(make_twiddles(&p->twx, p->Mx));
+  chk(make_twiddles32(&p->twz32, p->Mz));
+  chk(make_twiddles32(&p->twx32, p->Mx));
   chk(upload(&p->kx, d->kx, p->NKX));
   chk(upload(&p->kz, d->kz, p->NZ1));
   chk(upload(&p->d1j0, d->d1_j0, p->Ny));
@@ -781,7 +796,8 @@ extern "C" int dnsb_couette_rhs(dnsb_couette* p, const void* state, void* rhs,
   zi.kx = p->kx;
   zi.kz = p->kz;
   zi.plan = p->pz;
-  zi.tw = p->twz;
+  zi.tw = p->rhs_fp32 ? reinterpret_cast<const double2*>(p->twz32) : p->twz;
+  zi.fp32 = p->rhs_fp32;
   DNSB_LAUNCH(launch_zinv_curl(zi, p->span_max, st));
   XPassArgs xa{};
   xa.in = p->B;
@@ -800,7 +816,8 @@ extern "C" int dnsb_couette_rhs(dnsb_couette* p, const void* state, void* rhs,
   xa.nU = p->nU;
   xa.ny_grid = p->Ny;
   xa.plan = p->px;
-  xa.tw = p->twx;
+  xa.tw = p->rhs_fp32 ? reinterpret_cast<const double2*>(p->twx32) : p->twx;
+  xa.fp32 = p->rhs_fp32;
   DNSB_LAUNCH(launch_x_pass(xa, st));
   ColPassArgs zf{};
   zf.in = p->B;
@@ -815,8 +832,21 @@ extern "C" int dnsb_couette_rhs(dnsb_couette* p, const void* state, void* rhs,
   zf.nstored = p->NZ1;
   zf.inverse = 0;
   zf.plan = p->pz;
-  zf.tw = p->twz;
+  zf.tw = p->rhs_fp32 ? reinterpret_cast<const double2*>(p->twz32) : p->twz;
+  zf.fp32 = p->rhs_fp32;
   DNSB_LAUNCH(launch_col_pass(zf, 3, p->NKX, st));
+  return 0;
+}
+
+extern "C" int dnsb_couette_set_rhs_precision(dnsb_couette* p, int fp32) {
+  if (!p) return fail(DNSB_ERR_ARG, "null argument");
+  if (fp32) {
+    auto fixed = [](int L) { return L == 48 || L == 72 || L == 96 || L == 192; };
+    if (!fixed(p->Mz) || !fixed(p->Mx) || 3 * p->NKX != p->Mx)
+      return fail(DNSB_ERR_ARG,
+                  "FP32 RHS passes need padded sizes in {48, 72, 96, 192} with nx_p = 3 nx / 2");
+  }
+  p->rhs_fp32 = fp32 ? 1 : 0;
   return 0;
 }
 

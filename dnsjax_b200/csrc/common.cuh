@@ -9,6 +9,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 
 #define DNSB_MAX_RADIX 8
 #define DNSB_MAX_STAGES 12
@@ -40,6 +41,47 @@ __host__ __device__ __forceinline__ double2 ci(double2 z) {
   return make_double2(-z.y, z.x);
 }
 
+// Single-precision complex (the FP32 form of the Couette RHS passes).
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+  return make_float2(a.x + b.x, a.y + b.y);
+}
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  return make_float2(a.x - b.x, a.y - b.y);
+}
+__host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ float2 cscale(float2 a, float s) {
+  return make_float2(a.x * s, a.y * s);
+}
+
+// Complex type <-> real type and constructor.
+template <typename C>
+struct cplx;
+template <>
+struct cplx<double2> {
+  using real = double;
+  __host__ __device__ static double2 make(double x, double y) { return make_double2(x, y); }
+};
+template <>
+struct cplx<float2> {
+  using real = float;
+  __host__ __device__ static float2 make(float x, float y) { return make_float2(x, y); }
+};
+template <typename C>
+__host__ __device__ __forceinline__ C cmake(typename cplx<C>::real x, typename cplx<C>::real y) {
+  return cplx<C>::make(x, y);
+}
+// Conversions between the two precisions.
+__host__ __device__ __forceinline__ double2 to_c(double2 z, double2*) { return z; }
+__host__ __device__ __forceinline__ float2 to_c(double2 z, float2*) {
+  return make_float2((float)z.x, (float)z.y);
+}
+__host__ __device__ __forceinline__ double2 to_d(double2 z) { return z; }
+__host__ __device__ __forceinline__ double2 to_d(float2 z) {
+  return make_double2((double)z.x, (double)z.y);
+}
+
 // An FFT length L = product of radices (each 2, 3, 4 or 8), applied as
 // Stockham auto-sort stages so the output is in natural order.
 struct FFTPlan {
@@ -49,49 +91,56 @@ struct FFTPlan {
 };
 
 // ---- small DFTs in registers; sign = -1 forward, +1 inverse ------------
-__device__ __forceinline__ void dft2(double2* v) {
-  double2 a = v[0], b = v[1];
+// Generic over the complex type (double2, float2): the same operations in
+// either precision.
+template <typename C>
+__device__ __forceinline__ void dft2(C* v) {
+  C a = v[0], b = v[1];
   v[0] = cadd(a, b);
   v[1] = csub(a, b);
 }
 
-__device__ __forceinline__ void dft3(double2* v, int sign) {
-  const double s3 = 0.86602540378443864676;  // sin(2 pi / 3)
-  double2 t1 = cadd(v[1], v[2]);
-  double2 t2 = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
-  double2 d = csub(v[1], v[2]);
+template <typename C>
+__device__ __forceinline__ void dft3(C* v, int sign) {
+  using R = typename cplx<C>::real;
+  const R s3 = (R)0.86602540378443864676;  // sin(2 pi / 3)
+  const R half = (R)0.5;
+  C t1 = cadd(v[1], v[2]);
+  C t2 = cmake<C>(v[0].x - half * t1.x, v[0].y - half * t1.y);
+  C d = csub(v[1], v[2]);
   // i * sign * s3 * d
-  double2 t3 = make_double2(-sign * s3 * d.y, sign * s3 * d.x);
+  C t3 = cmake<C>(-sign * s3 * d.y, sign * s3 * d.x);
   v[0] = cadd(v[0], t1);
   v[1] = cadd(t2, t3);
   v[2] = csub(t2, t3);
 }
 
-__device__ __forceinline__ void dft4(double2* v, int sign) {
-  double2 a = cadd(v[0], v[2]);
-  double2 b = csub(v[0], v[2]);
-  double2 c = cadd(v[1], v[3]);
-  double2 d = csub(v[1], v[3]);
+template <typename C>
+__device__ __forceinline__ void dft4(C* v, int sign) {
+  C a = cadd(v[0], v[2]);
+  C b = csub(v[0], v[2]);
+  C c = cadd(v[1], v[3]);
+  C d = csub(v[1], v[3]);
   // i * sign * d
-  double2 isd = make_double2(-sign * d.y, sign * d.x);
+  C isd = cmake<C>(-sign * d.y, sign * d.x);
   v[0] = cadd(a, c);
   v[2] = csub(a, c);
   v[1] = cadd(b, isd);
   v[3] = csub(b, isd);
 }
 
-__device__ __forceinline__ void dft8(double2* v, int sign) {
-  const double h = 0.70710678118654752440;  // sqrt(2)/2
-  double2 e[4] = {v[0], v[2], v[4], v[6]};
-  double2 o[4] = {v[1], v[3], v[5], v[7]};
+template <typename C>
+__device__ __forceinline__ void dft8(C* v, int sign) {
+  using R = typename cplx<C>::real;
+  const R h = (R)0.70710678118654752440;  // sqrt(2)/2
+  C e[4] = {v[0], v[2], v[4], v[6]};
+  C o[4] = {v[1], v[3], v[5], v[7]};
   dft4(e, sign);
   dft4(o, sign);
   // twiddles w8^q = exp(sign * 2 pi i q / 8), q = 0..3
-  double2 t1 = make_double2(h * (o[1].x - sign * o[1].y),
-                            h * (o[1].y + sign * o[1].x));
-  double2 t2 = make_double2(-sign * o[2].y, sign * o[2].x);
-  double2 t3 = make_double2(h * (-o[3].x - sign * o[3].y),
-                            h * (-o[3].y + sign * o[3].x));
+  C t1 = cmake<C>(h * (o[1].x - sign * o[1].y), h * (o[1].y + sign * o[1].x));
+  C t2 = cmake<C>(-sign * o[2].y, sign * o[2].x);
+  C t3 = cmake<C>(h * (-o[3].x - sign * o[3].y), h * (-o[3].y + sign * o[3].x));
   v[0] = cadd(e[0], o[0]);
   v[4] = csub(e[0], o[0]);
   v[1] = cadd(e[1], t1);
@@ -249,19 +298,18 @@ __device__ __forceinline__ double2* fft_cols(double2* a, double2* b,
 // ---- register DFTs of size N = 3P (P in {2, 3, 4, 8}) --------------------
 // tw[m * TS] = exp(-2 pi i m / N) (a length-N*TS table); SIGN -1 forward,
 // +1 inverse; natural-order output in v.
-template <int P>
-__device__ __forceinline__ void dft_small(double2* v, int sign) {
+template <int P, typename C>
+__device__ __forceinline__ void dft_small(C* v, int sign) {
   if constexpr (P == 2) dft2(v);
   else if constexpr (P == 3) dft3(v, sign);
   else if constexpr (P == 4) dft4(v, sign);
   else dft8(v, sign);
 }
 
-template <int N, int SIGN>
-__device__ __forceinline__ void dft_3p(double2* v, const double2* __restrict__ tw,
-                                       int TS) {
+template <int N, int SIGN, typename C>
+__device__ __forceinline__ void dft_3p(C* v, const C* __restrict__ tw, int TS) {
   constexpr int P = N / 3;
-  double2 a[3][P];
+  C a[3][P];
 #pragma unroll
   for (int q = 0; q < 3; ++q)
 #pragma unroll
@@ -272,13 +320,13 @@ __device__ __forceinline__ void dft_3p(double2* v, const double2* __restrict__ t
   for (int q = 1; q < 3; ++q)
 #pragma unroll
     for (int k1 = 1; k1 < P; ++k1) {
-      double2 w = tw[(q * k1) * TS];
+      C w = tw[(q * k1) * TS];
       if (SIGN > 0) w.y = -w.y;
       a[q][k1] = cmul(a[q][k1], w);
     }
 #pragma unroll
   for (int k1 = 0; k1 < P; ++k1) {
-    double2 b[3] = {a[0][k1], a[1][k1], a[2][k1]};
+    C b[3] = {a[0][k1], a[1][k1], a[2][k1]};
     dft3(b, SIGN);
 #pragma unroll
     for (int k2 = 0; k2 < 3; ++k2) v[k1 + P * k2] = b[k2];
@@ -329,6 +377,13 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem)
                : "memory");
 }
+// One complex element, either precision.
+__device__ __forceinline__ void cp_async_elem(double2* smem, const double2* gmem) {
+  cp_async16(smem, gmem);
+}
+__device__ __forceinline__ void cp_async_elem(float2* smem, const float2* gmem) {
+  cp_async8(smem, gmem);
+}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
@@ -342,8 +397,8 @@ __device__ __forceinline__ void cp_async_wait_2() {
   asm volatile("cp.async.wait_group 2;\n" ::: "memory");
 }
 
-__device__ __forceinline__ void load_twiddles(double2* s, const double2* g,
-                                              int L) {
+template <typename C>
+__device__ __forceinline__ void load_twiddles(C* s, const C* g, int L) {
   for (int i = threadIdx.x; i < L; i += blockDim.x) s[i] = g[i];
 }
 

@@ -123,29 +123,33 @@ size_t col_pass2_smem(int M) {
   return sizeof(double2) * (size_t)(M * kC2Cols + M);
 }
 
-template <int ML, int SIGN>
+// T: the compute type and the element type of `in` (double, or float for the
+// FP32 form of the Couette RHS, whose pass buffer holds float2); `out` is
+// always complex128.
+template <int ML, int SIGN, typename T = double>
 __global__ void __launch_bounds__(kC2Threads)
 col_pass2_kernel(ColPassArgs a) {
+  using CT = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
   constexpr int M = ML, R1 = M / 8, C = kC2Cols;
-  extern __shared__ double2 sm[];
-  double2* X = sm;  // [t][C]
-  double2* tw = X + M * C;
+  extern __shared__ double2 sm_[];
+  CT* X = reinterpret_cast<CT*>(sm_);  // [t][C]
+  CT* tw = X + M * C;
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * C;
   const long long o = blockIdx.y;
   const long long f = blockIdx.z;
-  const double2* in = a.in + f * a.in_fs + o * a.in_os + i0;
+  const CT* in = reinterpret_cast<const CT*>(a.in) + f * a.in_fs + o * a.in_os + i0;
   double2* out = a.out + f * a.out_fs + o * a.out_os + i0;
   const int ni = min(C, a.nI - i0);
-  load_twiddles(tw, a.tw, M);
+  load_twiddles(tw, reinterpret_cast<const CT*>(a.tw), M);
   __syncthreads();
   for (int it = tid; it < 8 * C; it += kC2Threads) {
     const int c = it % C, j = it / C;
-    double2 v[R1];
+    CT v[R1];
 #pragma unroll
     for (int i = 0; i < R1; ++i) {
       const int t = j + 8 * i;
-      double2 z = make_double2(0.0, 0.0);
+      CT z = cmake<CT>(0, 0);
       if (c < ni) {
         if (SIGN > 0) {
           const int sidx = pos_to_stored(t, a.nstored, M);
@@ -164,12 +168,12 @@ col_pass2_kernel(ColPassArgs a) {
   const double sc = 1.0 / M;
   for (int it = tid; it < R1 * C; it += kC2Threads) {
     const int c = it % C, k = it / C;
-    double2 z[8];
+    CT z[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) z[i] = X[(k + R1 * i) * C + c];
 #pragma unroll
     for (int i = 1; i < 8; ++i) {
-      double2 w = tw[i * k];
+      CT w = tw[i * k];
       if (SIGN > 0) w.y = -w.y;
       z[i] = cmul(z[i], w);
     }
@@ -179,10 +183,10 @@ col_pass2_kernel(ColPassArgs a) {
       for (int i = 0; i < 8; ++i) {
         const int t = k + R1 * i;
         if (SIGN > 0) {
-          out[t * a.out_ts + c] = z[i];
+          out[t * a.out_ts + c] = to_d(z[i]);
         } else {
           const int sidx = pos_to_stored(t, a.nstored, M);
-          if (sidx >= 0) out[sidx * a.out_ts + c] = cscale(z[i], sc);
+          if (sidx >= 0) out[sidx * a.out_ts + c] = cscale(to_d(z[i]), sc);
         }
       }
     }
@@ -194,16 +198,19 @@ cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
   const int L = a.plan.L;
   if (L == 48 || L == 72 || L == 96 || L == 192) {
     dim3 g2((a.nI + kC2Cols - 1) / kC2Cols, nO, nfields);
-    const size_t sm2 = col_pass2_smem(L);
-#define DNSB_C2(LL)                                                           \
-  case LL:                                                                    \
-    if (a.inverse) col_pass2_kernel<LL, 1><<<g2, kC2Threads, sm2, st>>>(a);   \
-    else col_pass2_kernel<LL, -1><<<g2, kC2Threads, sm2, st>>>(a);            \
+    const size_t sm2 = a.fp32 ? col_pass2_smem(L) / 2 : col_pass2_smem(L);
+    if (a.fp32 && a.inverse) return cudaErrorInvalidValue;  // forward only
+#define DNSB_C2(LL)                                                              \
+  case LL:                                                                       \
+    if (a.fp32) col_pass2_kernel<LL, -1, float><<<g2, kC2Threads, sm2, st>>>(a);  \
+    else if (a.inverse) col_pass2_kernel<LL, 1><<<g2, kC2Threads, sm2, st>>>(a);  \
+    else col_pass2_kernel<LL, -1><<<g2, kC2Threads, sm2, st>>>(a);               \
     break;
     switch (L) { DNSB_C2(48) DNSB_C2(72) DNSB_C2(96) DNSB_C2(192) }
 #undef DNSB_C2
     return cudaGetLastError();
   }
+  if (a.fp32) return cudaErrorInvalidValue;  // compile-time sizes only
   dim3 grid((a.nI + kTile - 1) / kTile, nO, nfields);
   size_t sm = col_pass_smem(a.plan.L);
   DNSB_DISPATCH(a.plan.L, col_pass_kernel, grid, sm, st, a);
@@ -348,7 +355,7 @@ x_pass_kernel(XPassArgs a) {
   }
 }
 
-template <int ML>
+template <int ML, typename T = double>
 __global__ void __launch_bounds__(kX2Threads) x_pass2_kernel(XPassArgs a);
 
 cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
@@ -357,6 +364,16 @@ cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
   const int L = (a.nkx * 3 == a.plan.L) ? a.plan.L : -1;
   if (L == 48 || L == 72 || L == 96 || L == 192) {
     dim3 g2((a.nrows + kX2Rows - 1) / kX2Rows);
+    if (a.fp32) {
+      const size_t sm2 = x_pass2_smem(L, a.nkx) / 2;
+      switch (L) {
+        case 48: x_pass2_kernel<48, float><<<g2, kX2Threads, sm2, st>>>(a); break;
+        case 72: x_pass2_kernel<72, float><<<g2, kX2Threads, sm2, st>>>(a); break;
+        case 96: x_pass2_kernel<96, float><<<g2, kX2Threads, sm2, st>>>(a); break;
+        default: x_pass2_kernel<192, float><<<g2, kX2Threads, sm2, st>>>(a); break;
+      }
+      return cudaGetLastError();
+    }
     const size_t sm2 = x_pass2_smem(L, a.nkx);
     switch (L) {
       case 48: x_pass2_kernel<48><<<g2, kX2Threads, sm2, st>>>(a); break;
@@ -366,6 +383,7 @@ cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
     }
     return cudaGetLastError();
   }
+  if (a.fp32) return cudaErrorInvalidValue;  // compile-time sizes only
   DNSB_DISPATCH(L, x_pass_kernel, grid, x_pass_smem(a.plan.L), st, a);
   return cudaGetLastError();
 }
@@ -383,9 +401,12 @@ size_t x_pass2_smem(int M, int nkx) {
   return sizeof(double2) * ((S > Y ? S : Y) + X + M);
 }
 
-template <int ML>
+// T: the compute type and the element type of the pass buffer (double, or
+// float for the FP32 form of the Couette RHS).
+template <int ML, typename T>
 __global__ void __launch_bounds__(kX2Threads)
 x_pass2_kernel(XPassArgs a) {
+  using CT = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
   constexpr int M = ML, R1 = M / 8, R = kX2Rows, NKX = ML / 3;
   constexpr int CI = 3 * R, CF = 2 * R;
   // Stage outputs carry a skew of XS (X) / 1 (Y) slots per block of R1 (X)
@@ -395,11 +416,15 @@ x_pass2_kernel(XPassArgs a) {
   static_assert(R == 4, "the stage-A lane map assumes 4 rows");
   constexpr int SZ_S = 6 * NKX * R, SZ_Y = M * CF + R1;
   constexpr int SZ_SY = SZ_S > SZ_Y ? SZ_S : SZ_Y;
-  extern __shared__ double2 sm[];
-  double2* S = sm;            // staged half spectra, S[(f*NKX + k)*R + r]
-  double2* Y = sm;            // forward stage-1 output [t][CF] (after S dies)
-  double2* X = sm + SZ_SY;    // inverse stage-A output [t][CI]; later [t][CF]
-  double2* tw = X + M * CI + XS * 8;
+  extern __shared__ double2 sm_[];
+  CT* sm = reinterpret_cast<CT*>(sm_);
+  CT* S = sm;                 // staged half spectra, S[(f*NKX + k)*R + r]
+  CT* Y = sm;                 // forward stage-1 output [t][CF] (after S dies)
+  CT* X = sm + SZ_SY;         // inverse stage-A output [t][CI]; later [t][CF]
+  CT* tw = X + M * CI + XS * 8;
+  const CT* gin = reinterpret_cast<const CT*>(a.in);
+  const CT* gtw = reinterpret_cast<const CT*>(a.tw);
+  CT* gout = reinterpret_cast<CT*>(a.out);
   const int tid = threadIdx.x;
   const int r0 = blockIdx.x * R;
   const int nr = min(R, a.nrows - r0);
@@ -411,7 +436,7 @@ x_pass2_kernel(XPassArgs a) {
     s_off[tid] = (long long)outer * a.so + (long long)inner * a.si;
     s_y[tid] = a.y_outer ? outer : inner;
   }
-  for (int i = tid; i < M; i += kX2Threads) cp_async16(tw + i, a.tw + i);
+  for (int i = tid; i < M; i += kX2Threads) cp_async_elem(tw + i, gtw + i);
   __syncthreads();
   for (int idx = tid; idx < 6 * NKX * R; idx += kX2Threads) {
     int r, k, f;
@@ -424,9 +449,9 @@ x_pass2_kernel(XPassArgs a) {
       r = (idx / NKX) % R;
       f = idx / (R * NKX);
     }
-    double2* dst = S + (f * NKX + k) * R + r;
-    if (r < nr) cp_async16(dst, a.in + f * a.in_fs + s_off[r] + k * a.ks);
-    else *dst = make_double2(0.0, 0.0);
+    CT* dst = S + (f * NKX + k) * R + r;
+    if (r < nr) cp_async_elem(dst, gin + f * a.in_fs + s_off[r] + k * a.ks);
+    else *dst = cmake<CT>(0, 0);
   }
   cp_async_commit();
   cp_async_wait_all();
@@ -437,21 +462,21 @@ x_pass2_kernel(XPassArgs a) {
     const int r = it & 3, rest = it >> 3;
     const int pr = rest % 3, j = ((it >> 2) & 1) + 2 * (rest / 3);
     const int col = 3 * r + pr;
-    const double2* A = S + (2 * pr) * NKX * R + r;
-    const double2* B = S + (2 * pr + 1) * NKX * R + r;
-    double2 v[R1];
+    const CT* A = S + (2 * pr) * NKX * R + r;
+    const CT* B = S + (2 * pr + 1) * NKX * R + r;
+    CT v[R1];
 #pragma unroll
     for (int i = 0; i < R1; ++i) {
       const int t = j + 8 * i;
-      double2 z = make_double2(0.0, 0.0);
+      CT z = cmake<CT>(0, 0);
       if (t == 0) {
-        z = make_double2(A[0].x, B[0].x);
+        z = cmake<CT>(A[0].x, B[0].x);
       } else if (t < NKX) {
-        const double2 av = A[t * R], bv = B[t * R];
-        z = make_double2(av.x - bv.y, av.y + bv.x);
+        const CT av = A[t * R], bv = B[t * R];
+        z = cmake<CT>(av.x - bv.y, av.y + bv.x);
       } else if (M - t < NKX) {
-        const double2 av = A[(M - t) * R], bv = B[(M - t) * R];
-        z = make_double2(av.x + bv.y, -av.y + bv.x);
+        const CT av = A[(M - t) * R], bv = B[(M - t) * R];
+        z = cmake<CT>(av.x + bv.y, -av.y + bv.x);
       }
       v[i] = z;
     }
@@ -464,41 +489,41 @@ x_pass2_kernel(XPassArgs a) {
   // rotational product there; forward radix-8 stage (Ns = 1) on the same t.
   for (int it = tid; it < R1 * R; it += kX2Threads) {
     const int r = it % R, k = it / R;
-    double2 z[3][8];
+    CT z[3][8];
 #pragma unroll
     for (int pr = 0; pr < 3; ++pr) {
 #pragma unroll
       for (int i = 0; i < 8; ++i) z[pr][i] = X[(k + R1 * i) * CI + 3 * r + pr + XS * i];
 #pragma unroll
       for (int i = 1; i < 8; ++i) {
-        double2 w = tw[i * k];
+        CT w = tw[i * k];
         w.y = -w.y;
         z[pr][i] = cmul(z[pr][i], w);
       }
       dft8(z[pr], 1);
     }
-    double2 F0[8], F1[8];
+    CT F0[8], F1[8];
     const bool live = r < nr;
     const int y = s_y[r];
     const int ny = a.ny_grid;
-    const double U0 = live ? a.U[y] : 0.0, U1 = live ? a.U[ny + y] : 0.0,
-                 U2 = live ? a.U[2 * ny + y] : 0.0;
-    const double C0 = live ? a.cU[y] : 0.0, C1 = live ? a.cU[ny + y] : 0.0,
-                 C2 = live ? a.cU[2 * ny + y] : 0.0;
-    const double N0 = live ? a.nU[y] : 0.0, N1 = live ? a.nU[ny + y] : 0.0,
-                 N2 = live ? a.nU[2 * ny + y] : 0.0;
+    const T U0 = live ? (T)a.U[y] : T(0), U1 = live ? (T)a.U[ny + y] : T(0),
+            U2 = live ? (T)a.U[2 * ny + y] : T(0);
+    const T C0 = live ? (T)a.cU[y] : T(0), C1 = live ? (T)a.cU[ny + y] : T(0),
+            C2 = live ? (T)a.cU[2 * ny + y] : T(0);
+    const T N0 = live ? (T)a.nU[y] : T(0), N1 = live ? (T)a.nU[ny + y] : T(0),
+            N2 = live ? (T)a.nU[2 * ny + y] : T(0);
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const double u0 = z[0][i].x, u1 = z[0][i].y, u2 = z[1][i].x;
-      const double w0 = z[1][i].y, w1 = z[2][i].x, w2 = z[2][i].y;
-      const double n0 = u1 * w2 - u2 * w1;
-      const double n1 = u2 * w0 - u0 * w2;
-      const double n2 = u0 * w1 - u1 * w0;
-      const double b0 = (u1 * C2 - u2 * C1) + (U1 * w2 - U2 * w1) + N0;
-      const double b1 = (u2 * C0 - u0 * C2) + (U2 * w0 - U0 * w2) + N1;
-      const double b2 = (u0 * C1 - u1 * C0) + (U0 * w1 - U1 * w0) + N2;
-      F0[i] = live ? make_double2(n0 + b0, n1 + b1) : make_double2(0.0, 0.0);
-      F1[i] = live ? make_double2(n2 + b2, 0.0) : make_double2(0.0, 0.0);
+      const T u0 = z[0][i].x, u1 = z[0][i].y, u2 = z[1][i].x;
+      const T w0 = z[1][i].y, w1 = z[2][i].x, w2 = z[2][i].y;
+      const T n0 = u1 * w2 - u2 * w1;
+      const T n1 = u2 * w0 - u0 * w2;
+      const T n2 = u0 * w1 - u1 * w0;
+      const T b0 = (u1 * C2 - u2 * C1) + (U1 * w2 - U2 * w1) + N0;
+      const T b1 = (u2 * C0 - u0 * C2) + (U2 * w0 - U0 * w2) + N1;
+      const T b2 = (u0 * C1 - u1 * C0) + (U0 * w1 - U1 * w0) + N2;
+      F0[i] = live ? cmake<CT>(n0 + b0, n1 + b1) : cmake<CT>(0, 0);
+      F1[i] = live ? cmake<CT>(n2 + b2, 0) : cmake<CT>(0, 0);
     }
     dft8(F0, -1);
     dft8(F1, -1);
@@ -512,7 +537,7 @@ x_pass2_kernel(XPassArgs a) {
   // Stage C: forward radix R1 (Ns = 8), natural order into X[t][CF].
   for (int it = tid; it < 8 * CF; it += kX2Threads) {
     const int col = it % CF, j = it / CF;
-    double2 v[R1];
+    CT v[R1];
 #pragma unroll
     for (int i = 0; i < R1; ++i) v[i] = Y[(j + 8 * i) * CF + col + i];
 #pragma unroll
@@ -523,7 +548,7 @@ x_pass2_kernel(XPassArgs a) {
   }
   __syncthreads();
   // Unpack the real-field spectra, truncate to NKX, scale 1/M, store.
-  const double h = 0.5 / M;
+  const T h = (T)0.5 / M;
   for (int idx = tid; idx < 3 * NKX * R; idx += kX2Threads) {
     int r, k, f;
     if (a.rows_fast) {
@@ -537,15 +562,15 @@ x_pass2_kernel(XPassArgs a) {
     }
     if (r >= nr) continue;
     const int col = 2 * r + (f == 2 ? 1 : 0);
-    const double2 Z = X[k * CF + col];
-    const double2 Zm = X[((M - k) % M) * CF + col];
-    double2 v;
+    const CT Z = X[k * CF + col];
+    const CT Zm = X[((M - k) % M) * CF + col];
+    CT v;
     if (f == 1) {
-      v = make_double2((Z.y + Zm.y) * h, (Zm.x - Z.x) * h);
+      v = cmake<CT>((Z.y + Zm.y) * h, (Zm.x - Z.x) * h);
     } else {
-      v = make_double2((Z.x + Zm.x) * h, (Z.y - Zm.y) * h);
+      v = cmake<CT>((Z.x + Zm.x) * h, (Z.y - Zm.y) * h);
     }
-    a.out[f * a.out_fs + s_off[r] + k * a.ks] = v;
+    gout[f * a.out_fs + s_off[r] + k * a.ks] = v;
   }
 }
 
@@ -1022,8 +1047,8 @@ size_t zinv_curl2_smem(int M) {
   return sizeof(double2) * (size_t)(M * kZ2Cols + M);
 }
 
-template <int M, int F>
-__device__ __forceinline__ void zinv2_fill(const ZInvCurlArgs& a, double2* X,
+template <int M, int F, typename CT>
+__device__ __forceinline__ void zinv2_fill(const ZInvCurlArgs& a, CT* X,
                                            const double2* U, const double2* V,
                                            const double2* Wc, long long sstride,
                                            int y, double kx, bool live) {
@@ -1040,24 +1065,30 @@ __device__ __forceinline__ void zinv2_fill(const ZInvCurlArgs& a, double2* X,
       if (live && s >= 0) v[e] = zinv_field<F>(a, U, V, Wc, s * sstride, s, y, kx);
     }
 #pragma unroll
-    for (int e = 0; e < B; ++e) X[tid + (e0 + e) * kZ2Threads] = v[e];
+    for (int e = 0; e < B; ++e) X[tid + (e0 + e) * kZ2Threads] = to_c(v[e], (CT*)nullptr);
   }
 }
 
-template <int ML>
+// T: the compute type and the element type of the output pass buffer
+// (double, or float for the FP32 form of the Couette RHS); the state is
+// read, and the curl's fill computed, in FP64.
+template <int ML, typename T = double>
 __global__ void __launch_bounds__(kZ2Threads, 4)
 zinv_curl2_kernel(ZInvCurlArgs a) {
+  using CT = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
   constexpr int M = ML, R1 = M / 8, C = kZ2Cols;
-  extern __shared__ double2 sm[];
-  double2* X = sm;  // [t][C]
-  double2* tw = X + M * C;
+  extern __shared__ double2 sm_[];
+  CT* X = reinterpret_cast<CT*>(sm_);  // [t][C]
+  CT* tw = X + M * C;
+  const CT* gtw = reinterpret_cast<const CT*>(a.tw);
+  CT* gout = reinterpret_cast<CT*>(a.out);
   const int tid = threadIdx.x;
   const int NZ1 = a.NZ1, NKX = a.NKX, Ny = a.Ny;
   const long long ncol = (long long)NKX * Ny;
   const long long q0 = (long long)blockIdx.x * C;
   const int nq = (int)min((long long)C, ncol - q0);
   const long long cs = (long long)NZ1 * ncol;
-  for (int i = tid; i < M; i += kZ2Threads) cp_async16(tw + i, a.tw + i);
+  for (int i = tid; i < M; i += kZ2Threads) cp_async_elem(tw + i, gtw + i);
   cp_async_commit();
   // The fill column of this thread (the same for all its elements).
   const int cf = tid % C;
@@ -1084,7 +1115,7 @@ zinv_curl2_kernel(ZInvCurlArgs a) {
     // Stage 1: inverse radix R1 (Ns = 1) on positions t = j + 8 i of column c.
     {
       const int c = tid % C, j = tid / C;
-      double2 v[R1];
+      CT v[R1];
 #pragma unroll
       for (int i = 0; i < R1; ++i) v[i] = X[(j + 8 * i) * C + c];
       dft_3p<R1, 1>(v, tw, 8);
@@ -1096,12 +1127,12 @@ zinv_curl2_kernel(ZInvCurlArgs a) {
     // Stage 2: inverse radix 8 (Ns = R1) -> positions t = k + R1 i.
     for (int it = tid; it < R1 * C; it += kZ2Threads) {
       const int c = it % C, k = it / C;
-      double2 z[8];
+      CT z[8];
 #pragma unroll
       for (int i = 0; i < 8; ++i) z[i] = X[(k + R1 * i) * C + c];
 #pragma unroll
       for (int i = 1; i < 8; ++i) {
-        double2 w = tw[i * k];
+        CT w = tw[i * k];
         w.y = -w.y;
         z[i] = cmul(z[i], w);
       }
@@ -1109,7 +1140,7 @@ zinv_curl2_kernel(ZInvCurlArgs a) {
       if (c < nq) {
 #pragma unroll
         for (int i = 0; i < 8; ++i)
-          a.out[f * fs + (long long)(k + R1 * i) * ncol + q0 + c] = z[i];
+          gout[f * fs + (long long)(k + R1 * i) * ncol + q0 + c] = z[i];
       }
     }
     __syncthreads();  // X is refilled by the next field
@@ -1122,6 +1153,16 @@ cudaError_t launch_zinv_curl(const ZInvCurlArgs& a, int span_max,
   if (L == 48 || L == 72 || L == 96 || L == 192) {
     const long long ncol = (long long)a.NKX * a.Ny;
     const int grid = (int)((ncol + kZ2Cols - 1) / kZ2Cols);
+    if (a.fp32) {
+      const size_t sm = zinv_curl2_smem(L) / 2;
+      switch (L) {
+        case 48: zinv_curl2_kernel<48, float><<<grid, kZ2Threads, sm, st>>>(a); break;
+        case 72: zinv_curl2_kernel<72, float><<<grid, kZ2Threads, sm, st>>>(a); break;
+        case 96: zinv_curl2_kernel<96, float><<<grid, kZ2Threads, sm, st>>>(a); break;
+        default: zinv_curl2_kernel<192, float><<<grid, kZ2Threads, sm, st>>>(a); break;
+      }
+      return cudaGetLastError();
+    }
     const size_t sm = zinv_curl2_smem(L);
     switch (L) {
       case 48: zinv_curl2_kernel<48><<<grid, kZ2Threads, sm, st>>>(a); break;
@@ -1131,6 +1172,7 @@ cudaError_t launch_zinv_curl(const ZInvCurlArgs& a, int span_max,
     }
     return cudaGetLastError();
   }
+  if (a.fp32) return cudaErrorInvalidValue;  // compile-time sizes only
   dim3 grid((a.Ny + kZTile - 1) / kZTile, a.NKX);
   DNSB_DISPATCH(a.plan.L, zinv_curl_kernel, grid,
                 zinv_curl_smem(a.plan.L, a.NZ1, span_max), st, a, span_max);
@@ -1145,8 +1187,18 @@ cudaError_t set_pass_attributes(int max_smem) {
                        DNSB_ALL_SIZES(zinv_curl_kernel),
                        (const void*)zinv_curl2_kernel<48>, (const void*)zinv_curl2_kernel<72>,
                        (const void*)zinv_curl2_kernel<96>, (const void*)zinv_curl2_kernel<192>,
+                       (const void*)zinv_curl2_kernel<48, float>,
+                       (const void*)zinv_curl2_kernel<72, float>,
+                       (const void*)zinv_curl2_kernel<96, float>,
+                       (const void*)zinv_curl2_kernel<192, float>,
                        (const void*)x_pass2_kernel<48>, (const void*)x_pass2_kernel<72>,
                        (const void*)x_pass2_kernel<96>, (const void*)x_pass2_kernel<192>,
+                       (const void*)x_pass2_kernel<48, float>, (const void*)x_pass2_kernel<72, float>,
+                       (const void*)x_pass2_kernel<96, float>, (const void*)x_pass2_kernel<192, float>,
+                       (const void*)col_pass2_kernel<48, -1, float>,
+                       (const void*)col_pass2_kernel<72, -1, float>,
+                       (const void*)col_pass2_kernel<96, -1, float>,
+                       (const void*)col_pass2_kernel<192, -1, float>,
                        (const void*)col_pass2_kernel<48, 1>, (const void*)col_pass2_kernel<48, -1>,
                        (const void*)col_pass2_kernel<72, 1>, (const void*)col_pass2_kernel<72, -1>,
                        (const void*)col_pass2_kernel<96, 1>, (const void*)col_pass2_kernel<96, -1>,

@@ -30,6 +30,7 @@ struct ColPassArgs {
   int inverse;   // 1: spectral -> padded, inverse FFT; 0: forward, truncate
   FFTPlan plan;  // transform length M = plan.L
   const double2* tw;
+  int fp32;            // `in` and arithmetic in FP32 (compile-time sizes)
 };
 
 // x pass.  Rows are (outer, inner) pairs; row r = outer * inner_n + inner
@@ -48,7 +49,8 @@ struct XPassArgs {
   const double* nU;    // U x curl U
   int ny_grid;
   FFTPlan plan;        // Mx
-  const double2* tw;
+  const double2* tw;   // float2 table when fp32
+  int fp32;            // pass buffer and arithmetic in FP32 (compile-time sizes)
 };
 
 // x pass to physical space only (3 fields -> real [c] at row offsets
@@ -108,7 +110,8 @@ struct ZInvCurlArgs {
   const double* kx;
   const double* kz;
   FFTPlan plan;
-  const double2* tw;
+  const double2* tw;   // float2 table when fp32
+  int fp32;            // output pass buffer and FFT in FP32 (compile-time sizes)
 };
 
 constexpr int kZTile = 8;  // y values per CTA in the Couette z passes

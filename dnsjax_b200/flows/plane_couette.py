@@ -35,8 +35,10 @@ class PlaneCouetteFlow:
         d = derive(p)
         self.ly = float(d.ly if ly is None else ly)
         r = p.res
-        if p.res.double_precision is False:
-            raise NotImplementedError("the plain form computes in FP64")
+        # res.double_precision = False (parameters.py:63 of the reference)
+        # selects the mixed form: the RHS transforms and products in FP32,
+        # the state, the IMM (banded LU, 2x2 solve) and the norms in FP64.
+        self.rhs_fp32 = p.res.double_precision is False
         self.nx, self.ny, self.nz = r.nx, r.ny, r.nz
         self.nx_p, _, self.nz_p = padded_sizes(p)
         self.p = r.fd_order
@@ -77,6 +79,8 @@ class PlaneCouetteFlow:
         _lib.check(L.dnsb_couette_create(_lib.C.byref(desc), _lib.C.byref(h)))
         self._ctx = h
         self._L = L
+        if self.rhs_fp32:
+            _lib.check(L.dnsb_couette_set_rhs_precision(self._ctx, 1))
 
         if imm is None:
             imm = precompute_imm(self.ys, self.fourier.kx_global,

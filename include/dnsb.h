@@ -154,6 +154,13 @@ int dnsb_couette_bind_imm(dnsb_couette* ctx, const dnsb_imm_ops* ops);
 /* rhs = NL(u) on the padded grid (plane_couette.py:274-289) */
 int dnsb_couette_rhs(dnsb_couette* ctx, const void* state, void* rhs,
                      void* stream);
+/* Arithmetic of dnsb_couette_rhs (the reference's res.double_precision,
+ * parameters.py:63, __main__.py:287): fp32 = 1 runs the transforms and the
+ * rotational product in FP32 -- the state is read and the RHS written in
+ * complex128, the IMM, its banded substitutions and every norm stay FP64;
+ * fp32 = 0 (the default) is FP64 throughout.  FP32 needs padded sizes in
+ * {48, 72, 96, 192} with nx_p = 3 nx / 2 (DNSB_ERR_ARG otherwise). */
+int dnsb_couette_set_rhs_precision(dnsb_couette* ctx, int fp32);
 /* One influence-matrix iteration (plane_couette.py:376-504):
  * vel_new = IMM(vel_n, vel_j, nl_n, nl_j); corr_out = vel_new - vel_j
  * (nullable); err_dev[0] = Simpson norm of the correction (nullable).

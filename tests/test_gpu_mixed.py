@@ -1,0 +1,97 @@
+"""The mixed form of plane Couette (res.double_precision = False): the RHS
+transforms and rotational product in FP32, the state, the influence-matrix
+iteration (banded LU substitutions, 2x2 solve) and every norm in FP64.
+
+* The FP32 RHS at 128x129x128 against the FP64 oracle: relative L2 per
+  component below 2e-6, and not bit-equal to the FP64 path (so the FP32
+  kernels are the ones that ran).
+* Sizes the FP32 passes do not cover are refused.
+* Plane Couette 64x65x64 (p = 4, Re 400, dt 0.02), 20 steps of the reference
+  loop from the same seeded field, plain at tolerance 1e-10 and mixed at
+  1e-8: the FP32 rounding of the RHS puts a floor under the correction norm
+  (about 3e-10 here, about 3e-6 at 128x129x128), so the mixed form is run
+  to a tolerance it can reach; the kinetic energy agrees to 1e-6 relative,
+  the field to 1e-5 relative L2.
+"""
+
+from math import pi
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(a):
+    import torch
+
+    return torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+def couette_params(nx, ny, nz, p_ord, re, dt, fp64, tol=1e-10, max_iter=60):
+    # corrector tolerance: 1e-10 plain; the caller passes a reachable one for
+    # the mixed form
+    from dnsjax_b200.parameters import Parameters
+
+    return Parameters(phys=dict(system="plane-couette", re=re),
+                      geo=dict(lx=2 * pi, lz=pi),
+                      res=dict(nx=nx, ny=ny, nz=nz, fd_order=p_ord,
+                               double_precision=fp64),
+                      step=dict(dt=dt, corrector_tolerance=tol,
+                                max_corrector_iterations=max_iter))
+
+
+def test_couette_fp32_rhs_128():
+    from dnsjax_b200 import initial
+    from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
+    from oracle.config import Config
+    from oracle.couette import CouetteSetup
+
+    flow = PlaneCouetteFlow(couette_params(128, 129, 128, 6, 1000.0, 0.01, False))
+    assert flow.rhs_fp32
+    imm = {k: host(v) for k, v in flow.imm.items()}
+    imm["D1"], imm["D2"] = flow.D1, flow.D2
+    orc = CouetteSetup(Config(system="plane-couette", nx=128, ny=129, nz=128,
+                              lx=2 * pi, lz=pi, re=1000.0, dt=0.01, fd_order=6),
+                       imm=imm)
+    u0 = initial.couette_field(128, 129, 128, 2 * pi, pi, 6, 4, 32.0, 5e-2)
+    ref = orc.get_rhs(u0)
+    got = host(flow.get_rhs(dev(u0)))
+    errs = [rel_l2(got[c], ref[c]) for c in range(3)]
+    assert max(errs) < 2e-6, errs
+    assert max(errs) > 1e-12, errs  # FP32 arithmetic actually ran
+
+
+def test_couette_fp32_rejects_runtime_sizes():
+    from dnsjax_b200 import _lib
+    from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
+
+    # nx = nz = 16 pad to 24: no compile-time FP32 pass for that length
+    flow = PlaneCouetteFlow(couette_params(16, 17, 16, 4, 100.0, 0.01, True))
+    with pytest.raises(_lib.DnsbError):
+        _lib.check(flow._L.dnsb_couette_set_rhs_precision(flow._ctx, 1))
+
+
+def test_couette_mixed_trajectory_64():
+    from dnsjax_b200 import driver, initial
+    from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
+
+    u0 = initial.couette_field(64, 65, 64, 2 * pi, pi, 4, 1, 8.0, 1e-3)
+    plain = PlaneCouetteFlow(couette_params(64, 65, 64, 4, 400.0, 0.02, True))
+    mixed = PlaneCouetteFlow(couette_params(64, 65, 64, 4, 400.0, 0.02, False, tol=1e-8))
+    rp = driver.run(plain, dev(u0), 20)
+    rm = driver.run(mixed, dev(u0), 20)
+    assert rm.converged and rp.converged and rm.steps == rp.steps == 20
+    assert max(rm.errors) <= 1e-8
+    up, um = rp.state, rm.state
+    ke = lambda f, u: float(f.norm(u).item()) ** 2 / 2  # noqa: E731
+    assert abs(ke(mixed, um) - ke(plain, up)) <= 1e-6 * ke(plain, up)
+    a, b = host(um), host(up)
+    for c in range(3):
+        assert rel_l2(a[c], b[c]) <= 1e-5, c
