@@ -49,6 +49,30 @@ WORKLOADS = {
                           seed=2),
 }
 
+# Ensemble of 96 independent Kolmogorov trajectories of uneven resolution
+# (32 each at 32^3, 48^3, 64^3 spectral; 2 pi box, Re uniform in [30, 80],
+# dt 0.01, tol 1e-10; trajectory i seeded with i), advanced in lockstep.
+WORKLOADS["ensemble96"] = dict(system="ensemble", sizes=(32, 48, 64), per_size=32,
+                               re_range=(30.0, 80.0), dt=0.01, tol=1e-10,
+                               max_iter=10, energy=1e-2, seed=7)
+
+
+def ensemble_members(w):
+    import numpy as np
+
+    rng = np.random.default_rng(w["seed"])
+    out = []
+    for si, n in enumerate(w["sizes"]):
+        for k in range(w["per_size"]):
+            i = si * w["per_size"] + k
+            out.append(dict(system="kolmogorov", nx=n, ny=n, nz=n,
+                            re=float(rng.uniform(*w["re_range"])), dt=w["dt"],
+                            lx=2 * pi, lz=2 * pi, ly=2 * pi, tol=w["tol"],
+                            max_iter=w["max_iter"], energy=w["energy"],
+                            spectrum="cfg0", seed=i))
+    return out
+
+
 # Corrector iterations per step of the plain method on each workload's
 # first steps (deterministic; measured by the CUDA path and equal to the
 # oracle's).  Used only to turn the reference arm's bounded per-iteration
@@ -459,9 +483,183 @@ def cpu_sample(w, flow, u0, iters_per_step, imm=None):
                       "iterations per step"}
 
 
+def run_ensemble(a, w, rank, world):
+    """Ensemble trajectory-steps/s: all members in lockstep (one stream per
+    trajectory, one host synchronisation per corrector round) against the
+    same members stepped one after another."""
+    import torch
+
+    from dnsjax_b200 import _lib, driver
+    from dnsjax_b200.ensemble import Ensemble
+    from dnsjax_b200.flows.monochromatic import TriplyPeriodicFlow
+    from dnsjax_b200.replicas import max_over_ranks, total_steps
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    members = ensemble_members(w)
+    flows = [TriplyPeriodicFlow(params_for(m), ly=m["ly"]) for m in members]
+    u0s = [initial_state(m, m["seed"] + 1000 * rank) for m in members]
+    n = len(members)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    ens = Ensemble(flows, [torch.as_tensor(u, device="cuda") for u in u0s])
+    for _ in range(a.warmup):
+        ens.step()
+    iters = []
+    n0 = _lib.launch_count()
+    barrier()
+    with ClockSampler(local) as clk:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(a.steps):
+            iters.append(ens.step().corrector_iterations)
+        t1.record()
+        barrier()
+    launches = _lib.launch_count() - n0
+    ms = max_over_ranks(t0.elapsed_time(t1), dist, "cuda")
+
+    # The same members stepped one after another (the per-trajectory driver).
+    seq = [torch.as_tensor(u, device="cuda") for u in u0s]
+    steppers = [f.make_stepper() for f in flows]
+    for i in range(n):
+        for _ in range(a.warmup):
+            seq[i], _, _ = driver.step(flows[i], steppers[i], seq[i], members[i]["tol"],
+                                       members[i]["max_iter"])
+    barrier()
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for i in range(n):
+        for _ in range(a.steps):
+            seq[i], _, _ = driver.step(flows[i], steppers[i], seq[i], members[i]["tol"],
+                                       members[i]["max_iter"])
+    s1.record()
+    barrier()
+    ms_seq = max_over_ranks(s0.elapsed_time(s1), dist, "cuda")
+    # lockstep and sequential trajectories agree (same steps from the same fields)
+    agree = max(float((torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y)).item())
+                for x, y in zip(ens.states, seq))
+
+    # End to end: every member's state from pinned host memory each step and back.
+    host = [torch.empty(tuple(x.shape), dtype=x.dtype, pin_memory=True) for x in ens.states]
+    for h, x in zip(host, ens.states):
+        h.copy_(x)
+    bytes_state = sum(x.numel() * x.element_size() for x in ens.states)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        ens.states = [h.to("cuda", non_blocking=True) for h in host]
+        ens.step()
+        for h, x in zip(host, ens.states):
+            h.copy_(x, non_blocking=True)
+    e1.record()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+
+    steps_total = total_steps(a.steps, world) * n
+    value = steps_total / (ms * 1e-3)
+    # Aggregate roofline: algorithmic bytes of every RHS + corrector call.
+    byts = 0.0
+    for per_step in iters:
+        for m, c in zip(members, per_step):
+            ob = op_bytes(m)
+            byts += (2 + c) * (ob["rhs"] + ob["correct"])
+    peaks = measured_peaks()
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    achieved = byts / (ms * 1e-3) / 1e9
+    out = {
+        "metric": "trajectory-steps/s, 96-member Kolmogorov ensemble (32^3/48^3/64^3)",
+        "value": value,
+        "unit": "trajectory-steps/s",
+        "n_gpus": world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": ms / a.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded divergence-free spectral fields)",
+        "config": {
+            "workload": a.workload, "form": "plain-fp64, lockstep ensemble",
+            "members": n, "sizes": list(w["sizes"]), "re_range": list(w["re_range"]),
+            "sequential_trajectory_steps_per_s": n * a.steps / (ms_seq * 1e-3),
+            "speedup_vs_sequential": ms_seq / ms,
+            "lockstep_vs_sequential_rel_l2": agree,
+            "corrector_iterations_per_step": sum(sum(x) for x in iters) / (n * len(iters)),
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": "working set of the 96 members > 126 MB L2",
+        },
+        "roofline": {
+            "bound": "hbm", "kernel": "all step kernels of the ensemble (aggregate)",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "peak_source": "measured" if peaks else "fallback",
+            "algorithmic_bytes_per_launch": byts / len(iters), "avg_launch_ms": ms / a.steps,
+        },
+        "e2e": {"value": steps_total / (e2e_ms * 1e-3), "unit": "trajectory-steps/s",
+                "h2d_bytes_per_step": bytes_state, "d2h_bytes_per_step": bytes_state},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not a.no_cpu_baseline:
+        out["cpu_baseline"] = ensemble_cpu_sample(w)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def ensemble_cpu_sample(w):
+    """Oracle on one host core: one step of one member of each size (3
+    corrector iterations each, the plain method's count), as trajectory-steps/s
+    of the size mix."""
+    members = ensemble_members(w)
+    per = w["per_size"]
+    total = 0.0
+    parts = []
+    for si in range(len(w["sizes"])):
+        m = members[si * per]
+        u0 = initial_state(m, m["seed"])
+        r = cpu_sample(m, None, u0, PLAIN_ITERS_PER_STEP["kolmogorov32"])
+        total += 1.0 / r["value"]
+        parts.append(f"{m['nx']}^3 {1.0 / r['value']:.2f} s")
+    return {"value": len(w["sizes"]) / total, "unit": "trajectory-steps/s", "cores": 1,
+            "kind": "port",
+            "sample": "one step (1 RHS + 1 corrector, x(2 + 3)) of one member per size: "
+                      + ", ".join(parts)}
+
+
 def run_reference(a, w, rank, world):
     """The oracle port of the reference's CPU path, on the host cores."""
     if rank != 0:
+        return
+    if w["system"] == "ensemble":
+        cb = ensemble_cpu_sample(w)
+        print(json.dumps({
+            "metric": "trajectory-steps/s, 96-member Kolmogorov ensemble (32^3/48^3/64^3)",
+            "value": cb["value"], "unit": cb["unit"], "n_gpus": world, "steps": 1,
+            "warmup": 0, "ms_per_step": 1e3 / cb["value"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded divergence-free spectral fields)", "impl": "reference",
+            "config": {"workload": a.workload, "form": "plain-fp64"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
         return
     import numpy as np
 
@@ -532,6 +730,8 @@ def main():
     w = WORKLOADS[a.workload]
     if a.impl == "reference":
         run_reference(a, w, rank, world)
+    elif w["system"] == "ensemble":
+        run_ensemble(a, w, rank, world)
     else:
         run_ours(a, w, rank, world)
 
