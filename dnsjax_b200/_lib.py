@@ -71,6 +71,11 @@ SIGNATURES = {
     "dnsb_periodic_norm": (c_int, [c_void_p] * 4),
     "dnsb_periodic_correct_velocity": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "dnsb_periodic_energy_sums": (c_int, [c_void_p] * 4),
+    "dnsb_periodic_step_graph_create": (c_int, [c_void_p, c_void_p, c_double, c_int, c_int,
+                                                C.POINTER(c_void_p)]),
+    "dnsb_step_graph_launch": (c_int, [c_void_p, c_void_p]),
+    "dnsb_step_graph_status": (c_int, [c_void_p, P_int, P_double, c_void_p]),
+    "dnsb_step_graph_destroy": (c_int, [c_void_p]),
     "dnsb_periodic_spec_to_phys": (c_int, [c_void_p] * 4),
     "dnsb_periodic_phys_to_spec": (c_int, [c_void_p] * 4),
     "dnsb_couette_create": (c_int, [C.POINTER(CouetteDesc), C.POINTER(c_void_p)]),

@@ -371,6 +371,146 @@ extern "C" int dnsb_periodic_correct_velocity(dnsb_periodic* p, const void* v,
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// One full time step of a periodic context as a CUDA graph: predictor and
+// first correction, the corrector iterations as a device-controlled WHILE
+// node (the reference driver's loop, __main__.py:163-180: iterate while
+// error > tol and iterations < max_iter), then correct_velocity into the
+// state.  Fixed buffers: the state (in / out) and the graph's own
+// prediction, two RHS buffers and control words.
+// ---------------------------------------------------------------------------
+namespace dnsb {
+__global__ void step_ctl_kernel(cudaGraphConditionalHandle h, const double* err, int* ctl,
+                                double* err_last, double tol, int max_iter, int first) {
+  const int it = first ? 0 : ctl[0] + 1;
+  const double e = err[0];
+  ctl[0] = it;
+  err_last[0] = e;
+  cudaGraphSetConditional(h, (e > tol && it < max_iter) ? 1u : 0u);
+}
+}  // namespace dnsb
+
+struct dnsb_step_graph {
+  cudaGraphExec_t exec = nullptr;
+  long long k_fixed = 0, k_iter = 0;  // kernels per step outside / per corrector iteration
+  double2 *P = nullptr, *Ra = nullptr, *Rb = nullptr;
+  double* err = nullptr;  // [0] corrector error, [1] error of the last step
+  int* ctl = nullptr;     // corrector iterations of the last step
+};
+
+static void step_graph_free(dnsb_step_graph* g) {
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  void* ptrs[] = {g->P, g->Ra, g->Rb, g->err, g->ctl};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  delete g;
+}
+
+extern "C" int dnsb_periodic_step_graph_create(dnsb_periodic* p, void* state, double tol,
+                                               int max_iter, int divergence,
+                                               dnsb_step_graph** out) {
+  if (!p || !state || !out) return fail(DNSB_ERR_ARG, "null argument");
+  auto* g = new dnsb_step_graph();
+  const size_t n = 3 * (size_t)p->S;
+  if (cudaMalloc(&g->P, n * sizeof(double2)) || cudaMalloc(&g->Ra, n * sizeof(double2)) ||
+      cudaMalloc(&g->Rb, n * sizeof(double2)) || cudaMalloc(&g->err, 2 * sizeof(double)) ||
+      cudaMalloc(&g->ctl, sizeof(int))) {
+    step_graph_free(g);
+    return fail(DNSB_ERR_CUDA, "step graph allocation failed");
+  }
+  cudaStream_t s = nullptr, sb = nullptr;
+  cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  cudaStreamCreateWithFlags(&sb, cudaStreamNonBlocking);
+  int rc = 0;
+  auto ck = [&](cudaError_t e, const char* what) {
+    if (e != cudaSuccess && !rc) rc = fail(DNSB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  };
+  cudaGraph_t graph = nullptr;
+  ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+  cudaStreamCaptureStatus cs;
+  ck(cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, nullptr, nullptr), "capture info");
+  cudaGraphConditionalHandle h = 0;
+  ck(cudaGraphConditionalHandleCreate(&h, graph, 0, 0), "conditional handle");
+  // Captured calls count their launches; the graph's kernels are counted
+  // when they run (dnsb_step_graph_status), so the capture's count is undone.
+  const long long c0 = g_launches.load();
+  if (!rc) rc = dnsb_periodic_rhs(p, state, g->Ra, s);
+  if (!rc) rc = dnsb_periodic_predict(p, state, g->Ra, g->P, s);
+  if (!rc) rc = dnsb_periodic_rhs(p, g->P, g->Rb, s);
+  if (!rc) rc = dnsb_periodic_correct(p, g->P, g->Ra, g->Rb, g->P, nullptr, g->err, s);
+  dnsb::step_ctl_kernel<<<1, 1, 0, s>>>(h, g->err, g->ctl, g->err + 1, tol, max_iter, 1);
+  ck(cudaGetLastError(), "control kernel");
+  const long long c1 = g_launches.load() + 1;  // + the control kernel
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  ck(cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &ndeps), "capture info");
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t wn = nullptr;
+  if (!rc) ck(cudaGraphAddNode(&wn, graph, deps, ndeps, &cp), "while node");
+  if (!rc) {
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    ck(cudaStreamUpdateCaptureDependencies(s, &wn, 1, cudaStreamSetCaptureDependencies),
+       "capture dependencies");
+    ck(cudaStreamBeginCaptureToGraph(sb, body, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal), "body capture");
+    // one corrector iteration: rhs_next -> Ra, rhs_prev = Rb, then Ra -> Rb
+    if (!rc) rc = dnsb_periodic_rhs(p, g->P, g->Ra, sb);
+    if (!rc) rc = dnsb_periodic_correct(p, g->P, g->Rb, g->Ra, g->P, nullptr, g->err, sb);
+    ck(cudaMemcpyAsync(g->Rb, g->Ra, n * sizeof(double2), cudaMemcpyDeviceToDevice, sb),
+       "rhs copy");
+    dnsb::step_ctl_kernel<<<1, 1, 0, sb>>>(h, g->err, g->ctl, g->err + 1, tol, max_iter, 0);
+    ck(cudaGetLastError(), "control kernel");
+    cudaGraph_t bout = nullptr;
+    ck(cudaStreamEndCapture(sb, &bout), "end body capture");
+  }
+  const long long c2 = g_launches.load() + 1;  // + the body's control kernel
+  if (!rc) rc = dnsb_periodic_correct_velocity(p, g->P, state, divergence, s);
+  const long long c3 = g_launches.load();
+  g->k_iter = (c2 - c1) + 1;                    // body launches + its control kernel
+  g->k_fixed = (c1 - c0) + (c3 - c2 + 1);       // prologue (+ control) + epilogue
+  g_launches.fetch_sub(c3 - c0, std::memory_order_relaxed);
+  cudaGraph_t done = nullptr;
+  cudaError_t ee = cudaStreamEndCapture(s, &done);  // always end the capture
+  ck(ee, "end capture");
+  if (!rc) ck(cudaGraphInstantiate(&g->exec, done, 0), "instantiate");
+  if (done) cudaGraphDestroy(done);
+  cudaStreamDestroy(s);
+  cudaStreamDestroy(sb);
+  if (rc) {
+    step_graph_free(g);
+    return rc;
+  }
+  *out = g;
+  return 0;
+}
+
+extern "C" int dnsb_step_graph_launch(dnsb_step_graph* g, void* stream) {
+  if (!g) return fail(DNSB_ERR_ARG, "null argument");
+  DNSB_CUDA(cudaGraphLaunch(g->exec, as_stream(stream)));
+  return 0;
+}
+
+extern "C" int dnsb_step_graph_status(dnsb_step_graph* g, int* iters, double* err,
+                                      void* stream) {
+  if (!g || !iters || !err) return fail(DNSB_ERR_ARG, "null argument");
+  cudaStream_t st = as_stream(stream);
+  DNSB_CUDA(cudaMemcpyAsync(iters, g->ctl, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DNSB_CUDA(cudaMemcpyAsync(err, g->err + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+  DNSB_CUDA(cudaStreamSynchronize(st));
+  g_launches.fetch_add(g->k_fixed + (long long)*iters * g->k_iter, std::memory_order_relaxed);
+  return 0;
+}
+
+extern "C" int dnsb_step_graph_destroy(dnsb_step_graph* g) {
+  if (!g) return fail(DNSB_ERR_ARG, "null argument");
+  step_graph_free(g);
+  return 0;
+}
+
 extern "C" int dnsb_periodic_energy_sums(dnsb_periodic* p, const void* v,
                                          double* out_dev, void* stream) {
   if (!p || !v || !out_dev) return fail(DNSB_ERR_ARG, "null argument");

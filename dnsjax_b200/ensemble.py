@@ -24,22 +24,50 @@ class EnsembleStep:
 
 
 class Ensemble:
-    def __init__(self, flows, states, tol=None, max_iter=None):
+    """graphs=True (periodic flows): every trajectory's step is one CUDA graph
+    launch (predictor, device-controlled corrector loop, correct_velocity;
+    see StepGraph), and the host synchronises once per ensemble step to read
+    every trajectory's iterations and error."""
+
+    def __init__(self, flows, states, tol=None, max_iter=None, graphs=False):
         import torch
 
         if len(flows) != len(states):
             raise ValueError("one state per flow")
         self.flows = list(flows)
-        self.states = list(states)
+        self.states = [s.contiguous() for s in states]
         self.tol = [f.params.step.corrector_tolerance if tol is None else tol
                     for f in self.flows]
         self.max_iter = [f.params.step.max_corrector_iterations if max_iter is None
                          else max_iter for f in self.flows]
         self.steppers = [f.make_stepper() for f in self.flows]
         self.streams = [torch.cuda.Stream() for _ in self.flows]
+        self.graphs = ([f.make_step_graph(s, tol=t, max_iter=m) for f, s, t, m in
+                        zip(self.flows, self.states, self.tol, self.max_iter)]
+                       if graphs else None)
+
+    def _graph_step(self) -> EnsembleStep:
+        import torch
+
+        ready = torch.cuda.current_stream().record_event()
+        for g, st in zip(self.graphs, self.streams):
+            st.wait_event(ready)
+            g.launch(st)
+        for st in self.streams:
+            torch.cuda.current_stream().wait_stream(st)
+        torch.cuda.synchronize()
+        res = EnsembleStep()
+        for g, st in zip(self.graphs, self.streams):
+            it, e = g.status(st)
+            res.corrector_iterations.append(it)
+            res.errors.append(e)
+        return res
 
     def step(self) -> EnsembleStep:
         import torch
+
+        if self.graphs is not None:
+            return self._graph_step()
 
         n = len(self.flows)
         prev = list(self.states)

@@ -96,6 +96,26 @@ int dnsb_periodic_norm(dnsb_periodic* ctx, const void* v, double* out_dev,
  * (monochromatic.py:516-565).  out may alias v. */
 int dnsb_periodic_correct_velocity(dnsb_periodic* ctx, const void* v,
                                    void* out, int divergence, void* stream);
+/* One full time step as a CUDA graph, for callers that step without host
+ * synchronisation (the reference driver's step, __main__.py:125-203, with its
+ * corrector loop -- iterate while error > tol and iterations < max_iter,
+ * :163-180 -- as a device-controlled conditional node): predictor and first
+ * correction from `state`, corrector iterations, correct_velocity (with
+ * `divergence`) back into `state`.  The graph is bound to `state` (updated in
+ * place by every launch) and owns its prediction, RHS and control buffers;
+ * creation captures the context's launches and allocates, launching does
+ * neither. */
+typedef struct dnsb_step_graph dnsb_step_graph;
+int dnsb_periodic_step_graph_create(dnsb_periodic* ctx, void* state, double tol,
+                                    int max_iter, int divergence,
+                                    dnsb_step_graph** out);
+int dnsb_step_graph_launch(dnsb_step_graph* g, void* stream);
+/* Corrector iterations and final corrector error of the last launched step
+ * (host values; synchronises `stream`). */
+int dnsb_step_graph_status(dnsb_step_graph* g, int* iters, double* err,
+                           void* stream);
+int dnsb_step_graph_destroy(dnsb_step_graph* g);
+
 /* out_dev[0] = sum k_metric |v|^2, out_dev[1] = sum -lapl |v|^2 (the two
  * reductions of monochromatic.py:433-466). */
 int dnsb_periodic_energy_sums(dnsb_periodic* ctx, const void* v,

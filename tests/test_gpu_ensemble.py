@@ -1,7 +1,8 @@
-"""Lockstep ensembles: trajectories of different sizes advanced together
-(one stream each, one host synchronisation per corrector round) give exactly
-the states and corrector-iteration counts of the same trajectories stepped
-one after another."""
+"""Lockstep ensembles and step graphs: trajectories of different sizes
+advanced together (one stream each, one host synchronisation per corrector
+round, or one CUDA graph per step with the corrector loop on the device)
+give exactly the states and corrector-iteration counts of the same
+trajectories stepped one after another by the host-driven loop."""
 
 from math import pi
 
@@ -41,4 +42,50 @@ def test_lockstep_equals_sequential():
             s, c, e = driver.step(f, st, s, f.params.step.corrector_tolerance,
                                   f.params.step.max_corrector_iterations)
             assert c == lock_iters[k][i]
+        assert torch.equal(s, ens.states[i]), i
+
+
+def test_step_graph_equals_driver():
+    import torch
+
+    from dnsjax_b200 import driver
+
+    f, u = member(32, 40.0, 5)
+    s_eager = torch.as_tensor(u, device="cuda")
+    s_graph = torch.as_tensor(u, device="cuda")
+    g = f.make_step_graph(s_graph)
+    st = f.make_stepper()
+    for _ in range(3):
+        s_eager, c, e = driver.step(f, st, s_eager, f.params.step.corrector_tolerance,
+                                    f.params.step.max_corrector_iterations)
+        g.launch()
+        it, err = g.status()
+        assert it == c and err == e
+    assert torch.equal(s_eager, s_graph)
+    # a corrector cap below the needed count ends the loop at the cap
+    f2, u2 = member(32, 40.0, 5)
+    s2 = torch.as_tensor(u2, device="cuda")
+    g2 = f2.make_step_graph(s2, max_iter=1)
+    g2.launch()
+    assert g2.status()[0] == 1
+
+
+def test_graph_ensemble_equals_sequential():
+    import torch
+
+    from dnsjax_b200 import driver
+    from dnsjax_b200.ensemble import Ensemble
+
+    spec = [(32, 35.0, 0), (48, 60.0, 1), (64, 42.0, 3)]
+    built = [member(*s) for s in spec]
+    ens = Ensemble([f for f, _ in built], [torch.as_tensor(u, device="cuda") for _, u in built],
+                   graphs=True)
+    its = [ens.step().corrector_iterations for _ in range(3)]
+    for i, (f, u) in enumerate(built):
+        st = f.make_stepper()
+        s = torch.as_tensor(u, device="cuda")
+        for k in range(3):
+            s, c, e = driver.step(f, st, s, f.params.step.corrector_tolerance,
+                                  f.params.step.max_corrector_iterations)
+            assert c == its[k][i]
         assert torch.equal(s, ens.states[i]), i
