@@ -317,10 +317,13 @@ def run_ours(a, w, rank, world):
 
     iters = []
     errs = []
+    snap = state.clone()  # start of the timed segment, for the graph pass
+    # Eager pass: the host-driven reference loop, every RHS and corrector
+    # call bracketed by CUDA events (the per-op durations of the roofline).
     tf.on = True
     n0 = _lib.launch_count()
     barrier()
-    with ClockSampler(local) as clk:
+    with ClockSampler(local) as clk_eager:
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record()
@@ -330,10 +333,45 @@ def run_ours(a, w, rank, world):
             errs.append(e)
         t1.record()
         barrier()
-    launches = _lib.launch_count() - n0
+    eager_launches = _lib.launch_count() - n0
     tf.on = False
-    ms = max_over_ranks(t0.elapsed_time(t1), dist, "cuda")
+    eager_ms = max_over_ranks(t0.elapsed_time(t1), dist, "cuda")
+    ms, launches, clk = eager_ms, eager_launches, clk_eager
+    last_err = errs[-1]
 
+    graph = None
+    graph_check = None
+    if a.driver == "graph":
+        # Headline pass: every step is one step-graph launch (predictor,
+        # corrector loop on the device, correct_velocity) over the same K
+        # steps the eager pass took (from the same state); the host reads
+        # iterations and error per step.
+        gstate = snap.clone()
+        graph = flow.make_step_graph(gstate, tol=tol, max_iter=mi)
+        for _ in range(a.warmup):
+            graph.launch()
+            graph.status()
+        gstate.copy_(snap)
+        g_iters = []
+        n0 = _lib.launch_count()
+        barrier()
+        with ClockSampler(local) as clk:
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record()
+            for _ in range(a.steps):
+                graph.launch()
+                c, e = graph.status()
+                g_iters.append(c)
+            t1.record()
+            barrier()
+        launches = _lib.launch_count() - n0
+        ms = max_over_ranks(t0.elapsed_time(t1), dist, "cuda")
+        graph_check = {"same_iterations": g_iters == iters,
+                       "bitwise_equal_state": bool(torch.equal(gstate, state))}
+        last_err = e
+
+    traj_steps = a.warmup + a.steps  # the eager trajectory, for the mixed-form check
     # End to end through the public API: pinned host state in, new state out.
     host_in = torch.empty(state.shape, dtype=state.dtype, pin_memory=True)
     host_in.copy_(torch.as_tensor(u0))
@@ -343,13 +381,21 @@ def run_ours(a, w, rank, world):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(a.steps):
-        d_state = host_in.to("cuda", non_blocking=True)
-        d_state, c, e = driver.step(tf, steppers, d_state, tol, mi)
-        host_out.copy_(d_state, non_blocking=True)
+        if graph is not None:
+            gstate.copy_(host_in, non_blocking=True)  # the graph's bound state
+            graph.launch()
+            graph.status()
+            host_out.copy_(gstate, non_blocking=True)
+        else:
+            d_state = host_in.to("cuda", non_blocking=True)
+            d_state, c, e = driver.step(tf, steppers, d_state, tol, mi)
+            host_out.copy_(d_state, non_blocking=True)
         host_in, host_out = host_out, host_in
     e1.record()
     barrier()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+    if graph is not None:
+        graph.close()
     state_bytes = state.numel() * state.element_size()
 
     # Roofline of the dominant op (events inside the timed region).
@@ -382,18 +428,27 @@ def run_ours(a, w, rank, world):
         "config": {
             "workload": a.workload,
             "form": "mixed: FP32 RHS passes, FP64 state/IMM/norms" if mixed else "plain-fp64",
+            "driver": ("step graph per time step (corrector loop as a device-controlled "
+                       "conditional node)" if graph is not None else
+                       "host-driven reference loop"),
+            "eager_driver": {"steps_per_s": total_steps(a.steps, world) / (eager_ms * 1e-3),
+                             "gpu_launches": eager_launches,
+                             "note": "the same K steps from the same state through the "
+                                     "host-driven loop; per-op events of this pass give "
+                                     "op_ms and the roofline"},
+            "graph_vs_eager": graph_check,
             "grid": [w["nx"], w["ny"], w["nz"]],
             "fd_order": w.get("p"),
             "re": w["re"], "dt": w["dt"], "tol": tol,
             "max_corrector_iterations": w["max_iter"],
             "corrector_iterations_per_step": sum(iters) / len(iters),
-            "last_error": errs[-1],
+            "last_error": last_err,
             "grid_points_steps_per_s": value * grid_points(w),
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "l2": "working set (state, operators, workspace) > 126 MB L2",
             "op_ms": {"rhs": sum(rhs_ms) / max(1, len(rhs_ms)),
                       "imm_or_correct": sum(imm_ms) / max(1, len(imm_ms))},
-            "op_share": {k: v / ms for k, v in tot.items()},
+            "op_share": {k: v / eager_ms for k, v in tot.items()},
         },
         "roofline": {
             "bound": "hbm",
@@ -427,12 +482,12 @@ def run_ours(a, w, rank, world):
         plain = PlaneCouetteFlow(params_for(w, fp64=True))
         ps = plain.make_stepper()
         ref = torch.as_tensor(u0, device="cuda")
-        for _ in range(a.warmup + a.steps):
+        for _ in range(traj_steps):
             ref, _, _ = driver.step(plain, ps, ref, w["tol"], mi)
         ke_m = float(flow.norm(state).item()) ** 2 / 2
         ke_p = float(plain.norm(ref).item()) ** 2 / 2
         diff = torch.linalg.vector_norm(state - ref) / torch.linalg.vector_norm(ref)
-        out["config"]["vs_plain"] = {"steps": a.warmup + a.steps,
+        out["config"]["vs_plain"] = {"steps": traj_steps,
                                      "ke_rel_err": abs(ke_m - ke_p) / ke_p,
                                      "field_rel_l2": float(diff.item())}
         out["dtype"] = "f32 (RHS passes) + f64"
@@ -722,6 +777,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="couette128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--driver", default="graph", choices=["graph", "eager"],
+                    help="graph: one step graph launch per time step; eager: the "
+                         "host-driven predictor-corrector loop")
     ap.add_argument("--form", default="plain", choices=["plain", "mixed"],
                     help="mixed: FP32 RHS passes (plane Couette), FP64 elsewhere")
     ap.add_argument("--tol", type=float, default=None,

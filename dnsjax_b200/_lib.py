@@ -73,6 +73,8 @@ SIGNATURES = {
     "dnsb_periodic_energy_sums": (c_int, [c_void_p] * 4),
     "dnsb_periodic_step_graph_create": (c_int, [c_void_p, c_void_p, c_double, c_int, c_int,
                                                 C.POINTER(c_void_p)]),
+    "dnsb_couette_step_graph_create": (c_int, [c_void_p, c_void_p, c_double, c_int,
+                                               C.POINTER(c_void_p)]),
     "dnsb_step_graph_launch": (c_int, [c_void_p, c_void_p]),
     "dnsb_step_graph_status": (c_int, [c_void_p, P_int, P_double, c_void_p]),
     "dnsb_step_graph_destroy": (c_int, [c_void_p]),

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -406,24 +407,20 @@ static void step_graph_free(dnsb_step_graph* g) {
   delete g;
 }
 
-extern "C" int dnsb_periodic_step_graph_create(dnsb_periodic* p, void* state, double tol,
-                                               int max_iter, int divergence,
-                                               dnsb_step_graph** out) {
-  if (!p || !state || !out) return fail(DNSB_ERR_ARG, "null argument");
-  auto* g = new dnsb_step_graph();
-  const size_t n = 3 * (size_t)p->S;
-  if (cudaMalloc(&g->P, n * sizeof(double2)) || cudaMalloc(&g->Ra, n * sizeof(double2)) ||
-      cudaMalloc(&g->Rb, n * sizeof(double2)) || cudaMalloc(&g->err, 2 * sizeof(double)) ||
-      cudaMalloc(&g->ctl, sizeof(int))) {
-    step_graph_free(g);
-    return fail(DNSB_ERR_CUDA, "step graph allocation failed");
-  }
+// Captures prologue (predictor and first correction, error into g->err),
+// the corrector iteration `body` inside a WHILE node, and `epilogue`, with
+// the control kernel after the prologue and at the end of the body.
+static int build_step_graph(dnsb_step_graph* g, double tol, int max_iter,
+                            const std::function<int(cudaStream_t)>& prologue,
+                            const std::function<int(cudaStream_t)>& body,
+                            const std::function<int(cudaStream_t)>& epilogue) {
   cudaStream_t s = nullptr, sb = nullptr;
   cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
   cudaStreamCreateWithFlags(&sb, cudaStreamNonBlocking);
   int rc = 0;
   auto ck = [&](cudaError_t e, const char* what) {
-    if (e != cudaSuccess && !rc) rc = fail(DNSB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    if (e != cudaSuccess && !rc)
+      rc = fail(DNSB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
   };
   cudaGraph_t graph = nullptr;
   ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
@@ -434,10 +431,7 @@ extern "C" int dnsb_periodic_step_graph_create(dnsb_periodic* p, void* state, do
   // Captured calls count their launches; the graph's kernels are counted
   // when they run (dnsb_step_graph_status), so the capture's count is undone.
   const long long c0 = g_launches.load();
-  if (!rc) rc = dnsb_periodic_rhs(p, state, g->Ra, s);
-  if (!rc) rc = dnsb_periodic_predict(p, state, g->Ra, g->P, s);
-  if (!rc) rc = dnsb_periodic_rhs(p, g->P, g->Rb, s);
-  if (!rc) rc = dnsb_periodic_correct(p, g->P, g->Ra, g->Rb, g->P, nullptr, g->err, s);
+  if (!rc) rc = prologue(s);
   dnsb::step_ctl_kernel<<<1, 1, 0, s>>>(h, g->err, g->ctl, g->err + 1, tol, max_iter, 1);
   ck(cudaGetLastError(), "control kernel");
   const long long c1 = g_launches.load() + 1;  // + the control kernel
@@ -452,34 +446,70 @@ extern "C" int dnsb_periodic_step_graph_create(dnsb_periodic* p, void* state, do
   cudaGraphNode_t wn = nullptr;
   if (!rc) ck(cudaGraphAddNode(&wn, graph, deps, ndeps, &cp), "while node");
   if (!rc) {
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    cudaGraph_t bg = cp.conditional.phGraph_out[0];
     ck(cudaStreamUpdateCaptureDependencies(s, &wn, 1, cudaStreamSetCaptureDependencies),
        "capture dependencies");
-    ck(cudaStreamBeginCaptureToGraph(sb, body, nullptr, nullptr, 0,
+    ck(cudaStreamBeginCaptureToGraph(sb, bg, nullptr, nullptr, 0,
                                      cudaStreamCaptureModeThreadLocal), "body capture");
-    // one corrector iteration: rhs_next -> Ra, rhs_prev = Rb, then Ra -> Rb
-    if (!rc) rc = dnsb_periodic_rhs(p, g->P, g->Ra, sb);
-    if (!rc) rc = dnsb_periodic_correct(p, g->P, g->Rb, g->Ra, g->P, nullptr, g->err, sb);
-    ck(cudaMemcpyAsync(g->Rb, g->Ra, n * sizeof(double2), cudaMemcpyDeviceToDevice, sb),
-       "rhs copy");
+    if (!rc) rc = body(sb);
     dnsb::step_ctl_kernel<<<1, 1, 0, sb>>>(h, g->err, g->ctl, g->err + 1, tol, max_iter, 0);
     ck(cudaGetLastError(), "control kernel");
     cudaGraph_t bout = nullptr;
     ck(cudaStreamEndCapture(sb, &bout), "end body capture");
   }
   const long long c2 = g_launches.load() + 1;  // + the body's control kernel
-  if (!rc) rc = dnsb_periodic_correct_velocity(p, g->P, state, divergence, s);
+  if (!rc) rc = epilogue(s);
   const long long c3 = g_launches.load();
-  g->k_iter = (c2 - c1) + 1;                    // body launches + its control kernel
-  g->k_fixed = (c1 - c0) + (c3 - c2 + 1);       // prologue (+ control) + epilogue
+  g->k_iter = (c2 - c1) + 1;                   // body launches + its control kernel
+  g->k_fixed = (c1 - c0) + (c3 - c2 + 1);      // prologue (+ control) + epilogue
   g_launches.fetch_sub(c3 - c0, std::memory_order_relaxed);
   cudaGraph_t done = nullptr;
-  cudaError_t ee = cudaStreamEndCapture(s, &done);  // always end the capture
-  ck(ee, "end capture");
+  ck(cudaStreamEndCapture(s, &done), "end capture");  // always end the capture
   if (!rc) ck(cudaGraphInstantiate(&g->exec, done, 0), "instantiate");
   if (done) cudaGraphDestroy(done);
   cudaStreamDestroy(s);
   cudaStreamDestroy(sb);
+  return rc;
+}
+
+static dnsb_step_graph* new_step_graph(size_t n) {
+  auto* g = new dnsb_step_graph();
+  if (cudaMalloc(&g->P, n * sizeof(double2)) || cudaMalloc(&g->Ra, n * sizeof(double2)) ||
+      cudaMalloc(&g->Rb, n * sizeof(double2)) || cudaMalloc(&g->err, 2 * sizeof(double)) ||
+      cudaMalloc(&g->ctl, sizeof(int))) {
+    step_graph_free(g);
+    return nullptr;
+  }
+  return g;
+}
+
+extern "C" int dnsb_periodic_step_graph_create(dnsb_periodic* p, void* state, double tol,
+                                               int max_iter, int divergence,
+                                               dnsb_step_graph** out) {
+  if (!p || !state || !out) return fail(DNSB_ERR_ARG, "null argument");
+  const size_t n = 3 * (size_t)p->S;
+  dnsb_step_graph* g = new_step_graph(n);
+  if (!g) return fail(DNSB_ERR_CUDA, "step graph allocation failed");
+  auto prologue = [&](cudaStream_t s) {
+    int rc = dnsb_periodic_rhs(p, state, g->Ra, s);
+    if (!rc) rc = dnsb_periodic_predict(p, state, g->Ra, g->P, s);
+    if (!rc) rc = dnsb_periodic_rhs(p, g->P, g->Rb, s);
+    if (!rc) rc = dnsb_periodic_correct(p, g->P, g->Ra, g->Rb, g->P, nullptr, g->err, s);
+    return rc;
+  };
+  // one corrector iteration: rhs_next -> Ra, rhs_prev = Rb, then Ra -> Rb
+  auto body = [&](cudaStream_t s) {
+    int rc = dnsb_periodic_rhs(p, g->P, g->Ra, s);
+    if (!rc) rc = dnsb_periodic_correct(p, g->P, g->Rb, g->Ra, g->P, nullptr, g->err, s);
+    if (!rc && cudaMemcpyAsync(g->Rb, g->Ra, n * sizeof(double2), cudaMemcpyDeviceToDevice,
+                               s) != cudaSuccess)
+      rc = fail(DNSB_ERR_CUDA, "rhs copy");
+    return rc;
+  };
+  auto epilogue = [&](cudaStream_t s) {
+    return dnsb_periodic_correct_velocity(p, g->P, state, divergence, s);
+  };
+  const int rc = build_step_graph(g, tol, max_iter, prologue, body, epilogue);
   if (rc) {
     step_graph_free(g);
     return rc;
@@ -1117,6 +1147,49 @@ extern "C" int dnsb_couette_phys_to_spec(dnsb_couette* p, const double* phys,
   zf.plan = p->pz;
   zf.tw = p->twz;
   DNSB_LAUNCH(launch_col_pass(zf, 3, p->NKX, st));
+  return 0;
+}
+
+// One full plane-Couette time step as a CUDA graph (see
+// dnsb_periodic_step_graph_create): the predictor is the influence-matrix
+// iteration with (u^n, u^n, N^n, N^n), each correction the iteration with
+// (u^n, u^j, N_prev, N^j) (plane_couette.py:507-540); correct_velocity is
+// the identity (:575-582), so the epilogue copies the converged iterate
+// into the state.
+extern "C" int dnsb_couette_step_graph_create(dnsb_couette* p, void* state, double tol,
+                                              int max_iter, dnsb_step_graph** out) {
+  if (!p || !state || !out) return fail(DNSB_ERR_ARG, "null argument");
+  if (!p->bound) return fail(DNSB_ERR_ARG, "IMM operators not bound");
+  const size_t n = 3 * (size_t)p->NM * p->Ny;
+  dnsb_step_graph* g = new_step_graph(n);
+  if (!g) return fail(DNSB_ERR_CUDA, "step graph allocation failed");
+  auto prologue = [&](cudaStream_t s) {
+    int rc = dnsb_couette_rhs(p, state, g->Ra, s);
+    if (!rc) rc = dnsb_couette_imm(p, state, state, g->Ra, g->Ra, g->P, nullptr, nullptr, s);
+    if (!rc) rc = dnsb_couette_rhs(p, g->P, g->Rb, s);
+    if (!rc) rc = dnsb_couette_imm(p, state, g->P, g->Ra, g->Rb, g->P, nullptr, g->err, s);
+    return rc;
+  };
+  auto body = [&](cudaStream_t s) {
+    int rc = dnsb_couette_rhs(p, g->P, g->Ra, s);
+    if (!rc) rc = dnsb_couette_imm(p, state, g->P, g->Rb, g->Ra, g->P, nullptr, g->err, s);
+    if (!rc && cudaMemcpyAsync(g->Rb, g->Ra, n * sizeof(double2), cudaMemcpyDeviceToDevice,
+                               s) != cudaSuccess)
+      rc = fail(DNSB_ERR_CUDA, "rhs copy");
+    return rc;
+  };
+  auto epilogue = [&](cudaStream_t s) {
+    if (cudaMemcpyAsync(state, g->P, n * sizeof(double2), cudaMemcpyDeviceToDevice, s) !=
+        cudaSuccess)
+      return fail(DNSB_ERR_CUDA, "state copy");
+    return 0;
+  };
+  const int rc = build_step_graph(g, tol, max_iter, prologue, body, epilogue);
+  if (rc) {
+    step_graph_free(g);
+    return rc;
+  }
+  *out = g;
   return 0;
 }
 

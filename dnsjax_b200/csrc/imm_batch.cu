@@ -5,20 +5,21 @@
 //
 //   stages 0-1   one warp per (kz, kx) mode: d_hat = div u^n, then f_hat
 //                (D1 / D2 along y from shared memory) -> F      [NM][Ny]
-//   L_k solve    one thread per (mode, real column): p_P = L_k^-1 f_hat,
-//                in place in F
+//   L_k solve    p_P = L_k^-1 f_hat in place in F: a CTA per 16 items, one
+//                warp per component, lane = side * 16 + item (side 1 is the
+//                mirror mode (nz-1-s, kx) of item (s, kx) when it shares the
+//                item's factors), each lane one complex column
 //   stage 3      one warp per mode: R = H_k^- u^n - grad p_P + c N_j +
 //                (1-c) N_n -> R                                  [3][NM][Ny]
-//   H_k solve    one thread per (mode, real column), in place in R
+//   H_k solve    as the L_k solve, three components, in place in R
 //   stages 4-6   one warp per mode: wall divergence, influence-matrix
 //                weights, u^{j+1}, the correction and its Simpson norm
 //
-// The LU factors are repacked once, when the operators are bound, into a
-// record-major layout with the item index fastest, so a warp of 32 items
-// reads each factor of a substitution step with one coalesced load:
-//   fac[(j * RS + slot) * NP + item],  slots [0, kl) L multipliers of rows
-//   j+1..j+kl, [kl] 1/U_jj, [kl+i] U_{j-i,j}/U_jj (i = 1..NU);
-//   piv[j * NP + item] = ipiv[j] - j (validated, 0..kl).
+// The LU factors are repacked once, when the operators are bound, into
+// 16-item tiles whose rows are contiguous (layout below), so a block of
+// substitution steps of one tile is one bulk copy into shared memory; the
+// substitution kernels stream those blocks through a ring of slots, each
+// lane fetching its own entering rows with cp.async.
 // An item is mode (s, kx) with s <= (nz-1)/2; when the factors of (s, kx)
 // and its mirror (nz-1-s, kx) are bit-identical (same k^2; checked at bind
 // time) the mirror reads the item's records, else every mode is an item.
@@ -53,14 +54,14 @@ __device__ __forceinline__ double2 band_row(const double2* x, const int* __restr
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// Bind time: repack one operator's factors into 32-item tiles, each tile's
+// Bind time: repack one operator's factors into 16-item tiles, each tile's
 // rows contiguous so a block of substitution steps is one contiguous copy:
-//   facL[tile][j][i/2][32][2]       (rows j < Ny, then W zero rows)  L
+//   facL[tile][j][i/2][16][2]       (rows j < Ny, then W zero rows)  L
 //                                   multipliers of rows j+1..j+kl
-//   facU[tile][j + WB][i/2][32][2]  (WB zero rows first; NUP = NU+1 rounded
+//   facU[tile][j + WB][i/2][16][2]  (WB zero rows first; NUP = NU+1 rounded
 //                                   up to even) i = 0: 1/U_jj, i > 0:
 //                                   U_{j-i,j} / U_jj
-//   dp[tile][j][32]            ipiv[j] - j, validated (a bad pivot is flagged
+//   dp[tile][j][16]            ipiv[j] - j, validated (a bad pivot is flagged
 //                              and replaced by 0)
 // Item p is mode p (modes (s, kx) with s <= (nz-1)/2 when mirrors share
 // factors).  The arrays must be zeroed before the call (padding rows and

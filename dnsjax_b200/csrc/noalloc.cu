@@ -2,8 +2,7 @@
 //
 // Some callers cannot allocate device memory: a JAX/XLA FFI handler runs
 // inside memory that XLA's allocator already owns (a cudaMalloc there can
-// fail or stall the runtime), and code recorded into a CUDA graph by stream
-// capture may not call cudaMalloc at all.  Such callers also cannot create a
+// fail or stall the runtime).  Such callers also cannot create a
 // dnsb_couette context (creation allocates its workspace).  This entry
 // point computes the same quantity as dnsb_couette_norm -- the reference's
 // sqrt(Simpson_y(sum conj(v) k_metric v) / ly) -- from the caller's field
@@ -22,8 +21,7 @@
 //     never used.
 //   * host code cannot use the array's name as a device address; the first
 //     call on each device looks the address up with cudaGetSymbolAddress
-//     (with that device current) and caches it, so make the first call on a
-//     device before any stream capture.
+//     (with that device current) and caches it.
 #include <mutex>
 #include <string>
 

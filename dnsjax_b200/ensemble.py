@@ -24,9 +24,9 @@ class EnsembleStep:
 
 
 class Ensemble:
-    """graphs=True (periodic flows): every trajectory's step is one CUDA graph
+    """graphs=True: every trajectory's step is one CUDA graph
     launch (predictor, device-controlled corrector loop, correct_velocity;
-    see StepGraph), and the host synchronises once per ensemble step to read
+    see timestep.StepGraph), and the host synchronises once per ensemble step to read
     every trajectory's iterations and error."""
 
     def __init__(self, flows, states, tol=None, max_iter=None, graphs=False):

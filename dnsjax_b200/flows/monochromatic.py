@@ -18,7 +18,7 @@ import numpy as np
 from .. import _lib
 from ..geometries.triply_periodic import Fourier
 from ..parameters import Parameters, derive, monochromatic_systems, padded_sizes
-from ..timestep import make_fused_stepper, make_stepper
+from ..timestep import StepGraph, make_fused_stepper, make_stepper
 
 
 class TriplyPeriodicFlow:
@@ -204,9 +204,10 @@ class TriplyPeriodicFlow:
         if divergence is None:
             dbg = self.params.debug
             divergence = True if dbg is None else dbg.correct_divergence
-        return StepGraph(self, state, st.corrector_tolerance if tol is None else tol,
-                         st.max_corrector_iterations if max_iter is None else max_iter,
-                         divergence)
+        tol = st.corrector_tolerance if tol is None else tol
+        max_iter = st.max_corrector_iterations if max_iter is None else max_iter
+        return StepGraph(self._L, state, lambda h: self._L.dnsb_periodic_step_graph_create(
+            self._ctx, self._check(state), float(tol), int(max_iter), int(divergence), h))
 
     def get_stats(self, state) -> dict:
         """E, I, D, E' (monochromatic.py:433-505)."""
@@ -281,41 +282,6 @@ def _flow() -> TriplyPeriodicFlow:
         flow = TriplyPeriodicFlow(params, ly=derived_params.ly)
         _steppers = flow.make_stepper(fused=True)
     return flow
-
-
-class StepGraph:
-    """One full time step (predictor, device-controlled corrector loop,
-    correct_velocity) captured as a CUDA graph on the flow's context; every
-    launch advances the bound state in place without host synchronisation.
-    status() returns the corrector iterations and error of the last step."""
-
-    def __init__(self, flow, state, tol, max_iter, divergence):
-        self._flow, self.state = flow, state
-        h = _lib.C.c_void_p()
-        _lib.check(flow._L.dnsb_periodic_step_graph_create(
-            flow._ctx, flow._check(state), float(tol), int(max_iter), int(divergence),
-            _lib.C.byref(h)))
-        self._h = h
-
-    def launch(self, stream=None):
-        _lib.check(self._flow._L.dnsb_step_graph_launch(self._h, _lib.stream_handle(stream)))
-
-    def status(self, stream=None):
-        it, err = _lib.C.c_int(), _lib.C.c_double()
-        _lib.check(self._flow._L.dnsb_step_graph_status(
-            self._h, _lib.C.byref(it), _lib.C.byref(err), _lib.stream_handle(stream)))
-        return it.value, err.value
-
-    def close(self):
-        if getattr(self, "_h", None):
-            self._flow._L.dnsb_step_graph_destroy(self._h)
-            self._h = None
-
-    def __del__(self):
-        try:
-            self.close()
-        except Exception:
-            pass
 
 
 def predict_and_correct(state):

@@ -23,7 +23,7 @@ from .. import _lib
 from ..fd import build_diff_matrices, cgl_grid, diff_bands
 from ..geometries.cartesian import Fourier, precompute_imm, simpson_weights
 from ..parameters import Parameters, derive, padded_sizes
-from ..timestep import make_fused_stepper, make_stepper
+from ..timestep import StepGraph, make_fused_stepper, make_stepper
 
 
 class PlaneCouetteFlow:
@@ -165,6 +165,16 @@ class PlaneCouetteFlow:
     def correct_velocity(self, state):
         """plane_couette.py:575-582: pass-through."""
         return state, None
+
+    def make_step_graph(self, state, tol: float | None = None,
+                        max_iter: int | None = None):
+        """A CUDA graph of one full time step bound to `state` (updated in
+        place by every launch); see StepGraph."""
+        st = self.params.step
+        tol = st.corrector_tolerance if tol is None else tol
+        max_iter = st.max_corrector_iterations if max_iter is None else max_iter
+        return StepGraph(self._L, state, lambda h: self._L.dnsb_couette_step_graph_create(
+            self._ctx, self._check(state), float(tol), int(max_iter), h))
 
     def get_stats(self, state) -> dict:
         """plane_couette.py:591-613: E' = ||u||^2 / 2."""

@@ -65,3 +65,43 @@ def make_fused_stepper(flow):
         return prediction, rhs_next, err
 
     return predict_and_correct, iterate_correction
+
+
+class StepGraph:
+    """One full time step (predictor, device-controlled corrector loop,
+    correct_velocity) captured as a CUDA graph on a flow's context; every
+    launch advances the bound state in place without host synchronisation.
+    status() returns the corrector iterations and error of the last step.
+    ``create(handle_ref)`` is the flow's dnsb_*_step_graph_create call."""
+
+    def __init__(self, lib, state, create):
+        from . import _lib
+
+        self._L, self.state = lib, state
+        h = _lib.C.c_void_p()
+        _lib.check(create(_lib.C.byref(h)))
+        self._h = h
+
+    def launch(self, stream=None):
+        from . import _lib
+
+        _lib.check(self._L.dnsb_step_graph_launch(self._h, _lib.stream_handle(stream)))
+
+    def status(self, stream=None):
+        from . import _lib
+
+        it, err = _lib.C.c_int(), _lib.C.c_double()
+        _lib.check(self._L.dnsb_step_graph_status(
+            self._h, _lib.C.byref(it), _lib.C.byref(err), _lib.stream_handle(stream)))
+        return it.value, err.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.dnsb_step_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

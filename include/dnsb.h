@@ -206,10 +206,20 @@ int dnsb_couette_phys_to_spec(dnsb_couette* ctx, const double* phys,
  * kernel gave up (its results are then invalid), else 0. */
 int dnsb_couette_check(dnsb_couette* ctx, void* stream);
 
+/* One full plane-Couette time step as a CUDA graph, like
+ * dnsb_periodic_step_graph_create: predictor (the IMM iteration with
+ * (u^n, u^n, N^n, N^n), plane_couette.py:507-519), first correction, and
+ * corrector iterations (plane_couette.py:522-540) in a device-controlled
+ * loop while error > tol and iterations < max_iter (__main__.py:163-180);
+ * correct_velocity is the identity for this flow (plane_couette.py:575-582),
+ * so the converged iterate is copied back into `state`.  Needs bound IMM
+ * operators; launch/status/destroy through dnsb_step_graph_*. */
+int dnsb_couette_step_graph_create(dnsb_couette* ctx, void* state, double tol,
+                                   int max_iter, dnsb_step_graph** out);
+
 /* Allocation-free Couette norm (no counterpart in the reference; it exists
  * for callers that cannot allocate device memory, such as an XLA FFI handler
- * working inside memory its framework owns, or code recorded by CUDA stream
- * capture).  Computes what dnsb_couette_norm computes, from the field alone
+ * working inside memory its framework owns).  Computes what dnsb_couette_norm computes, from the field alone
  * (the CGL grid and its Simpson weights are generated in the kernel), with
  * the per-mode partial sums kept in a file-scope device array instead of
  * context workspace:
@@ -219,7 +229,7 @@ int dnsb_couette_check(dnsb_couette* ctx, void* stream);
  *   device that loads the library until exit; every call shares it, so calls
  *   that may overlap on the GPU race and must be ordered by the caller.  The
  *   first call on a device looks up the array's device address (with that
- *   device current); make it before any stream capture. */
+ *   device current) and caches it. */
 int dnsb_couette_norm_noalloc(const void* v, int nx, int ny, int nz, double ly,
                               double* out_dev, void* stream);
 

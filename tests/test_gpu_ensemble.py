@@ -2,7 +2,8 @@
 advanced together (one stream each, one host synchronisation per corrector
 round, or one CUDA graph per step with the corrector loop on the device)
 give exactly the states and corrector-iteration counts of the same
-trajectories stepped one after another by the host-driven loop."""
+trajectories stepped one after another by the host-driven loop.  Step graphs
+are checked for the triply periodic flows and for plane Couette."""
 
 from math import pi
 
@@ -85,6 +86,63 @@ def test_graph_ensemble_equals_sequential():
         st = f.make_stepper()
         s = torch.as_tensor(u, device="cuda")
         for k in range(3):
+            s, c, e = driver.step(f, st, s, f.params.step.corrector_tolerance,
+                                  f.params.step.max_corrector_iterations)
+            assert c == its[k][i]
+        assert torch.equal(s, ens.states[i]), i
+
+
+def couette_member(n, re, seed):
+    from dnsjax_b200 import initial
+    from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
+    from dnsjax_b200.parameters import Parameters
+
+    p = Parameters(phys=dict(system="plane-couette", re=re),
+                   geo=dict(lx=2 * pi, lz=pi), res=dict(nx=n, ny=n + 1, nz=n, fd_order=4),
+                   step=dict(dt=0.02, corrector_tolerance=1e-10))
+    u0 = initial.couette_field(n, n + 1, n, 2 * pi, pi, 4, seed, 8.0, 1e-3)
+    return PlaneCouetteFlow(p), u0
+
+
+def test_couette_step_graph_equals_driver():
+    import torch
+
+    from dnsjax_b200 import driver
+
+    f, u = couette_member(64, 400.0, 2)
+    s_eager = torch.as_tensor(u, device="cuda")
+    s_graph = torch.as_tensor(u, device="cuda")
+    g = f.make_step_graph(s_graph)
+    st = f.make_stepper()
+    for _ in range(3):
+        s_eager, c, e = driver.step(f, st, s_eager, f.params.step.corrector_tolerance,
+                                    f.params.step.max_corrector_iterations)
+        g.launch()
+        it, err = g.status()
+        assert it == c and err == e
+    f.check_status()
+    assert torch.equal(s_eager, s_graph)
+    g.close()
+    g2 = f.make_step_graph(torch.as_tensor(u, device="cuda"), max_iter=0)
+    g2.launch()
+    assert g2.status()[0] == 0
+
+
+def test_couette_graph_ensemble_equals_sequential():
+    import torch
+
+    from dnsjax_b200 import driver
+    from dnsjax_b200.ensemble import Ensemble
+
+    spec = [(32, 300.0, 1), (48, 500.0, 3), (32, 200.0, 4)]
+    built = [couette_member(*s) for s in spec]
+    ens = Ensemble([f for f, _ in built], [torch.as_tensor(u, device="cuda") for _, u in built],
+                   graphs=True)
+    its = [ens.step().corrector_iterations for _ in range(2)]
+    for i, (f, u) in enumerate(built):
+        st = f.make_stepper()
+        s = torch.as_tensor(u, device="cuda")
+        for k in range(2):
             s, c, e = driver.step(f, st, s, f.params.step.corrector_tolerance,
                                   f.params.step.max_corrector_iterations)
             assert c == its[k][i]

@@ -1,8 +1,7 @@
 """dnsb_couette_norm_noalloc: the allocation-free Couette norm.
 
-Callers that cannot allocate device memory -- an XLA FFI handler working in
-memory its framework owns, or code recorded by CUDA stream capture -- cannot
-create a dnsb_couette context either; this entry point gives them the same
+Callers that cannot allocate device memory -- such as an XLA FFI handler
+working in memory its framework owns -- cannot create a dnsb_couette context either; this entry point gives them the same
 norm from the field alone, keeping its partial sums in a fixed-size array
 inside the library.  It must agree with the context-based dnsb_couette_norm
 call after call (the array keeps the previous call's contents, which must
