@@ -375,7 +375,7 @@ extern "C" int dnsb_periodic_correct_velocity(dnsb_periodic* p, const void* v,
 // ---------------------------------------------------------------------------
 // One full time step of a periodic context as a CUDA graph: predictor and
 // first correction, the corrector iterations as a device-controlled WHILE
-// node (the reference driver's loop, __main__.py:163-180: iterate while
+// node (the reference driver's loop, __main__.py:166-180: iterate while
 // error > tol and iterations < max_iter), then correct_velocity into the
 // state.  Fixed buffers: the state (in / out) and the graph's own
 // prediction, two RHS buffers and control words.

@@ -99,7 +99,7 @@ int dnsb_periodic_correct_velocity(dnsb_periodic* ctx, const void* v,
 /* One full time step as a CUDA graph, for callers that step without host
  * synchronisation (the reference driver's step, __main__.py:125-203, with its
  * corrector loop -- iterate while error > tol and iterations < max_iter,
- * :163-180 -- as a device-controlled conditional node): predictor and first
+ * :166-180 -- as a device-controlled conditional node): predictor and first
  * correction from `state`, corrector iterations, correct_velocity (with
  * `divergence`) back into `state`.  The graph is bound to `state` (updated in
  * place by every launch) and owns its prediction, RHS and control buffers;
@@ -210,7 +210,7 @@ int dnsb_couette_check(dnsb_couette* ctx, void* stream);
  * dnsb_periodic_step_graph_create: predictor (the IMM iteration with
  * (u^n, u^n, N^n, N^n), plane_couette.py:507-519), first correction, and
  * corrector iterations (plane_couette.py:522-540) in a device-controlled
- * loop while error > tol and iterations < max_iter (__main__.py:163-180);
+ * loop while error > tol and iterations < max_iter (__main__.py:166-180);
  * correct_velocity is the identity for this flow (plane_couette.py:575-582),
  * so the converged iterate is copied back into `state`.  Needs bound IMM
  * operators; launch/status/destroy through dnsb_step_graph_*. */
