@@ -373,21 +373,30 @@ extern "C" int dnsb_periodic_correct_velocity(dnsb_periodic* p, const void* v,
 }
 
 // ---------------------------------------------------------------------------
-// One full time step of a periodic context as a CUDA graph: predictor and
-// first correction, the corrector iterations as a device-controlled WHILE
-// node (the reference driver's loop, __main__.py:166-180: iterate while
-// error > tol and iterations < max_iter), then correct_velocity into the
-// state.  Fixed buffers: the state (in / out) and the graph's own
-// prediction, two RHS buffers and control words.
+// One full time step as a CUDA graph: predictor and first correction, the
+// corrector iterations as a device-controlled WHILE node (the reference
+// driver's loop, __main__.py:166-180: iterate while error > tol and
+// iterations < max_iter), then correct_velocity into the state.  Fixed
+// buffers: the state (in / out) and the graph's own prediction, two RHS
+// buffers and control words.  The WHILE body holds two iterations, the
+// second inside an IF node, so the two RHS buffers alternate as previous
+// and next without a copy: iteration A (RHS into Ra, previous Rb), then, if
+// A did not end the loop, iteration B (RHS into Rb, previous Ra).
 // ---------------------------------------------------------------------------
 namespace dnsb {
-__global__ void step_ctl_kernel(cudaGraphConditionalHandle h, const double* err, int* ctl,
-                                double* err_last, double tol, int max_iter, int first) {
+// After a correction: count the iteration (first: the predictor's), keep
+// the error, and set the loop's condition -- and, after iteration A, the IF
+// node's (set_if) -- to "iterate again".
+__global__ void step_ctl_kernel(cudaGraphConditionalHandle h, cudaGraphConditionalHandle h_if,
+                                int set_if, const double* err, int* ctl, double* err_last,
+                                double tol, int max_iter, int first) {
   const int it = first ? 0 : ctl[0] + 1;
   const double e = err[0];
+  const unsigned cont = (e > tol && it < max_iter) ? 1u : 0u;
   ctl[0] = it;
   err_last[0] = e;
-  cudaGraphSetConditional(h, (e > tol && it < max_iter) ? 1u : 0u);
+  cudaGraphSetConditional(h, cont);
+  if (set_if) cudaGraphSetConditional(h_if, cont);
 }
 }  // namespace dnsb
 
@@ -408,67 +417,95 @@ static void step_graph_free(dnsb_step_graph* g) {
 }
 
 // Captures prologue (predictor and first correction, error into g->err),
-// the corrector iteration `body` inside a WHILE node, and `epilogue`, with
-// the control kernel after the prologue and at the end of the body.
+// the corrector iterations `body(stream, 0)` (A) and `body(stream, 1)` (B)
+// inside the WHILE node, and `epilogue`, with the control kernel after the
+// prologue and after each iteration.
 static int build_step_graph(dnsb_step_graph* g, double tol, int max_iter,
                             const std::function<int(cudaStream_t)>& prologue,
-                            const std::function<int(cudaStream_t)>& body,
+                            const std::function<int(cudaStream_t, int)>& body,
                             const std::function<int(cudaStream_t)>& epilogue) {
-  cudaStream_t s = nullptr, sb = nullptr;
+  cudaStream_t s = nullptr, sb = nullptr, si = nullptr;
   cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
   cudaStreamCreateWithFlags(&sb, cudaStreamNonBlocking);
+  cudaStreamCreateWithFlags(&si, cudaStreamNonBlocking);
   int rc = 0;
   auto ck = [&](cudaError_t e, const char* what) {
     if (e != cudaSuccess && !rc)
       rc = fail(DNSB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
   };
+  // Adds a conditional node of `type` after the work captured so far on
+  // `st` (in graph `gr`), makes it the stream's dependency, and returns its
+  // body graph.
+  auto add_cond = [&](cudaStream_t st, cudaGraph_t gr, cudaGraphConditionalHandle hd,
+                      cudaGraphConditionalNodeType type) -> cudaGraph_t {
+    if (rc) return nullptr;
+    cudaStreamCaptureStatus cst;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    ck(cudaStreamGetCaptureInfo(st, &cst, nullptr, nullptr, &deps, &ndeps), "capture info");
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hd;
+    cp.conditional.type = type;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if (!rc) ck(cudaGraphAddNode(&node, gr, deps, ndeps, &cp), "conditional node");
+    if (!rc)
+      ck(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies),
+         "capture dependencies");
+    return rc ? nullptr : cp.conditional.phGraph_out[0];
+  };
   cudaGraph_t graph = nullptr;
   ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
   cudaStreamCaptureStatus cs;
   ck(cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, nullptr, nullptr), "capture info");
-  cudaGraphConditionalHandle h = 0;
+  cudaGraphConditionalHandle h = 0, h_if = 0;
   ck(cudaGraphConditionalHandleCreate(&h, graph, 0, 0), "conditional handle");
   // Captured calls count their launches; the graph's kernels are counted
   // when they run (dnsb_step_graph_status), so the capture's count is undone.
   const long long c0 = g_launches.load();
   if (!rc) rc = prologue(s);
-  dnsb::step_ctl_kernel<<<1, 1, 0, s>>>(h, g->err, g->ctl, g->err + 1, tol, max_iter, 1);
+  dnsb::step_ctl_kernel<<<1, 1, 0, s>>>(h, 0, 0, g->err, g->ctl, g->err + 1, tol, max_iter, 1);
   ck(cudaGetLastError(), "control kernel");
   const long long c1 = g_launches.load() + 1;  // + the control kernel
-  const cudaGraphNode_t* deps = nullptr;
-  size_t ndeps = 0;
-  ck(cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &ndeps), "capture info");
-  cudaGraphNodeParams cp = {};
-  cp.type = cudaGraphNodeTypeConditional;
-  cp.conditional.handle = h;
-  cp.conditional.type = cudaGraphCondTypeWhile;
-  cp.conditional.size = 1;
-  cudaGraphNode_t wn = nullptr;
-  if (!rc) ck(cudaGraphAddNode(&wn, graph, deps, ndeps, &cp), "while node");
+  long long c2 = c1;
+  cudaGraph_t bg = add_cond(s, graph, h, cudaGraphCondTypeWhile);
   if (!rc) {
-    cudaGraph_t bg = cp.conditional.phGraph_out[0];
-    ck(cudaStreamUpdateCaptureDependencies(s, &wn, 1, cudaStreamSetCaptureDependencies),
-       "capture dependencies");
+    ck(cudaGraphConditionalHandleCreate(&h_if, bg, 0, 0), "conditional handle");
     ck(cudaStreamBeginCaptureToGraph(sb, bg, nullptr, nullptr, 0,
                                      cudaStreamCaptureModeThreadLocal), "body capture");
-    if (!rc) rc = body(sb);
-    dnsb::step_ctl_kernel<<<1, 1, 0, sb>>>(h, g->err, g->ctl, g->err + 1, tol, max_iter, 0);
+    if (!rc) rc = body(sb, 0);
+    dnsb::step_ctl_kernel<<<1, 1, 0, sb>>>(h, h_if, 1, g->err, g->ctl, g->err + 1, tol,
+                                           max_iter, 0);
     ck(cudaGetLastError(), "control kernel");
+    c2 = g_launches.load() + 1;  // + the control kernel of iteration A
+    cudaGraph_t ig = add_cond(sb, bg, h_if, cudaGraphCondTypeIf);
+    if (!rc) {
+      ck(cudaStreamBeginCaptureToGraph(si, ig, nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeThreadLocal), "IF body capture");
+      if (!rc) rc = body(si, 1);
+      dnsb::step_ctl_kernel<<<1, 1, 0, si>>>(h, 0, 0, g->err, g->ctl, g->err + 1, tol,
+                                             max_iter, 0);
+      ck(cudaGetLastError(), "control kernel");
+      cudaGraph_t iout = nullptr;
+      ck(cudaStreamEndCapture(si, &iout), "end IF body capture");
+    }
     cudaGraph_t bout = nullptr;
     ck(cudaStreamEndCapture(sb, &bout), "end body capture");
   }
-  const long long c2 = g_launches.load() + 1;  // + the body's control kernel
+  const long long c3 = g_launches.load();  // after both iterations
   if (!rc) rc = epilogue(s);
-  const long long c3 = g_launches.load();
-  g->k_iter = (c2 - c1) + 1;                   // body launches + its control kernel
-  g->k_fixed = (c1 - c0) + (c3 - c2 + 1);      // prologue (+ control) + epilogue
-  g_launches.fetch_sub(c3 - c0, std::memory_order_relaxed);
+  const long long c4 = g_launches.load();
+  g->k_iter = c2 - c1;                      // one iteration + its control kernel
+  g->k_fixed = (c1 - c0) + (c4 - c3);       // prologue (+ control) + epilogue
+  g_launches.fetch_sub(c4 - c0, std::memory_order_relaxed);
   cudaGraph_t done = nullptr;
   ck(cudaStreamEndCapture(s, &done), "end capture");  // always end the capture
   if (!rc) ck(cudaGraphInstantiate(&g->exec, done, 0), "instantiate");
   if (done) cudaGraphDestroy(done);
   cudaStreamDestroy(s);
   cudaStreamDestroy(sb);
+  cudaStreamDestroy(si);
   return rc;
 }
 
@@ -497,13 +534,13 @@ extern "C" int dnsb_periodic_step_graph_create(dnsb_periodic* p, void* state, do
     if (!rc) rc = dnsb_periodic_correct(p, g->P, g->Ra, g->Rb, g->P, nullptr, g->err, s);
     return rc;
   };
-  // one corrector iteration: rhs_next -> Ra, rhs_prev = Rb, then Ra -> Rb
-  auto body = [&](cudaStream_t s) {
-    int rc = dnsb_periodic_rhs(p, g->P, g->Ra, s);
-    if (!rc) rc = dnsb_periodic_correct(p, g->P, g->Rb, g->Ra, g->P, nullptr, g->err, s);
-    if (!rc && cudaMemcpyAsync(g->Rb, g->Ra, n * sizeof(double2), cudaMemcpyDeviceToDevice,
-                               s) != cudaSuccess)
-      rc = fail(DNSB_ERR_CUDA, "rhs copy");
+  // one corrector iteration: A (parity 0) rhs_next -> Ra with rhs_prev Rb,
+  // B (parity 1) the other way round
+  auto body = [&](cudaStream_t s, int parity) {
+    double2* nx = parity ? g->Rb : g->Ra;
+    double2* pv = parity ? g->Ra : g->Rb;
+    int rc = dnsb_periodic_rhs(p, g->P, nx, s);
+    if (!rc) rc = dnsb_periodic_correct(p, g->P, pv, nx, g->P, nullptr, g->err, s);
     return rc;
   };
   auto epilogue = [&](cudaStream_t s) {
@@ -1170,12 +1207,11 @@ extern "C" int dnsb_couette_step_graph_create(dnsb_couette* p, void* state, doub
     if (!rc) rc = dnsb_couette_imm(p, state, g->P, g->Ra, g->Rb, g->P, nullptr, g->err, s);
     return rc;
   };
-  auto body = [&](cudaStream_t s) {
-    int rc = dnsb_couette_rhs(p, g->P, g->Ra, s);
-    if (!rc) rc = dnsb_couette_imm(p, state, g->P, g->Rb, g->Ra, g->P, nullptr, g->err, s);
-    if (!rc && cudaMemcpyAsync(g->Rb, g->Ra, n * sizeof(double2), cudaMemcpyDeviceToDevice,
-                               s) != cudaSuccess)
-      rc = fail(DNSB_ERR_CUDA, "rhs copy");
+  auto body = [&](cudaStream_t s, int parity) {
+    double2* nx = parity ? g->Rb : g->Ra;
+    double2* pv = parity ? g->Ra : g->Rb;
+    int rc = dnsb_couette_rhs(p, g->P, nx, s);
+    if (!rc) rc = dnsb_couette_imm(p, state, g->P, pv, nx, g->P, nullptr, g->err, s);
     return rc;
   };
   auto epilogue = [&](cudaStream_t s) {

@@ -69,6 +69,17 @@ def test_step_graph_equals_driver():
     g2 = f2.make_step_graph(s2, max_iter=1)
     g2.launch()
     assert g2.status()[0] == 1
+    # a cap of 2 ends the loop in the second iteration of the graph's body;
+    # the state matches the host loop with the same cap
+    f3, u3 = member(32, 40.0, 5)
+    s3 = torch.as_tensor(u3, device="cuda")
+    s3_eager = torch.as_tensor(u3, device="cuda")
+    g3 = f3.make_step_graph(s3, max_iter=2)
+    g3.launch()
+    assert g3.status()[0] == 2
+    s3_eager, c, _ = driver.step(f3, f3.make_stepper(), s3_eager,
+                                 f3.params.step.corrector_tolerance, 2)
+    assert c == 2 and torch.equal(s3_eager, s3)
 
 
 def test_graph_ensemble_equals_sequential():
