@@ -92,6 +92,8 @@ SIGNATURES = {
     "dnsb_couette_phys_to_spec": (c_int, [c_void_p] * 4),
     "dnsb_couette_check": (c_int, [c_void_p, c_void_p]),
     "dnsb_couette_set_rhs_precision": (c_int, [c_void_p, c_int]),
+    "dnsb_imm_precompute": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_int,
+                                    c_int, c_double, c_double, c_double] + [c_void_p] * 13),
     "dnsb_couette_norm_noalloc": (c_int, [c_void_p, c_int, c_int, c_int, c_double,
                                           c_void_p, c_void_p]),
     "dnsb_banded_solve": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int,

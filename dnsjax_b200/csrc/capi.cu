@@ -1241,6 +1241,41 @@ extern "C" int dnsb_couette_check(dnsb_couette* p, void* stream) {
 }
 
 // ===========================================================================
+// Influence-matrix precompute on the GPU
+// ===========================================================================
+extern "C" int dnsb_imm_precompute(const double* D1, const double* D2, const double* kx,
+                                   int nkx, const double* kz, int nkz, int ny, int p,
+                                   double dt, double c, double nu, double* p1, double* p2,
+                                   double* v1, double* v2, double* q1, double* q2,
+                                   double* M_inv, double* Lk_ab, int* Lk_piv, double* Hk_ab,
+                                   int* Hk_piv, int* info_dev, void* stream) {
+  if (!D1 || !D2 || !kx || !kz || !p1 || !p2 || !v1 || !v2 || !q1 || !q2 || !M_inv ||
+      !Lk_ab || !Lk_piv || !Hk_ab || !Hk_piv || !info_dev)
+    return fail(DNSB_ERR_ARG, "null argument");
+  if (nkx < 1 || nkz < 1 || ny < 3 || p < 1 || p >= ny || !(dt > 0.0))
+    return fail(DNSB_ERR_ARG, "invalid sizes");
+  cudaStream_t st = as_stream(stream);
+  const size_t nmy = (size_t)nkx * nkz * ny;
+  double* bp = nullptr;
+  double* bv = nullptr;
+  DNSB_CUDA(cudaMallocAsync(&bp, nmy * 2 * sizeof(double), st));
+  if (cudaMallocAsync(&bv, nmy * 4 * sizeof(double), st) != cudaSuccess) {
+    cudaFreeAsync(bp, st);
+    return fail(DNSB_ERR_CUDA, "precompute workspace allocation failed");
+  }
+  ImmPrecomputeArgs a{D1, D2, kx, kz, nkx, nkz, ny, p, dt, c, nu, p1, p2, v1, v2, q1, q2,
+                      M_inv, Lk_ab, Lk_piv, Hk_ab, Hk_piv, info_dev, info_dev};
+  int nl = 0;
+  const cudaError_t e = launch_imm_precompute(a, bp, bv, st, &nl);
+  g_launches.fetch_add(nl, std::memory_order_relaxed);
+  cudaFreeAsync(bp, st);
+  cudaFreeAsync(bv, st);
+  if (e != cudaSuccess)
+    return fail(DNSB_ERR_CUDA, std::string("IMM precompute: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+// ===========================================================================
 // Standalone banded solve
 // ===========================================================================
 extern "C" int dnsb_banded_solve(const double* ab, const int* ipiv, double* b,

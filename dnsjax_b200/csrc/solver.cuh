@@ -122,6 +122,28 @@ struct ImmBatch {
   double2* F;
   double2* R;
 };
+// Influence-matrix precompute (csrc/precompute.cu); every pointer is device
+// memory, D1 / D2 dense (ny, ny) row-major, outputs in the reference's
+// layouts ([nkz][nkx][...]).
+struct ImmPrecomputeArgs {
+  const double* D1;
+  const double* D2;
+  const double* kx;  // [nkx]
+  const double* kz;  // [nkz]
+  int nkx, nkz, ny, p;
+  double dt, c, nu;
+  double *p1, *p2, *v1, *v2, *q1, *q2;  // [nkz][nkx][ny]
+  double* M_inv;                         // [nkz][nkx][2][2]
+  double* Lk_ab;                         // [nkz][nkx][3p+1][ny]
+  int* Lk_piv;                           // [nkz][nkx][ny], 0-based
+  double* Hk_ab;
+  int* Hk_piv;
+  int* info;    // bit 1: zero pivot in some L_k, bit 2: in some H_k
+  int* status;  // bit 0: a pivot out of range in a substitution
+};
+// bp: nkz*nkx*ny*2 doubles, bv: nkz*nkx*ny*4 doubles of workspace.
+cudaError_t launch_imm_precompute(const ImmPrecomputeArgs& a, double* bp, double* bv,
+                                  cudaStream_t st, int* launches);
 bool imm_batch_supported(int kl, int ny);
 size_t imm_batch_stage_smem(int Ny);
 int imm_nu(int kl, int row0);

@@ -21,13 +21,14 @@ import numpy as np
 
 from .. import _lib
 from ..fd import build_diff_matrices, cgl_grid, diff_bands
-from ..geometries.cartesian import Fourier, precompute_imm, simpson_weights
+from ..geometries.cartesian import Fourier, precompute_imm, precompute_imm_gpu, simpson_weights
 from ..parameters import Parameters, derive, padded_sizes
 from ..timestep import StepGraph, make_fused_stepper, make_stepper
 
 
 class PlaneCouetteFlow:
-    def __init__(self, p: Parameters, imm: dict | None = None, ly: float | None = None):
+    def __init__(self, p: Parameters, imm: dict | None = None, ly: float | None = None,
+                 precompute: str = "gpu"):
         import torch
 
         L = _lib.lib()
@@ -82,17 +83,30 @@ class PlaneCouetteFlow:
         if self.rhs_fp32:
             _lib.check(L.dnsb_couette_set_rhs_precision(self._ctx, 1))
 
+        # Influence-matrix data (cartesian.py:575-801): given, or computed
+        # once here -- on the GPU ("gpu") or on the host as the reference
+        # does ("host").
         if imm is None:
-            imm = precompute_imm(self.ys, self.fourier.kx_global,
-                                 self.fourier.kz_global, self.p, self.dt,
-                                 self.c, self.nu, self.D1, self.D2)
+            if precompute == "gpu":
+                imm = precompute_imm_gpu(self.fourier.kx_global, self.fourier.kz_global,
+                                         self.p, self.dt, self.c, self.nu, self.D1, self.D2)
+            elif precompute == "host":
+                imm = precompute_imm(self.ys, self.fourier.kx_global,
+                                     self.fourier.kz_global, self.p, self.dt,
+                                     self.c, self.nu, self.D1, self.D2)
+            else:
+                raise ValueError(f"precompute must be 'gpu' or 'host', got {precompute!r}")
+
+        def to_dev(a, dt_np, dt_t):
+            if isinstance(a, torch.Tensor):
+                return a.to(device="cuda", dtype=dt_t).contiguous()
+            return torch.as_tensor(np.ascontiguousarray(a, dt_np), device="cuda")
+
         dev = {}
         for k in ("Lk_ab", "Hk_ab", "v1", "v2", "q1", "q2", "M_inv", "p1", "p2"):
-            dev[k] = torch.as_tensor(np.ascontiguousarray(imm[k], np.float64),
-                                     device="cuda")
+            dev[k] = to_dev(imm[k], np.float64, torch.float64)
         for k in ("Lk_piv", "Hk_piv"):
-            dev[k] = torch.as_tensor(np.ascontiguousarray(imm[k], np.int32),
-                                     device="cuda")
+            dev[k] = to_dev(imm[k], np.int32, torch.int32)
         self.imm = dev
         ops = _lib.ImmOps(*[_lib.ptr(dev[k]) for k in (
             "Lk_ab", "Lk_piv", "Hk_ab", "Hk_piv", "v1", "v2", "q1", "q2", "M_inv")])

@@ -5,9 +5,11 @@ Host-side setup mirrors the reference (src/dnsjax/geometries/cartesian.py):
 * ``Fourier`` -- ``kx``, ``kz``, ``k_metric``, ``k2`` (cartesian.py:17-69);
 * ``precompute_imm`` -- per-(kz, kx) influence-matrix data and LAPACK
   ``gbtrf`` banded LU factors of ``L_k`` (Neumann) and ``H_k`` (Dirichlet)
-  in the reference's ``ab`` layout (cartesian.py:491-801).  Like the
-  reference it runs once, on the host, before time stepping; this version
-  batches the dense homogeneous solves across modes;
+  in the reference's ``ab`` layout (cartesian.py:491-801), on the host as
+  the reference runs it (this version batches the dense homogeneous solves
+  across modes);
+* ``precompute_imm_gpu`` -- the same arrays computed on the GPU
+  (``dnsb_imm_precompute``);
 * ``simpson_weights`` -- the non-uniform composite Simpson rule of
   cartesian.py:106-140 as a linear functional.
 
@@ -160,6 +162,48 @@ def precompute_imm(y, kx_vals, kz_vals, p, dt, c, nu, D1, D2,
             out["Hk_ab"][s + i], out["Hk_piv"][s + i] = banded_lu(Hab[i], kl, ku)
     for k, v in out.items():
         out[k] = v.reshape((nkz, nkx) + v.shape[1:])
+    out["D1"], out["D2"] = D1, D2
+    return out
+
+
+IMM_KEYS_F64 = ("p1", "p2", "v1", "v2", "q1", "q2", "M_inv", "Lk_ab", "Hk_ab")
+
+
+def precompute_imm_gpu(kx_vals, kz_vals, p, dt, c, nu, D1, D2) -> dict:
+    """``precompute_imm`` on the GPU (``dnsb_imm_precompute``): the same keys
+    and shapes as device tensors (cartesian.py:575-801).  The operators are
+    built and factored per mode exactly as the reference packs and factors
+    them (LAPACK dgbtf2 with partial pivoting); p, v, q are solved with the
+    banded factors instead of dense LU, so they agree to rounding.  Raises
+    ValueError on a zero pivot, as the reference does for LAPACK info > 0."""
+    import torch
+
+    from .. import _lib
+
+    L = _lib.lib()
+    ny, nkx, nkz = D1.shape[0], len(kx_vals), len(kz_vals)
+
+    def dev(a):
+        return torch.as_tensor(np.ascontiguousarray(a, np.float64), device="cuda")
+
+    d1, d2, kx, kz = dev(D1), dev(D2), dev(kx_vals), dev(kz_vals)
+    f64 = dict(dtype=torch.float64, device="cuda")
+    out = {k: torch.empty((nkz, nkx, ny), **f64) for k in ("p1", "p2", "v1", "v2", "q1", "q2")}
+    out["M_inv"] = torch.empty((nkz, nkx, 2, 2), **f64)
+    for k in ("Lk", "Hk"):
+        out[k + "_ab"] = torch.empty((nkz, nkx, 3 * p + 1, ny), **f64)
+        out[k + "_piv"] = torch.empty((nkz, nkx, ny), dtype=torch.int32, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ptr = _lib.ptr
+    _lib.check(L.dnsb_imm_precompute(
+        ptr(d1), ptr(d2), ptr(kx), nkx, ptr(kz), nkz, ny, p, float(dt), float(c), float(nu),
+        *[ptr(out[k]) for k in ("p1", "p2", "v1", "v2", "q1", "q2", "M_inv", "Lk_ab",
+                                 "Lk_piv", "Hk_ab", "Hk_piv")],
+        ptr(info), _lib.stream_handle()))
+    bad = int(info.item())
+    if bad & 6:
+        which = " and ".join(n for b, n in ((2, "L_k"), (4, "H_k")) if bad & b)
+        raise ValueError(f"dgbtrf failed: zero pivot in some {which}")
     out["D1"], out["D2"] = D1, D2
     return out
 

@@ -234,6 +234,37 @@ int dnsb_couette_norm_noalloc(const void* v, int nx, int ny, int nz, double ly,
                               double* out_dev, void* stream);
 
 /* ------------------------------------------------------------------ */
+/* Influence-matrix precompute on the GPU (precompute_imm, banded      */
+/* backend, geometries/cartesian.py:575-801).  For every (kz, kx) mode  */
+/* (k2 = kx^2 + kz^2): L_k = D2 - k2 I with Neumann wall rows (row 0    */
+/* pinned to e_0 when k2 = 0; build_Lk_neumann, :491-526) and           */
+/* H_k = I/dt - c nu (D2 - k2 I) with identity wall rows               */
+/* (build_Hk_dirichlet, :529-572), packed as LAPACK ab (:291-320) and  */
+/* factored by banded LU with partial pivoting (LAPACK dgbtf2, what    */
+/* SciPy's gbtrf runs for these bandwidths; :323-357); p1, p2 = L_k^-1 */
+/* e_0, e_{ny-1}; v1, v2 = H_k^-1 (-D1 p1), H_k^-1 (-D1 p2) and q1,    */
+/* q2 = H_k^-1 p1, H_k^-1 p2 (wall rows of the right-hand sides zero); */
+/* M_inv = inverse of [D1[0].v1 D1[0].v2; D1[ny-1].v1 D1[ny-1].v2]      */
+/* ([[0, 0], [0, 1/M11]] when k2 = 0).  The p, v, q solves use the     */
+/* banded factors (the reference uses dense LU), so they agree with    */
+/* the reference to rounding.  kl = ku = p.                            */
+/*   D1, D2 : (ny, ny) float64 row-major; kx (nkx), kz (nkz) float64   */
+/*   p1..q2 : (nkz, nkx, ny) float64; M_inv (nkz, nkx, 2, 2) float64   */
+/*   Lk_ab, Hk_ab : (nkz, nkx, 3p+1, ny) float64; Lk_piv, Hk_piv       */
+/*          (nkz, nkx, ny) int32, 0-based                              */
+/*   info_dev : device int, zeroed by the caller; OR'ed with 2 when    */
+/*          some L_k, 4 when some H_k has a zero pivot (the reference  */
+/*          raises ValueError for LAPACK info > 0)                     */
+/* Every array is device memory; the call allocates stream-ordered    */
+/* workspace (6 nkz nkx ny doubles) and frees it before returning.     */
+/* ------------------------------------------------------------------ */
+int dnsb_imm_precompute(const double* D1, const double* D2, const double* kx, int nkx,
+                        const double* kz, int nkz, int ny, int p, double dt, double c,
+                        double nu, double* p1, double* p2, double* v1, double* v2,
+                        double* q1, double* q2, double* M_inv, double* Lk_ab, int* Lk_piv,
+                        double* Hk_ab, int* Hk_piv, int* info_dev, void* stream);
+
+/* ------------------------------------------------------------------ */
 /* Per-mode banded LU substitution (PerModeBandedOperator.solve,       */
 /* cartesian.py:444-488; dgbtrs 'N').                                  */
 /*   ab   : (nmodes, 2kl+ku+1, ny) float64, LAPACK ab packing          */
