@@ -259,6 +259,13 @@ class TriplyPeriodicFlow:
         return self.phys_to_spec(torch.as_tensor(np.ascontiguousarray(arr),
                                                  device="cuda"))
 
+    def save_snapshot(self, path, state) -> None:
+        """Write ``state`` as an npz snapshot the reference's init_state
+        reads (monochromatic.py:302-311): ``velocity_phys`` = the physical
+        perturbation velocity plus the base flow."""
+        phys = self.spec_to_phys(state).cpu().numpy()
+        np.savez(path, velocity_phys=phys + self.base_flow[:, :, None, None])
+
     def make_stepper(self, fused: bool = True):
         if fused:
             return make_fused_stepper(self)
@@ -304,3 +311,7 @@ def get_stats(state) -> dict:
 
 def init_state(snapshot=None):
     return _flow().init_state(snapshot)
+
+
+def save_snapshot(path, state) -> None:
+    _flow().save_snapshot(path, state)

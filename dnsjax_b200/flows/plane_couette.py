@@ -226,6 +226,12 @@ class PlaneCouetteFlow:
         arr = np.load(snapshot)["velocity_phys_nonexpanded"].astype(np.float64)
         return self.phys_to_spec(torch.as_tensor(arr, device="cuda"))
 
+    def save_snapshot(self, path, state) -> None:
+        """Write ``state`` as an npz snapshot the reference's init_state
+        reads (plane_couette.py:233-242): ``velocity_phys_nonexpanded`` =
+        the physical perturbation velocity (no base flow)."""
+        np.savez(path, velocity_phys_nonexpanded=self.spec_to_phys(state).cpu().numpy())
+
     # -- stepper ---------------------------------------------------------------
     def make_stepper(self, fused: bool = True):
         if fused:
@@ -272,3 +278,7 @@ def get_stats(state) -> dict:
 
 def init_state(snapshot=None):
     return _flow().init_state(snapshot)
+
+
+def save_snapshot(path, state) -> None:
+    _flow().save_snapshot(path, state)
