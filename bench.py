@@ -514,6 +514,154 @@ def run_ours(a, w, rank, world):
         print(json.dumps(out), flush=True)
 
 
+def run_learned(a, w, rank, world):
+    """The learned-guess forms (plane Couette): plain FP64 or mixed, each step
+    started from predictor + the MLP's guess, the network trained online on
+    every step's pair.  Timed over K steps including inference and training;
+    compared with the plain FP64 host loop over the same steps."""
+    import torch
+
+    from dnsjax_b200 import _lib, driver, learned
+    from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
+
+    if w["system"] != "plane-couette":
+        raise SystemExit("--form learned is built for plane Couette")
+    if world > 1:
+        raise SystemExit("--form learned runs on one GPU")
+    torch.cuda.set_device(0)
+    mixed = a.form == "learned-mixed"
+    flow = PlaneCouetteFlow(params_for(w, fp64=not mixed))
+    tol, mi = (w["tol"] if a.tol is None else a.tol), w["max_iter"]
+    u0 = initial_state(w, w["seed"])
+    lg = learned.LearnedGuess(flow, hidden=512, train_iters=a.train_iters)
+    state = torch.as_tensor(u0, device="cuda")
+    dprev = None
+    for _ in range(a.warmup):
+        state, dprev, _ = lg.step(state, dprev, tol, mi)
+    steps = []
+    n0 = _lib.launch_count()
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clk:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(a.steps):
+            state, dprev, st = lg.step(state, dprev, tol, mi)
+            steps.append(st)
+        t1.record()
+        torch.cuda.synchronize()
+    launches = _lib.launch_count() - n0
+    ms = t0.elapsed_time(t1)
+
+    # the plain FP64 host loop over the same steps from the same field
+    plain = PlaneCouetteFlow(params_for(w, fp64=True))
+    ps = plain.make_stepper()
+    ref = torch.as_tensor(u0, device="cuda")
+    for _ in range(a.warmup):
+        ref, _, _ = driver.step(plain, ps, ref, w["tol"], mi)
+    p_iters = []
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        ref, c, _ = driver.step(plain, ps, ref, w["tol"], mi)
+        p_iters.append(c)
+    e1.record()
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    ke = lambda f, u: float(f.norm(u).item()) ** 2 / 2  # noqa: E731
+    ke_l, ke_p = ke(plain, state), ke(plain, ref)
+    field = float(torch.linalg.vector_norm(state - ref) / torch.linalg.vector_norm(ref))
+
+    # the network alone: one inference and one training iteration, timed
+    net = lg.net
+    flops_fwd = 2.0 * net.M * (net.K1p * net.H + net.H * net.N2)
+    q0 = torch.cuda.Event(enable_timing=True)
+    q1 = torch.cuda.Event(enable_timing=True)
+    reps = 10
+    q0.record()
+    for _ in range(reps):
+        net.forward()
+        net.loss()
+        net.backward()
+    q1.record()
+    torch.cuda.synchronize()
+    train_ms = q0.elapsed_time(q1) / reps
+    peaks = measured_peaks()
+    bf16_peak = (peaks or {}).get("bf16_tflops", 1590.0)
+    achieved = 3 * flops_fwd / (train_ms * 1e-3) / 1e12
+
+    # end to end: pinned host state in and out every step
+    host_in = torch.empty(state.shape, dtype=state.dtype, pin_memory=True)
+    host_in.copy_(torch.as_tensor(u0))
+    host_out = torch.empty_like(host_in, pin_memory=True)
+    dp = None
+    torch.cuda.synchronize()
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g0.record()
+    for _ in range(a.steps):
+        d_state = host_in.to("cuda", non_blocking=True)
+        d_state, dp, _ = lg.step(d_state, dp, tol, mi)
+        host_out.copy_(d_state, non_blocking=True)
+        host_in, host_out = host_out, host_in
+    g1.record()
+    torch.cuda.synchronize()
+    e2e_ms = g0.elapsed_time(g1)
+    state_bytes = state.numel() * state.element_size()
+    value = a.steps / (ms * 1e-3)
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "steps/s",
+        "n_gpus": 1,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": ms / a.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (RHS passes) + f64, bf16 MLP" if mixed else "f64, bf16 MLP",
+        "data": "synthetic (seeded divergence-free spectral field)",
+        "config": {
+            "workload": a.workload,
+            "form": ("learned+mixed" if mixed else "learned") + ": per-mode MLP guess of the "
+                    "converged correction, trained online; corrector to tolerance",
+            "grid": [w["nx"], w["ny"], w["nz"]], "fd_order": w.get("p"),
+            "re": w["re"], "dt": w["dt"], "tol": tol,
+            "network": {"parameters": net.parameters, "layers": [net.K1, net.H, net.N2],
+                        "train_iters_per_step": lg.train_iters},
+            "corrector_iterations_per_step": sum(s.corrector_iterations for s in steps) / a.steps,
+            "plain_corrector_iterations_per_step": sum(p_iters) / a.steps,
+            "guessed_fraction": sum(s.guessed for s in steps) / a.steps,
+            "guess_rel_error_last": steps[-1].guess_rel_error,
+            "plain_fp64_host_loop_steps_per_s": a.steps / (plain_ms * 1e-3),
+            "speedup_vs_plain_fp64_host_loop": plain_ms / ms,
+            "vs_plain_fp64": {"steps": a.warmup + a.steps, "ke_rel_err": abs(ke_l - ke_p) / ke_p,
+                              "field_rel_l2": field},
+            "all_steps_converged": all(s.error <= tol for s in steps),
+        },
+        "roofline": {
+            "bound": "tensor",
+            "kernel": "MLP forward + backward (6 BF16 GEMMs, mma.sync)",
+            "achieved": achieved,
+            "peak": bf16_peak,
+            "unit": "TFLOP/s",
+            "frac": achieved / bf16_peak,
+            "traffic": None,
+            "peak_source": "measured" if peaks else "fallback",
+            "flops_per_train_iteration": 3 * flops_fwd,
+            "avg_train_iteration_ms": train_ms,
+        },
+        "e2e": {"value": a.steps / (e2e_ms * 1e-3), "unit": "steps/s",
+                "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(out), flush=True)
+
+
 def cpu_sample(w, flow, u0, iters_per_step, imm=None):
     """Oracle (NumPy FP64 port) timed on one host core: one RHS + one
     corrector evaluation of the same workload, turned into steps/s with the
@@ -794,8 +942,12 @@ def main():
     ap.add_argument("--driver", default="graph", choices=["graph", "eager"],
                     help="graph: one step graph launch per time step; eager: the "
                          "host-driven predictor-corrector loop")
-    ap.add_argument("--form", default="plain", choices=["plain", "mixed"],
-                    help="mixed: FP32 RHS passes (plane Couette), FP64 elsewhere")
+    ap.add_argument("--form", default="plain",
+                    choices=["plain", "mixed", "learned", "learned-mixed"],
+                    help="mixed: FP32 RHS passes (plane Couette), FP64 elsewhere; "
+                         "learned[-mixed]: each step started from the MLP's guess")
+    ap.add_argument("--train-iters", type=int, default=2,
+                    help="learned forms: training iterations per time step")
     ap.add_argument("--tol", type=float, default=None,
                     help="corrector tolerance of the timed run (default: the workload's)")
     a = ap.parse_args()
@@ -806,6 +958,8 @@ def main():
         run_reference(a, w, rank, world)
     elif w["system"] == "ensemble":
         run_ensemble(a, w, rank, world)
+    elif a.form.startswith("learned"):
+        run_learned(a, w, rank, world)
     else:
         run_ours(a, w, rank, world)
 

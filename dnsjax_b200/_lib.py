@@ -92,6 +92,19 @@ SIGNATURES = {
     "dnsb_couette_phys_to_spec": (c_int, [c_void_p] * 4),
     "dnsb_couette_check": (c_int, [c_void_p, c_void_p]),
     "dnsb_couette_set_rhs_precision": (c_int, [c_void_p, c_int]),
+    "dnsb_mlp_gemm": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p,
+                              c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_int,
+                              c_void_p]),
+    "dnsb_learned_features": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_double,
+                                      c_double, c_double, c_void_p, c_int, c_void_p, c_int,
+                                      c_void_p, c_void_p]),
+    "dnsb_learned_guess": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                                   c_void_p]),
+    "dnsb_mlp_loss_grad": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p,
+                                   c_void_p, c_void_p, c_void_p]),
+    "dnsb_mlp_colsum": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "dnsb_mlp_adam": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, C.c_longlong,
+                              C.c_float, C.c_float, C.c_float, C.c_float, c_int, c_void_p]),
     "dnsb_imm_precompute": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_int,
                                     c_int, c_double, c_double, c_double] + [c_void_p] * 13),
     "dnsb_couette_norm_noalloc": (c_int, [c_void_p, c_int, c_int, c_int, c_double,

@@ -1241,6 +1241,71 @@ extern "C" int dnsb_couette_check(dnsb_couette* p, void* stream) {
 }
 
 // ===========================================================================
+// Learned corrector guess (plane Couette): BF16 MLP kernels
+// ===========================================================================
+extern "C" int dnsb_mlp_gemm(int ta, int tb, int M, int N, int K, const void* A, int lda,
+                             const void* B, int ldb, const float* bias, int relu,
+                             const void* mask, int ldm, float* Cf, void* Cb, int ldc,
+                             void* stream) {
+  if (!A || !B || (!Cf && !Cb)) return fail(DNSB_ERR_ARG, "null argument");
+  if (M < 1 || N < 1 || K < 1 || lda < 1 || ldb < 1 || ldc < N || (mask && ldm < N))
+    return fail(DNSB_ERR_ARG, "invalid GEMM sizes");
+  if ((ta ? lda < M : lda < K) || (tb ? ldb < N : ldb < K))
+    return fail(DNSB_ERR_ARG, "leading dimension smaller than the operand");
+  DNSB_LAUNCH(launch_mlp_gemm(ta, tb, M, N, K, A, lda, B, ldb, bias, relu, mask, ldm, Cf, Cb,
+                              ldc, as_stream(stream)));
+  return 0;
+}
+
+extern "C" int dnsb_learned_features(dnsb_couette* p, const void* un, const void* up,
+                                     const void* dprev, const void* target, double kx_max,
+                                     double kz_max, double s_floor, void* X, int ldx, float* T,
+                                     int ldt, float* scale, void* stream) {
+  if (!p || !un || !up || !X || !scale || (target && !T)) return fail(DNSB_ERR_ARG, "null argument");
+  if (ldx < 12 * p->Ny + 2 || (target && ldt < 6 * p->Ny) || !(kx_max > 0.0) || !(kz_max > 0.0))
+    return fail(DNSB_ERR_ARG, "invalid feature sizes");
+  DNSB_LAUNCH(launch_learned_features(
+      (const double2*)un, (const double2*)up, (const double2*)dprev, (const double2*)target,
+      p->kx, p->kz, p->NKX, p->NZ1, p->Ny, kx_max, kz_max, s_floor, X, ldx, T, ldt, scale,
+      as_stream(stream)));
+  return 0;
+}
+
+extern "C" int dnsb_learned_guess(dnsb_couette* p, const void* up, const float* Y, int ldy,
+                                  const float* scale, void* out, void* stream) {
+  if (!p || !up || !Y || !scale || !out) return fail(DNSB_ERR_ARG, "null argument");
+  if (ldy < 6 * p->Ny) return fail(DNSB_ERR_ARG, "invalid output stride");
+  DNSB_LAUNCH(launch_learned_guess((const double2*)up, Y, ldy, scale, p->NM, p->Ny,
+                                   (double2*)out, as_stream(stream)));
+  return 0;
+}
+
+extern "C" int dnsb_mlp_loss_grad(const float* Y, const float* T, int M, int N, int ld,
+                                  float* dYf, void* dYb, float* err, float* ref, void* stream) {
+  if (!Y || !T || !dYf || !dYb || !err || !ref) return fail(DNSB_ERR_ARG, "null argument");
+  if (M < 1 || N < 1 || ld < N) return fail(DNSB_ERR_ARG, "invalid sizes");
+  DNSB_LAUNCH(launch_mlp_loss_grad(Y, T, M, N, ld, dYf, dYb, err, ref, as_stream(stream)));
+  return 0;
+}
+
+extern "C" int dnsb_mlp_colsum(const void* A, int bf16, int M, int N, int lda, float* out,
+                               void* stream) {
+  if (!A || !out) return fail(DNSB_ERR_ARG, "null argument");
+  if (M < 1 || N < 1 || lda < N) return fail(DNSB_ERR_ARG, "invalid sizes");
+  DNSB_LAUNCH(launch_mlp_colsum(A, bf16, M, N, lda, out, as_stream(stream)));
+  return 0;
+}
+
+extern "C" int dnsb_mlp_adam(float* w, float* m, float* v, const float* grad, void* wb,
+                             long long n, float lr, float b1, float b2, float eps, int step,
+                             void* stream) {
+  if (!w || !m || !v || !grad) return fail(DNSB_ERR_ARG, "null argument");
+  if (n < 1 || step < 1) return fail(DNSB_ERR_ARG, "invalid sizes");
+  DNSB_LAUNCH(launch_mlp_adam(w, m, v, grad, wb, n, lr, b1, b2, eps, step, as_stream(stream)));
+  return 0;
+}
+
+// ===========================================================================
 // Influence-matrix precompute on the GPU
 // ===========================================================================
 extern "C" int dnsb_imm_precompute(const double* D1, const double* D2, const double* kx,

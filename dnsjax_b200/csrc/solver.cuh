@@ -144,6 +144,25 @@ struct ImmPrecomputeArgs {
 // bp: nkz*nkx*ny*2 doubles, bv: nkz*nkx*ny*4 doubles of workspace.
 cudaError_t launch_imm_precompute(const ImmPrecomputeArgs& a, double* bp, double* bv,
                                   cudaStream_t st, int* launches);
+// Learned corrector guess (csrc/learned.cu): BF16 MLP kernels.
+cudaError_t launch_mlp_gemm(int ta, int tb, int M, int N, int K, const void* A, int lda,
+                            const void* B, int ldb, const float* bias, int relu,
+                            const void* mask, int ldm, float* Cf, void* Cb, int ldc,
+                            cudaStream_t st);
+cudaError_t launch_learned_features(const double2* un, const double2* up, const double2* dprev,
+                                    const double2* target, const double* kx, const double* kz,
+                                    int NKX, int NZ1, int Ny, double kx_max, double kz_max,
+                                    double s_floor, void* X, int ldx, float* T, int ldt,
+                                    float* scale, cudaStream_t st);
+cudaError_t launch_learned_guess(const double2* up, const float* Y, int ldy, const float* scale,
+                                 int NM, int Ny, double2* out, cudaStream_t st);
+cudaError_t launch_mlp_loss_grad(const float* Y, const float* T, int M, int N, int ld, float* dYf,
+                                 void* dYb, float* err, float* ref, cudaStream_t st);
+cudaError_t launch_mlp_colsum(const void* A, int bf16, int M, int N, int lda, float* out,
+                              cudaStream_t st);
+cudaError_t launch_mlp_adam(float* w, float* m, float* v, const float* grad, void* wb,
+                            long long n, float lr, float b1, float b2, float eps, int step,
+                            cudaStream_t st);
 bool imm_batch_supported(int kl, int ny);
 size_t imm_batch_stage_smem(int Ny);
 int imm_nu(int kl, int row0);

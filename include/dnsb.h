@@ -234,6 +234,46 @@ int dnsb_couette_norm_noalloc(const void* v, int nx, int ny, int nz, double ly,
                               double* out_dev, void* stream);
 
 /* ------------------------------------------------------------------ */
+/* Learned corrector guess for plane Couette (no counterpart in the     */
+/* reference): kernels of a per-(kz, kx)-mode MLP, BF16 weights and     */
+/* activations, FP32 accumulation, trained online on the pairs          */
+/* (predictor -> converged correction) the solver generates.  The       */
+/* guess replaces the predictor's output before the first correction;   */
+/* the corrector still iterates to the tolerance from it.  Every array  */
+/* is device memory.                                                    */
+/* ------------------------------------------------------------------ */
+/* C[m][n] = sum_k A(m, k) B(n, k) on the tensor cores (BF16 operands,
+ * FP32 accumulation); A(m, k) = ta ? A[k lda + m] : A[m lda + k],
+ * B(n, k) = tb ? B[k ldb + n] : B[n ldb + k].  Epilogue: + bias[n] (FP32,
+ * optional), max(., 0) when relu, times (mask[m ldm + n] > 0) when mask
+ * (BF16) is given; written to Cf (FP32) and / or Cb (BF16) at [m ldc + n]. */
+int dnsb_mlp_gemm(int ta, int tb, int M, int N, int K, const void* A, int lda, const void* B,
+                  int ldb, const float* bias, int relu, const void* mask, int ldm, float* Cf,
+                  void* Cb, int ldc, void* stream);
+/* Features of every mode m (spectral layout (3, nz-1, nx/2, ny) complex128):
+ * X[m][((F*3 + c)*ny + y)*2 + part] (BF16) with F = 0: (up - un) / s_m,
+ * F = 1: dprev / s_m (zero when dprev is NULL), then kx / kx_max,
+ * kz / kz_max at 12 ny, 12 ny + 1; scale[m] = s_m = rms of up - un over
+ * the mode, at least s_floor; T[m][(c*ny + y)*2 + part] = target / s_m (FP32) when target is
+ * given.  ldx >= 12 ny + 2, ldt >= 6 ny. */
+int dnsb_learned_features(dnsb_couette* ctx, const void* un, const void* up, const void* dprev,
+                          const void* target, double kx_max, double kz_max, double s_floor,
+                          void* X, int ldx, float* T, int ldt, float* scale, void* stream);
+/* out = up + scale[m] * Y[m][(c*ny + y)*2 + part] (complex128 out). */
+int dnsb_learned_guess(dnsb_couette* ctx, const void* up, const float* Y, int ldy,
+                       const float* scale, void* out, void* stream);
+/* Mean-squared-error gradient dY = 2 (Y - T) / M (FP32 dYf and BF16 dYb),
+ * err[m] = sum_n (Y - T)^2, ref[m] = sum_n T^2. */
+int dnsb_mlp_loss_grad(const float* Y, const float* T, int M, int N, int ld, float* dYf,
+                       void* dYb, float* err, float* ref, void* stream);
+/* out[n] = sum_m A[m lda + n]; A is BF16 when bf16 != 0, else FP32. */
+int dnsb_mlp_colsum(const void* A, int bf16, int M, int N, int lda, float* out, void* stream);
+/* One Adam update (step >= 1, bias-corrected) of FP32 weights w with
+ * moments m, v from grad; wb (BF16, optional) gets the rounded weights. */
+int dnsb_mlp_adam(float* w, float* m, float* v, const float* grad, void* wb, long long n,
+                  float lr, float b1, float b2, float eps, int step, void* stream);
+
+/* ------------------------------------------------------------------ */
 /* Influence-matrix precompute on the GPU (precompute_imm, banded      */
 /* backend, geometries/cartesian.py:575-801).  For every (kz, kx) mode  */
 /* (k2 = kx^2 + kz^2): L_k = D2 - k2 I with Neumann wall rows (row 0    */
