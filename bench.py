@@ -111,20 +111,24 @@ def grid_points(w):
     return nxp * nyp * nzp
 
 
-def op_bytes(w):
-    """Algorithmic HBM bytes of one RHS and one corrector IMM launch."""
+def op_bytes(w, fp32=False):
+    """Algorithmic HBM bytes of one RHS and one corrector IMM launch.  The
+    state read and the RHS write are complex128 (cb = 16 bytes); the pass
+    buffers between the transform passes are complex64 (8 bytes) in the
+    mixed form (fp32)."""
     cb = 16
+    pb = 8 if fp32 else 16
     nkx, ny, nz = w["nx"] // 2, w["ny"], w["nz"]
     if w["system"] == "plane-couette":
         nkz, mz, p = nz - 1, 3 * nz // 2, w["p"]
         K = nkz * nkx
-        rhs = cb * nkx * ny * (6 * nkz + 18 * mz)
+        rhs = nkx * ny * (cb * 6 * nkz + pb * 18 * mz)
         imm = K * ny * (12 * cb + 2 * (3 * p + 1) * 8 + 2 * 4 + 4 * 8 + 3 * cb) + 32 * K
         return {"rhs": rhs, "imm": imm}
     ny1, nz1 = ny - 1, nz - 1
     my, mz = 3 * ny // 2, 3 * nz // 2
     S, A1, A2 = ny1 * nz1 * nkx, my * nz1 * nkx, my * mz * nkx
-    return {"rhs": cb * (6 * S + 18 * A1 + 18 * A2), "correct": cb * 12 * S}
+    return {"rhs": cb * 6 * S + pb * (18 * A1 + 18 * A2), "correct": cb * 12 * S}
 
 
 # DRAM bytes (read + write) of one call, summed over the call's kernels, from
@@ -289,8 +293,6 @@ def run_ours(a, w, rank, world):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     mixed = a.form == "mixed"
-    if mixed and w["system"] != "plane-couette":
-        raise SystemExit("--form mixed is built for plane Couette")
     p = params_for(w, fp64=not mixed)
     if w["system"] == "plane-couette":
         from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
@@ -399,7 +401,7 @@ def run_ours(a, w, rank, world):
     state_bytes = state.numel() * state.element_size()
 
     # Roofline of the dominant op (events inside the timed region).
-    ob = op_bytes(w)
+    ob = op_bytes(w, fp32=mixed)
     rhs_ms = tf.durations_ms("rhs")
     imm_ms = tf.durations_ms("imm")
     tot = {"rhs": sum(rhs_ms), "imm": sum(imm_ms)}
@@ -460,7 +462,7 @@ def run_ours(a, w, rank, world):
             "peak": peak,
             "unit": "GB/s",
             "frac": achieved / peak,
-            "traffic": MEASURED_TRAFFIC.get(a.workload, {}).get(dom),
+            "traffic": None if mixed else MEASURED_TRAFFIC.get(a.workload, {}).get(dom),
             "peak_source": "measured" if peaks else "fallback",
             "algorithmic_bytes_per_launch": bytes_,
             "avg_launch_ms": dur,
@@ -477,9 +479,10 @@ def run_ours(a, w, rank, world):
     if mixed:
         # Error of the mixed form after the warm-up + timed steps, against the
         # plain FP64 form advanced the same number of steps from the same field.
-        from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
-
-        plain = PlaneCouetteFlow(params_for(w, fp64=True))
+        if w["system"] == "plane-couette":
+            plain = PlaneCouetteFlow(params_for(w, fp64=True))
+        else:
+            plain = TriplyPeriodicFlow(params_for(w, fp64=True), ly=w["ly"])
         ps = plain.make_stepper()
         ref = torch.as_tensor(u0, device="cuda")
         for _ in range(traj_steps):
@@ -490,6 +493,9 @@ def run_ours(a, w, rank, world):
         out["config"]["vs_plain"] = {"steps": traj_steps,
                                      "ke_rel_err": abs(ke_m - ke_p) / ke_p,
                                      "field_rel_l2": float(diff.item())}
+        if w["system"] != "plane-couette":
+            d_m, d_p = plain.get_stats(state)["D"], plain.get_stats(ref)["D"]
+            out["config"]["vs_plain"]["dissipation_rel_err"] = abs(d_m - d_p) / abs(d_p)
         out["dtype"] = "f32 (RHS passes) + f64"
     if w["system"] == "plane-couette":
         # Setup: the influence-matrix operators of this workload on the GPU

@@ -91,6 +91,7 @@ SIGNATURES = {
     "dnsb_couette_spec_to_phys": (c_int, [c_void_p] * 4),
     "dnsb_couette_phys_to_spec": (c_int, [c_void_p] * 4),
     "dnsb_couette_check": (c_int, [c_void_p, c_void_p]),
+    "dnsb_periodic_set_rhs_precision": (c_int, [c_void_p, c_int]),
     "dnsb_couette_set_rhs_precision": (c_int, [c_void_p, c_int]),
     "dnsb_mlp_gemm": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p,
                               c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_int,

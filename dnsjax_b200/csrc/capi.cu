@@ -99,12 +99,14 @@ struct dnsb_periodic {
   double c;
   FFTPlan py, pz, px;
   double2 *twy = nullptr, *twz = nullptr, *twx = nullptr;
+  float2 *twy32 = nullptr, *twz32 = nullptr, *twx32 = nullptr;
   double *kx = nullptr, *ky = nullptr, *kz = nullptr;
   double *U = nullptr, *cU = nullptr, *nU = nullptr;
   double *ldt1 = nullptr, *ildt2 = nullptr, *lapl = nullptr, *inv_lapl = nullptr;
   double2 *A = nullptr, *B = nullptr;
   double* partials = nullptr;
   size_t ws_bytes = 0;
+  int rhs_fp32 = 0;  // RHS transforms and product in FP32 (pass buffers float2)
 
   PeriodicPointArgs point() const {
     PeriodicPointArgs a;
@@ -125,9 +127,9 @@ struct dnsb_periodic {
 };
 
 static void periodic_free(dnsb_periodic* p) {
-  void* ptrs[] = {p->twy, p->twz, p->twx, p->kx, p->ky, p->kz, p->U, p->cU,
-                  p->nU, p->ldt1, p->ildt2, p->lapl, p->inv_lapl, p->A, p->B,
-                  p->partials};
+  void* ptrs[] = {p->twy, p->twz, p->twx, p->twy32, p->twz32, p->twx32, p->kx, p->ky,
+                  p->kz, p->U, p->cU, p->nU, p->ldt1, p->ildt2, p->lapl, p->inv_lapl,
+                  p->A, p->B, p->partials};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete p;
@@ -163,7 +165,7 @@ extern "C" int dnsb_periodic_create(const dnsb_periodic_desc* d,
   const int smax = max_smem_optin();
   const size_t need[] = {col_pass_smem(p->Mz), x_pass_smem(p->Mx),
                          x_phys_smem(p->Mx), x_fwd_smem(p->Mx),
-                         yinv_smem(p->My, p->NY1), yfwd_smem(p->My, p->NY1)};
+                         yinv_smem(p->My, p->NY1, 0), yfwd_smem(p->My, p->NY1, 0)};
   for (size_t n : need)
     if ((int)n > smax) {
       periodic_free(p);
@@ -176,6 +178,9 @@ extern "C" int dnsb_periodic_create(const dnsb_periodic_desc* d,
   chk(make_twiddles(&p->twy, p->My));
   chk(make_twiddles(&p->twz, p->Mz));
   chk(make_twiddles(&p->twx, p->Mx));
+  chk(make_twiddles32(&p->twy32, p->My));
+  chk(make_twiddles32(&p->twz32, p->Mz));
+  chk(make_twiddles32(&p->twx32, p->Mx));
   chk(upload(&p->kx, d->kx, p->NKX));
   chk(upload(&p->ky, d->ky, p->NY1));
   chk(upload(&p->kz, d->kz, p->NZ1));
@@ -286,9 +291,14 @@ extern "C" int dnsb_periodic_rhs(dnsb_periodic* p, const void* state,
   yi.ky = p->ky;
   yi.kz = p->kz;
   yi.plan = p->py;
-  yi.tw = p->twy;
+  const int f32 = p->rhs_fp32;
+  yi.tw = f32 ? reinterpret_cast<const double2*>(p->twy32) : p->twy;
+  yi.fp32 = f32;
   DNSB_LAUNCH(launch_yinv(yi, st));
-  DNSB_LAUNCH(launch_col_pass(periodic_zinv(p), 6, p->My, st));
+  ColPassArgs zi = periodic_zinv(p);
+  zi.fp32 = zi.out32 = f32;
+  if (f32) zi.tw = reinterpret_cast<const double2*>(p->twz32);
+  DNSB_LAUNCH(launch_col_pass(zi, 6, p->My, st));
   XPassArgs xa{};
   xa.in = p->B;
   xa.out = p->B;
@@ -306,9 +316,13 @@ extern "C" int dnsb_periodic_rhs(dnsb_periodic* p, const void* state,
   xa.nU = p->nU;
   xa.ny_grid = p->My;
   xa.plan = p->px;
-  xa.tw = p->twx;
+  xa.tw = f32 ? reinterpret_cast<const double2*>(p->twx32) : p->twx;
+  xa.fp32 = f32;
   DNSB_LAUNCH(launch_x_pass(xa, st));
-  DNSB_LAUNCH(launch_col_pass(periodic_zfwd(p), 3, p->My, st));
+  ColPassArgs zf = periodic_zfwd(p);
+  zf.fp32 = zf.out32 = f32;
+  if (f32) zf.tw = reinterpret_cast<const double2*>(p->twz32);
+  DNSB_LAUNCH(launch_col_pass(zf, 3, p->My, st));
   YFwdArgs yf{};
   yf.in = p->A;
   yf.out = (double2*)rhs;
@@ -321,8 +335,21 @@ extern "C" int dnsb_periodic_rhs(dnsb_periodic* p, const void* state,
   yf.kz = p->kz;
   yf.inv_lapl = p->inv_lapl;
   yf.plan = p->py;
-  yf.tw = p->twy;
+  yf.tw = f32 ? reinterpret_cast<const double2*>(p->twy32) : p->twy;
+  yf.fp32 = f32;
   DNSB_LAUNCH(launch_yfwd(yf, st));
+  return 0;
+}
+
+extern "C" int dnsb_periodic_set_rhs_precision(dnsb_periodic* p, int fp32) {
+  if (!p) return fail(DNSB_ERR_ARG, "null argument");
+  if (fp32) {
+    auto fixed = [](int L) { return L == 48 || L == 72 || L == 96 || L == 192; };
+    if (!fixed(p->My) || !fixed(p->Mz) || !fixed(p->Mx) || 3 * p->NKX != p->Mx)
+      return fail(DNSB_ERR_ARG,
+                  "FP32 RHS passes need padded sizes in {48, 72, 96, 192} with nx_p = 3 nx / 2");
+  }
+  p->rhs_fp32 = fp32 ? 1 : 0;
   return 0;
 }
 

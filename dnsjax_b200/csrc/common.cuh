@@ -228,10 +228,11 @@ __host__ __device__ constexpr int cplan_nst(int L) {
   return s;
 }
 
-template <int L, int R, int C, int NS, int SIGN, int NT>
-__device__ __forceinline__ void fft_stage_t(const double2* __restrict__ in,
-                                            double2* __restrict__ out,
-                                            const double2* __restrict__ tw) {
+// CT: the complex type of the columns and twiddles (double2, or float2).
+template <int L, int R, int C, int NS, int SIGN, int NT, typename CT = double2>
+__device__ __forceinline__ void fft_stage_t(const CT* __restrict__ in,
+                                            CT* __restrict__ out,
+                                            const CT* __restrict__ tw) {
   constexpr int NB = L / R;
   constexpr int STEP = L / (NS * R);
   constexpr int TOTAL = NB * C;
@@ -240,13 +241,13 @@ __device__ __forceinline__ void fft_stage_t(const double2* __restrict__ in,
     const int c = idx % C;
     const int j = idx / C;
     const int k = j % NS;
-    double2 v[R];
+    CT v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = in[(j + r * NB) * C + c];
     if (NS > 1) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        double2 w = tw[r * k * STEP];
+        CT w = tw[r * k * STEP];
         if (SIGN > 0) w.y = -w.y;
         v[r] = cmul(v[r], w);
       }
@@ -261,36 +262,34 @@ __device__ __forceinline__ void fft_stage_t(const double2* __restrict__ in,
   }
 }
 
-template <int L, int C, int SIGN, int NT, int S = 0, int NS = 1>
-__device__ __forceinline__ double2* fft_stages_t(double2* a, double2* b,
-                                                 const double2* tw) {
+template <int L, int C, int SIGN, int NT, int S = 0, int NS = 1, typename CT = double2>
+__device__ __forceinline__ CT* fft_stages_t(CT* a, CT* b, const CT* tw) {
   if constexpr (S >= cplan_nst(L)) {
     return a;
   } else {
     constexpr int R = cplan_radix(L, S);
-    fft_stage_t<L, R, C, NS, SIGN, NT>(a, b, tw);
+    fft_stage_t<L, R, C, NS, SIGN, NT, CT>(a, b, tw);
     __syncthreads();
-    return fft_stages_t<L, C, SIGN, NT, S + 1, NS * R>(b, a, tw);
+    return fft_stages_t<L, C, SIGN, NT, S + 1, NS * R, CT>(b, a, tw);
   }
 }
 
 // Compile-time-planned version of fft_columns (blockDim.x must equal NT).
-template <int L, int C, int SIGN, int NT>
-__device__ __forceinline__ double2* fft_columns_t(double2* a, double2* b,
-                                                  const double2* tw) {
-  return fft_stages_t<L, C, SIGN, NT>(a, b, tw);
+template <int L, int C, int SIGN, int NT, typename CT = double2>
+__device__ __forceinline__ CT* fft_columns_t(CT* a, CT* b, const CT* tw) {
+  return fft_stages_t<L, C, SIGN, NT, 0, 1, CT>(a, b, tw);
 }
 
 // Dispatch: ML > 0 uses the compile-time plan for length ML, ML == 0 the
-// runtime plan.
-template <int ML, int C, int NT>
-__device__ __forceinline__ double2* fft_cols(double2* a, double2* b,
-                                             const FFTPlan& P, int sign,
-                                             const double2* tw) {
+// runtime plan (FP64 only).
+template <int ML, int C, int NT, typename CT = double2>
+__device__ __forceinline__ CT* fft_cols(CT* a, CT* b, const FFTPlan& P, int sign,
+                                        const CT* tw) {
   if constexpr (ML > 0) {
-    if (sign > 0) return fft_columns_t<ML, C, 1, NT>(a, b, tw);
-    return fft_columns_t<ML, C, -1, NT>(a, b, tw);
+    if (sign > 0) return fft_columns_t<ML, C, 1, NT, CT>(a, b, tw);
+    return fft_columns_t<ML, C, -1, NT, CT>(a, b, tw);
   } else {
+    static_assert(std::is_same<CT, double2>::value, "runtime-planned FFTs are FP64");
     return fft_columns(a, b, P, C, sign, tw);
   }
 }

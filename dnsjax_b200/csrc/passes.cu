@@ -124,9 +124,9 @@ size_t col_pass2_smem(int M) {
 }
 
 // T: the compute type and the element type of `in` (double, or float for the
-// FP32 form of the Couette RHS, whose pass buffer holds float2); `out` is
-// always complex128.
-template <int ML, int SIGN, typename T = double>
+// FP32 forms, whose pass buffers hold float2); `out` is complex128, or with
+// OUT32 (FP32 only) an FP32 pass buffer.
+template <int ML, int SIGN, typename T = double, bool OUT32 = false>
 __global__ void __launch_bounds__(kC2Threads)
 col_pass2_kernel(ColPassArgs a) {
   using CT = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
@@ -139,7 +139,9 @@ col_pass2_kernel(ColPassArgs a) {
   const long long o = blockIdx.y;
   const long long f = blockIdx.z;
   const CT* in = reinterpret_cast<const CT*>(a.in) + f * a.in_fs + o * a.in_os + i0;
+  // FP64 output, or (OUT32, FP32 arithmetic) an FP32 pass buffer
   double2* out = a.out + f * a.out_fs + o * a.out_os + i0;
+  CT* out_c = reinterpret_cast<CT*>(a.out) + f * a.out_fs + o * a.out_os + i0;
   const int ni = min(C, a.nI - i0);
   load_twiddles(tw, reinterpret_cast<const CT*>(a.tw), M);
   __syncthreads();
@@ -183,10 +185,14 @@ col_pass2_kernel(ColPassArgs a) {
       for (int i = 0; i < 8; ++i) {
         const int t = k + R1 * i;
         if (SIGN > 0) {
-          out[t * a.out_ts + c] = to_d(z[i]);
+          if (OUT32) out_c[t * a.out_ts + c] = z[i];
+          else out[t * a.out_ts + c] = to_d(z[i]);
         } else {
           const int sidx = pos_to_stored(t, a.nstored, M);
-          if (sidx >= 0) out[sidx * a.out_ts + c] = cscale(to_d(z[i]), sc);
+          if (sidx >= 0) {
+            if (OUT32) out_c[sidx * a.out_ts + c] = cscale(z[i], (T)sc);
+            else out[sidx * a.out_ts + c] = cscale(to_d(z[i]), sc);
+          }
         }
       }
     }
@@ -199,12 +205,19 @@ cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
   if (L == 48 || L == 72 || L == 96 || L == 192) {
     dim3 g2((a.nI + kC2Cols - 1) / kC2Cols, nO, nfields);
     const size_t sm2 = a.fp32 ? col_pass2_smem(L) / 2 : col_pass2_smem(L);
-    if (a.fp32 && a.inverse) return cudaErrorInvalidValue;  // forward only
-#define DNSB_C2(LL)                                                              \
-  case LL:                                                                       \
-    if (a.fp32) col_pass2_kernel<LL, -1, float><<<g2, kC2Threads, sm2, st>>>(a);  \
-    else if (a.inverse) col_pass2_kernel<LL, 1><<<g2, kC2Threads, sm2, st>>>(a);  \
-    else col_pass2_kernel<LL, -1><<<g2, kC2Threads, sm2, st>>>(a);               \
+    if (a.fp32 && a.inverse && !a.out32) return cudaErrorInvalidValue;
+#define DNSB_C2(LL)                                                                     \
+  case LL:                                                                              \
+    if (a.fp32 && a.inverse)                                                            \
+      col_pass2_kernel<LL, 1, float, true><<<g2, kC2Threads, sm2, st>>>(a);             \
+    else if (a.fp32 && a.out32)                                                         \
+      col_pass2_kernel<LL, -1, float, true><<<g2, kC2Threads, sm2, st>>>(a);            \
+    else if (a.fp32)                                                                    \
+      col_pass2_kernel<LL, -1, float><<<g2, kC2Threads, sm2, st>>>(a);                  \
+    else if (a.inverse)                                                                 \
+      col_pass2_kernel<LL, 1><<<g2, kC2Threads, sm2, st>>>(a);                          \
+    else                                                                                \
+      col_pass2_kernel<LL, -1><<<g2, kC2Threads, sm2, st>>>(a);                         \
     break;
     switch (L) { DNSB_C2(48) DNSB_C2(72) DNSB_C2(96) DNSB_C2(192) }
 #undef DNSB_C2
@@ -731,26 +744,30 @@ cudaError_t launch_x_fwd(const XPhysArgs& a, const double* phys, double2* spec,
 // ---------------------------------------------------------------------------
 // Periodic first inverse pass (y) with the spectral curl fused.
 // ---------------------------------------------------------------------------
-size_t yinv_smem(int My, int NY1) {
-  return sizeof(double2) * (size_t)(3 * NY1 * kTile + 2 * My * kTile + My);
+// FP32 form: the state columns and the curl stay FP64 (su); the transform
+// buffers, twiddles and the output pass buffer are FP32.
+size_t yinv_smem(int My, int NY1, int fp32) {
+  const size_t cb = fp32 ? sizeof(float2) : sizeof(double2);
+  return sizeof(double2) * (size_t)(3 * NY1 * kTile) + cb * (size_t)(2 * My * kTile + My);
 }
 
-template <int ML>
+template <int ML, typename T = double>
 __global__ void __launch_bounds__(kPassThreads)
 yinv_kernel(YInvArgs a) {
+  using CT = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
   extern __shared__ double2 sm[];
   const int M = ML > 0 ? ML : a.plan.L;
   const int C = kTile;
   const int NY1 = a.NY1, NZ1 = a.NZ1, NKX = a.NKX;
   double2* su = sm;                       // [3][NY1][C]
-  double2* bufA = su + 3 * NY1 * C;
-  double2* bufB = bufA + M * C;
-  double2* tw = bufB + M * C;
+  CT* bufA = reinterpret_cast<CT*>(su + 3 * NY1 * C);
+  CT* bufB = bufA + M * C;
+  CT* tw = bufB + M * C;
   const int i0 = blockIdx.x * C;
   const int iz = blockIdx.y;
   const int ni = min(C, NKX - i0);
   const long long cs = (long long)NY1 * NZ1 * NKX;
-  load_twiddles(tw, a.tw, M);
+  load_twiddles(tw, reinterpret_cast<const CT*>(a.tw), M);
   for (int idx = threadIdx.x; idx < 3 * NY1 * C; idx += blockDim.x) {
     const int c = idx % C, s = (idx / C) % NY1, comp = idx / (C * NY1);
     double2 v = make_double2(0.0, 0.0);
@@ -781,11 +798,11 @@ yinv_kernel(YInvArgs a) {
           default: v = ci(make_double2(kx * vv.x - ky * u.x, kx * vv.y - ky * u.y)); break;
         }
       }
-      bufA[idx] = v;
+      bufA[idx] = to_c(v, (CT*)nullptr);
     }
     __syncthreads();
-    const double2* res = fft_cols<ML, C, kPassThreads>(bufA, bufB, a.plan, 1, tw);
-    double2* out = a.out + f * fs + (long long)iz * NKX + i0;
+    const CT* res = fft_cols<ML, C, kPassThreads, CT>(bufA, bufB, a.plan, 1, tw);
+    CT* out = reinterpret_cast<CT*>(a.out) + f * fs + (long long)iz * NKX + i0;
     for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
       const int c = idx % C, t = idx / C;
       if (c < ni) out[(long long)t * NZ1 * NKX + c] = res[idx];
@@ -796,48 +813,64 @@ yinv_kernel(YInvArgs a) {
 
 cudaError_t launch_yinv(const YInvArgs& a, cudaStream_t st) {
   dim3 grid((a.NKX + kTile - 1) / kTile, a.NZ1);
-  DNSB_DISPATCH(a.plan.L, yinv_kernel, grid, yinv_smem(a.plan.L, a.NY1), st, a);
+  if (a.fp32) {
+    const size_t sm = yinv_smem(a.plan.L, a.NY1, 1);
+    switch (a.plan.L) {
+      case 48: yinv_kernel<48, float><<<grid, kPassThreads, sm, st>>>(a); break;
+      case 72: yinv_kernel<72, float><<<grid, kPassThreads, sm, st>>>(a); break;
+      case 96: yinv_kernel<96, float><<<grid, kPassThreads, sm, st>>>(a); break;
+      case 192: yinv_kernel<192, float><<<grid, kPassThreads, sm, st>>>(a); break;
+      default: return cudaErrorInvalidValue;  // compile-time sizes only
+    }
+    return cudaGetLastError();
+  }
+  DNSB_DISPATCH(a.plan.L, yinv_kernel, grid, yinv_smem(a.plan.L, a.NY1, 0), st, a);
   return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
 // Periodic last forward pass (y) with the pressure projection fused.
 // ---------------------------------------------------------------------------
-size_t yfwd_smem(int My, int NY1) {
-  return sizeof(double2) * (size_t)(3 * NY1 * kTile + 2 * My * kTile + My);
+// FP32 form: the input pass buffer, transform buffers and twiddles are
+// FP32; the transformed rows are scaled into FP64 (snl) and the projection
+// and the output RHS are FP64.
+size_t yfwd_smem(int My, int NY1, int fp32) {
+  const size_t cb = fp32 ? sizeof(float2) : sizeof(double2);
+  return sizeof(double2) * (size_t)(3 * NY1 * kTile) + cb * (size_t)(2 * My * kTile + My);
 }
 
-template <int ML>
+template <int ML, typename T = double>
 __global__ void __launch_bounds__(kPassThreads)
 yfwd_kernel(YFwdArgs a) {
+  using CT = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
   extern __shared__ double2 sm[];
   const int M = ML > 0 ? ML : a.plan.L;
   const int C = kTile;
   const int NY1 = a.NY1, NZ1 = a.NZ1, NKX = a.NKX;
   double2* snl = sm;  // [3][NY1][C]
-  double2* bufA = snl + 3 * NY1 * C;
-  double2* bufB = bufA + M * C;
-  double2* tw = bufB + M * C;
+  CT* bufA = reinterpret_cast<CT*>(snl + 3 * NY1 * C);
+  CT* bufB = bufA + M * C;
+  CT* tw = bufB + M * C;
   const int i0 = blockIdx.x * C;
   const int iz = blockIdx.y;
   const int ni = min(C, NKX - i0);
-  load_twiddles(tw, a.tw, M);
+  load_twiddles(tw, reinterpret_cast<const CT*>(a.tw), M);
   const long long fs = (long long)M * NZ1 * NKX;
   const double sc = 1.0 / M;
   for (int f = 0; f < 3; ++f) {
-    const double2* in = a.in + f * fs + (long long)iz * NKX + i0;
+    const CT* in = reinterpret_cast<const CT*>(a.in) + f * fs + (long long)iz * NKX + i0;
     for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
       const int c = idx % C, t = idx / C;
-      double2 v = make_double2(0.0, 0.0);
+      CT v = cmake<CT>(0, 0);
       if (c < ni) v = in[(long long)t * NZ1 * NKX + c];
       bufA[idx] = v;
     }
     __syncthreads();
-    const double2* res = fft_cols<ML, C, kPassThreads>(bufA, bufB, a.plan, -1, tw);
+    const CT* res = fft_cols<ML, C, kPassThreads, CT>(bufA, bufB, a.plan, -1, tw);
     for (int idx = threadIdx.x; idx < NY1 * C; idx += blockDim.x) {
       const int c = idx % C, s = idx / C;
       const int t = stored_to_pos(s, NY1, M);
-      snl[(f * NY1 + s) * C + c] = cscale(res[t * C + c], sc);
+      snl[(f * NY1 + s) * C + c] = cscale(to_d(res[t * C + c]), sc);
     }
     __syncthreads();
   }
@@ -869,7 +902,18 @@ yfwd_kernel(YFwdArgs a) {
 
 cudaError_t launch_yfwd(const YFwdArgs& a, cudaStream_t st) {
   dim3 grid((a.NKX + kTile - 1) / kTile, a.NZ1);
-  DNSB_DISPATCH(a.plan.L, yfwd_kernel, grid, yfwd_smem(a.plan.L, a.NY1), st, a);
+  if (a.fp32) {
+    const size_t sm = yfwd_smem(a.plan.L, a.NY1, 1);
+    switch (a.plan.L) {
+      case 48: yfwd_kernel<48, float><<<grid, kPassThreads, sm, st>>>(a); break;
+      case 72: yfwd_kernel<72, float><<<grid, kPassThreads, sm, st>>>(a); break;
+      case 96: yfwd_kernel<96, float><<<grid, kPassThreads, sm, st>>>(a); break;
+      case 192: yfwd_kernel<192, float><<<grid, kPassThreads, sm, st>>>(a); break;
+      default: return cudaErrorInvalidValue;  // compile-time sizes only
+    }
+    return cudaGetLastError();
+  }
+  DNSB_DISPATCH(a.plan.L, yfwd_kernel, grid, yfwd_smem(a.plan.L, a.NY1, 0), st, a);
   return cudaGetLastError();
 }
 
@@ -1202,7 +1246,14 @@ cudaError_t set_pass_attributes(int max_smem) {
                        (const void*)col_pass2_kernel<48, 1>, (const void*)col_pass2_kernel<48, -1>,
                        (const void*)col_pass2_kernel<72, 1>, (const void*)col_pass2_kernel<72, -1>,
                        (const void*)col_pass2_kernel<96, 1>, (const void*)col_pass2_kernel<96, -1>,
-                       (const void*)col_pass2_kernel<192, 1>, (const void*)col_pass2_kernel<192, -1>};
+                       (const void*)col_pass2_kernel<192, 1>, (const void*)col_pass2_kernel<192, -1>,
+#define DNSB_F32_PASSES(L)                                                          \
+  (const void*)yinv_kernel<L, float>, (const void*)yfwd_kernel<L, float>,           \
+      (const void*)col_pass2_kernel<L, 1, float, true>,                             \
+      (const void*)col_pass2_kernel<L, -1, float, true>
+                       DNSB_F32_PASSES(48), DNSB_F32_PASSES(72), DNSB_F32_PASSES(96),
+                       DNSB_F32_PASSES(192)};
+#undef DNSB_F32_PASSES
   for (const void* f : fns) {
     cudaError_t r = allow_dynamic_smem(f, max_smem);
     if (r != cudaSuccess) e = r;

@@ -31,6 +31,7 @@ struct ColPassArgs {
   FFTPlan plan;  // transform length M = plan.L
   const double2* tw;
   int fp32;            // `in` and arithmetic in FP32 (compile-time sizes)
+  int out32;           // with fp32: `out` is an FP32 pass buffer (always for inverse)
 };
 
 // x pass.  Rows are (outer, inner) pairs; row r = outer * inner_n + inner
@@ -79,6 +80,7 @@ struct YInvArgs {
   const double* kz;
   FFTPlan plan;
   const double2* tw;
+  int fp32;  // FP32 transform and output pass buffer (tw: float2 table)
 };
 
 // Periodic last forward pass (y), projection fused: [3][My][NZ1][NKX] ->
@@ -94,6 +96,7 @@ struct YFwdArgs {
   const double* inv_lapl;  // [NY1][NZ1][NKX]
   FFTPlan plan;
   const double2* tw;
+  int fp32;  // FP32 input pass buffer and transform (tw: float2 table)
 };
 
 // Couette first inverse pass (z), FD curl fused: spectral
@@ -119,8 +122,8 @@ constexpr int kZTile = 8;  // y values per CTA in the Couette z passes
 size_t col_pass_smem(int M);
 size_t x_pass_smem(int Mx);
 size_t x_phys_smem(int Mx);
-size_t yinv_smem(int My, int NY1);
-size_t yfwd_smem(int My, int NY1);
+size_t yinv_smem(int My, int NY1, int fp32);
+size_t yfwd_smem(int My, int NY1, int fp32);
 size_t zinv_curl_smem(int Mz, int NZ1, int span_max);
 size_t zinv_curl2_smem(int M);
 

@@ -33,8 +33,11 @@ class TriplyPeriodicFlow:
             d.ly = ly
         self.ly = float(d.ly)
         r = p.res
-        if r.double_precision is False:
-            raise NotImplementedError("the plain form computes in FP64")
+        # res.double_precision = False (parameters.py:63 of the reference)
+        # selects the mixed form: the RHS transforms and product in FP32,
+        # the state, the curl, the projection, the corrector and the norms in
+        # FP64.
+        self.rhs_fp32 = r.double_precision is False
         self.system = p.phys.system
         self.nx, self.ny, self.nz = r.nx, r.ny, r.nz
         self.nx_p, self.ny_p, self.nz_p = padded_sizes(p)
@@ -69,6 +72,8 @@ class TriplyPeriodicFlow:
         _lib.check(L.dnsb_periodic_create(_lib.C.byref(desc), _lib.C.byref(h)))
         self._ctx = h
         self._L = L
+        if self.rhs_fp32:
+            _lib.check(L.dnsb_periodic_set_rhs_precision(self._ctx, 1))
         self._scratch = torch.empty(2, dtype=torch.float64, device="cuda")
 
     def _setup_base_flow(self, d) -> None:

@@ -79,6 +79,13 @@ size_t dnsb_periodic_workspace_bytes(const dnsb_periodic* ctx);
 /* rhs = NL(u) - grad lapl^-1 div NL(u)   (monochromatic.py:366-386) */
 int dnsb_periodic_rhs(dnsb_periodic* ctx, const void* state, void* rhs,
                       void* stream);
+/* res.double_precision = False for the periodic flows (parameters.py:63):
+ * with fp32 != 0 the RHS transforms (y, z, x passes) and the rotational
+ * product run in FP32 on FP32 pass buffers; the state is read, the curl
+ * formed and the projection applied in FP64, and the RHS is written in
+ * complex128.  Only for padded sizes in {48, 72, 96, 192} with
+ * nx_p = 3 nx / 2 (else DNSB_ERR_ARG). */
+int dnsb_periodic_set_rhs_precision(dnsb_periodic* ctx, int fp32);
 /* out = (state ldt_1 + rhs) ildt_2       (monochromatic.py:320-333) */
 int dnsb_periodic_predict(dnsb_periodic* ctx, const void* state,
                           const void* rhs, void* out, void* stream);

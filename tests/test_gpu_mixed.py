@@ -1,4 +1,4 @@
-"""The mixed form of plane Couette (res.double_precision = False): the RHS
+"""The mixed forms (res.double_precision = False): for plane Couette the RHS
 transforms and rotational product in FP32, the state, the influence-matrix
 iteration (banded LU substitutions, 2x2 solve) and every norm in FP64.
 
@@ -12,6 +12,9 @@ iteration (banded LU substitutions, 2x2 solve) and every norm in FP64.
   (about 3e-10 here, about 3e-6 at 128x129x128), so the mixed form is run
   to a tolerance it can reach; the kinetic energy agrees to 1e-6 relative,
   the field to 1e-5 relative L2.
+* The periodic flows (Kolmogorov): the same checks for the FP32 y, z and x
+  passes, the curl and projection staying FP64, with the dissipation
+  compared too.
 """
 
 from math import pi
@@ -93,5 +96,69 @@ def test_couette_mixed_trajectory_64():
     ke = lambda f, u: float(f.norm(u).item()) ** 2 / 2  # noqa: E731
     assert abs(ke(mixed, um) - ke(plain, up)) <= 1e-6 * ke(plain, up)
     a, b = host(um), host(up)
+    for c in range(3):
+        assert rel_l2(a[c], b[c]) <= 1e-5, c
+
+
+# -- the periodic flows (Kolmogorov) ---------------------------------------------
+def kolmogorov_params(n, re, dt, fp64, tol=1e-10, max_iter=60):
+    from dnsjax_b200.parameters import Parameters
+
+    return Parameters(phys=dict(system="kolmogorov", re=re),
+                      geo=dict(lx=2 * pi, lz=2 * pi),
+                      res=dict(nx=n, ny=n, nz=n, double_precision=fp64),
+                      step=dict(dt=dt, corrector_tolerance=tol,
+                                max_corrector_iterations=max_iter))
+
+
+def test_periodic_fp32_rhs_128():
+    """The FP32 RHS passes at 128^3 (padded 192^3) against the FP64 RHS
+    (itself pinned to the oracle by the parity tests): relative L2 per
+    component below 2e-6, and not bit-equal."""
+    from dnsjax_b200 import initial
+    from dnsjax_b200.flows.monochromatic import TriplyPeriodicFlow
+
+    u0 = dev(initial.periodic_field(128, 128, 128, 2 * pi, 2 * pi, 2 * pi, 2,
+                                    initial.kolmogorov_spectrum_k53, 0.5))
+    f64 = TriplyPeriodicFlow(kolmogorov_params(128, 100.0, 0.005, True), ly=2 * pi)
+    f32 = TriplyPeriodicFlow(kolmogorov_params(128, 100.0, 0.005, False), ly=2 * pi)
+    assert f32.rhs_fp32 and not f64.rhs_fp32
+    ref = host(f64.get_rhs(u0))
+    got = host(f32.get_rhs(u0))
+    errs = [rel_l2(got[c], ref[c]) for c in range(3)]
+    assert max(errs) < 2e-6, errs
+    assert max(errs) > 1e-12, errs
+
+
+def test_periodic_fp32_rejects_runtime_sizes():
+    from dnsjax_b200 import _lib
+    from dnsjax_b200.flows.monochromatic import TriplyPeriodicFlow
+
+    # n = 16 pads to 24: no compile-time FP32 pass for that length
+    flow = TriplyPeriodicFlow(kolmogorov_params(16, 40.0, 0.01, True), ly=2 * pi)
+    with pytest.raises(_lib.DnsbError):
+        _lib.check(flow._L.dnsb_periodic_set_rhs_precision(flow._ctx, 1))
+
+
+def test_periodic_mixed_trajectory_64():
+    """Kolmogorov 64^3 (padded 96^3), Re 100, dt 0.005, 20 steps: plain at
+    tolerance 1e-10, mixed at 1e-8 (a tolerance above its FP32 floor);
+    kinetic energy and dissipation within 1e-6 relative, the field within
+    1e-5 relative L2."""
+    from dnsjax_b200 import driver, initial
+    from dnsjax_b200.flows.monochromatic import TriplyPeriodicFlow
+
+    u0 = initial.periodic_field(64, 64, 64, 2 * pi, 2 * pi, 2 * pi, 3,
+                                initial.kolmogorov_spectrum_k53, 0.5)
+    plain = TriplyPeriodicFlow(kolmogorov_params(64, 100.0, 0.005, True), ly=2 * pi)
+    mixed = TriplyPeriodicFlow(kolmogorov_params(64, 100.0, 0.005, False, tol=1e-8),
+                               ly=2 * pi)
+    rp = driver.run(plain, dev(u0), 20)
+    rm = driver.run(mixed, dev(u0), 20)
+    assert rp.converged and rm.converged and rp.steps == rm.steps == 20
+    sp, sm = plain.get_stats(rp.state), plain.get_stats(rm.state)
+    assert abs(sm["E'"] - sp["E'"]) <= 1e-6 * sp["E'"]
+    assert abs(sm["D"] - sp["D"]) <= 1e-6 * abs(sp["D"])
+    a, b = host(rm.state), host(rp.state)
     for c in range(3):
         assert rel_l2(a[c], b[c]) <= 1e-5, c
