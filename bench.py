@@ -582,7 +582,7 @@ def run_learned(a, w, rank, world):
 
     # the network alone: one inference and one training iteration, timed
     net = lg.net
-    flops_fwd = 2.0 * net.M * (net.K1p * net.H + net.H * net.N2)
+    flops_fwd = 2.0 * net.M * (net.K1p * net.H + net.H * net.N2p)
     q0 = torch.cuda.Event(enable_timing=True)
     q1 = torch.cuda.Event(enable_timing=True)
     reps = 10

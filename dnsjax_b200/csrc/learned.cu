@@ -20,6 +20,8 @@
 #include <cuda_bf16.h>
 
 #include <cmath>
+#include <algorithm>
+#include <cstdint>
 
 #include "solver.cuh"
 
@@ -122,6 +124,150 @@ gemm_bf16_kernel(int M, int N, int K, const __nv_bfloat16* __restrict__ A, int l
         const int n = n0 + wn * 32 + nt * 8 + 2 * t + (q & 1);
         if (m >= M || n >= N) continue;
         float v = acc[mt][nt][q];
+        if (bias) v += bias[n];
+        if (relu) v = fmaxf(v, 0.0f);
+        if (mask && !(__bfloat162float(mask[(long long)m * ldm + n]) > 0.0f)) v = 0.0f;
+        if (Cf) Cf[(long long)m * ldc + n] = v;
+        if (Cb) Cb[(long long)m * ldc + n] = __float2bfloat16(v);
+      }
+}
+
+// The same product with 128 x 128 CTA tiles (8 warps of 64 x 32), 16-byte
+// operand loads (8 consecutive BF16 along the operand's contiguous index,
+// which needs lda, ldb multiples of 8 and 16-byte aligned bases) staged
+// through registers one k-tile ahead of the tensor-core loop.  With
+// gridDim.z > 1 (split K, plain FP32 output only) CTA z reduces k in
+// [z kc, (z + 1) kc) and adds its partial sums into Cf atomically.
+constexpr int kBM2 = 128, kBN2 = 128, kBK2 = 32;
+
+template <bool T_, int ROWS>
+struct TileLoad {
+  // One k-tile of an operand X(r, k) (r < ROWS tile rows, k < kBK2): two
+  // 16-byte chunks per thread.  !T_: X[r ld + k] (k contiguous); T_:
+  // X[k ld + r] (r contiguous).
+  uint4 v[2];
+  int r[2], k[2];
+  bool full[2];
+  __device__ __forceinline__ void load(const __nv_bfloat16* X, int ld, int R0, int K0, int nR,
+                                       int nK) {
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int c = threadIdx.x + q * 256;
+      if (!T_) {
+        r[q] = c / (kBK2 / 8);
+        k[q] = (c % (kBK2 / 8)) * 8;
+      } else {
+        // a warp's 32 chunks: 32 different k at one r, so the transposing
+        // shared-memory stores of a warp fall in 16 different banks
+        k[q] = c % kBK2;
+        r[q] = (c / kBK2) * 8;
+      }
+      const int gr = R0 + r[q], gk = K0 + k[q];
+      full[q] = !T_ ? (gr < nR && gk + 8 <= nK) : (gk < nK && gr + 8 <= nR);
+      if (full[q]) {
+        const __nv_bfloat16* src = !T_ ? X + (long long)gr * ld + gk : X + (long long)gk * ld + gr;
+        v[q] = *reinterpret_cast<const uint4*>(src);
+      } else {
+        // ragged edge: element loads, zero outside the operand
+        union {
+          uint4 u;
+          __nv_bfloat16 h[8];
+        } e;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int rr = !T_ ? gr : gr + i, kk = !T_ ? gk + i : gk;
+          e.h[i] = (rr < nR && kk < nK)
+                       ? (!T_ ? X[(long long)rr * ld + kk] : X[(long long)kk * ld + rr])
+                       : __float2bfloat16(0.0f);
+        }
+        v[q] = e.u;
+      }
+    }
+  }
+  __device__ __forceinline__ void store(__nv_bfloat16 (*S)[kBK2 + kPad]) const {
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      if (!T_) {
+        *reinterpret_cast<uint4*>(&S[r[q]][k[q]]) = v[q];
+      } else {
+        union {
+          uint4 u;
+          __nv_bfloat16 h[8];
+        } e;
+        e.u = v[q];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) S[r[q] + i][k[q]] = e.h[i];
+      }
+    }
+  }
+};
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(256)
+gemm_bf16_v2_kernel(int M, int N, int K, const __nv_bfloat16* __restrict__ A, int lda,
+                    const __nv_bfloat16* __restrict__ B, int ldb, const float* __restrict__ bias,
+                    int relu, const __nv_bfloat16* __restrict__ mask, int ldm, float* Cf,
+                    __nv_bfloat16* Cb, int ldc, int kc) {
+  __shared__ __align__(16) __nv_bfloat16 As[kBM2][kBK2 + kPad];
+  __shared__ __align__(16) __nv_bfloat16 Bs[kBN2][kBK2 + kPad];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps, 64 x 32 each
+  const int g = lane >> 2, t = lane & 3;
+  const int m0 = blockIdx.y * kBM2, n0 = blockIdx.x * kBN2;
+  float acc[4][4][4] = {};
+  const int kb = blockIdx.z * kc, ke = min(K, kb + kc);
+  TileLoad<TA, kBM2> la;
+  TileLoad<TB, kBN2> lb;
+  if (kb < ke) {
+    la.load(A, lda, m0, kb, M, ke);
+    lb.load(B, ldb, n0, kb, N, ke);
+  }
+  for (int k0 = kb; k0 < ke; k0 += kBK2) {
+    la.store(As);
+    lb.store(Bs);
+    __syncthreads();
+    if (k0 + kBK2 < ke) {  // next tile in flight during this one's products
+      la.load(A, lda, m0, k0 + kBK2, M, ke);
+      lb.load(B, ldb, n0, k0 + kBK2, N, ke);
+    }
+#pragma unroll
+    for (int ks = 0; ks < kBK2; ks += 16) {
+      unsigned af[4][4], bf[4][2];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) {
+        const int r = wm * 64 + mt * 16 + g;
+        af[mt][0] = pack_bf16(&As[r][ks + 2 * t]);
+        af[mt][1] = pack_bf16(&As[r + 8][ks + 2 * t]);
+        af[mt][2] = pack_bf16(&As[r][ks + 2 * t + 8]);
+        af[mt][3] = pack_bf16(&As[r + 8][ks + 2 * t + 8]);
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int c = wn * 32 + nt * 8 + g;
+        bf[nt][0] = pack_bf16(&Bs[c][ks + 2 * t]);
+        bf[nt][1] = pack_bf16(&Bs[c][ks + 2 * t + 8]);
+      }
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) mma_bf16(acc[mt][nt], af[mt], bf[nt]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int m = m0 + wm * 64 + mt * 16 + g + (q >= 2 ? 8 : 0);
+        const int n = n0 + wn * 32 + nt * 8 + 2 * t + (q & 1);
+        if (m >= M || n >= N) continue;
+        float v = acc[mt][nt][q];
+        if (gridDim.z > 1) {
+          atomicAdd(&Cf[(long long)m * ldc + n], v);
+          continue;
+        }
         if (bias) v += bias[n];
         if (relu) v = fmaxf(v, 0.0f);
         if (mask && !(__bfloat162float(mask[(long long)m * ldm + n]) > 0.0f)) v = 0.0f;
@@ -244,19 +390,20 @@ __global__ void loss_grad_kernel(const float* __restrict__ Y, const float* __res
   }
 }
 
-// out[n] = sum_m A[m lda + n] (FP32 or BF16 input).
+// out[n] += sum over rows m = blockIdx.y, blockIdx.y + gridDim.y, ... of
+// A[m lda + n] (FP32 or BF16 input); out is zeroed by the launcher.
 template <typename T>
 __global__ void colsum_kernel(const T* __restrict__ A, int M, int N, int lda, float* out) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
   float s = 0.0f;
-  for (int m = 0; m < M; ++m) {
+  for (int m = blockIdx.y; m < M; m += gridDim.y) {
     if constexpr (sizeof(T) == 4)
       s += A[(long long)m * lda + n];
     else
       s += __bfloat162float(A[(long long)m * lda + n]);
   }
-  out[n] = s;
+  atomicAdd(&out[n], s);
 }
 
 // Adam on FP32 master weights w with moments mo, ve; BF16 copy wb.
@@ -282,11 +429,37 @@ cudaError_t launch_mlp_gemm(int ta, int tb, int M, int N, int K, const void* A, 
                             const void* B, int ldb, const float* bias, int relu,
                             const void* mask, int ldm, float* Cf, void* Cb, int ldc,
                             cudaStream_t st) {
-  const dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM);
   const auto* a = static_cast<const __nv_bfloat16*>(A);
   const auto* b = static_cast<const __nv_bfloat16*>(B);
   const auto* mk = static_cast<const __nv_bfloat16*>(mask);
   auto* cb = static_cast<__nv_bfloat16*>(Cb);
+  const bool vec = lda % 8 == 0 && ldb % 8 == 0 && reinterpret_cast<uintptr_t>(A) % 16 == 0 &&
+                   reinterpret_cast<uintptr_t>(B) % 16 == 0;
+  if (vec) {
+    // split K when the output tiles cannot fill the GPU and the epilogue is
+    // a plain FP32 store: about two CTAs per SM, at least 512 k per split
+    const int tiles = ((N + kBN2 - 1) / kBN2) * ((M + kBM2 - 1) / kBM2);
+    int splits = 1;
+    if (Cf && !Cb && !bias && !relu && !mask && tiles < 296)
+      splits = std::max(1, std::min(296 / tiles, K / 512));
+    const int kc = ((K + splits - 1) / splits + kBK2 - 1) / kBK2 * kBK2;
+    splits = (K + kc - 1) / kc;
+    if (splits > 1) {
+      const cudaError_t z = cudaMemset2DAsync(Cf, sizeof(float) * ldc, 0, sizeof(float) * N, M, st);
+      if (z != cudaSuccess) return z;
+    }
+    const dim3 g2((N + kBN2 - 1) / kBN2, (M + kBM2 - 1) / kBM2, splits);
+#define DNSB_V2(TA_, TB_)                                                                      \
+  gemm_bf16_v2_kernel<TA_, TB_><<<g2, 256, 0, st>>>(M, N, K, a, lda, b, ldb, bias, relu, mk,  \
+                                                    ldm, Cf, cb, ldc, kc)
+    if (!ta && !tb) DNSB_V2(false, false);
+    else if (ta && tb) DNSB_V2(true, true);
+    else if (!ta && tb) DNSB_V2(false, true);
+    else DNSB_V2(true, false);
+#undef DNSB_V2
+    return cudaGetLastError();
+  }
+  const dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM);
   if (!ta && !tb)
     gemm_bf16_kernel<false, false><<<grid, 128, 0, st>>>(M, N, K, a, lda, b, ldb, bias, relu, mk,
                                                          ldm, Cf, cb, ldc);
@@ -328,12 +501,14 @@ cudaError_t launch_mlp_loss_grad(const float* Y, const float* T, int M, int N, i
 
 cudaError_t launch_mlp_colsum(const void* A, int bf16, int M, int N, int lda, float* out,
                               cudaStream_t st) {
+  const cudaError_t z = cudaMemsetAsync(out, 0, sizeof(float) * N, st);
+  if (z != cudaSuccess) return z;
+  const dim3 grid((N + 127) / 128, std::max(1, std::min(M, 128)));
   if (bf16)
-    colsum_kernel<__nv_bfloat16><<<(N + 127) / 128, 128, 0, st>>>(
-        static_cast<const __nv_bfloat16*>(A), M, N, lda, out);
+    colsum_kernel<__nv_bfloat16><<<grid, 128, 0, st>>>(static_cast<const __nv_bfloat16*>(A), M,
+                                                       N, lda, out);
   else
-    colsum_kernel<float><<<(N + 127) / 128, 128, 0, st>>>(static_cast<const float*>(A), M, N,
-                                                          lda, out);
+    colsum_kernel<float><<<grid, 128, 0, st>>>(static_cast<const float*>(A), M, N, lda, out);
   return cudaGetLastError();
 }
 

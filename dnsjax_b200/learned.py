@@ -53,16 +53,21 @@ class MLP:
 
         self.L = _lib.lib()
         self.M, self.K1, self.H, self.N2 = M, K1, H, N2
+        # operand widths padded to multiples of 8 (16-byte rows for the GEMM's
+        # vector loads); padded inputs, weights and targets are zero
         self.K1p = (K1 + 7) // 8 * 8
+        self.N2p = (N2 + 7) // 8 * 8
+        N2p = self.N2p
         self.lr = lr
         g = torch.Generator(device="cpu").manual_seed(seed)
         f32 = dict(dtype=torch.float32, device="cuda")
         bf = dict(dtype=torch.bfloat16, device="cuda")
         W1 = torch.randn(H, self.K1p, generator=g) * sqrt(2.0 / K1)
         W1[:, K1:] = 0.0
-        W2 = torch.randn(N2, H, generator=g) * (out_scale / sqrt(H))
+        W2 = torch.zeros(N2p, H)
+        W2[:N2] = torch.randn(N2, H, generator=g) * (out_scale / sqrt(H))
         self.w = {"W1": W1.to(**f32), "b1": torch.zeros(H, **f32),
-                  "W2": W2.to(**f32), "b2": torch.zeros(N2, **f32)}
+                  "W2": W2.to(**f32), "b2": torch.zeros(N2p, **f32)}
         self.wb = {k: self.w[k].to(torch.bfloat16) for k in ("W1", "W2")}
         self.m = {k: torch.zeros_like(v) for k, v in self.w.items()}
         self.v = {k: torch.zeros_like(v) for k, v in self.w.items()}
@@ -70,10 +75,10 @@ class MLP:
         self.X = torch.zeros(M, self.K1p, **bf)
         self.Hb = torch.empty(M, H, **bf)
         self.dHb = torch.empty(M, H, **bf)
-        self.Y = torch.empty(M, N2, **f32)
-        self.T = torch.zeros(M, N2, **f32)
-        self.dYf = torch.empty(M, N2, **f32)
-        self.dYb = torch.empty(M, N2, **bf)
+        self.Y = torch.empty(M, N2p, **f32)
+        self.T = torch.zeros(M, N2p, **f32)
+        self.dYf = torch.empty(M, N2p, **f32)
+        self.dYb = torch.empty(M, N2p, **bf)
         self.err = torch.empty(M, **f32)
         self.ref = torch.empty(M, **f32)
         self.adam_step = 0
@@ -94,26 +99,26 @@ class MLP:
         M = self.M
         self._gemm(0, 0, M, self.H, self.K1p, self.X, self.K1p, self.wb["W1"], self.K1p,
                    bias=self.w["b1"], relu=1, Cb=self.Hb, ldc=self.H)
-        self._gemm(0, 0, M, self.N2, self.H, self.Hb, self.H, self.wb["W2"], self.H,
-                   bias=self.w["b2"], Cf=self.Y, ldc=self.N2)
+        self._gemm(0, 0, M, self.N2p, self.H, self.Hb, self.H, self.wb["W2"], self.H,
+                   bias=self.w["b2"], Cf=self.Y, ldc=self.N2p)
 
     def loss(self):
         """Mean-squared-error gradient into dYf / dYb; returns the per-row
         (err, ref) sums of squares."""
         p = _lib.ptr
         _lib.check(self.L.dnsb_mlp_loss_grad(
-            p(self.Y), p(self.T), self.M, self.N2, self.N2, p(self.dYf), p(self.dYb),
+            p(self.Y), p(self.T), self.M, self.N2p, self.N2p, p(self.dYf), p(self.dYb),
             p(self.err), p(self.ref), _lib.stream_handle()))
         return self.err, self.ref
 
     def backward(self):
         p = _lib.ptr
         M = self.M
-        self._gemm(1, 1, self.N2, self.H, M, self.dYb, self.N2, self.Hb, self.H,
+        self._gemm(1, 1, self.N2p, self.H, M, self.dYb, self.N2p, self.Hb, self.H,
                    Cf=self.g["W2"], ldc=self.H)
-        _lib.check(self.L.dnsb_mlp_colsum(p(self.dYf), 0, M, self.N2, self.N2, p(self.g["b2"]),
+        _lib.check(self.L.dnsb_mlp_colsum(p(self.dYf), 0, M, self.N2p, self.N2p, p(self.g["b2"]),
                                           _lib.stream_handle()))
-        self._gemm(0, 1, M, self.H, self.N2, self.dYb, self.N2, self.wb["W2"], self.H,
+        self._gemm(0, 1, M, self.H, self.N2p, self.dYb, self.N2p, self.wb["W2"], self.H,
                    mask=self.Hb, ldm=self.H, Cb=self.dHb, ldc=self.H)
         self._gemm(1, 1, self.H, self.K1p, M, self.dHb, self.H, self.X, self.K1p,
                    Cf=self.g["W1"], ldc=self.K1p)
@@ -166,12 +171,12 @@ class LearnedGuess:
         _lib.check(self.flow._L.dnsb_learned_features(
             self.flow._ctx, p(un), p(up), p(dprev) if dprev is not None else None,
             p(target) if target is not None else None, self.kx_max, self.kz_max,
-            float(s_floor), p(n.X), n.K1p, p(n.T), n.N2, p(self.scale), _lib.stream_handle()))
+            float(s_floor), p(n.X), n.K1p, p(n.T), n.N2p, p(self.scale), _lib.stream_handle()))
 
     def guess(self, up, out):
         p = _lib.ptr
         _lib.check(self.flow._L.dnsb_learned_guess(self.flow._ctx, p(up), p(self.net.Y),
-                                                   self.net.N2, p(self.scale), p(out),
+                                                   self.net.N2p, p(self.scale), p(out),
                                                    _lib.stream_handle()))
         return out
 

@@ -34,15 +34,18 @@ def as64(t):
     return t.float().cpu().numpy().astype(np.float64)
 
 
+# (70, 45, 100): unaligned leading dimensions, the 64 x 64 kernel; (200,
+# 136, 264): the 128 x 128 kernel with ragged tiles; (64, 96, 4096): its
+# split-K path.
+@pytest.mark.parametrize("M,N,K", [(70, 45, 100), (200, 136, 264), (64, 96, 4096)])
 @pytest.mark.parametrize("ta,tb", [(0, 0), (1, 1), (0, 1)])
-def test_mlp_gemm_layouts(ta, tb):
+def test_mlp_gemm_layouts(ta, tb, M, N, K):
     import torch
 
     from dnsjax_b200 import _lib
 
     L = _lib.lib()
     rng = np.random.default_rng(ta * 2 + tb)
-    M, N, K = 70, 45, 100
     Am = rng.standard_normal((M, K))
     Bn = rng.standard_normal((N, K))
     A = bf16_tensor(Am.T if ta else Am).contiguous()
@@ -79,7 +82,7 @@ def test_mlp_gradients_match_oracle():
     X[:, net.K1:] = 0.0
     net.X.copy_(bf16_tensor(X))
     T = rng.standard_normal((150, 30))
-    net.T.copy_(torch.as_tensor(T, dtype=torch.float32))
+    net.T[:, :30] = torch.as_tensor(T, dtype=torch.float32)
     net.forward()
     err, _ = net.loss()
     net.backward()
@@ -87,6 +90,7 @@ def test_mlp_gradients_match_oracle():
     loss, g = om.loss_and_grads(as64(net.X), w["W1"], w["b1"], w["W2"], w["b2"],
                                 net.T.double().cpu().numpy())
     assert abs(float(err.double().sum()) / 150 - loss) <= 1e-4 * loss
+    assert net.N2p == 32 and float(net.g["W2"][30:].abs().max()) == 0.0
     for k in ("W1", "b1", "W2", "b2"):
         got = net.g[k].double().cpu().numpy()
         rel = np.linalg.norm(got - g[k]) / np.linalg.norm(g[k])
