@@ -306,9 +306,11 @@ def run_ours(a, w, rank, world):
 
     u0 = initial_state(w, replica_seed(w["seed"], rank))
     tf = Timed(flow)
-    steppers = tf.make_stepper()
     tol, mi = (w["tol"] if a.tol is None else a.tol), w["max_iter"]
     state = torch.as_tensor(u0, device="cuda")
+    # pass variants timed on this workload before anything else runs
+    tuning = None if a.no_autotune else flow.autotune(state)
+    steppers = tf.make_stepper()
     for _ in range(a.warmup):
         state, c, e = driver.step(tf, steppers, state, tol, mi)
 
@@ -430,6 +432,7 @@ def run_ours(a, w, rank, world):
         "config": {
             "workload": a.workload,
             "form": "mixed: FP32 RHS passes, FP64 state/IMM/norms" if mixed else "plain-fp64",
+            "autotune": tuning,
             "driver": ("step graph per time step (corrector loop as a device-controlled "
                        "conditional node)" if graph is not None else
                        "host-driven reference loop"),
@@ -737,7 +740,8 @@ def run_ensemble(a, w, rank, world):
             dist.barrier()
         torch.cuda.synchronize()
 
-    ens = Ensemble(flows, [torch.as_tensor(u, device="cuda") for u in u0s], graphs=True)
+    ens = Ensemble(flows, [torch.as_tensor(u, device="cuda") for u in u0s], graphs=True,
+                   autotune=not a.no_autotune)
     for _ in range(a.warmup):
         ens.step()
     iters = []
@@ -822,6 +826,7 @@ def run_ensemble(a, w, rank, world):
         "config": {
             "workload": a.workload, "form": "plain-fp64, ensemble of step graphs",
             "members": n, "sizes": list(w["sizes"]), "re_range": list(w["re_range"]),
+            "autotune": {f"{k[1]}^3": v["variants"] for k, v in ens.tuning.items()},
             "sequential_trajectory_steps_per_s": n * a.steps / (ms_seq * 1e-3),
             "speedup_vs_sequential": ms_seq / ms,
             "lockstep_vs_sequential_rel_l2": agree,
@@ -952,6 +957,8 @@ def main():
                     choices=["plain", "mixed", "learned", "learned-mixed"],
                     help="mixed: FP32 RHS passes (plane Couette), FP64 elsewhere; "
                          "learned[-mixed]: each step started from the MLP's guess")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default pass variants instead of timing them first")
     ap.add_argument("--train-iters", type=int, default=2,
                     help="learned forms: training iterations per time step")
     ap.add_argument("--tol", type=float, default=None,

@@ -93,6 +93,10 @@ SIGNATURES = {
     "dnsb_couette_check": (c_int, [c_void_p, c_void_p]),
     "dnsb_periodic_set_rhs_precision": (c_int, [c_void_p, c_int]),
     "dnsb_couette_set_rhs_precision": (c_int, [c_void_p, c_int]),
+    "dnsb_periodic_autotune": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "dnsb_couette_autotune": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "dnsb_periodic_set_variants": (c_int, [c_void_p, c_void_p]),
+    "dnsb_couette_set_variants": (c_int, [c_void_p, c_void_p]),
     "dnsb_mlp_gemm": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p,
                               c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_int,
                               c_void_p]),

@@ -107,6 +107,7 @@ struct dnsb_periodic {
   double* partials = nullptr;
   size_t ws_bytes = 0;
   int rhs_fp32 = 0;  // RHS transforms and product in FP32 (pass buffers float2)
+  int var[5] = {0, 0, 0, 0, 0};  // pass variants: y inverse, z inverse, x, z forward, y forward
 
   PeriodicPointArgs point() const {
     PeriodicPointArgs a;
@@ -276,10 +277,10 @@ static ColPassArgs periodic_zfwd(const dnsb_periodic* p) {
   return a;
 }
 
-extern "C" int dnsb_periodic_rhs(dnsb_periodic* p, const void* state,
-                                 void* rhs, void* stream) {
-  if (!p || !state || !rhs) return fail(DNSB_ERR_ARG, "null argument");
-  cudaStream_t st = as_stream(stream);
+// The five passes of the periodic RHS; bit k of `mask` runs pass k (y
+// inverse, z inverse, x, z forward, y forward), each with its variant.
+static int periodic_rhs_impl(dnsb_periodic* p, const void* state, void* rhs, unsigned mask,
+                             cudaStream_t st) {
   YInvArgs yi{};
   yi.u = (const double2*)state;
   yi.out = p->A;
@@ -294,11 +295,13 @@ extern "C" int dnsb_periodic_rhs(dnsb_periodic* p, const void* state,
   const int f32 = p->rhs_fp32;
   yi.tw = f32 ? reinterpret_cast<const double2*>(p->twy32) : p->twy;
   yi.fp32 = f32;
-  DNSB_LAUNCH(launch_yinv(yi, st));
+  yi.variant = p->var[0];
+  if (mask & 1u) DNSB_LAUNCH(launch_yinv(yi, st));
   ColPassArgs zi = periodic_zinv(p);
   zi.fp32 = zi.out32 = f32;
   if (f32) zi.tw = reinterpret_cast<const double2*>(p->twz32);
-  DNSB_LAUNCH(launch_col_pass(zi, 6, p->My, st));
+  zi.variant = p->var[1];
+  if (mask & 2u) DNSB_LAUNCH(launch_col_pass(zi, 6, p->My, st));
   XPassArgs xa{};
   xa.in = p->B;
   xa.out = p->B;
@@ -318,11 +321,13 @@ extern "C" int dnsb_periodic_rhs(dnsb_periodic* p, const void* state,
   xa.plan = p->px;
   xa.tw = f32 ? reinterpret_cast<const double2*>(p->twx32) : p->twx;
   xa.fp32 = f32;
-  DNSB_LAUNCH(launch_x_pass(xa, st));
+  xa.variant = p->var[2];
+  if (mask & 4u) DNSB_LAUNCH(launch_x_pass(xa, st));
   ColPassArgs zf = periodic_zfwd(p);
   zf.fp32 = zf.out32 = f32;
   if (f32) zf.tw = reinterpret_cast<const double2*>(p->twz32);
-  DNSB_LAUNCH(launch_col_pass(zf, 3, p->My, st));
+  zf.variant = p->var[3];
+  if (mask & 8u) DNSB_LAUNCH(launch_col_pass(zf, 3, p->My, st));
   YFwdArgs yf{};
   yf.in = p->A;
   yf.out = (double2*)rhs;
@@ -337,8 +342,15 @@ extern "C" int dnsb_periodic_rhs(dnsb_periodic* p, const void* state,
   yf.plan = p->py;
   yf.tw = f32 ? reinterpret_cast<const double2*>(p->twy32) : p->twy;
   yf.fp32 = f32;
-  DNSB_LAUNCH(launch_yfwd(yf, st));
+  yf.variant = p->var[4];
+  if (mask & 16u) DNSB_LAUNCH(launch_yfwd(yf, st));
   return 0;
+}
+
+extern "C" int dnsb_periodic_rhs(dnsb_periodic* p, const void* state, void* rhs,
+                                 void* stream) {
+  if (!p || !state || !rhs) return fail(DNSB_ERR_ARG, "null argument");
+  return periodic_rhs_impl(p, state, rhs, 31u, as_stream(stream));
 }
 
 extern "C" int dnsb_periodic_set_rhs_precision(dnsb_periodic* p, int fp32) {
@@ -710,6 +722,7 @@ struct dnsb_couette {
   int* status = nullptr;
   dnsb_imm_ops ops{};
   bool bound = false;
+  int var[4] = {0, 0, 0, 0};  // variants: z inverse, x, z forward passes; IMM
   int ab_row0 = 0;
   int pair_modes = 0;
   size_t ws_bytes = 0;
@@ -1012,10 +1025,10 @@ extern "C" int dnsb_couette_bind_imm(dnsb_couette* p, const dnsb_imm_ops* ops) {
   return 0;
 }
 
-extern "C" int dnsb_couette_rhs(dnsb_couette* p, const void* state, void* rhs,
-                                void* stream) {
-  if (!p || !state || !rhs) return fail(DNSB_ERR_ARG, "null argument");
-  cudaStream_t st = as_stream(stream);
+// The three passes of the Couette RHS; bit k of `mask` runs pass k (z
+// inverse with the curl, x, z forward), each with its variant.
+static int couette_rhs_impl(dnsb_couette* p, const void* state, void* rhs, unsigned mask,
+                            cudaStream_t st) {
   ZInvCurlArgs zi{};
   zi.u = (const double2*)state;
   zi.out = p->B;
@@ -1032,7 +1045,8 @@ extern "C" int dnsb_couette_rhs(dnsb_couette* p, const void* state, void* rhs,
   zi.plan = p->pz;
   zi.tw = p->rhs_fp32 ? reinterpret_cast<const double2*>(p->twz32) : p->twz;
   zi.fp32 = p->rhs_fp32;
-  DNSB_LAUNCH(launch_zinv_curl(zi, p->span_max, st));
+  zi.variant = p->var[0];
+  if (mask & 1u) DNSB_LAUNCH(launch_zinv_curl(zi, p->span_max, st));
   XPassArgs xa{};
   xa.in = p->B;
   xa.out = p->B;
@@ -1052,7 +1066,8 @@ extern "C" int dnsb_couette_rhs(dnsb_couette* p, const void* state, void* rhs,
   xa.plan = p->px;
   xa.tw = p->rhs_fp32 ? reinterpret_cast<const double2*>(p->twx32) : p->twx;
   xa.fp32 = p->rhs_fp32;
-  DNSB_LAUNCH(launch_x_pass(xa, st));
+  xa.variant = p->var[1];
+  if (mask & 2u) DNSB_LAUNCH(launch_x_pass(xa, st));
   ColPassArgs zf{};
   zf.in = p->B;
   zf.out = (double2*)rhs;
@@ -1068,8 +1083,15 @@ extern "C" int dnsb_couette_rhs(dnsb_couette* p, const void* state, void* rhs,
   zf.plan = p->pz;
   zf.tw = p->rhs_fp32 ? reinterpret_cast<const double2*>(p->twz32) : p->twz;
   zf.fp32 = p->rhs_fp32;
-  DNSB_LAUNCH(launch_col_pass(zf, 3, p->NKX, st));
+  zf.variant = p->var[2];
+  if (mask & 4u) DNSB_LAUNCH(launch_col_pass(zf, 3, p->NKX, st));
   return 0;
+}
+
+extern "C" int dnsb_couette_rhs(dnsb_couette* p, const void* state, void* rhs,
+                                void* stream) {
+  if (!p || !state || !rhs) return fail(DNSB_ERR_ARG, "null argument");
+  return couette_rhs_impl(p, state, rhs, 7u, as_stream(stream));
 }
 
 extern "C" int dnsb_couette_set_rhs_precision(dnsb_couette* p, int fp32) {
@@ -1095,13 +1117,13 @@ extern "C" int dnsb_couette_imm(dnsb_couette* p, const void* vel_n,
   if (vel_new == vel_n)
     return fail(DNSB_ERR_ARG, "vel_new must not alias vel_n");
   cudaStream_t st = as_stream(stream);
-  if (p->batch_ready) {
+  if (p->batch_ready && p->var[3] == 0) {
     DNSB_LAUNCH(launch_imm_batch(p->imm(), p->batch, (const double2*)vel_n,
                                  (const double2*)vel_j, (const double2*)nl_n,
                                  (const double2*)nl_j, (double2*)vel_new,
                                  (double2*)corr_out, err_dev ? p->partials : nullptr, st));
     count_launches(4);  // five kernels
-  } else if (imm_v2_supported(p->p, p->Ny)) {
+  } else if (imm_v2_supported(p->p, p->Ny) && p->var[3] <= 1) {
     DNSB_LAUNCH(launch_imm_v2(p->imm(), (const double2*)vel_n, (const double2*)vel_j,
                               (const double2*)nl_n, (const double2*)nl_j,
                               (double2*)vel_new, (double2*)corr_out,
@@ -1265,6 +1287,140 @@ extern "C" int dnsb_couette_check(dnsb_couette* p, void* stream) {
   if (h & 1) return fail(DNSB_ERR_PIVOT, "pivot index outside [j, j+kl]");
   if (h & 2) return fail(DNSB_ERR_CUDA, "IMM substitution: a shared-memory ring wait timed out");
   return 0;
+}
+
+// ===========================================================================
+// Autotuning: per-pass kernel variants picked by timing on the context's
+// own sizes and buffers
+// ===========================================================================
+namespace {
+// Mean milliseconds of `reps` calls of f on st (after one untimed call).
+template <typename F>
+int time_calls(F&& f, int reps, cudaStream_t st, float* ms) {
+  int rc = f();
+  if (rc) return rc;
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, st);
+  for (int r = 0; r < reps && !rc; ++r) rc = f();
+  cudaEventRecord(b, st);
+  const cudaError_t e = cudaEventSynchronize(b);
+  float t = 0.0f;
+  if (!rc && e == cudaSuccess) cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (!rc && e != cudaSuccess) rc = fail(DNSB_ERR_CUDA, cudaGetErrorString(e));
+  *ms = t / (float)(reps > 0 ? reps : 1);
+  return rc;
+}
+
+// Tunes pass k over `variants` (count nv): for each, `prefix` rebuilds the
+// pass's input, then the pass alone is timed; var[k] keeps the fastest.
+template <typename Prefix, typename Pass>
+int tune_one(int* var, int k, const int* variants, int nv, int reps, cudaStream_t st,
+             float* ms_out, Prefix&& prefix, Pass&& pass) {
+  float best = 0.0f;
+  int pick = var[k];
+  for (int i = 0; i < nv; ++i) {
+    var[k] = variants[i];
+    int rc = prefix();
+    float t = 0.0f;
+    if (!rc) rc = time_calls(pass, reps, st, &t);
+    if (rc) return rc;
+    ms_out[variants[i]] = t;
+    if (i == 0 || t < best) {
+      best = t;
+      pick = variants[i];
+    }
+  }
+  var[k] = pick;
+  return 0;
+}
+}  // namespace
+
+extern "C" int dnsb_periodic_set_variants(dnsb_periodic* p, const int* var) {
+  if (!p || !var) return fail(DNSB_ERR_ARG, "null argument");
+  for (int k = 0; k < 5; ++k)
+    if (var[k] < 0 || var[k] > 2 || (p->rhs_fp32 && var[k] != 0))
+      return fail(DNSB_ERR_ARG, "pass variants are 0, 1 or 2 (0 only in FP32)");
+  for (int k = 0; k < 5; ++k) p->var[k] = var[k];
+  return 0;
+}
+
+extern "C" int dnsb_couette_set_variants(dnsb_couette* p, const int* var) {
+  if (!p || !var) return fail(DNSB_ERR_ARG, "null argument");
+  for (int k = 0; k < 4; ++k)
+    if (var[k] < 0 || var[k] > 2 || (k < 3 && p->rhs_fp32 && var[k] != 0))
+      return fail(DNSB_ERR_ARG, "variants are 0, 1 or 2 (passes: 0 only in FP32)");
+  if (var[3] == 1 && !imm_v2_supported(p->p, p->Ny))
+    return fail(DNSB_ERR_ARG, "the register-window IMM does not cover these sizes");
+  for (int k = 0; k < 4; ++k) p->var[k] = var[k];
+  return 0;
+}
+
+extern "C" int dnsb_periodic_autotune(dnsb_periodic* p, const void* state, int reps,
+                                      int* chosen, float* ms, void* stream) {
+  if (!p || !state || !chosen || !ms) return fail(DNSB_ERR_ARG, "null argument");
+  if (reps < 1) return fail(DNSB_ERR_ARG, "reps must be positive");
+  cudaStream_t st = as_stream(stream);
+  for (int i = 0; i < 15; ++i) ms[i] = -1.0f;
+  double2* rhs = nullptr;
+  DNSB_CUDA(cudaMallocAsync(&rhs, 3 * (size_t)p->S * sizeof(double2), st));
+  const int all[] = {0, 1, 2}, ypass[] = {0, 2}, only0[] = {0};
+  int rc = 0;
+  for (int k = 0; k < 5 && !rc; ++k) {
+    const int* vs = p->rhs_fp32 ? only0 : (k == 0 || k == 4) ? ypass : all;
+    const int nv = p->rhs_fp32 ? 1 : (k == 0 || k == 4) ? 2 : 3;
+    const unsigned before = (1u << k) - 1u, self = 1u << k;
+    rc = tune_one(
+        p->var, k, vs, nv, reps, st, ms + 3 * k,
+        [&] { return before ? periodic_rhs_impl(p, state, rhs, before, st) : 0; },
+        [&] { return periodic_rhs_impl(p, state, rhs, self, st); });
+  }
+  cudaFreeAsync(rhs, st);
+  for (int k = 0; k < 5; ++k) chosen[k] = p->var[k];
+  return rc;
+}
+
+extern "C" int dnsb_couette_autotune(dnsb_couette* p, const void* state, int reps, int* chosen,
+                                     float* ms, void* stream) {
+  if (!p || !state || !chosen || !ms) return fail(DNSB_ERR_ARG, "null argument");
+  if (reps < 1) return fail(DNSB_ERR_ARG, "reps must be positive");
+  cudaStream_t st = as_stream(stream);
+  for (int i = 0; i < 12; ++i) ms[i] = -1.0f;
+  const size_t n = 3 * (size_t)p->NM * p->Ny;
+  double2 *rhs = nullptr, *out = nullptr;
+  double* err = nullptr;
+  DNSB_CUDA(cudaMallocAsync(&rhs, n * sizeof(double2), st));
+  DNSB_CUDA(cudaMallocAsync(&out, n * sizeof(double2), st));
+  DNSB_CUDA(cudaMallocAsync(&err, sizeof(double), st));
+  const int all[] = {0, 1, 2}, only0[] = {0};
+  int rc = 0;
+  for (int k = 0; k < 3 && !rc; ++k) {
+    const unsigned before = (1u << k) - 1u, self = 1u << k;
+    rc = tune_one(
+        p->var, k, p->rhs_fp32 ? only0 : all, p->rhs_fp32 ? 1 : 3, reps, st, ms + 3 * k,
+        [&] { return before ? couette_rhs_impl(p, state, rhs, before, st) : 0; },
+        [&] { return couette_rhs_impl(p, state, rhs, self, st); });
+  }
+  if (!rc && p->bound) {
+    // the IMM with the correction norm, as a corrector iteration calls it
+    int vs[3], nv = 0;
+    if (p->batch_ready) vs[nv++] = 0;
+    if (imm_v2_supported(p->p, p->Ny)) vs[nv++] = 1;
+    vs[nv++] = 2;
+    rc = couette_rhs_impl(p, state, rhs, 7u, st);
+    if (!rc)
+      rc = tune_one(
+          p->var, 3, vs, nv, reps, st, ms + 9, [] { return 0; },
+          [&] { return dnsb_couette_imm(p, state, state, rhs, rhs, out, nullptr, err, st); });
+  }
+  cudaFreeAsync(rhs, st);
+  cudaFreeAsync(out, st);
+  cudaFreeAsync(err, st);
+  for (int k = 0; k < 4; ++k) chosen[k] = p->var[k];
+  return rc;
 }
 
 // ===========================================================================

@@ -20,6 +20,14 @@ namespace dnsb {
     case 192: KERNEL<192><<<GRID, kPassThreads, SMEM, ST>>>(__VA_ARGS__); break; \
     default: KERNEL<0><<<GRID, kPassThreads, SMEM, ST>>>(__VA_ARGS__); break; \
   }
+// Variant 2 (runtime-planned stages) takes KERNEL<0> whatever L is.
+#define DNSB_DISPATCH_V(VAR, L, KERNEL, GRID, SMEM, ST, ...)                  \
+  do {                                                                      \
+    if ((VAR) == 2)                                                         \
+      KERNEL<0><<<GRID, kPassThreads, SMEM, ST>>>(__VA_ARGS__);             \
+    else                                                                    \
+      DNSB_DISPATCH(L, KERNEL, GRID, SMEM, ST, __VA_ARGS__);                \
+  } while (0)
 #define DNSB_ALL_SIZES(KERNEL)                                                \
   (const void*)KERNEL<0>, (const void*)KERNEL<48>, (const void*)KERNEL<72>,   \
       (const void*)KERNEL<96>, (const void*)KERNEL<192>
@@ -202,7 +210,7 @@ col_pass2_kernel(ColPassArgs a) {
 cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
                             cudaStream_t st) {
   const int L = a.plan.L;
-  if (L == 48 || L == 72 || L == 96 || L == 192) {
+  if (a.variant == 0 && (L == 48 || L == 72 || L == 96 || L == 192)) {
     dim3 g2((a.nI + kC2Cols - 1) / kC2Cols, nO, nfields);
     const size_t sm2 = a.fp32 ? col_pass2_smem(L) / 2 : col_pass2_smem(L);
     if (a.fp32 && a.inverse && !a.out32) return cudaErrorInvalidValue;
@@ -223,10 +231,10 @@ cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
 #undef DNSB_C2
     return cudaGetLastError();
   }
-  if (a.fp32) return cudaErrorInvalidValue;  // compile-time sizes only
+  if (a.fp32) return cudaErrorInvalidValue;  // two-stage compile-time passes only
   dim3 grid((a.nI + kTile - 1) / kTile, nO, nfields);
   size_t sm = col_pass_smem(a.plan.L);
-  DNSB_DISPATCH(a.plan.L, col_pass_kernel, grid, sm, st, a);
+  DNSB_DISPATCH_V(a.variant, a.plan.L, col_pass_kernel, grid, sm, st, a);
   return cudaGetLastError();
 }
 
@@ -375,7 +383,7 @@ cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
   dim3 grid((a.nrows + kXRows - 1) / kXRows);
   // The compile-time variants assume nx/2 = M/3 (3/2 oversampling).
   const int L = (a.nkx * 3 == a.plan.L) ? a.plan.L : -1;
-  if (L == 48 || L == 72 || L == 96 || L == 192) {
+  if (a.variant == 0 && (L == 48 || L == 72 || L == 96 || L == 192)) {
     dim3 g2((a.nrows + kX2Rows - 1) / kX2Rows);
     if (a.fp32) {
       const size_t sm2 = x_pass2_smem(L, a.nkx) / 2;
@@ -396,8 +404,8 @@ cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
     }
     return cudaGetLastError();
   }
-  if (a.fp32) return cudaErrorInvalidValue;  // compile-time sizes only
-  DNSB_DISPATCH(L, x_pass_kernel, grid, x_pass_smem(a.plan.L), st, a);
+  if (a.fp32) return cudaErrorInvalidValue;  // two-stage compile-time passes only
+  DNSB_DISPATCH_V(a.variant, L, x_pass_kernel, grid, x_pass_smem(a.plan.L), st, a);
   return cudaGetLastError();
 }
 
@@ -824,7 +832,7 @@ cudaError_t launch_yinv(const YInvArgs& a, cudaStream_t st) {
     }
     return cudaGetLastError();
   }
-  DNSB_DISPATCH(a.plan.L, yinv_kernel, grid, yinv_smem(a.plan.L, a.NY1, 0), st, a);
+  DNSB_DISPATCH_V(a.variant, a.plan.L, yinv_kernel, grid, yinv_smem(a.plan.L, a.NY1, 0), st, a);
   return cudaGetLastError();
 }
 
@@ -913,7 +921,7 @@ cudaError_t launch_yfwd(const YFwdArgs& a, cudaStream_t st) {
     }
     return cudaGetLastError();
   }
-  DNSB_DISPATCH(a.plan.L, yfwd_kernel, grid, yfwd_smem(a.plan.L, a.NY1, 0), st, a);
+  DNSB_DISPATCH_V(a.variant, a.plan.L, yfwd_kernel, grid, yfwd_smem(a.plan.L, a.NY1, 0), st, a);
   return cudaGetLastError();
 }
 
@@ -1194,7 +1202,7 @@ zinv_curl2_kernel(ZInvCurlArgs a) {
 cudaError_t launch_zinv_curl(const ZInvCurlArgs& a, int span_max,
                              cudaStream_t st) {
   const int L = a.plan.L;
-  if (L == 48 || L == 72 || L == 96 || L == 192) {
+  if (a.variant == 0 && (L == 48 || L == 72 || L == 96 || L == 192)) {
     const long long ncol = (long long)a.NKX * a.Ny;
     const int grid = (int)((ncol + kZ2Cols - 1) / kZ2Cols);
     if (a.fp32) {
@@ -1216,10 +1224,10 @@ cudaError_t launch_zinv_curl(const ZInvCurlArgs& a, int span_max,
     }
     return cudaGetLastError();
   }
-  if (a.fp32) return cudaErrorInvalidValue;  // compile-time sizes only
+  if (a.fp32) return cudaErrorInvalidValue;  // two-stage compile-time passes only
   dim3 grid((a.Ny + kZTile - 1) / kZTile, a.NKX);
-  DNSB_DISPATCH(a.plan.L, zinv_curl_kernel, grid,
-                zinv_curl_smem(a.plan.L, a.NZ1, span_max), st, a, span_max);
+  DNSB_DISPATCH_V(a.variant, a.plan.L, zinv_curl_kernel, grid,
+                  zinv_curl_smem(a.plan.L, a.NZ1, span_max), st, a, span_max);
   return cudaGetLastError();
 }
 

@@ -32,6 +32,8 @@ struct ColPassArgs {
   const double2* tw;
   int fp32;            // `in` and arithmetic in FP32 (compile-time sizes)
   int out32;           // with fp32: `out` is an FP32 pass buffer (always for inverse)
+  int variant;         // 0: two-stage register pass when compiled for L, 1: Stockham
+                       // stages (compile-time plan when compiled for L), 2: runtime plan
 };
 
 // x pass.  Rows are (outer, inner) pairs; row r = outer * inner_n + inner
@@ -52,6 +54,8 @@ struct XPassArgs {
   FFTPlan plan;        // Mx
   const double2* tw;   // float2 table when fp32
   int fp32;            // pass buffer and arithmetic in FP32 (compile-time sizes)
+  int variant;         // 0: two-stage register pass when compiled for L, 1: Stockham
+                       // stages (compile-time plan when compiled for L), 2: runtime plan
 };
 
 // x pass to physical space only (3 fields -> real [c] at row offsets
@@ -81,6 +85,7 @@ struct YInvArgs {
   FFTPlan plan;
   const double2* tw;
   int fp32;  // FP32 transform and output pass buffer (tw: float2 table)
+  int variant;  // 0 / 1: compile-time plan when compiled for L, 2: runtime plan
 };
 
 // Periodic last forward pass (y), projection fused: [3][My][NZ1][NKX] ->
@@ -97,6 +102,7 @@ struct YFwdArgs {
   FFTPlan plan;
   const double2* tw;
   int fp32;  // FP32 input pass buffer and transform (tw: float2 table)
+  int variant;  // 0 / 1: compile-time plan when compiled for L, 2: runtime plan
 };
 
 // Couette first inverse pass (z), FD curl fused: spectral
@@ -115,6 +121,8 @@ struct ZInvCurlArgs {
   FFTPlan plan;
   const double2* tw;   // float2 table when fp32
   int fp32;            // output pass buffer and FFT in FP32 (compile-time sizes)
+  int variant;         // 0: two-stage register pass when compiled for L, 1: Stockham
+                       // stages (compile-time plan when compiled for L), 2: runtime plan
 };
 
 constexpr int kZTile = 8;  // y values per CTA in the Couette z passes

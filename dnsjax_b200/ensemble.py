@@ -24,12 +24,15 @@ class EnsembleStep:
 
 
 class Ensemble:
-    """graphs=True: every trajectory's step is one CUDA graph
+    """autotune=True: the pass variants of every member are picked by timing
+    (one tuning per distinct size; see flow.autotune).
+
+    graphs=True: every trajectory's step is one CUDA graph
     launch (predictor, device-controlled corrector loop, correct_velocity;
     see timestep.StepGraph), and the host synchronises once per ensemble step to read
     every trajectory's iterations and error."""
 
-    def __init__(self, flows, states, tol=None, max_iter=None, graphs=False):
+    def __init__(self, flows, states, tol=None, max_iter=None, graphs=False, autotune=False):
         import torch
 
         if len(flows) != len(states):
@@ -40,6 +43,17 @@ class Ensemble:
                     for f in self.flows]
         self.max_iter = [f.params.step.max_corrector_iterations if max_iter is None
                          else max_iter for f in self.flows]
+        # autotune: pass variants timed once per distinct member size (the
+        # first member of each size), shared by the others of that size,
+        # before any step graph is captured
+        self.tuning = {}
+        if autotune:
+            for f, st in zip(self.flows, self.states):
+                key = (type(f).__name__, f.nx, f.ny, f.nz, bool(getattr(f, "rhs_fp32", False)))
+                if key in self.tuning:
+                    f.set_variants(self.tuning[key]["variants"])
+                else:
+                    self.tuning[key] = f.autotune(st)
         self.steppers = [f.make_stepper() for f in self.flows]
         self.streams = [torch.cuda.Stream() for _ in self.flows]
         self.graphs = ([f.make_step_graph(s, tol=t, max_iter=m) for f, s, t, m in

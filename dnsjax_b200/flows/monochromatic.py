@@ -214,6 +214,23 @@ class TriplyPeriodicFlow:
         return StepGraph(self._L, state, lambda h: self._L.dnsb_periodic_step_graph_create(
             self._ctx, self._check(state), float(tol), int(max_iter), int(divergence), h))
 
+    # -- variants of the passes (no counterpart in the reference) ----------------
+    def autotune(self, state, reps: int = 5) -> dict:
+        """Times every kernel variant of each pass (and, for Couette, the
+        IMM) on this flow's sizes from `state` and keeps the fastest (see
+        dnsb_periodic_autotune); returns the choices and the mean times."""
+        n = 5
+        chosen = (_lib.C.c_int * n)()
+        ms = (_lib.C.c_float * (3 * n))()
+        _lib.check(self._L.dnsb_periodic_autotune(self._ctx, self._check(state), int(reps),
+                                                 chosen, ms, _lib.stream_handle()))
+        return {"variants": list(chosen), "ms": [list(ms[3 * k:3 * k + 3]) for k in range(n)],
+                 "stages": ["y inverse", "z inverse", "x", "z forward", "y forward"]}
+
+    def set_variants(self, variants) -> None:
+        arr = (_lib.C.c_int * 5)(*[int(v) for v in variants])
+        _lib.check(self._L.dnsb_periodic_set_variants(self._ctx, arr))
+
     def get_stats(self, state) -> dict:
         """E, I, D, E' (monochromatic.py:433-505)."""
         _lib.check(self._L.dnsb_periodic_energy_sums(

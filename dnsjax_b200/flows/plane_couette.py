@@ -190,6 +190,23 @@ class PlaneCouetteFlow:
         return StepGraph(self._L, state, lambda h: self._L.dnsb_couette_step_graph_create(
             self._ctx, self._check(state), float(tol), int(max_iter), h))
 
+    # -- variants of the passes (no counterpart in the reference) ----------------
+    def autotune(self, state, reps: int = 5) -> dict:
+        """Times every kernel variant of each pass (and, for Couette, the
+        IMM) on this flow's sizes from `state` and keeps the fastest (see
+        dnsb_couette_autotune); returns the choices and the mean times."""
+        n = 4
+        chosen = (_lib.C.c_int * n)()
+        ms = (_lib.C.c_float * (3 * n))()
+        _lib.check(self._L.dnsb_couette_autotune(self._ctx, self._check(state), int(reps),
+                                                 chosen, ms, _lib.stream_handle()))
+        return {"variants": list(chosen), "ms": [list(ms[3 * k:3 * k + 3]) for k in range(n)],
+                 "stages": ["z inverse", "x", "z forward", "IMM"]}
+
+    def set_variants(self, variants) -> None:
+        arr = (_lib.C.c_int * 4)(*[int(v) for v in variants])
+        _lib.check(self._L.dnsb_couette_set_variants(self._ctx, arr))
+
     def get_stats(self, state) -> dict:
         """plane_couette.py:591-613: E' = ||u||^2 / 2."""
         _lib.check(self._L.dnsb_couette_norm2(

@@ -241,6 +241,31 @@ int dnsb_couette_norm_noalloc(const void* v, int nx, int ny, int nz, double ly,
                               double* out_dev, void* stream);
 
 /* ------------------------------------------------------------------ */
+/* Autotuning (no counterpart in the reference).  Times every kernel    */
+/* variant of each pass on the context's own sizes and buffers, from    */
+/* `state` (spectral, complex128), `reps` calls each after one warm-up  */
+/* call, and keeps the fastest for the context's later calls (and for   */
+/* step graphs created afterwards).  Variants: 0 the two-stage register */
+/* pass where it is compiled for the length (the default), 1 Stockham   */
+/* stages with the compile-time plan, 2 Stockham stages with the        */
+/* runtime plan; the FP32 forms have variant 0 only.                   */
+/*   periodic: chosen[5] for the y inverse, z inverse, x, z forward and */
+/*     y forward passes (the y passes: 0 or 2); ms[5][3] mean times     */
+/*     (-1 where not tried).                                            */
+/*   Couette: chosen[4] for the z inverse, x and z forward passes and   */
+/*     the IMM (0 five-kernel batched form, 1 one-kernel register-window */
+/*     form, 2 one-kernel form); ms[4][3].                              */
+/* Results of different variants agree to rounding, not bit for bit.   */
+/* ------------------------------------------------------------------ */
+int dnsb_periodic_autotune(dnsb_periodic* ctx, const void* state, int reps, int* chosen,
+                           float* ms, void* stream);
+/* Sets the variants directly (same meaning and order as `chosen`). */
+int dnsb_periodic_set_variants(dnsb_periodic* ctx, const int* variants);
+int dnsb_couette_set_variants(dnsb_couette* ctx, const int* variants);
+int dnsb_couette_autotune(dnsb_couette* ctx, const void* state, int reps, int* chosen,
+                          float* ms, void* stream);
+
+/* ------------------------------------------------------------------ */
 /* Learned corrector guess for plane Couette (no counterpart in the     */
 /* reference): kernels of a per-(kz, kx)-mode MLP, BF16 weights and     */
 /* activations, FP32 accumulation, trained online on the pairs          */
