@@ -305,8 +305,50 @@ __device__ __forceinline__ void dft_small(C* v, int sign) {
   else dft8(v, sign);
 }
 
+// Modular inverse of a mod m (a, m coprime), by search (compile time).
+__host__ __device__ constexpr int inv_mod(int a, int m) {
+  int r = 1;
+  while ((a * r) % m != 1) ++r;
+  return r;
+}
+
 template <int N, int SIGN, typename C>
+__device__ __forceinline__ void dft_3p_ct(C* v, const C* __restrict__ tw, int TS);
+
+// PFA: with 3 and P coprime, the prime-factor form (no twiddles); else the
+// Cooley-Tukey form with the twiddle table.
+template <int N, int SIGN, typename C, bool PFA = false>
 __device__ __forceinline__ void dft_3p(C* v, const C* __restrict__ tw, int TS) {
+  constexpr int P = N / 3;
+  if constexpr (PFA && P % 3 != 0) {
+    // 3 and P coprime: prime-factor (Good-Thomas) DFT, no twiddles.  Input
+    // n = (P n1 + 3 n2) mod N; P-point DFTs over n2, 3-point DFTs over n1;
+    // output k = (P (P^-1 mod 3) k1 + 3 (3^-1 mod P) k2) mod N (Chinese
+    // remainder map).
+    constexpr int A = P * inv_mod(P % 3, 3), B = 3 * inv_mod(3 % P, P);
+    (void)tw;
+    (void)TS;
+    C a[3][P];
+#pragma unroll
+    for (int n1 = 0; n1 < 3; ++n1)
+#pragma unroll
+      for (int n2 = 0; n2 < P; ++n2) a[n1][n2] = v[(P * n1 + 3 * n2) % N];
+#pragma unroll
+    for (int n1 = 0; n1 < 3; ++n1) dft_small<P>(a[n1], SIGN);
+#pragma unroll
+    for (int k2 = 0; k2 < P; ++k2) {
+      C b[3] = {a[0][k2], a[1][k2], a[2][k2]};
+      dft3(b, SIGN);
+#pragma unroll
+      for (int k1 = 0; k1 < 3; ++k1) v[(A * k1 + B * k2) % N] = b[k1];
+    }
+  } else {
+    dft_3p_ct<N, SIGN>(v, tw, TS);
+  }
+}
+
+template <int N, int SIGN, typename C>
+__device__ __forceinline__ void dft_3p_ct(C* v, const C* __restrict__ tw, int TS) {
   constexpr int P = N / 3;
   C a[3][P];
 #pragma unroll

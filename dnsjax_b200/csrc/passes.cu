@@ -501,7 +501,7 @@ x_pass2_kernel(XPassArgs a) {
       }
       v[i] = z;
     }
-    dft_3p<R1, 1>(v, tw, 8);
+    dft_3p<R1, 1, CT, true>(v, tw, 8);
 #pragma unroll
     for (int i = 0; i < R1; ++i) X[(j * R1 + i) * CI + col + XS * j] = v[i];
   }
@@ -563,7 +563,7 @@ x_pass2_kernel(XPassArgs a) {
     for (int i = 0; i < R1; ++i) v[i] = Y[(j + 8 * i) * CF + col + i];
 #pragma unroll
     for (int i = 1; i < R1; ++i) v[i] = cmul(v[i], tw[i * j]);
-    dft_3p<R1, -1>(v, tw, 8);
+    dft_3p<R1, -1, CT, true>(v, tw, 8);
 #pragma unroll
     for (int i = 0; i < R1; ++i) X[(j + 8 * i) * CF + col] = v[i];
   }
