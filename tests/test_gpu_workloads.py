@@ -95,6 +95,23 @@ def test_couette_64_one_step():
     assert abs(res.errors[-1] - ref.errors[-1]) <= 1e-6 * ref.errors[-1]
 
 
+def test_couette_tall_wall_normal_grid():
+    """ny = 193 is beyond the batched IMM's wall-normal limit (160), so the
+    one-kernel IMM runs, and nx = nz = 16 (padded 24) takes the
+    runtime-planned passes: two steps against the oracle."""
+    from dnsjax_b200 import driver, initial
+    from oracle.stepper import run
+
+    flow, orc = couette(16, 193, 16, 4, 400.0, 0.01, max_iter=60)
+    u0 = initial.couette_field(16, 193, 16, 2 * pi, pi, 4, 3, 4.0, 1e-3)
+    res = driver.run(flow, dev(u0), 2)
+    ref = run(orc, u0, 2)
+    assert res.corrector_iterations == ref.corrector_iterations
+    got = host(res.state)
+    for c in range(3):
+        assert rel_l2(got[c], ref.state[c]) <= 1e-10, c
+
+
 @pytest.fixture(scope="module")
 def couette128():
     from dnsjax_b200 import initial
