@@ -1,0 +1,46 @@
+"""Host logic of bench.py, on the CPU: the algorithmic bytes behind every
+roofline figure (pinned to the per-workload values of the measurement
+plan), the segmenting of long timed runs, and strict-JSON output."""
+
+import json
+
+import pytest
+
+
+def test_algorithmic_bytes():
+    import bench
+
+    W = bench.WORKLOADS
+    mb = lambda x: round(x / 1e6, 2)  # noqa: E731
+    c128 = bench.op_bytes(W["couette128"])
+    assert (mb(c128["rhs"]), mb(c128["imm"])) == (557.18, 612.59)
+    c64 = bench.op_bytes(W["couette64"])
+    assert (mb(c64["rhs"]), mb(c64["imm"])) == (70.09, 64.01)
+    k32 = bench.op_bytes(W["kolmogorov32"])
+    assert (mb(k32["rhs"]), mb(k32["correct"])) == (18.95, 2.95)
+    assert mb(bench.op_bytes(W["kolmogorov128"])["rhs"]) == 1228.02
+    # mixed form: the state read and the RHS write stay complex128, the pass
+    # buffers are complex64
+    k128 = W["kolmogorov128"]
+    S = (k128["ny"] - 1) * (k128["nz"] - 1) * k128["nx"] // 2
+    f32 = bench.op_bytes(k128, fp32=True)["rhs"]
+    assert f32 == 16 * 6 * S + (bench.op_bytes(k128)["rhs"] - 16 * 6 * S) // 2
+
+
+@pytest.mark.parametrize("k,want", [(0, []), (1, [1]), (30, [30]), (31, [30, 1]),
+                                    (70, [30, 30, 10])])
+def test_segments(k, want):
+    import bench
+
+    assert bench.segments(k) == want
+    assert all(s <= bench.SEGMENT for s in want)
+
+
+def test_strict_json(capsys):
+    import bench
+
+    bench.emit({"value": float("nan"), "e2e": {"value": float("inf"), "n": 3},
+                "list": [1.0, float("-inf")]})
+    line = capsys.readouterr().out.strip()
+    d = json.loads(line)
+    assert d == {"value": None, "e2e": {"value": None, "n": 3}, "list": [1.0, None]}
