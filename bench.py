@@ -420,6 +420,29 @@ def run_ours(a, w, rank, world):
                        "bitwise_equal_state": bool(torch.equal(gstate, state))}
         last_err = e
 
+    # Kernel-level duration of each op: 10 back-to-back calls, no host
+    # synchronisation between them (the per-op events of the host loop can
+    # also hold host time between a call's launches).
+    reps = 10
+    rb = flow.get_rhs(snap)
+    ob = torch.empty_like(snap)
+    eb = torch.empty(1, dtype=torch.float64, device="cuda")
+
+    def time_op(fn):
+        fn()
+        torch.cuda.synchronize()
+        q0 = torch.cuda.Event(enable_timing=True)
+        q1 = torch.cuda.Event(enable_timing=True)
+        q0.record()
+        for _ in range(reps):
+            fn()
+        q1.record()
+        torch.cuda.synchronize()
+        return max_over_ranks(q0.elapsed_time(q1) / reps, dist, "cuda")
+
+    op_b2b = {"rhs": time_op(lambda: flow.get_rhs(snap, out=rb)),
+              "imm": time_op(lambda: flow.correct_fused(snap, snap, rb, rb, eb, out=ob))}
+
     traj_steps = a.warmup + segs[-1]  # the eager trajectory, for the mixed-form check
     # End to end through the public API: pinned host state in, new state out.
     host_in = torch.empty(state.shape, dtype=state.dtype, pin_memory=True)
@@ -454,8 +477,10 @@ def run_ours(a, w, rank, world):
     rhs_ms = tf.durations_ms("rhs")
     imm_ms = tf.durations_ms("imm")
     tot = {"rhs": sum(rhs_ms), "imm": sum(imm_ms)}
-    dom = max(tot, key=tot.get)
-    dur = (sum(imm_ms) / len(imm_ms)) if dom == "imm" else (sum(rhs_ms) / len(rhs_ms))
+    # dominant op: calls per run (host loop) x back-to-back duration
+    calls = {"rhs": len(rhs_ms), "imm": len(imm_ms)}
+    dom = max(op_b2b, key=lambda k: op_b2b[k] * calls[k])
+    dur = op_b2b[dom]
     corr_bytes = ob.get("imm", ob.get("correct"))
     bytes_ = corr_bytes if dom == "imm" else ob["rhs"]
     peaks = measured_peaks()
@@ -500,6 +525,7 @@ def run_ours(a, w, rank, world):
             "l2": "working set (state, operators, workspace) > 126 MB L2",
             "op_ms": {"rhs": sum(rhs_ms) / max(1, len(rhs_ms)),
                       "imm_or_correct": sum(imm_ms) / max(1, len(imm_ms))},
+            "op_ms_back_to_back": {"rhs": op_b2b["rhs"], "imm_or_correct": op_b2b["imm"]},
             "op_share": {k: v / eager_ms for k, v in tot.items()},
         },
         "roofline": {
@@ -516,6 +542,7 @@ def run_ours(a, w, rank, world):
             "peak_source": "measured" if peaks else "fallback",
             "algorithmic_bytes_per_launch": bytes_,
             "avg_launch_ms": dur,
+            "timing": "mean of 10 back-to-back calls of the op, CUDA events",
         },
         "e2e": {
             "value": nsteps / (e2e_ms * 1e-3),

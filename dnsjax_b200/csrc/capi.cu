@@ -296,7 +296,33 @@ static int periodic_rhs_impl(dnsb_periodic* p, const void* state, void* rhs, uns
   yi.tw = f32 ? reinterpret_cast<const double2*>(p->twy32) : p->twy;
   yi.fp32 = f32;
   yi.variant = p->var[0];
-  if (mask & 1u) DNSB_LAUNCH(launch_yinv(yi, st));
+  auto fixed = [](int L) { return L == 48 || L == 72 || L == 96 || L == 192; };
+  if ((mask & 1u) && p->var[0] == 0 && fixed(p->My)) {
+    // y inverse with the curl as a two-stage column pass: state
+    // [comp][ky][kz][kx] -> A[f][y][kz][kx]
+    ColPassArgs yc{};
+    yc.in = (const double2*)state;
+    yc.out = p->A;
+    yc.in_fs = (long long)p->NY1 * p->NZ1 * p->NKX;
+    yc.out_fs = (long long)p->My * p->NZ1 * p->NKX;
+    yc.in_os = p->NKX;
+    yc.out_os = p->NKX;
+    yc.in_ts = (long long)p->NZ1 * p->NKX;
+    yc.out_ts = (long long)p->NZ1 * p->NKX;
+    yc.nI = p->NKX;
+    yc.nstored = p->NY1;
+    yc.inverse = 1;
+    yc.plan = p->py;
+    yc.tw = yi.tw;
+    yc.fp32 = yc.out32 = f32;
+    yc.curl = 1;
+    yc.kx = p->kx;
+    yc.ky = p->ky;
+    yc.kz = p->kz;
+    DNSB_LAUNCH(launch_col_pass(yc, 6, p->NZ1, st));
+  } else if (mask & 1u) {
+    DNSB_LAUNCH(launch_yinv(yi, st));
+  }
   ColPassArgs zi = periodic_zinv(p);
   zi.fp32 = zi.out32 = f32;
   if (f32) zi.tw = reinterpret_cast<const double2*>(p->twz32);
@@ -1370,8 +1396,8 @@ extern "C" int dnsb_periodic_autotune(dnsb_periodic* p, const void* state, int r
   const int all[] = {0, 1, 2}, ypass[] = {0, 2}, only0[] = {0};
   int rc = 0;
   for (int k = 0; k < 5 && !rc; ++k) {
-    const int* vs = p->rhs_fp32 ? only0 : (k == 0 || k == 4) ? ypass : all;
-    const int nv = p->rhs_fp32 ? 1 : (k == 0 || k == 4) ? 2 : 3;
+    const int* vs = p->rhs_fp32 ? only0 : (k == 4) ? ypass : all;
+    const int nv = p->rhs_fp32 ? 1 : (k == 4) ? 2 : 3;
     const unsigned before = (1u << k) - 1u, self = 1u << k;
     rc = tune_one(
         p->var, k, vs, nv, reps, st, ms + 3 * k,

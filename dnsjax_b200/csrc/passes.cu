@@ -133,8 +133,10 @@ size_t col_pass2_smem(int M) {
 
 // T: the compute type and the element type of `in` (double, or float for the
 // FP32 forms, whose pass buffers hold float2); `out` is complex128, or with
-// OUT32 (FP32 only) an FP32 pass buffer.
-template <int ML, int SIGN, typename T = double, bool OUT32 = false>
+// OUT32 (FP32 only) an FP32 pass buffer.  CURL (inverse): `in` is the FP64
+// spectral state and field f of the 6 is u, v, w (f < 3) or the spectral
+// curl i (k x u) (triply_periodic.py:122-132), formed in FP64 at the load.
+template <int ML, int SIGN, typename T = double, bool OUT32 = false, bool CURL = false>
 __global__ void __launch_bounds__(kC2Threads)
 col_pass2_kernel(ColPassArgs a) {
   using CT = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
@@ -163,7 +165,26 @@ col_pass2_kernel(ColPassArgs a) {
       if (c < ni) {
         if (SIGN > 0) {
           const int sidx = pos_to_stored(t, a.nstored, M);
-          if (sidx >= 0) z = in[sidx * a.in_ts + c];
+          if (sidx >= 0) {
+            if constexpr (CURL) {
+              const double2* st = reinterpret_cast<const double2*>(a.in) + o * a.in_os + i0 +
+                                  (long long)sidx * a.in_ts + c;
+              const double2 u = st[0], vv = st[a.in_fs], w = st[2 * a.in_fs];
+              const double kx = a.kx[i0 + c], ky = a.ky[sidx], kz = a.kz[o];
+              double2 q;
+              switch (f) {
+                case 0: q = u; break;
+                case 1: q = vv; break;
+                case 2: q = w; break;
+                case 3: q = ci(make_double2(ky * w.x - kz * vv.x, ky * w.y - kz * vv.y)); break;
+                case 4: q = ci(make_double2(kz * u.x - kx * w.x, kz * u.y - kx * w.y)); break;
+                default: q = ci(make_double2(kx * vv.x - ky * u.x, kx * vv.y - ky * u.y)); break;
+              }
+              z = to_c(q, (CT*)nullptr);
+            } else {
+              z = in[sidx * a.in_ts + c];
+            }
+          }
         } else {
           z = in[t * a.in_ts + c];
         }
@@ -216,7 +237,11 @@ cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
     if (a.fp32 && a.inverse && !a.out32) return cudaErrorInvalidValue;
 #define DNSB_C2(LL)                                                                     \
   case LL:                                                                              \
-    if (a.fp32 && a.inverse)                                                            \
+    if (a.curl && a.fp32)                                                               \
+      col_pass2_kernel<LL, 1, float, true, true><<<g2, kC2Threads, sm2, st>>>(a);       \
+    else if (a.curl)                                                                    \
+      col_pass2_kernel<LL, 1, double, false, true><<<g2, kC2Threads, sm2, st>>>(a);     \
+    else if (a.fp32 && a.inverse)                                                       \
       col_pass2_kernel<LL, 1, float, true><<<g2, kC2Threads, sm2, st>>>(a);             \
     else if (a.fp32 && a.out32)                                                         \
       col_pass2_kernel<LL, -1, float, true><<<g2, kC2Threads, sm2, st>>>(a);            \
@@ -231,7 +256,7 @@ cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
 #undef DNSB_C2
     return cudaGetLastError();
   }
-  if (a.fp32) return cudaErrorInvalidValue;  // two-stage compile-time passes only
+  if (a.fp32 || a.curl) return cudaErrorInvalidValue;  // two-stage compile-time passes only
   dim3 grid((a.nI + kTile - 1) / kTile, nO, nfields);
   size_t sm = col_pass_smem(a.plan.L);
   DNSB_DISPATCH_V(a.variant, a.plan.L, col_pass_kernel, grid, sm, st, a);
@@ -1258,7 +1283,9 @@ cudaError_t set_pass_attributes(int max_smem) {
 #define DNSB_F32_PASSES(L)                                                          \
   (const void*)yinv_kernel<L, float>, (const void*)yfwd_kernel<L, float>,           \
       (const void*)col_pass2_kernel<L, 1, float, true>,                             \
-      (const void*)col_pass2_kernel<L, -1, float, true>
+      (const void*)col_pass2_kernel<L, -1, float, true>,                            \
+      (const void*)col_pass2_kernel<L, 1, float, true, true>,                       \
+      (const void*)col_pass2_kernel<L, 1, double, false, true>
                        DNSB_F32_PASSES(48), DNSB_F32_PASSES(72), DNSB_F32_PASSES(96),
                        DNSB_F32_PASSES(192)};
 #undef DNSB_F32_PASSES

@@ -34,6 +34,13 @@ struct ColPassArgs {
   int out32;           // with fp32: `out` is an FP32 pass buffer (always for inverse)
   int variant;         // 0: two-stage register pass when compiled for L, 1: Stockham
                        // stages (compile-time plan when compiled for L), 2: runtime plan
+  // curl (inverse only, two-stage pass): `in` is the FP64 spectral state
+  // [3][nstored][nO][nI] (component stride in_fs) and the 6 output fields are
+  // u, v, w and i (k x u) with k = (kx[inner], ky[stored], kz[outer])
+  int curl;
+  const double* kx;
+  const double* ky;
+  const double* kz;
 };
 
 // x pass.  Rows are (outer, inner) pairs; row r = outer * inner_n + inner

@@ -249,9 +249,9 @@ int dnsb_couette_norm_noalloc(const void* v, int nx, int ny, int nz, double ly,
 /* pass where it is compiled for the length (the default), 1 Stockham   */
 /* stages with the compile-time plan, 2 Stockham stages with the        */
 /* runtime plan; the FP32 forms have variant 0 only.                   */
-/*   periodic: chosen[5] for the y inverse, z inverse, x, z forward and */
-/*     y forward passes (the y passes: 0 or 2); ms[5][3] mean times     */
-/*     (-1 where not tried).                                            */
+/*   periodic: chosen[5] for the y inverse (0: two-stage pass with the  */
+/*     curl formed at the load), z inverse, x, z forward and y forward  */
+/*     (0 or 2) passes; ms[5][3] mean times (-1 where not tried).       */
 /*   Couette: chosen[4] for the z inverse, x and z forward passes and   */
 /*     the IMM (0 five-kernel batched form, 1 one-kernel register-window */
 /*     form, 2 one-kernel form); ms[4][3].                              */
