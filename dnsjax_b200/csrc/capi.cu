@@ -369,7 +369,29 @@ static int periodic_rhs_impl(dnsb_periodic* p, const void* state, void* rhs, uns
   yf.tw = f32 ? reinterpret_cast<const double2*>(p->twy32) : p->twy;
   yf.fp32 = f32;
   yf.variant = p->var[4];
-  if (mask & 16u) DNSB_LAUNCH(launch_yfwd(yf, st));
+  if ((mask & 16u) && p->var[4] == 0 && fixed(p->My)) {
+    // y forward as a two-stage column pass with truncation, A[f][y][kz][kx]
+    // -> rhs[comp][ky][kz][kx] (complex128), then the projection in place
+    ColPassArgs yc{};
+    yc.in = p->A;
+    yc.out = (double2*)rhs;
+    yc.in_fs = (long long)p->My * p->NZ1 * p->NKX;
+    yc.out_fs = p->S;
+    yc.in_os = p->NKX;
+    yc.out_os = p->NKX;
+    yc.in_ts = (long long)p->NZ1 * p->NKX;
+    yc.out_ts = (long long)p->NZ1 * p->NKX;
+    yc.nI = p->NKX;
+    yc.nstored = p->NY1;
+    yc.inverse = 0;
+    yc.plan = p->py;
+    yc.tw = yf.tw;
+    yc.fp32 = f32;
+    DNSB_LAUNCH(launch_col_pass(yc, 3, p->NZ1, st));
+    DNSB_LAUNCH(launch_periodic_project(p->point(), (double2*)rhs, st));
+  } else if (mask & 16u) {
+    DNSB_LAUNCH(launch_yfwd(yf, st));
+  }
   return 0;
 }
 
@@ -1393,11 +1415,11 @@ extern "C" int dnsb_periodic_autotune(dnsb_periodic* p, const void* state, int r
   for (int i = 0; i < 15; ++i) ms[i] = -1.0f;
   double2* rhs = nullptr;
   DNSB_CUDA(cudaMallocAsync(&rhs, 3 * (size_t)p->S * sizeof(double2), st));
-  const int all[] = {0, 1, 2}, ypass[] = {0, 2}, only0[] = {0};
+  const int all[] = {0, 1, 2}, only0[] = {0};
   int rc = 0;
   for (int k = 0; k < 5 && !rc; ++k) {
-    const int* vs = p->rhs_fp32 ? only0 : (k == 4) ? ypass : all;
-    const int nv = p->rhs_fp32 ? 1 : (k == 4) ? 2 : 3;
+    const int* vs = p->rhs_fp32 ? only0 : all;
+    const int nv = p->rhs_fp32 ? 1 : 3;
     const unsigned before = (1u << k) - 1u, self = 1u << k;
     rc = tune_one(
         p->var, k, vs, nv, reps, st, ms + 3 * k,

@@ -156,10 +156,10 @@ cudaError_t launch_periodic_stats(const PeriodicPointArgs& a,
   return cudaGetLastError();
 }
 
-// u - grad(inv_lapl div u), then the mean mode set to zero.
+// u - grad(inv_lapl div u), then (zero_mean) the mean mode set to zero.
 __global__ void periodic_cv_kernel(PeriodicPointArgs a,
                                    const double2* in, double2* out,
-                                   int divergence) {
+                                   int divergence, int zero_mean) {
   const int S = a.S;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S;
        s += gridDim.x * blockDim.x) {
@@ -177,7 +177,7 @@ __global__ void periodic_cv_kernel(PeriodicPointArgs a,
       u1 = cadd(u1, make_double2(-g1.x, -g1.y));
       u2 = cadd(u2, make_double2(-g2.x, -g2.y));
     }
-    if (s == 0) {
+    if (s == 0 && zero_mean) {
       u0 = u1 = u2 = make_double2(0.0, 0.0);
     }
     out[s] = u0;
@@ -189,7 +189,15 @@ __global__ void periodic_cv_kernel(PeriodicPointArgs a,
 cudaError_t launch_periodic_correct_velocity(const PeriodicPointArgs& a,
                                              const double2* in, double2* out,
                                              int divergence, cudaStream_t st) {
-  periodic_cv_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(a, in, out, divergence);
+  periodic_cv_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(a, in, out, divergence, 1);
+  return cudaGetLastError();
+}
+
+// The RHS projection NL - grad(inv_lapl div NL) (monochromatic.py:377-385),
+// in place, the mean mode kept.
+cudaError_t launch_periodic_project(const PeriodicPointArgs& a, double2* rhs,
+                                   cudaStream_t st) {
+  periodic_cv_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(a, rhs, rhs, 1, 0);
   return cudaGetLastError();
 }
 

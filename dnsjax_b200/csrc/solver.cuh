@@ -45,6 +45,8 @@ cudaError_t launch_periodic_norm2(const PeriodicPointArgs& a,
 cudaError_t launch_periodic_correct_velocity(const PeriodicPointArgs& a,
                                              const double2* in, double2* out,
                                              int divergence, cudaStream_t st);
+cudaError_t launch_periodic_project(const PeriodicPointArgs& a, double2* rhs,
+                                   cudaStream_t st);
 // partials[0..kRedBlocks) of k_metric|u|^2, partials[kRedBlocks..2 kRedBlocks)
 // of -lapl |u|^2.
 cudaError_t launch_periodic_stats(const PeriodicPointArgs& a,

@@ -251,7 +251,8 @@ int dnsb_couette_norm_noalloc(const void* v, int nx, int ny, int nz, double ly,
 /* runtime plan; the FP32 forms have variant 0 only.                   */
 /*   periodic: chosen[5] for the y inverse (0: two-stage pass with the  */
 /*     curl formed at the load), z inverse, x, z forward and y forward  */
-/*     (0 or 2) passes; ms[5][3] mean times (-1 where not tried).       */
+/*     (0: two-stage pass, then the projection as a separate pointwise  */
+/*     kernel) passes; ms[5][3] mean times (-1 where not tried).        */
 /*   Couette: chosen[4] for the z inverse, x and z forward passes and   */
 /*     the IMM (0 five-kernel batched form, 1 one-kernel register-window */
 /*     form, 2 one-kernel form); ms[4][3].                              */

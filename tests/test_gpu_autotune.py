@@ -45,7 +45,8 @@ def couette(n):
     return PlaneCouetteFlow(p), torch.as_tensor(u, device="cuda")
 
 
-@pytest.mark.parametrize("var", [[1, 0, 0, 0, 2], [2, 1, 1, 1, 0], [0, 2, 2, 2, 0]])
+@pytest.mark.parametrize("var", [[1, 0, 0, 0, 2], [2, 1, 1, 1, 0], [0, 2, 2, 2, 0],
+                                 [0, 0, 0, 0, 1]])
 def test_periodic_pass_variants(var):
     f, u = periodic(48)
     ref = f.get_rhs(u)
@@ -70,7 +71,7 @@ def test_autotune_choices_and_results():
     f, u = periodic(48)
     ref = f.get_rhs(u)
     t = f.autotune(u, reps=3)
-    assert len(t["variants"]) == 5 and t["variants"][4] in (0, 2)
+    assert len(t["variants"]) == 5 and all(v in (0, 1, 2) for v in t["variants"])
     for k, v in enumerate(t["variants"]):
         assert t["ms"][k][v] > 0 and t["ms"][k][v] == min(x for x in t["ms"][k] if x >= 0)
     assert rel(f.get_rhs(u), ref) < 1e-12
