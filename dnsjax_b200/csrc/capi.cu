@@ -1363,8 +1363,10 @@ int time_calls(F&& f, int reps, cudaStream_t st, float* ms) {
   return rc;
 }
 
-// Tunes pass k over `variants` (count nv): for each, `prefix` rebuilds the
-// pass's input, then the pass alone is timed; var[k] keeps the fastest.
+// Tunes pass k over `variants` (count nv, the default first): for each,
+// `prefix` rebuilds the pass's input, then the pass alone is timed; var[k]
+// keeps the fastest, but the default unless another is 5% faster (timing
+// noise does not move a pass to a variant of about the same speed).
 template <typename Prefix, typename Pass>
 int tune_one(int* var, int k, const int* variants, int nv, int reps, cudaStream_t st,
              float* ms_out, Prefix&& prefix, Pass&& pass) {
@@ -1382,6 +1384,7 @@ int tune_one(int* var, int k, const int* variants, int nv, int reps, cudaStream_
       pick = variants[i];
     }
   }
+  if (pick != variants[0] && best > 0.95f * ms_out[variants[0]]) pick = variants[0];
   var[k] = pick;
   return 0;
 }

@@ -244,8 +244,9 @@ int dnsb_couette_norm_noalloc(const void* v, int nx, int ny, int nz, double ly,
 /* Autotuning (no counterpart in the reference).  Times every kernel    */
 /* variant of each pass on the context's own sizes and buffers, from    */
 /* `state` (spectral, complex128), `reps` calls each after one warm-up  */
-/* call, and keeps the fastest for the context's later calls (and for   */
-/* step graphs created afterwards).  Variants: 0 the two-stage register */
+/* call, and keeps the fastest (the default unless another is 5%       */
+/* faster) for the context's later calls and later step graphs.        */
+/* Variants: 0 the two-stage register                                   */
 /* pass where it is compiled for the length (the default), 1 Stockham   */
 /* stages with the compile-time plan, 2 Stockham stages with the        */
 /* runtime plan; the FP32 forms have variant 0 only.                   */

@@ -73,7 +73,9 @@ def test_autotune_choices_and_results():
     t = f.autotune(u, reps=3)
     assert len(t["variants"]) == 5 and all(v in (0, 1, 2) for v in t["variants"])
     for k, v in enumerate(t["variants"]):
-        assert t["ms"][k][v] > 0 and t["ms"][k][v] == min(x for x in t["ms"][k] if x >= 0)
+        # the fastest, or the default when none is 5% faster than it
+        fastest = min(x for x in t["ms"][k] if x >= 0)
+        assert t["ms"][k][v] == fastest or (v == 0 and fastest > 0.95 * t["ms"][k][0])
     assert rel(f.get_rhs(u), ref) < 1e-12
 
     c, uc = couette(32)
