@@ -2,7 +2,6 @@
 
 import os
 
-import pytest
 import torch.multiprocessing as mp
 
 
