@@ -33,6 +33,41 @@ constexpr int kTile = 16;       // items per substitution CTA (two sides per ite
 constexpr int kStageWarps = 4;  // modes per CTA in the stage kernels
 constexpr int kSYM = 5;         // y values per lane: y = lane + 32 k, Ny <= 160
 
+// L2 residency of the workspaces F and R (K Ny and 3 K Ny complex, 67 MB at
+// 128x129x128, each touched about three times per call): their writes and
+// the substitutions' accesses carry an evict_last policy, and their last
+// reads (F in stage 3, R in stage 6) evict_first, so the streamed inputs do
+// not push them out of the 126 MB L2 between the kernels of one call.
+__device__ __forceinline__ unsigned long long l2_keep() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ unsigned long long l2_drop() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ void st_l2(double2* g, double2 v, unsigned long long pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;\n" ::"l"(g), "d"(v.x),
+               "d"(v.y), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ double2 ld_l2(const double2* g, unsigned long long pol) {
+  double2 v;
+  asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;\n"
+               : "=d"(v.x), "=d"(v.y)
+               : "l"(g), "l"(pol)
+               : "memory");
+  return v;
+}
+__device__ __forceinline__ void cp_async16_l2(void* smem, const void* g, unsigned long long pol) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(s), "l"(g),
+               "l"(pol)
+               : "memory");
+}
+
 // Banded stencil row y applied to x: sum_m w[m][y] x[j0[y] + m], with the
 // weights stored tap-major ([S][Ny]) so the lanes of a warp (consecutive y)
 // read each tap's weights contiguously.
@@ -138,6 +173,7 @@ imm_stage01_kernel(ImmArgs a, const double2* __restrict__ vel_n,
   const double kx = a.kx[ix], kz = a.kz[iz];
   const double k2 = kx * kx + kz * kz;
   const double c = a.c, dt = a.dt, omc = 1.0 - c, omc_nu = omc * a.nu;
+  const unsigned long long keep = l2_keep();
   double2 ua[YM], wa[YM], uj[YM], wj[YM], un[YM], wn[YM];
 #pragma unroll
   for (int k = 0; k < YM; ++k) {
@@ -177,7 +213,7 @@ imm_stage01_kernel(ImmArgs a, const double2* __restrict__ vel_n,
       const double2 dd = make_double2(dy.x / dt, dy.y / dt);
       fy = cadd(cadd(cadd(dd, cscale(divNj, c)), cscale(divNn, omc)), cscale(Lkd, omc_nu));
     }
-    F[mo + y] = fy;
+    st_l2(F + mo + y, fy, keep);
   }
 }
 
@@ -198,11 +234,12 @@ imm_stage3_kernel(ImmArgs a, const double2* __restrict__ vel_n,
   double2* T = sm + wq * 4 * Ny;  // u^n, v^n, w^n
   double2* Pp = T + 3 * Ny;       // p_P
   const long long CS = (long long)NM * Ny, mo = (long long)m * Ny;
+  const unsigned long long keep = l2_keep(), drop = l2_drop();
   for (int y = lane; y < Ny; y += 32) {
     cp_async16(T + y, vel_n + mo + y);
     cp_async16(T + Ny + y, vel_n + CS + mo + y);
     cp_async16(T + 2 * Ny + y, vel_n + 2 * CS + mo + y);
-    cp_async16(Pp + y, P + mo + y);
+    cp_async16_l2(Pp + y, P + mo + y, drop);
   }
   cp_async_commit();
   const int iz = m / NKX, ix = m % NKX;
@@ -244,9 +281,9 @@ imm_stage3_kernel(ImmArgs a, const double2* __restrict__ vel_n,
       rv = cadd(cadd(csub(hv, dyp), cscale(nj[1][k], c)), cscale(nn[1][k], omc));
       rw = cadd(cadd(csub(hw, dzp), cscale(nj[2][k], c)), cscale(nn[2][k], omc));
     }
-    R[mo + y] = ru;
-    R[CS + mo + y] = rv;
-    R[2 * CS + mo + y] = rw;
+    st_l2(R + mo + y, ru, keep);
+    st_l2(R + CS + mo + y, rv, keep);
+    st_l2(R + 2 * CS + mo + y, rw, keep);
   }
 }
 
@@ -269,6 +306,7 @@ imm_stage6_kernel(ImmArgs a, const double2* __restrict__ R, const double2* vel_j
   const double k2 = kx * kx + kz * kz;
   double2 vj[3][YM], ra[3][YM];
   double c1[YM], c2[YM], e1[YM], e2[YM];
+  const unsigned long long drop = l2_drop();
 #pragma unroll
   for (int k = 0; k < YM; ++k) {
     const int y = lane + 32 * k;
@@ -276,7 +314,7 @@ imm_stage6_kernel(ImmArgs a, const double2* __restrict__ R, const double2* vel_j
 #pragma unroll
       for (int cpt = 0; cpt < 3; ++cpt) {
         vj[cpt][k] = vel_j[cpt * CS + mo + y];
-        ra[cpt][k] = R[cpt * CS + mo + y];
+        ra[cpt][k] = ld_l2(R + cpt * CS + mo + y, drop);
       }
       c1[k] = a.v1[mo + y];
       c2[k] = a.v2[mo + y];
@@ -440,7 +478,8 @@ template <int KL, int NCP, int MW, int MODE, bool TAIL>
 __device__ __forceinline__ void tile_fwd_block(double2* const (&col)[NCP], int j0, int nsteps,
                                                int Ny, bool live, double (&w)[2 * NCP][KL + 1],
                                                const double2* Lp, const int (&dr)[KL + 1],
-                                               const double2* ent, int ES) {
+                                               const double2* ent, int ES,
+                                               unsigned long long pol) {
   constexpr int W = KL + 1;
 #pragma unroll
   for (int ph = 0; ph < W; ++ph) {
@@ -458,7 +497,8 @@ __device__ __forceinline__ void tile_fwd_block(double2* const (&col)[NCP], int j
       for (int c = 0; c < 2 * NCP; ++c) bp[c] = pivot_take<KL, MODE>(w[c], ph, dr[ph]);
       if (live) {
 #pragma unroll
-        for (int cc = 0; cc < NCP; ++cc) col[cc][j] = make_double2(bp[2 * cc], bp[2 * cc + 1]);
+        for (int cc = 0; cc < NCP; ++cc)
+          st_l2(col[cc] + j, make_double2(bp[2 * cc], bp[2 * cc + 1]), pol);
       }
 #pragma unroll
       for (int c = 0; c < 2 * NCP; ++c) {
@@ -480,7 +520,8 @@ __device__ __forceinline__ void tile_fwd_block(double2* const (&col)[NCP], int j
 template <int NU, int NCP, int MW, bool TAIL>
 __device__ __forceinline__ void tile_bwd_block(double2* const (&col)[NCP], int j0, bool live,
                                                double (&w)[2 * NCP][NU + 1], const double2* Up,
-                                               const double2* ent, int ES) {
+                                               const double2* ent, int ES,
+                                               unsigned long long pol) {
   constexpr int WB = NU + 1, NUP = (NU + 2) & ~1;
 #pragma unroll
   for (int ph = 0; ph < WB; ++ph) {
@@ -501,7 +542,7 @@ __device__ __forceinline__ void tile_bwd_block(double2* const (&col)[NCP], int j
       if (live) {
 #pragma unroll
         for (int cc = 0; cc < NCP; ++cc)
-          col[cc][j] = make_double2(bj[2 * cc] * U[0], bj[2 * cc + 1] * U[0]);
+          st_l2(col[cc] + j, make_double2(bj[2 * cc] * U[0], bj[2 * cc + 1] * U[0]), pol);
       }
 #pragma unroll
       for (int i = 1; i <= NU; ++i) {
@@ -539,6 +580,7 @@ imm_solve_kernel(SolveArgs a) {
   const long long NyF = Ny + W, NyB = Ny + WB;
   int m;
   const bool live = item_mode(a, tile * kTile + it, side, &m);
+  const unsigned long long keep = l2_keep();
   double2* col[NCP];
 #pragma unroll
   for (int cc = 0; cc < NCP; ++cc) col[cc] = a.X + ((long long)(cw + cc) * a.NM + m) * Ny;
@@ -576,7 +618,7 @@ imm_solve_kernel(SolveArgs a) {
           for (int ph = 0; ph < W; ++ph) {
             const int e = j0 + W + ph;
             if (e < Ny)
-              for (int cc = 0; cc < NCP; ++cc) cp_async16(ent + (cc * MW + ph) * nthr, col[cc] + e);
+              for (int cc = 0; cc < NCP; ++cc) cp_async16_l2(ent + (cc * MW + ph) * nthr, col[cc] + e, keep);
           }
         }
       } else {
@@ -590,7 +632,7 @@ imm_solve_kernel(SolveArgs a) {
           for (int ph = 0; ph < WB; ++ph) {
             const int e = j0 - WB - ph;
             if (e >= 0)
-              for (int cc = 0; cc < NCP; ++cc) cp_async16(ent + (cc * MW + ph) * nthr, col[cc] + e);
+              for (int cc = 0; cc < NCP; ++cc) cp_async16_l2(ent + (cc * MW + ph) * nthr, col[cc] + e, keep);
           }
         }
       }
@@ -615,7 +657,7 @@ imm_solve_kernel(SolveArgs a) {
     for (int cc = 0; cc < NCP; ++cc) {
 #pragma unroll
       for (int o = 0; o < W; ++o) {
-        const double2 v = (o < Ny) ? col[cc][o] : make_double2(0.0, 0.0);
+        const double2 v = (o < Ny) ? ld_l2(col[cc] + o, keep) : make_double2(0.0, 0.0);
         w[2 * cc][o] = v.x;
         w[2 * cc + 1][o] = v.y;
       }
@@ -637,13 +679,13 @@ imm_solve_kernel(SolveArgs a) {
       dm = __reduce_max_sync(0xffffffffu, dm);
       const int j0 = k * W;
       if (j0 + W > nsteps)
-        tile_fwd_block<KL, NCP, MW, 2, true>(col, j0, nsteps, Ny, live, w, Lp, dr, ent, nthr);
+        tile_fwd_block<KL, NCP, MW, 2, true>(col, j0, nsteps, Ny, live, w, Lp, dr, ent, nthr, keep);
       else if (dm == 0)
-        tile_fwd_block<KL, NCP, MW, 0, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent, nthr);
+        tile_fwd_block<KL, NCP, MW, 0, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent, nthr, keep);
       else if (dm == 1)
-        tile_fwd_block<KL, NCP, MW, 1, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent, nthr);
+        tile_fwd_block<KL, NCP, MW, 1, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent, nthr, keep);
       else
-        tile_fwd_block<KL, NCP, MW, 2, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent, nthr);
+        tile_fwd_block<KL, NCP, MW, 2, false>(col, j0, nsteps, Ny, live, w, Lp, dr, ent, nthr, keep);
       __syncthreads();  // the slot is refilled by the next issue
       if (s_fail) {
         ok = false;
@@ -661,7 +703,7 @@ imm_solve_kernel(SolveArgs a) {
           v0 = w[2 * cc][s];
           v1 = w[2 * cc + 1][s];
         }
-      if (live && ok) col[cc][Ny - 1] = make_double2(v0, v1);
+      if (live && ok) st_l2(col[cc] + Ny - 1, make_double2(v0, v1), keep);
     }
   }
 
@@ -675,7 +717,7 @@ imm_solve_kernel(SolveArgs a) {
 #pragma unroll
       for (int o = 0; o < WB; ++o) {
         const int idx = Ny - 1 - NU + o;
-        const double2 v = (idx >= 0) ? col[cc][idx] : make_double2(0.0, 0.0);
+        const double2 v = (idx >= 0) ? ld_l2(col[cc] + idx, keep) : make_double2(0.0, 0.0);
         w[2 * cc][o] = v.x;
         w[2 * cc + 1][o] = v.y;
       }
@@ -688,9 +730,9 @@ imm_solve_kernel(SolveArgs a) {
       const double2* ent = reinterpret_cast<const double2*>(slot + SB - EB) + tid;
       const int j0 = Ny - 1 - k * WB;
       if (j0 - WB + 1 < 0)
-        tile_bwd_block<NU, NCP, MW, true>(col, j0, live, w, Up, ent, nthr);
+        tile_bwd_block<NU, NCP, MW, true>(col, j0, live, w, Up, ent, nthr, keep);
       else
-        tile_bwd_block<NU, NCP, MW, false>(col, j0, live, w, Up, ent, nthr);
+        tile_bwd_block<NU, NCP, MW, false>(col, j0, live, w, Up, ent, nthr, keep);
       __syncthreads();
       if (s_fail) {
         ok = false;
