@@ -425,6 +425,72 @@ __device__ __forceinline__ void cp_async_elem(double2* smem, const double2* gmem
 __device__ __forceinline__ void cp_async_elem(float2* smem, const float2* gmem) {
   cp_async8(smem, gmem);
 }
+// L2 eviction priority of global accesses: a policy from createpolicy,
+// carried by .L2::cache_hint loads, stores and cp.async copies.  l2_keep:
+// every line evict_last; l2_keep_half: evict_last on half of the lines
+// (address-hashed), the rest unchanged; l2_drop: evict_first.
+__device__ __forceinline__ unsigned long long l2_keep() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ unsigned long long l2_keep_half() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_last.L2::evict_unchanged.b64 %0, 0.5;\n"
+               : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ unsigned long long l2_drop() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ void st_l2(double2* g, double2 v, unsigned long long pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;\n" ::"l"(g), "d"(v.x),
+               "d"(v.y), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void st_l2(float2* g, float2 v, unsigned long long pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;\n" ::"l"(g), "f"(v.x),
+               "f"(v.y), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ double2 ld_l2(const double2* g, unsigned long long pol) {
+  double2 v;
+  asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;\n"
+               : "=d"(v.x), "=d"(v.y)
+               : "l"(g), "l"(pol)
+               : "memory");
+  return v;
+}
+__device__ __forceinline__ float2 ld_l2(const float2* g, unsigned long long pol) {
+  float2 v;
+  asm volatile("ld.global.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;\n"
+               : "=f"(v.x), "=f"(v.y)
+               : "l"(g), "l"(pol)
+               : "memory");
+  return v;
+}
+__device__ __forceinline__ void cp_async16_l2(void* smem, const void* g, unsigned long long pol) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(s), "l"(g),
+               "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8_l2(void* smem, const void* g, unsigned long long pol) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 8, %2;\n" ::"r"(s), "l"(g),
+               "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_elem_l2(double2* smem, const double2* g,
+                                                 unsigned long long pol) {
+  cp_async16_l2(smem, g, pol);
+}
+__device__ __forceinline__ void cp_async_elem_l2(float2* smem, const float2* g,
+                                                 unsigned long long pol) {
+  cp_async8_l2(smem, g, pol);
+}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }

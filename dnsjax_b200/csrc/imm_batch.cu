@@ -37,36 +37,8 @@ constexpr int kSYM = 5;         // y values per lane: y = lane + 32 k, Ny <= 160
 // 128x129x128, each touched about three times per call): their writes and
 // the substitutions' accesses carry an evict_last policy, and their last
 // reads (F in stage 3, R in stage 6) evict_first, so the streamed inputs do
-// not push them out of the 126 MB L2 between the kernels of one call.
-__device__ __forceinline__ unsigned long long l2_keep() {
-  unsigned long long p;
-  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
-  return p;
-}
-__device__ __forceinline__ unsigned long long l2_drop() {
-  unsigned long long p;
-  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
-  return p;
-}
-__device__ __forceinline__ void st_l2(double2* g, double2 v, unsigned long long pol) {
-  asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;\n" ::"l"(g), "d"(v.x),
-               "d"(v.y), "l"(pol)
-               : "memory");
-}
-__device__ __forceinline__ double2 ld_l2(const double2* g, unsigned long long pol) {
-  double2 v;
-  asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;\n"
-               : "=d"(v.x), "=d"(v.y)
-               : "l"(g), "l"(pol)
-               : "memory");
-  return v;
-}
-__device__ __forceinline__ void cp_async16_l2(void* smem, const void* g, unsigned long long pol) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(s), "l"(g),
-               "l"(pol)
-               : "memory");
-}
+// not push them out of the 126 MB L2 between the kernels of one call
+// (l2_keep / l2_drop and the hinted accesses are in common.cuh).
 
 // Banded stencil row y applied to x: sum_m w[m][y] x[j0[y] + m], with the
 // weights stored tap-major ([S][Ny]) so the lanes of a warp (consecutive y)

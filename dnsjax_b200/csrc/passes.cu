@@ -153,6 +153,7 @@ col_pass2_kernel(ColPassArgs a) {
   double2* out = a.out + f * a.out_fs + o * a.out_os + i0;
   CT* out_c = reinterpret_cast<CT*>(a.out) + f * a.out_fs + o * a.out_os + i0;
   const int ni = min(C, a.nI - i0);
+  const unsigned long long drop = l2_drop();
   load_twiddles(tw, reinterpret_cast<const CT*>(a.tw), M);
   __syncthreads();
   for (int it = tid; it < 8 * C; it += kC2Threads) {
@@ -186,7 +187,7 @@ col_pass2_kernel(ColPassArgs a) {
             }
           }
         } else {
-          z = in[t * a.in_ts + c];
+          z = ld_l2(in + t * a.in_ts + c, drop);  // the input's last use
         }
       }
       v[i] = z;
@@ -484,6 +485,9 @@ x_pass2_kernel(XPassArgs a) {
   }
   for (int i = tid; i < M; i += kX2Threads) cp_async_elem(tw + i, gtw + i);
   __syncthreads();
+  // The input's last use (evict_first); the output is the next pass's input
+  // (evict_last).
+  const unsigned long long drop = l2_drop(), keep = l2_keep();
   for (int idx = tid; idx < 6 * NKX * R; idx += kX2Threads) {
     int r, k, f;
     if (a.rows_fast) {
@@ -496,7 +500,7 @@ x_pass2_kernel(XPassArgs a) {
       f = idx / (R * NKX);
     }
     CT* dst = S + (f * NKX + k) * R + r;
-    if (r < nr) cp_async_elem(dst, gin + f * a.in_fs + s_off[r] + k * a.ks);
+    if (r < nr) cp_async_elem_l2(dst, gin + f * a.in_fs + s_off[r] + k * a.ks, drop);
     else *dst = cmake<CT>(0, 0);
   }
   cp_async_commit();
@@ -616,7 +620,7 @@ x_pass2_kernel(XPassArgs a) {
     } else {
       v = cmake<CT>((Z.x + Zm.x) * h, (Z.y - Zm.y) * h);
     }
-    gout[f * a.out_fs + s_off[r] + k * a.ks] = v;
+    st_l2(gout + f * a.out_fs + s_off[r] + k * a.ks, v, keep);
   }
 }
 
@@ -1178,6 +1182,9 @@ zinv_curl2_kernel(ZInvCurlArgs a) {
   const double2* Wc = U + 2 * cs;
   const int nf = a.curl ? 6 : 3;
   const long long fs = (long long)M * ncol;
+  // Half of the pass buffer's lines stay in L2 for the x pass that reads
+  // them next (all of them would not fit beside the rest).
+  const unsigned long long keep = l2_keep_half();
   for (int f = 0; f < nf; ++f) {
     switch (f) {
       case 0: zinv2_fill<M, 0>(a, X, U, V, Wc, ncol, y, kx, live); break;
@@ -1217,7 +1224,7 @@ zinv_curl2_kernel(ZInvCurlArgs a) {
       if (c < nq) {
 #pragma unroll
         for (int i = 0; i < 8; ++i)
-          gout[f * fs + (long long)(k + R1 * i) * ncol + q0 + c] = z[i];
+          st_l2(gout + f * fs + (long long)(k + R1 * i) * ncol + q0 + c, z[i], keep);
       }
     }
     __syncthreads();  // X is refilled by the next field
