@@ -17,6 +17,8 @@ from __future__ import annotations
 import numpy as np
 from scipy.linalg.lapack import get_lapack_funcs
 
+from . import parallel
+
 from .config import Config
 from .fft import (
     complex_harmonics,
@@ -127,7 +129,17 @@ def banded_solve(ab, ipiv, b, kl, ku):
     """cartesian.py:360-441 (dgbtrs 'N'), vectorised over leading axes.
 
     ``ab``: (..., 2kl+ku+1, Ny); ``ipiv``: (..., Ny); ``b``: (..., Ny) real.
+    With oracle.parallel threads, the modes of the first leading axis are
+    split over them.
     """
+    ab, ipiv, b = np.asarray(ab), np.asarray(ipiv), np.asarray(b)
+    if ab.ndim >= 3 and ab.shape[:-2] == ipiv.shape[:-1] == b.shape[:-1]:
+        return parallel.split(lambda a_, p_, b_: _banded_solve_serial(a_, p_, b_, kl, ku),
+                              (ab, ipiv, b), 0, n=parallel.SOLVE_THREADS_MAX)
+    return _banded_solve_serial(ab, ipiv, b, kl, ku)
+
+
+def _banded_solve_serial(ab, ipiv, b, kl, ku):
     ab = np.asarray(ab)
     Ny = ab.shape[-1]
     lead = ab.shape[:-2]
@@ -272,8 +284,8 @@ class CouetteSetup:
     def curl(self, s):
         """plane_couette.py:251-271: D1 in y, i k in x and z."""
         u, v, w = s
-        dy_u = np.einsum("ij,zxj->zxi", self.D1, u)
-        dy_w = np.einsum("ij,zxj->zxi", self.D1, w)
+        dy_u = parallel.einsum_y(self.D1, u)
+        dy_w = parallel.einsum_y(self.D1, w)
         kx, kz = self.kx, self.kz
         return np.array(
             [dy_w - 1j * kz * v, 1j * kz * u - 1j * kx * w, 1j * kx * v - dy_u]
@@ -294,7 +306,7 @@ class CouetteSetup:
 
     def lk_matvec(self, u):
         """plane_couette.py:299-338."""
-        D2u = np.einsum("ij,zxj->zxi", self.D2, u)
+        D2u = parallel.einsum_y(self.D2, u)
         out = D2u - self.k2 * u
         bot_n = np.einsum("j,zxj->zx", self.D1_bnd[0], u)
         bot = np.where(self.k2_is_zero[..., 0], u[..., 0], bot_n)
@@ -307,7 +319,7 @@ class CouetteSetup:
     def hk_minus_matvec(self, u):
         """plane_couette.py:341-373."""
         c, dt, nu = self.cfg.implicitness, self.cfg.dt, self.nu
-        D2u = np.einsum("ij,zxj->zxi", self.D2, u)
+        D2u = parallel.einsum_y(self.D2, u)
         out = (1.0 / dt) * u + (1.0 - c) * nu * (D2u - self.k2 * u)
         out = out.copy()
         out[..., 0] = u[..., 0]
@@ -323,10 +335,10 @@ class CouetteSetup:
         Nu_n, Nv_n, Nw_n = nl_n
         Nu_j, Nv_j, Nw_j = nl_j
         D1 = self.D1
-        dy_v_n = np.einsum("ij,zxj->zxi", D1, v_n)
+        dy_v_n = parallel.einsum_y(D1, v_n)
         d_hat = 1j * kx * u_n + dy_v_n + 1j * kz * w_n
-        div_Nj = 1j * kx * Nu_j + np.einsum("ij,zxj->zxi", D1, Nv_j) + 1j * kz * Nw_j
-        div_Nn = 1j * kx * Nu_n + np.einsum("ij,zxj->zxi", D1, Nv_n) + 1j * kz * Nw_n
+        div_Nj = 1j * kx * Nu_j + parallel.einsum_y(D1, Nv_j) + 1j * kz * Nw_j
+        div_Nn = 1j * kx * Nu_n + parallel.einsum_y(D1, Nv_n) + 1j * kz * Nw_n
         Lk_d = self.lk_matvec(d_hat)
         f_hat = d_hat / dt + c * div_Nj + (1 - c) * div_Nn + (1 - c) * nu * Lk_d
         f_hat = f_hat.copy()
@@ -334,7 +346,7 @@ class CouetteSetup:
         f_hat[..., -1] = 0.0
         pP = banded_solve_complex(imm["Lk_ab"], imm["Lk_piv"], f_hat, kl, ku)
         dx_p = 1j * kx * pP
-        dy_p = np.einsum("ij,zxj->zxi", D1, pP)
+        dy_p = parallel.einsum_y(D1, pP)
         dz_p = 1j * kz * pP
         Ru = self.hk_minus_matvec(u_n) - dx_p + c * Nu_j + (1 - c) * Nu_n
         Rv = self.hk_minus_matvec(v_n) - dy_p + c * Nv_j + (1 - c) * Nv_n

@@ -5,12 +5,15 @@ Restates ``src/dnsjax/fft.py`` and the transform wrappers of
 transform divides by N, the inverse applies no factor.  Nyquist modes are
 never stored.  ``numpy.fft`` implements the same transform definitions as
 ``jax.numpy.fft`` (the reference's FFT dependency, jax 0.10.0 per
-``uv.lock:42-58``).
+``uv.lock:42-58``).  With oracle.parallel threads, each transform's lines
+are split over them (bitwise the same result).
 """
 
 from __future__ import annotations
 
 import numpy as np
+
+from . import parallel
 
 NORM = "forward"
 
@@ -68,31 +71,31 @@ def truncate_rfft(a: np.ndarray, n: int) -> np.ndarray:
 
 def rfft3d(x: np.ndarray, nx: int, ny: int, nz: int) -> np.ndarray:
     """fft.py:291-348: physical [y,z,x] -> spectral [ky,kz,kx], x->z->y."""
-    y = truncate_rfft(np.fft.rfft(x, axis=2, norm=NORM), nx // 2)
-    y = truncate_fft(np.fft.fft(y, axis=1, norm=NORM), nz, 1)
-    y = truncate_fft(np.fft.fft(y, axis=0, norm=NORM), ny, 0)
+    y = truncate_rfft(parallel.fft(np.fft.rfft, x, 2, norm=NORM), nx // 2)
+    y = truncate_fft(parallel.fft(np.fft.fft, y, 1, norm=NORM), nz, 1)
+    y = truncate_fft(parallel.fft(np.fft.fft, y, 0, norm=NORM), ny, 0)
     return y
 
 
 def irfft3d(x: np.ndarray, nx_p: int, ny_p: int, nz_p: int) -> np.ndarray:
     """fft.py:351-408: spectral [ky,kz,kx] -> physical [y,z,x], y->z->x."""
-    y = np.fft.ifft(zeropad_fft(x, ny_p, 0), axis=0, norm=NORM)
-    y = np.fft.ifft(zeropad_fft(y, nz_p, 1), axis=1, norm=NORM)
+    y = parallel.fft(np.fft.ifft, zeropad_fft(x, ny_p, 0), 0, norm=NORM)
+    y = parallel.fft(np.fft.ifft, zeropad_fft(y, nz_p, 1), 1, norm=NORM)
     y = zeropad_rfft(y, nx_p // 2 + 1)
-    return np.fft.irfft(y, axis=2, norm=NORM)
+    return parallel.fft(np.fft.irfft, y, 2, norm=NORM)
 
 
 def rfft2d(x: np.ndarray, nx: int, nz: int) -> np.ndarray:
     """fft.py:193-240: physical [y,z,x] -> [y,kz,kx], x then z."""
-    y = truncate_rfft(np.fft.rfft(x, axis=2, norm=NORM), nx // 2)
-    return truncate_fft(np.fft.fft(y, axis=1, norm=NORM), nz, 1)
+    y = truncate_rfft(parallel.fft(np.fft.rfft, x, 2, norm=NORM), nx // 2)
+    return truncate_fft(parallel.fft(np.fft.fft, y, 1, norm=NORM), nz, 1)
 
 
 def irfft2d(x: np.ndarray, nx_p: int, nz_p: int) -> np.ndarray:
     """fft.py:243-288: [y,kz,kx] -> physical [y,z,x], z then x."""
-    y = np.fft.ifft(zeropad_fft(x, nz_p, 1), axis=1, norm=NORM)
+    y = parallel.fft(np.fft.ifft, zeropad_fft(x, nz_p, 1), 1, norm=NORM)
     y = zeropad_rfft(y, nx_p // 2 + 1)
-    return np.fft.irfft(y, axis=2, norm=NORM)
+    return parallel.fft(np.fft.irfft, y, 2, norm=NORM)
 
 
 # operators.py:59-146: vmapped wrappers over the 3 velocity components.
