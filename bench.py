@@ -746,11 +746,13 @@ def run_learned(a, w, rank, world):
 
 
 def host_threads() -> int:
-    """Host threads this process may run on."""
+    """Host threads this process may run on, at most 32 (the oracle's slices
+    of 127 or 128 rows stop shrinking usefully beyond that)."""
     try:
-        return len(os.sched_getaffinity(0))
+        n = len(os.sched_getaffinity(0))
     except (AttributeError, OSError):
-        return os.cpu_count() or 1
+        n = os.cpu_count() or 1
+    return max(1, min(n, 32))
 
 
 THREADS_NOTE = ("FFT lines, y-stencils and banded solves split over the threads, "

@@ -47,7 +47,8 @@ def split(fn, arrays, axis: int, n: int | None = None):
     along the same axis of the result."""
     n = _threads if n is None else min(n, _threads)
     size = arrays[0].shape[axis]
-    if n <= 1 or _pool is None or size < 2 * n:
+    n = min(n, size // 2)  # slices of at least two rows
+    if n <= 1 or _pool is None:
         return fn(*arrays)
     edges = np.linspace(0, size, n + 1).astype(int)
 

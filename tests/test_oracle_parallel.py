@@ -63,8 +63,13 @@ def test_split_falls_back_to_the_serial_call():
     parallel.set_threads(4)
     try:
         x = np.arange(6.0).reshape(3, 2)
-        # 3 rows cannot make 4 slices of at least 2: the serial call
+        # 3 rows make one slice of at least 2 rows: the serial call
         assert np.array_equal(parallel.split(lambda a: a * 2, (x,), 0), x * 2)
+        # 5 rows make two slices (not four)
+        y = np.arange(10.0).reshape(5, 2)
+        sizes = []
+        parallel.split(lambda a: sizes.append(a.shape[0]) or a, (y,), 0)
+        assert sorted(sizes) == [2, 3]
     finally:
         parallel.set_threads(1)
     assert parallel.threads() == 1
