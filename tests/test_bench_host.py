@@ -1,6 +1,7 @@
 """Host logic of bench.py, on the CPU: the algorithmic bytes behind every
 roofline figure (pinned to the per-workload values of the measurement
-plan), the segmenting of long timed runs, and strict-JSON output."""
+plan), the segmenting of long timed runs, strict-JSON output, and the
+threads of the oracle's cpu_baseline leg."""
 
 import json
 
@@ -44,3 +45,17 @@ def test_strict_json(capsys):
     line = capsys.readouterr().out.strip()
     d = json.loads(line)
     assert d == {"value": None, "e2e": {"value": None, "n": 3}, "list": [1.0, None]}
+
+
+def test_cpu_sample_uses_the_host_threads():
+    """The cpu_baseline leg on the oracle: threads reported as cores, the
+    pool back at one thread afterwards."""
+    import bench
+    from oracle import parallel
+
+    w = bench.WORKLOADS["kolmogorov32"]
+    r = bench.cpu_sample(w, None, bench.initial_state(w, w["seed"]), 3)
+    assert r["kind"] == "port" and r["value"] > 0
+    assert r["cores"] == bench.host_threads() and 1 <= r["cores"] <= 32
+    assert f"{r['cores']} host threads" in r["sample"]
+    assert parallel.threads() == 1
