@@ -2,9 +2,10 @@
 
 Same sections, field names, defaults and validation as
 ``src/dnsjax/parameters.py:26-133`` (``dist``, ``phys``, ``geo``, ``res``,
-``init``, ``outs``, ``step``, ``stop``, ``debug``, ``solver``), with one
-addition: ``solver.backend`` accepts ``"cuda"``, which selects this
-package's kernels (and is this package's default).  ``update_parameters``
+``init``, ``outs``, ``step``, ``stop``, ``debug``, ``solver``), with two
+differences: ``solver.backend`` accepts ``"cuda"``, which selects this
+package's kernels (and is this package's default), and ``dist.platform``
+defaults to ``"cuda"`` (the reference's default is ``"cpu"``).  ``update_parameters``
 applies only explicitly-set fields and recomputes the derived values as the
 reference does (``parameters.py:173-211``), including the reset of ``ly`` to
 4 (periodic) or 2 (walled); a caller that needs another ``ly`` (e.g. a
