@@ -781,24 +781,28 @@ def cpu_sample(w, flow, u0, iters_per_step, imm=None):
         from oracle.periodic import PeriodicSetup
 
         S = PeriodicSetup(cfg)
-    nthr = host_threads()
-    parallel.set_threads(nthr)
-    try:
+    def once():
         t0 = time.perf_counter()
         r0 = S.get_rhs(u0)
         t1 = time.perf_counter()
         new, corr = S.correct(u0, u0, r0, r0)
         S.norm(corr)
-        t2 = time.perf_counter()
+        return t1 - t0, time.perf_counter() - t1
+
+    nthr = host_threads()
+    parallel.set_threads(nthr)
+    try:
+        t_rhs, t_cor = once()
     finally:
         parallel.set_threads(1)
-    per_iter = t2 - t0
-    per_step = per_iter * (2 + iters_per_step)
-    return {"value": 1.0 / per_step, "unit": "steps/s", "cores": nthr,
-            "kind": "port",
-            "sample": f"1 RHS ({t1 - t0:.2f} s) + 1 corrector ({t2 - t1:.2f} s) "
+    t1_rhs, t1_cor = once()  # the reference's CPU mode: one thread per process
+    steps = 2 + iters_per_step
+    return {"value": 1.0 / ((t_rhs + t_cor) * steps), "unit": "steps/s", "cores": nthr,
+            "kind": "port", "value_1_thread": 1.0 / ((t1_rhs + t1_cor) * steps),
+            "sample": f"1 RHS ({t_rhs:.2f} s) + 1 corrector ({t_cor:.2f} s) "
                       f"of the workload on {nthr} host threads ({THREADS_NOTE}), "
-                      f"x(2 + {iters_per_step:.1f}) iterations per step"}
+                      f"x(2 + {iters_per_step:.1f}) iterations per step; value_1_thread: "
+                      f"the same on one thread ({t1_rhs:.2f} s + {t1_cor:.2f} s)"}
 
 
 def run_ensemble(a, w, rank, world):
@@ -1020,6 +1024,9 @@ def run_reference(a, w, rank, world):
         sample()
     dt_iter = (time.perf_counter() - t0) / a.steps
     parallel.set_threads(1)
+    t0 = time.perf_counter()
+    sample()  # once on one thread: the reference's CPU mode
+    dt_1 = time.perf_counter() - t0
     per_step = dt_iter * (2 + iters)
     value = 1.0 / per_step
     out = {
@@ -1032,10 +1039,13 @@ def run_reference(a, w, rank, world):
                    "grid": [w["nx"], w["ny"], w["nz"]]},
         "cpu_baseline": {
             "value": value, "unit": "steps/s", "cores": nthr, "kind": "port",
+            "value_1_thread": 1.0 / (dt_1 * (2 + iters)),
             "sample": f"each step = 1 RHS + 1 corrector of the workload "
                       f"({dt_iter:.2f} s), scaled by 2 + {iters} iterations/step; "
                       f"NumPy FP64 restatement of the reference (JAX absent) on "
-                      f"{nthr} host threads ({THREADS_NOTE})"},
+                      f"{nthr} host threads ({THREADS_NOTE}); value_1_thread: one "
+                      f"such sample on one thread ({dt_1:.2f} s), the reference's "
+                      "CPU mode"},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

@@ -58,4 +58,5 @@ def test_cpu_sample_uses_the_host_threads():
     assert r["kind"] == "port" and r["value"] > 0
     assert r["cores"] == bench.host_threads() and 1 <= r["cores"] <= 32
     assert f"{r['cores']} host threads" in r["sample"]
+    assert r["value_1_thread"] > 0
     assert parallel.threads() == 1
