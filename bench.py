@@ -505,6 +505,7 @@ def run_ours(a, w, rank, world):
             "workload": a.workload,
             "form": "mixed: FP32 RHS passes, FP64 state/IMM/norms" if mixed else "plain-fp64",
             "autotune": tuning,
+            "x_pass_flops": x_pass_flops(w, tuning, fp32=bool(mixed)),
             "driver": ("step graph per time step (corrector loop as a device-controlled "
                        "conditional node)" if graph is not None else
                        "host-driven reference loop"),
@@ -743,6 +744,31 @@ def run_learned(a, w, rank, world):
         "clocks": clk.summary(),
     }
     emit(out)
+
+
+def x_pass_flops(w, tuning, fp32=False):
+    """Flop rate of the fused x pass, from the tuner's time of the variant it
+    kept (None without the tuner).  The x pass is close to the FP64 ridge, so
+    its rate is reported beside the bandwidth roofline.  Flops by
+    convention: 5 M log2 M per complex length-M FFT, with two real fields
+    packed per complex transform (3 inverse for the six fields, 2 forward
+    for the three outputs), plus 40 per physical point for the rotational
+    product; rows = (y, z) lines of the padded grid."""
+    try:
+        if not tuning:
+            return None
+        k = tuning["stages"].index("x")
+        ms = float(tuning["ms"][k][tuning["variants"][k]])
+        M = 3 * w["nx"] // 2
+        my = w["ny"] if w["system"] == "plane-couette" else 3 * w["ny"] // 2
+        rows = my * (3 * w["nz"] // 2)
+        flops = rows * (5 * 5 * M * math.log2(M) + 40 * M)
+        return {"tflops": flops / (ms * 1e-3) / 1e12, "flops_per_call": flops, "ms": ms,
+                "dtype": "f32" if fp32 else "f64",
+                "convention": "5 M log2 M per complex FFT (3 inverse + 2 forward per row) "
+                              "+ 40 per point for the product"}
+    except Exception:  # a reported figure never fails the run
+        return None
 
 
 def host_threads() -> int:

@@ -60,3 +60,23 @@ def test_cpu_sample_uses_the_host_threads():
     assert f"{r['cores']} host threads" in r["sample"]
     assert r["value_1_thread"] > 0
     assert parallel.threads() == 1
+
+
+def test_x_pass_flops():
+    """The x pass's flop rate from the tuner's timing (Couette 128x129x128:
+    129 x 192 rows of 5 length-192 complex FFTs plus the product)."""
+    import math
+
+    import bench
+
+    w = bench.WORKLOADS["couette128"]
+    tuning = {"variants": [0, 0, 0, 0], "ms": [[0.09, 0.1, 0.1], [0.1063, 0.25, 0.3],
+                                               [0.03, 0.05, 0.05], [0.24, 0.32, 1.7]],
+              "stages": ["z inverse", "x", "z forward", "IMM"]}
+    r = bench.x_pass_flops(w, tuning)
+    flops = 129 * 192 * (25 * 192 * math.log2(192) + 40 * 192)
+    assert r["flops_per_call"] == flops and r["dtype"] == "f64"
+    assert abs(r["tflops"] - flops / 0.1063e-3 / 1e12) < 1e-9
+    assert 10.0 < r["tflops"] < 11.0
+    assert bench.x_pass_flops(w, None) is None
+    assert bench.x_pass_flops(w, {"stages": ["x"], "ms": [[]], "variants": [0]}) is None
