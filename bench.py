@@ -137,6 +137,25 @@ def op_bytes(w, fp32=False):
     return {"rhs": cb * 6 * S + pb * (18 * A1 + 18 * A2), "correct": cb * 12 * S}
 
 
+def step_roofline(w, iters, steps_per_s_per_gpu, peak, fp32=False):
+    """Whole-step bandwidth: algorithmic bytes of one time step, (2 + c)
+    RHS and corrector calls with c the corrector iterations per step (plus
+    the divergence correction, 6S complex, for the periodic flows), times
+    the steps per second of one GPU, against the HBM peak."""
+    try:
+        ob = op_bytes(w, fp32=fp32)
+        per = ob["rhs"] + ob.get("imm", ob.get("correct"))
+        extra = 0
+        if w["system"] != "plane-couette":
+            extra = 16 * 6 * (w["ny"] - 1) * (w["nz"] - 1) * (w["nx"] // 2)
+        b = (2 + iters) * per + extra
+        gbs = b * steps_per_s_per_gpu / 1e9
+        return {"bytes_per_step": b, "achieved_gbs": gbs, "frac": gbs / peak,
+                "unit": "GB/s"}
+    except Exception:  # a reported figure never fails the run
+        return None
+
+
 # DRAM bytes (read + write) of one call, summed over the call's kernels, from
 # one ncu capture of this workload (profiles/couette128_step_kernels_ncu.md);
 # None where no capture exists.
@@ -528,6 +547,8 @@ def run_ours(a, w, rank, world):
                       "imm_or_correct": sum(imm_ms) / max(1, len(imm_ms))},
             "op_ms_back_to_back": {"rhs": op_b2b["rhs"], "imm_or_correct": op_b2b["imm"]},
             "op_share": {k: v / eager_ms for k, v in tot.items()},
+            "step_roofline": step_roofline(w, sum(iters) / len(iters), value / world, peak,
+                                           fp32=bool(mixed)),
         },
         "roofline": {
             "bound": "hbm",

@@ -80,3 +80,21 @@ def test_x_pass_flops():
     assert 10.0 < r["tflops"] < 11.0
     assert bench.x_pass_flops(w, None) is None
     assert bench.x_pass_flops(w, {"stages": ["x"], "ms": [[]], "variants": [0]}) is None
+
+
+def test_step_roofline():
+    """Whole-step bytes (2 + c) x (RHS + corrector call), plus the divergence
+    correction for the periodic flows."""
+    import bench
+
+    w = bench.WORKLOADS["couette128"]
+    ob = bench.op_bytes(w)
+    r = bench.step_roofline(w, 11.0, 100.0, 6534.5)
+    assert r["bytes_per_step"] == 13 * (ob["rhs"] + ob["imm"])
+    assert abs(r["achieved_gbs"] - r["bytes_per_step"] * 100.0 / 1e9) < 1e-9
+    assert abs(r["frac"] - r["achieved_gbs"] / 6534.5) < 1e-12
+    k = bench.WORKLOADS["kolmogorov32"]
+    okb = bench.op_bytes(k)
+    rk = bench.step_roofline(k, 3.0, 1.0, 1.0)
+    assert rk["bytes_per_step"] == 5 * (okb["rhs"] + okb["correct"]) + 16 * 6 * 31 * 31 * 16
+    assert bench.step_roofline({"system": "plane-couette"}, 1.0, 1.0, 1.0) is None
