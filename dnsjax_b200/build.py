@@ -33,16 +33,29 @@ def needs_build(out: Path = OUT) -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile every source to an object in parallel (the translation units
+    share no device symbols), then link the shared library."""
+    import tempfile
+    from concurrent.futures import ThreadPoolExecutor
+
     if not force and not needs_build():
         return OUT
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17",
-           "-Xcompiler", "-fPIC", "-shared", "-o", str(OUT)]
+    flags = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
     if verbose:
-        cmd += ["-Xptxas", "-v"]
-    cmd += [str(CSRC / s) for s in SOURCES]
-    tmp = OUT.with_suffix(".so.tmp")
-    cmd[cmd.index(str(OUT))] = str(tmp)
-    subprocess.run(cmd, check=True)
+        flags += ["-Xptxas", "-v"]
+    with tempfile.TemporaryDirectory(prefix="dnsb_build_") as tmpdir:
+        objs = [Path(tmpdir) / (Path(s).stem + ".o") for s in SOURCES]
+
+        def compile_one(k):
+            subprocess.run([nvcc(), *flags, "-c", str(CSRC / SOURCES[k]), "-o",
+                            str(objs[k])], check=True)
+
+        workers = max(1, min(len(SOURCES), os.cpu_count() or 1))
+        with ThreadPoolExecutor(max_workers=workers) as pool:
+            list(pool.map(compile_one, range(len(SOURCES))))
+        tmp = OUT.with_suffix(".so.tmp")
+        subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp),
+                        *[str(o) for o in objs]], check=True)
     tmp.replace(OUT)
     return OUT
 

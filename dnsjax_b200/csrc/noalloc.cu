@@ -19,9 +19,16 @@
 //     the caller.  Each call writes every partial it later reads, so no
 //     clearing is needed between calls and a previous call's leftovers are
 //     never used.
-//   * host code cannot use the array's name as a device address; the first
+//   * host code cannot use the array's name as a device address.  The first
 //     call on each device looks the address up with cudaGetSymbolAddress
-//     (with that device current) and caches it.
+//     (with that device current) and caches it together with the unique ID
+//     of the CUDA context it came from.  A later call from a different
+//     context on that device (after cudaDeviceReset, or with another
+//     driver-API context current) repeats the look-up, so a stale address
+//     is never used.  Do that first call on a device (and the first call
+//     after a reset) before any stream capture.
+#include <cuda.h>  // CUcontext / CUresult types; the driver functions are
+                   // fetched at run time, the library does not link libcuda
 #include <mutex>
 #include <string>
 
@@ -77,7 +84,41 @@ __global__ void couette_mode_norm2_kernel(const double2* __restrict__ v, int nm,
 namespace {
 
 std::mutex g_noalloc_mutex;
-double* g_noalloc_ptr[dnsb::kNoallocMaxDevices] = {};
+
+struct NoallocAddress {
+  unsigned long long ctx_id = 0;  // context the address belongs to (0: none)
+  double* ptr = nullptr;
+};
+NoallocAddress g_noalloc_addr[dnsb::kNoallocMaxDevices];
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Unique ID of the current context (IDs are never reused within a process);
+// 0 if the driver does not provide one.
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool fetched = false;
+  if (!fetched) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault,
+                                         &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault,
+                                         &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+    fetched = true;
+  }
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx ||
+      get_id(ctx, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
 
 }  // namespace
 
@@ -95,23 +136,34 @@ extern "C" int dnsb_couette_norm_noalloc(const void* v, int nx, int ny, int nz,
                           "(nz-1)*(nx/2) exceeds the 32768 modes of the static "
                           "scratch of dnsb_couette_norm_noalloc");
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices)
-    return set_last_error(DNSB_ERR_CUDA, "cudaGetDevice failed");
+  const cudaError_t de = cudaGetDevice(&dev);
+  if (de != cudaSuccess)
+    return set_last_error(DNSB_ERR_CUDA,
+                          std::string("cudaGetDevice: ") + cudaGetErrorString(de));
+  if (dev < 0 || dev >= kNoallocMaxDevices)
+    return set_last_error(DNSB_ERR_ARG,
+                          "device ordinal " + std::to_string(dev) +
+                              " beyond the 64 devices dnsb_couette_norm_noalloc "
+                              "keeps scratch addresses for");
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
-      // First call on this device (current): host code needs the symbol's
-      // device address; the array's host-side name is not one.
+    const unsigned long long ctx_id = current_context_id();
+    NoallocAddress& a = g_noalloc_addr[dev];
+    if (!a.ptr || ctx_id == 0 || a.ctx_id != ctx_id) {
+      // First call on this device, or from another context than the cached
+      // address came from: host code needs the symbol's device address in
+      // the current context; the array's host-side name is not one.
       void* p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
       if (e != cudaSuccess || !p)
         return set_last_error(DNSB_ERR_CUDA,
                               std::string("cudaGetSymbolAddress: ") +
                                   cudaGetErrorString(e));
-      g_noalloc_ptr[dev] = static_cast<double*>(p);
+      a.ptr = static_cast<double*>(p);
+      a.ctx_id = ctx_id;
     }
-    scratch = g_noalloc_ptr[dev];
+    scratch = a.ptr;
   }
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const int warps = 4;

@@ -236,7 +236,12 @@ int dnsb_couette_step_graph_create(dnsb_couette* ctx, void* state, double tol,
  *   device that loads the library until exit; every call shares it, so calls
  *   that may overlap on the GPU race and must be ordered by the caller.  The
  *   first call on a device looks up the array's device address (with that
- *   device current) and caches it. */
+ *   device current) and caches it with the ID of the current CUDA context;
+ *   the cache assumes that the address stays valid while that context
+ *   lives, and a call from another context (after cudaDeviceReset, or with
+ *   a different driver-API context current) looks it up again.  Make the
+ *   first call on a device, and the first after a reset, before any stream
+ *   capture.  Device ordinals of 64 and above return DNSB_ERR_ARG. */
 int dnsb_couette_norm_noalloc(const void* v, int nx, int ny, int nz, double ly,
                               double* out_dev, void* stream);
 
