@@ -99,7 +99,8 @@ SIGNATURES = {
     "dnsb_couette_set_variants": (c_int, [c_void_p, c_void_p]),
     "dnsb_mlp_gemm": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p,
                               c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_int,
-                              c_void_p]),
+                              c_void_p, C.c_longlong, c_void_p, c_void_p]),
+    "dnsb_mlp_transpose": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_void_p]),
     "dnsb_learned_features": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_double,
                                       c_double, c_double, c_void_p, c_int, c_void_p, c_int,
                                       c_void_p, c_void_p]),
@@ -107,7 +108,8 @@ SIGNATURES = {
                                    c_void_p]),
     "dnsb_mlp_loss_grad": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p,
                                    c_void_p, c_void_p, c_void_p]),
-    "dnsb_mlp_colsum": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "dnsb_mlp_colsum": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
+                                C.c_longlong, c_void_p]),
     "dnsb_mlp_adam": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, C.c_longlong,
                               C.c_float, C.c_float, C.c_float, C.c_float, c_int, c_void_p]),
     "dnsb_imm_precompute": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_int,

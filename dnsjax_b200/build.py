@@ -11,7 +11,8 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 OUT = HERE / "libdnsb.so"
-SOURCES = ["passes.cu", "solver.cu", "imm.cu", "imm_batch.cu", "noalloc.cu", "precompute.cu", "learned.cu", "capi.cu"]
+SOURCES = ["passes.cu", "solver.cu", "imm.cu", "imm_batch.cu", "noalloc.cu", "precompute.cu",
+           "learned.cu", "mlp_tc.cu", "capi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

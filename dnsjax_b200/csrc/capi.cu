@@ -1480,14 +1480,28 @@ extern "C" int dnsb_couette_autotune(dnsb_couette* p, const void* state, int rep
 extern "C" int dnsb_mlp_gemm(int ta, int tb, int M, int N, int K, const void* A, int lda,
                              const void* B, int ldb, const float* bias, int relu,
                              const void* mask, int ldm, float* Cf, void* Cb, int ldc,
-                             void* stream) {
+                             float* work, long long work_elems, int* status, void* stream) {
   if (!A || !B || (!Cf && !Cb)) return fail(DNSB_ERR_ARG, "null argument");
   if (M < 1 || N < 1 || K < 1 || lda < 1 || ldb < 1 || ldc < N || (mask && ldm < N))
     return fail(DNSB_ERR_ARG, "invalid GEMM sizes");
   if ((ta ? lda < M : lda < K) || (tb ? ldb < N : ldb < K))
     return fail(DNSB_ERR_ARG, "leading dimension smaller than the operand");
-  DNSB_LAUNCH(launch_mlp_gemm(ta, tb, M, N, K, A, lda, B, ldb, bias, relu, mask, ldm, Cf, Cb,
-                              ldc, as_stream(stream)));
+  if (work_elems < 0 || (work_elems > 0 && !work))
+    return fail(DNSB_ERR_ARG, "invalid workspace");
+  int n = 1;
+  const cudaError_t e = launch_mlp_gemm(ta, tb, M, N, K, A, lda, B, ldb, bias, relu, mask, ldm,
+                                        Cf, Cb, ldc, work_elems > 0 ? work : nullptr, work_elems,
+                                        status, as_stream(stream), &n);
+  count_launches(n);
+  if (e != cudaSuccess) return fail(DNSB_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+extern "C" int dnsb_mlp_transpose(const void* A, int R, int C, int lda, void* out, int ldo,
+                                  void* stream) {
+  if (!A || !out) return fail(DNSB_ERR_ARG, "null argument");
+  if (R < 1 || C < 1 || lda < C || ldo < R) return fail(DNSB_ERR_ARG, "invalid sizes");
+  DNSB_LAUNCH(launch_bf16_transpose(A, R, C, lda, out, ldo, as_stream(stream)));
   return 0;
 }
 
@@ -1523,10 +1537,14 @@ extern "C" int dnsb_mlp_loss_grad(const float* Y, const float* T, int M, int N, 
 }
 
 extern "C" int dnsb_mlp_colsum(const void* A, int bf16, int M, int N, int lda, float* out,
-                               void* stream) {
-  if (!A || !out) return fail(DNSB_ERR_ARG, "null argument");
+                               float* work, long long work_elems, void* stream) {
+  if (!A || !out || !work) return fail(DNSB_ERR_ARG, "null argument");
   if (M < 1 || N < 1 || lda < N) return fail(DNSB_ERR_ARG, "invalid sizes");
-  DNSB_LAUNCH(launch_mlp_colsum(A, bf16, M, N, lda, out, as_stream(stream)));
+  if (work_elems < (long long)colsum_groups(M) * N)
+    return fail(DNSB_ERR_ARG, "colsum workspace smaller than min(M, 128) x N floats");
+  const cudaError_t e = launch_colsum_det(A, bf16, M, N, lda, out, work, as_stream(stream));
+  count_launches(2);
+  if (e != cudaSuccess) return fail(DNSB_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
   return 0;
 }
 

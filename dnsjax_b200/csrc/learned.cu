@@ -8,14 +8,15 @@
 //   h = relu(W1 x + b1),  y = W2 h + b2.
 // Training is online on the pairs the solver generates (mean squared error,
 // Adam).  The kernels:
-//   gemm        C[M][N] = sum_k A(m, k) B(n, k) on the tensor cores
-//               (mma.sync m16n8k16 BF16 -> FP32), 64 x 64 CTA tiles;
-//               operands read as stored or transposed; epilogue with bias,
-//               relu, a relu-derivative mask, FP32 and / or BF16 output
+//   gemm        C[M][N] = sum_k A(m, k) B(n, k): with both operands
+//               K-contiguous, the tcgen05 kernel of csrc/mlp_tc.cu (TMA,
+//               TMEM accumulator); operands stored transposed take the
+//               mma.sync m16n8k16 BF16 -> FP32 kernels below; epilogue with
+//               bias, relu, a relu-derivative mask, FP32 and / or BF16 output
 //   features    x and the target from the spectral fields
 //   guess       u_p + scale * y
 //   loss_grad   dy = 2 (y - t) / M as BF16 and FP32 copies, per-row error
-//   colsum      bias gradients
+//   colsum      bias gradients (fixed-order two-stage sums, csrc/mlp_tc.cu)
 //   adam        FP32 master weights, BF16 copies
 #include <cuda_bf16.h>
 
@@ -135,9 +136,7 @@ gemm_bf16_kernel(int M, int N, int K, const __nv_bfloat16* __restrict__ A, int l
 // The same product with 128 x 128 CTA tiles (8 warps of 64 x 32), 16-byte
 // operand loads (8 consecutive BF16 along the operand's contiguous index,
 // which needs lda, ldb multiples of 8 and 16-byte aligned bases) staged
-// through registers one k-tile ahead of the tensor-core loop.  With
-// gridDim.z > 1 (split K, plain FP32 output only) CTA z reduces k in
-// [z kc, (z + 1) kc) and adds its partial sums into Cf atomically.
+// through registers one k-tile ahead of the tensor-core loop.
 constexpr int kBM2 = 128, kBN2 = 128, kBK2 = 32;
 
 template <bool T_, int ROWS>
@@ -207,7 +206,7 @@ __global__ void __launch_bounds__(256)
 gemm_bf16_v2_kernel(int M, int N, int K, const __nv_bfloat16* __restrict__ A, int lda,
                     const __nv_bfloat16* __restrict__ B, int ldb, const float* __restrict__ bias,
                     int relu, const __nv_bfloat16* __restrict__ mask, int ldm, float* Cf,
-                    __nv_bfloat16* Cb, int ldc, int kc) {
+                    __nv_bfloat16* Cb, int ldc) {
   __shared__ __align__(16) __nv_bfloat16 As[kBM2][kBK2 + kPad];
   __shared__ __align__(16) __nv_bfloat16 Bs[kBN2][kBK2 + kPad];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -215,7 +214,7 @@ gemm_bf16_v2_kernel(int M, int N, int K, const __nv_bfloat16* __restrict__ A, in
   const int g = lane >> 2, t = lane & 3;
   const int m0 = blockIdx.y * kBM2, n0 = blockIdx.x * kBN2;
   float acc[4][4][4] = {};
-  const int kb = blockIdx.z * kc, ke = min(K, kb + kc);
+  const int kb = 0, ke = K;
   TileLoad<TA, kBM2> la;
   TileLoad<TB, kBN2> lb;
   if (kb < ke) {
@@ -264,10 +263,6 @@ gemm_bf16_v2_kernel(int M, int N, int K, const __nv_bfloat16* __restrict__ A, in
         const int n = n0 + wn * 32 + nt * 8 + 2 * t + (q & 1);
         if (m >= M || n >= N) continue;
         float v = acc[mt][nt][q];
-        if (gridDim.z > 1) {
-          atomicAdd(&Cf[(long long)m * ldc + n], v);
-          continue;
-        }
         if (bias) v += bias[n];
         if (relu) v = fmaxf(v, 0.0f);
         if (mask && !(__bfloat162float(mask[(long long)m * ldm + n]) > 0.0f)) v = 0.0f;
@@ -390,22 +385,6 @@ __global__ void loss_grad_kernel(const float* __restrict__ Y, const float* __res
   }
 }
 
-// out[n] += sum over rows m = blockIdx.y, blockIdx.y + gridDim.y, ... of
-// A[m lda + n] (FP32 or BF16 input); out is zeroed by the launcher.
-template <typename T>
-__global__ void colsum_kernel(const T* __restrict__ A, int M, int N, int lda, float* out) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  float s = 0.0f;
-  for (int m = blockIdx.y; m < M; m += gridDim.y) {
-    if constexpr (sizeof(T) == 4)
-      s += A[(long long)m * lda + n];
-    else
-      s += __bfloat162float(A[(long long)m * lda + n]);
-  }
-  atomicAdd(&out[n], s);
-}
-
 // Adam on FP32 master weights w with moments mo, ve; BF16 copy wb.
 __global__ void adam_kernel(float* w, float* mo, float* ve, const float* __restrict__ grad,
                             __nv_bfloat16* wb, long long n, float lr, float b1, float b2,
@@ -427,8 +406,12 @@ __global__ void adam_kernel(float* w, float* mo, float* ve, const float* __restr
 
 cudaError_t launch_mlp_gemm(int ta, int tb, int M, int N, int K, const void* A, int lda,
                             const void* B, int ldb, const float* bias, int relu,
-                            const void* mask, int ldm, float* Cf, void* Cb, int ldc,
-                            cudaStream_t st) {
+                            const void* mask, int ldm, float* Cf, void* Cb, int ldc, float* work,
+                            long long work_elems, int* status, cudaStream_t st, int* launches) {
+  if (!ta && !tb && tc_gemm_supported(A, lda, B, ldb))
+    return launch_tc_gemm(M, N, K, A, lda, B, ldb, bias, relu, mask, ldm, Cf, Cb, ldc, work,
+                          work_elems, status, st, launches);
+  if (launches) *launches = 1;
   const auto* a = static_cast<const __nv_bfloat16*>(A);
   const auto* b = static_cast<const __nv_bfloat16*>(B);
   const auto* mk = static_cast<const __nv_bfloat16*>(mask);
@@ -436,22 +419,10 @@ cudaError_t launch_mlp_gemm(int ta, int tb, int M, int N, int K, const void* A, 
   const bool vec = lda % 8 == 0 && ldb % 8 == 0 && reinterpret_cast<uintptr_t>(A) % 16 == 0 &&
                    reinterpret_cast<uintptr_t>(B) % 16 == 0;
   if (vec) {
-    // split K when the output tiles cannot fill the GPU and the epilogue is
-    // a plain FP32 store: about two CTAs per SM, at least 512 k per split
-    const int tiles = ((N + kBN2 - 1) / kBN2) * ((M + kBM2 - 1) / kBM2);
-    int splits = 1;
-    if (Cf && !Cb && !bias && !relu && !mask && tiles < 296)
-      splits = std::max(1, std::min(296 / tiles, K / 512));
-    const int kc = ((K + splits - 1) / splits + kBK2 - 1) / kBK2 * kBK2;
-    splits = (K + kc - 1) / kc;
-    if (splits > 1) {
-      const cudaError_t z = cudaMemset2DAsync(Cf, sizeof(float) * ldc, 0, sizeof(float) * N, M, st);
-      if (z != cudaSuccess) return z;
-    }
-    const dim3 g2((N + kBN2 - 1) / kBN2, (M + kBM2 - 1) / kBM2, splits);
+    const dim3 g2((N + kBN2 - 1) / kBN2, (M + kBM2 - 1) / kBM2);
 #define DNSB_V2(TA_, TB_)                                                                      \
   gemm_bf16_v2_kernel<TA_, TB_><<<g2, 256, 0, st>>>(M, N, K, a, lda, b, ldb, bias, relu, mk,  \
-                                                    ldm, Cf, cb, ldc, kc)
+                                                    ldm, Cf, cb, ldc)
     if (!ta && !tb) DNSB_V2(false, false);
     else if (ta && tb) DNSB_V2(true, true);
     else if (!ta && tb) DNSB_V2(false, true);
@@ -496,19 +467,6 @@ cudaError_t launch_mlp_loss_grad(const float* Y, const float* T, int M, int N, i
                                  void* dYb, float* err, float* ref, cudaStream_t st) {
   loss_grad_kernel<<<M, 256, 0, st>>>(Y, T, M, N, ld, dYf, static_cast<__nv_bfloat16*>(dYb),
                                       err, ref);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_mlp_colsum(const void* A, int bf16, int M, int N, int lda, float* out,
-                              cudaStream_t st) {
-  const cudaError_t z = cudaMemsetAsync(out, 0, sizeof(float) * N, st);
-  if (z != cudaSuccess) return z;
-  const dim3 grid((N + 127) / 128, std::max(1, std::min(M, 128)));
-  if (bf16)
-    colsum_kernel<__nv_bfloat16><<<grid, 128, 0, st>>>(static_cast<const __nv_bfloat16*>(A), M,
-                                                       N, lda, out);
-  else
-    colsum_kernel<float><<<grid, 128, 0, st>>>(static_cast<const float*>(A), M, N, lda, out);
   return cudaGetLastError();
 }
 

@@ -149,8 +149,19 @@ cudaError_t launch_imm_precompute(const ImmPrecomputeArgs& a, double* bp, double
 // Learned corrector guess (csrc/learned.cu): BF16 MLP kernels.
 cudaError_t launch_mlp_gemm(int ta, int tb, int M, int N, int K, const void* A, int lda,
                             const void* B, int ldb, const float* bias, int relu,
-                            const void* mask, int ldm, float* Cf, void* Cb, int ldc,
-                            cudaStream_t st);
+                            const void* mask, int ldm, float* Cf, void* Cb, int ldc, float* work,
+                            long long work_elems, int* status, cudaStream_t st, int* launches);
+// tcgen05 GEMM C = A B^T with K-contiguous BF16 operands (csrc/mlp_tc.cu).
+bool tc_gemm_supported(const void* A, int lda, const void* B, int ldb);
+cudaError_t launch_tc_gemm(int M, int N, int K, const void* A, int lda, const void* B, int ldb,
+                           const float* bias, int relu, const void* mask, int ldm, float* Cf,
+                           void* Cb, int ldc, float* work, long long work_elems, int* status,
+                           cudaStream_t st, int* launches);
+cudaError_t launch_bf16_transpose(const void* in, int R, int C, int ldi, void* out, int ldo,
+                                  cudaStream_t st);
+int colsum_groups(int M);
+cudaError_t launch_colsum_det(const void* A, int bf16, int M, int N, int lda, float* out,
+                              float* work, cudaStream_t st);
 cudaError_t launch_learned_features(const double2* un, const double2* up, const double2* dprev,
                                     const double2* target, const double* kx, const double* kz,
                                     int NKX, int NZ1, int Ny, double kx_max, double kz_max,
@@ -160,8 +171,6 @@ cudaError_t launch_learned_guess(const double2* up, const float* Y, int ldy, con
                                  int NM, int Ny, double2* out, cudaStream_t st);
 cudaError_t launch_mlp_loss_grad(const float* Y, const float* T, int M, int N, int ld, float* dYf,
                                  void* dYb, float* err, float* ref, cudaStream_t st);
-cudaError_t launch_mlp_colsum(const void* A, int bf16, int M, int N, int lda, float* out,
-                              cudaStream_t st);
 cudaError_t launch_mlp_adam(float* w, float* m, float* v, const float* grad, void* wb,
                             long long n, float lr, float b1, float b2, float eps, int step,
                             cudaStream_t st);

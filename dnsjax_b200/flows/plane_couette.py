@@ -176,6 +176,13 @@ class PlaneCouetteFlow:
                                              _lib.ptr(out), _lib.stream_handle()))
         return out
 
+    def set_rhs_precision(self, fp32: bool) -> None:
+        """FP32 (True) or FP64 (False) RHS passes for the following RHS calls
+        (the ``res.double_precision`` switch, applied per call)."""
+        if bool(fp32) != self.rhs_fp32:
+            _lib.check(self._L.dnsb_couette_set_rhs_precision(self._ctx, int(bool(fp32))))
+            self.rhs_fp32 = bool(fp32)
+
     def correct_velocity(self, state):
         """plane_couette.py:575-582: pass-through."""
         return state, None

@@ -1,22 +1,32 @@
 """Learned corrector guess for plane Couette.
 
-A per-(kz, kx)-mode MLP, 1.19M parameters at 128x129x128 (12 Ny + 2 ->
-``hidden`` = 512 -> 6 Ny), with BF16 weights and activations and FP32
-accumulation on the tensor cores (``dnsb_mlp_*``, ``csrc/learned.cu``).
-For every mode it guesses the converged corrector correction u^{n+1} - u_p
-(u_p: the predictor's output) from the predictor increment u_p - u^n and
-the previous step's converged correction, both scaled by the mode's rms of
-u_p - u^n.  It is trained online, on the GPU, on the pairs the solver
-generates each step (mean squared error, Adam).
+A per-(kz, kx)-mode MLP with two hidden layers (12 Ny + 2 -> 640 -> 640 ->
+6 Ny; 1.9M parameters at 128x129x128), BF16 weights and activations and
+FP32 accumulation on the tcgen05 tensor cores (``dnsb_mlp_*``,
+``csrc/mlp_tc.cu``, ``csrc/learned.cu``).  For every mode it guesses the
+converged corrector correction u^{n+1} - u_p (u_p: the predictor's output)
+from the predictor increment u_p - u^n and the previous step's converged
+correction, both scaled by the mode's rms of u_p - u^n.
+
+Training: ``LearnedGuess.collect`` runs the plain FP64 solver (the
+reference's loop) from seeded initial fields and keeps every step's
+per-mode (predictor, previous correction, converged correction) triples on
+the GPU; ``pretrain`` fits the network to them (mean squared error, Adam),
+all with this package's own forward and backward kernels.  ``step`` can
+also keep training online on each step's pair.
 
 ``step`` is the reference's time step (src/dnsjax/__main__.py:159-190 with
-plane_couette.py:507-582) with one change: the first correction starts
-from u_p + guess instead of u_p.  The corrector still iterates to
-``corrector_tolerance`` from there, so the guess only moves the starting
-point of the same fixed-point iteration.  The guess is applied only while
-its measured error on the latest step (before training on that step) is
-below ``gate`` times the correction's norm, i.e. while it is closer to the
-converged state than the plain predictor.
+plane_couette.py:507-582) started from the guessed state u_p + guess: the
+corrector iterations of ``iterate_correction`` (timestep.py:96-120) run
+from there to ``corrector_tolerance``, so the guess only moves the starting
+point of the same fixed-point iteration and the converged state is the
+same to within the tolerance.  With ``restart`` (the default) the guessed
+state is treated as the previous iterate, so its own RHS fills both RHS
+slots of the first correction (the reference's predict_and_correct keeps
+N(u^n) in the first slot).  With ``switch`` set (the mixed form), the RHS
+runs in FP32 until the correction norm falls below ``switch`` and in FP64
+from then on within the step, so the iteration ends at an FP64 fixed point
+while its early iterations cost less.
 """
 
 from __future__ import annotations
@@ -34,6 +44,8 @@ class LearnedStep:
     guessed: bool
     guess_rel_error: float | None  # |guess - target| / |target| of this step
     first_correction: float        # norm of the first correction
+    rhs_fp32: int = 0              # RHS evaluations of the step in FP32
+    rhs_fp64: int = 0              # and in FP64
 
 
 @dataclass
@@ -41,66 +53,139 @@ class LearnedStats:
     steps: list = field(default_factory=list)
 
 
-class MLP:
-    """h = relu(x W1^T + b1), y = h W2^T + b2 over M rows, BF16 weights and
-    activations, FP32 accumulation and master weights, Adam; every step of
-    the forward and backward pass is a ``dnsb_mlp_*`` kernel.  X (M x
-    K1p, BF16) and T (M x N2, FP32) are filled by the caller."""
+def _pad8(n: int) -> int:
+    return (n + 7) // 8 * 8
 
-    def __init__(self, M: int, K1: int, H: int, N2: int, lr: float = 1e-3, seed: int = 0,
-                 out_scale: float = 0.1):
+
+class MLP:
+    """y = W_L relu(... relu(W_1 x + b_1) ...) + b_L over M rows, BF16
+    weights and activations, FP32 accumulation and master weights, Adam;
+    every step of the forward and backward pass is a ``dnsb_mlp_*`` kernel.
+    ``sizes`` = [inputs, hidden..., outputs].  X (M x K1p, BF16) and T (M x
+    N2p, FP32) are filled by the caller; widths are padded to multiples of
+    8 (16-byte rows), the padding of inputs, weights and targets is zero.
+
+    Every product is C = A B^T with both operands K-contiguous (the tcgen05
+    kernel); the backward pass feeds it transposed copies of the
+    activations and gradients (``dnsb_mlp_transpose``) and keeps a
+    transposed BF16 copy of every weight matrix.  Reductions (split-K
+    partials, bias gradients) run in a fixed order, so training is
+    reproducible run to run."""
+
+    def __init__(self, M: int, sizes, lr: float = 1e-3, seed: int = 0, out_scale: float = 0.1):
         import torch
 
         self.L = _lib.lib()
-        self.M, self.K1, self.H, self.N2 = M, K1, H, N2
-        # operand widths padded to multiples of 8 (16-byte rows for the GEMM's
-        # vector loads); padded inputs, weights and targets are zero
-        self.K1p = (K1 + 7) // 8 * 8
-        self.N2p = (N2 + 7) // 8 * 8
-        N2p = self.N2p
+        sizes = [int(s) for s in sizes]
+        if len(sizes) < 2:
+            raise ValueError("sizes = [inputs, hidden..., outputs]")
+        self.M, self.sizes = M, sizes
+        self.dims = [_pad8(s) for s in sizes]
+        self.K1, self.N2 = sizes[0], sizes[-1]
+        self.K1p, self.N2p = self.dims[0], self.dims[-1]
+        self.H = sizes[1] if len(sizes) > 2 else None
+        self.nl = len(sizes) - 1
         self.lr = lr
         g = torch.Generator(device="cpu").manual_seed(seed)
         f32 = dict(dtype=torch.float32, device="cuda")
         bf = dict(dtype=torch.bfloat16, device="cuda")
-        W1 = torch.randn(H, self.K1p, generator=g) * sqrt(2.0 / K1)
-        W1[:, K1:] = 0.0
-        W2 = torch.zeros(N2p, H)
-        W2[:N2] = torch.randn(N2, H, generator=g) * (out_scale / sqrt(H))
-        self.w = {"W1": W1.to(**f32), "b1": torch.zeros(H, **f32),
-                  "W2": W2.to(**f32), "b2": torch.zeros(N2p, **f32)}
-        self.wb = {k: self.w[k].to(torch.bfloat16) for k in ("W1", "W2")}
+        self.w = {}
+        for l in range(self.nl):
+            din, dout = sizes[l], sizes[l + 1]
+            W = torch.zeros(self.dims[l + 1], self.dims[l])
+            if l < self.nl - 1:
+                W[:dout, :din] = torch.randn(dout, din, generator=g) * sqrt(2.0 / din)
+            else:
+                W[:dout, :din] = torch.randn(dout, din, generator=g) * (out_scale / sqrt(din))
+            self.w[f"W{l + 1}"] = W.to(**f32)
+            self.w[f"b{l + 1}"] = torch.zeros(self.dims[l + 1], **f32)
+        self.wb = {f"W{l + 1}": self.w[f"W{l + 1}"].to(torch.bfloat16) for l in range(self.nl)}
+        self.wt = {k: v.t().contiguous() for k, v in self.wb.items()}
         self.m = {k: torch.zeros_like(v) for k, v in self.w.items()}
         self.v = {k: torch.zeros_like(v) for k, v in self.w.items()}
         self.g = {k: torch.zeros_like(v) for k, v in self.w.items()}
-        self.X = torch.zeros(M, self.K1p, **bf)
-        self.Hb = torch.empty(M, H, **bf)
-        self.dHb = torch.empty(M, H, **bf)
-        self.Y = torch.empty(M, N2p, **f32)
-        self.T = torch.zeros(M, N2p, **f32)
-        self.dYf = torch.empty(M, N2p, **f32)
-        self.dYb = torch.empty(M, N2p, **bf)
+        # activations: acts[0] = X (input), acts[l] = hidden layer l output
+        self.acts = [torch.zeros(M, self.dims[0], **bf)]
+        for l in range(1, self.nl):
+            self.acts.append(torch.empty(M, self.dims[l], **bf))
+        self.X = self.acts[0]
+        self.dacts = [None] + [torch.empty(M, self.dims[l], **bf) for l in range(1, self.nl)]
+        self.Y = torch.empty(M, self.N2p, **f32)
+        self.T = torch.zeros(M, self.N2p, **f32)
+        self.dYf = torch.empty(M, self.N2p, **f32)
+        self.dYb = torch.empty(M, self.N2p, **bf)
         self.err = torch.empty(M, **f32)
         self.ref = torch.empty(M, **f32)
+        dmax = max(self.dims)
+        self.tA = torch.empty(dmax * M, **bf)  # transposed gradient
+        self.tB = torch.empty(dmax * M, **bf)  # transposed activation
+        wmax = max(self.dims[l] * self.dims[l + 1] for l in range(self.nl))
+        self.work = torch.empty(max(4 * wmax, 128 * dmax), **f32)
+        self.status = torch.zeros(1, dtype=torch.int32, device="cuda")
         self.adam_step = 0
 
     @property
     def parameters(self) -> int:
-        return self.H * self.K1 + self.H + self.N2 * self.H + self.N2
+        return sum(self.sizes[l] * self.sizes[l + 1] + self.sizes[l + 1] for l in range(self.nl))
 
-    def _gemm(self, ta, tb, M, N, K, A, lda, B, ldb, bias=None, relu=0, mask=None, ldm=0,
-              Cf=None, Cb=None, ldc=0):
+    @property
+    def layers(self) -> list:
+        return list(self.sizes)
+
+    def _gemm(self, M, N, K, A, lda, B, ldb, bias=None, relu=0, mask=None, ldm=0, Cf=None,
+              Cb=None, ldc=0, split=False):
+        """C[M][N] = sum_k A[m][k] B[n][k] (both K-contiguous)."""
         p = _lib.ptr
+        work, nwork = (p(self.work), self.work.numel()) if split else (None, 0)
         _lib.check(self.L.dnsb_mlp_gemm(
-            ta, tb, M, N, K, p(A), lda, p(B), ldb, p(bias) if bias is not None else None, relu,
+            0, 0, M, N, K, p(A), lda, p(B), ldb, p(bias) if bias is not None else None, relu,
             p(mask) if mask is not None else None, ldm, p(Cf) if Cf is not None else None,
-            p(Cb) if Cb is not None else None, ldc, _lib.stream_handle()))
+            p(Cb) if Cb is not None else None, ldc, work, nwork, p(self.status),
+            _lib.stream_handle()))
+
+    def _transpose(self, A, R, C, out):
+        _lib.check(self.L.dnsb_mlp_transpose(_lib.ptr(A), R, C, C, _lib.ptr(out), R,
+                                             _lib.stream_handle()))
+
+    def _colsum(self, A, bf16, N, out):
+        p = _lib.ptr
+        _lib.check(self.L.dnsb_mlp_colsum(p(A), int(bf16), self.M, N, N, p(out), p(self.work),
+                                          self.work.numel(), _lib.stream_handle()))
 
     def forward(self):
-        M = self.M
-        self._gemm(0, 0, M, self.H, self.K1p, self.X, self.K1p, self.wb["W1"], self.K1p,
-                   bias=self.w["b1"], relu=1, Cb=self.Hb, ldc=self.H)
-        self._gemm(0, 0, M, self.N2p, self.H, self.Hb, self.H, self.wb["W2"], self.H,
-                   bias=self.w["b2"], Cf=self.Y, ldc=self.N2p)
+        M, d = self.M, self.dims
+        for l in range(self.nl):
+            W, b = self.wb[f"W{l + 1}"], self.w[f"b{l + 1}"]
+            if l < self.nl - 1:
+                self._gemm(M, d[l + 1], d[l], self.acts[l], d[l], W, d[l], bias=b, relu=1,
+                           Cb=self.acts[l + 1], ldc=d[l + 1])
+            else:
+                self._gemm(M, d[l + 1], d[l], self.acts[l], d[l], W, d[l], bias=b, Cf=self.Y,
+                           ldc=d[l + 1])
+
+    def capture_forward(self):
+        """Capture ``forward`` (its GEMM launches, bound to this network's
+        buffers) as a CUDA graph; ``replay_forward`` then runs it with one
+        launch.  Re-capture is not needed after training: the graph reads the
+        weight buffers, which Adam updates in place."""
+        import torch
+
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            self.forward()  # first launches (kernel attributes) outside the capture
+        torch.cuda.current_stream().wait_stream(side)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.forward()
+        self._fwd_graph = g
+
+    def replay_forward(self):
+        g = getattr(self, "_fwd_graph", None)
+        if g is None:
+            self.forward()
+        else:
+            g.replay()
 
     def loss(self):
         """Mean-squared-error gradient into dYf / dYb; returns the per-row
@@ -112,18 +197,24 @@ class MLP:
         return self.err, self.ref
 
     def backward(self):
-        p = _lib.ptr
-        M = self.M
-        self._gemm(1, 1, self.N2p, self.H, M, self.dYb, self.N2p, self.Hb, self.H,
-                   Cf=self.g["W2"], ldc=self.H)
-        _lib.check(self.L.dnsb_mlp_colsum(p(self.dYf), 0, M, self.N2p, self.N2p, p(self.g["b2"]),
-                                          _lib.stream_handle()))
-        self._gemm(0, 1, M, self.H, self.N2p, self.dYb, self.N2p, self.wb["W2"], self.H,
-                   mask=self.Hb, ldm=self.H, Cb=self.dHb, ldc=self.H)
-        self._gemm(1, 1, self.H, self.K1p, M, self.dHb, self.H, self.X, self.K1p,
-                   Cf=self.g["W1"], ldc=self.K1p)
-        _lib.check(self.L.dnsb_mlp_colsum(p(self.dHb), 1, M, self.H, self.H, p(self.g["b1"]),
-                                          _lib.stream_handle()))
+        M, d = self.M, self.dims
+        cur = self.dYb
+        for l in range(self.nl - 1, -1, -1):
+            dout, din = d[l + 1], d[l]
+            # weight gradient g[o][i] = sum_m cur[m][o] acts[l][m][i]
+            self._transpose(cur, M, dout, self.tA)
+            self._transpose(self.acts[l], M, din, self.tB)
+            self._gemm(dout, din, M, self.tA, M, self.tB, M, Cf=self.g[f"W{l + 1}"], ldc=din,
+                       split=True)
+            if l == self.nl - 1:
+                self._colsum(self.dYf, False, dout, self.g[f"b{l + 1}"])
+            else:
+                self._colsum(cur, True, dout, self.g[f"b{l + 1}"])
+            if l > 0:
+                # input gradient (cur W) masked by the relu of layer l
+                self._gemm(M, din, dout, cur, dout, self.wt[f"W{l + 1}"], dout,
+                           mask=self.acts[l], ldm=din, Cb=self.dacts[l], ldc=din)
+                cur = self.dacts[l]
 
     def update(self):
         p = _lib.ptr
@@ -134,8 +225,13 @@ class MLP:
                 p(w), p(self.m[k]), p(self.v[k]), p(self.g[k]),
                 p(wb) if wb is not None else None, w.numel(), self.lr, 0.9, 0.999, 1e-8,
                 self.adam_step, _lib.stream_handle()))
+            if wb is not None:
+                R, C = wb.shape
+                self._transpose(wb, R, C, self.wt[k])
 
     def train(self, iters: int):
+        """``iters`` Adam iterations on the current X, T (the first reuses
+        the forward pass and loss the caller ran)."""
         for it in range(iters):
             if it:
                 self.forward()
@@ -143,27 +239,41 @@ class MLP:
             self.backward()
             self.update()
 
+    def pipeline_status(self) -> int:
+        """Bit 0: a tensor-core pipeline wait gave up (synchronises)."""
+        return int(self.status.item())
+
 
 class LearnedGuess:
     """The MLP bound to a plane-Couette flow: features from the spectral
-    fields, the guessed prediction, and the learned time step."""
+    fields, the guessed prediction, data collection, pretraining and the
+    learned time step."""
 
-    def __init__(self, flow, hidden: int = 512, lr: float = 1e-3, train_iters: int = 2,
-                 gate: float = 0.9, mode_gate: float | None = None, seed: int = 0):
+    def __init__(self, flow, hidden=(640, 640), lr: float = 1e-3, seed: int = 0,
+                 restart: bool = True, switch: float | None = None, gate: float | None = 0.9,
+                 train_iters: int = 0):
         import torch
 
         if not hasattr(flow, "imm"):
             raise ValueError("the learned guess is built for plane Couette")
+        if isinstance(hidden, int):
+            hidden = (hidden,)
         self.flow = flow
         self.ny = flow.ny
         self.NM = (flow.nz - 1) * (flow.nx // 2)
-        self.net = MLP(self.NM, 12 * self.ny + 2, hidden, 6 * self.ny, lr=lr, seed=seed)
-        self.train_iters, self.gate, self.mode_gate = train_iters, gate, mode_gate
-        self.mode_ok = None  # per mode: 1 where its latest guess error was below mode_gate
+        self.net = MLP(self.NM, [12 * self.ny + 2, *hidden, 6 * self.ny], lr=lr, seed=seed)
+        self.restart, self.switch, self.gate = restart, switch, gate
+        self.stall = 0.8      # FP32 iterations stop when e > stall * previous e
+        self.recheck = 8      # while gated off, measure the guess every recheck steps
+        self.trace = None     # list: (iteration, error, fp32) of every correction
+        self._since = 0
+        self.train_iters = train_iters
         self.kx_max = float(max(abs(flow.fourier.kx_global).max(), 1e-30))
         self.kz_max = float(max(abs(flow.fourier.kz_global).max(), 1e-30))
         self.scale = torch.empty(self.NM, dtype=torch.float32, device="cuda")
-        self.last_rel = None  # guess error of the latest step, before training on it
+        self.last_rel = None  # guess error of the latest step, measured after it
+        self.enabled = True   # False: the same step with no guess (u_p as start)
+        self.data = []        # (X, T, scale) of collected steps
 
     def features(self, un, up, dprev=None, target=None, s_floor=0.0):
         p = _lib.ptr
@@ -180,51 +290,145 @@ class LearnedGuess:
                                                    _lib.stream_handle()))
         return out
 
-    # -- one time step -----------------------------------------------------------
-    def step(self, state, dprev, tol, max_iter):
-        """One reference time step with the guessed starting point; returns
-        (new state, converged correction u^{n+1} - u_p, LearnedStep)."""
+    def _s_floor(self, up, state):
+        import torch
+
+        inc = torch.linalg.vector_norm(up - state)
+        return 1e-3 * float(inc) / sqrt(up.numel())
+
+    def measure(self, state, up, dprev, delta, s_floor) -> float:
+        """Relative error of the network's guess of ``delta`` (= converged
+        state - u_p) on this step; leaves the step's features and target in
+        the network's X, T."""
+        import torch
+
+        self.features(state, up, dprev, target=delta, s_floor=s_floor)
+        self.net.replay_forward()
+        er, rf = self.net.loss()
+        s2 = self.scale.double() ** 2
+        return float(torch.sqrt((er.double() * s2).sum()
+                                / (rf.double() * s2).sum().clamp_min(1e-300)))
+
+    # -- data and pretraining --------------------------------------------------
+    def collect(self, state, steps: int, tol: float, max_iter: int):
+        """Run ``steps`` plain FP64 reference steps from ``state`` and keep each
+        step's training triple (features of u^n, u_p, previous correction;
+        target u^{n+1} - u_p) on the GPU.  Returns the final state."""
         import torch
 
         f = self.flow
         err = torch.empty(1, dtype=torch.float64, device="cuda")
-        r0 = f.get_rhs(state)
+        was32 = f.rhs_fp32
+        f.set_rhs_precision(False)
+        dprev = None
+        try:
+            for _ in range(steps):
+                r0 = f.get_rhs(state)
+                up = f.predict(state, r0)
+                rn = f.get_rhs(up)
+                cur = f.correct_fused(state, up.clone(), r0, rn, err)
+                c, e = 0, float(err.item())
+                while e > tol and c < max_iter:
+                    rp, rn = rn, f.get_rhs(cur)
+                    cur = f.correct_fused(state, cur, rp, rn, err, out=cur)
+                    c, e = c + 1, float(err.item())
+                if not e <= tol:
+                    break
+                cur, _ = f.correct_velocity(cur)
+                delta = cur - up
+                self.features(state, up, dprev, target=delta, s_floor=self._s_floor(up, state))
+                self.data.append((self.net.X.clone(), self.net.T.clone(), self.scale.clone()))
+                dprev, state = delta, cur
+        finally:
+            f.set_rhs_precision(was32)
+        return state
+
+    def pretrain(self, epochs: int) -> list:
+        """``epochs`` passes over the collected steps, one Adam iteration per
+        step; returns the mean loss of each epoch (synchronises once per
+        epoch)."""
+        import torch
+
+        n = self.net
+        losses = []
+        for _ in range(epochs):
+            tot = torch.zeros((), dtype=torch.float64, device="cuda")
+            for X, T, _s in self.data:
+                n.X.copy_(X)
+                n.T.copy_(T)
+                n.forward()
+                er, _ = n.loss()
+                tot += er.double().sum()
+                n.backward()
+                n.update()
+            losses.append(float(tot) / max(1, len(self.data) * n.M))
+        n.capture_forward()
+        return losses
+
+    # -- one time step -----------------------------------------------------------
+    def step(self, state, dprev, tol, max_iter, measure: bool | None = None):
+        """One time step started from the guessed state; returns (new state,
+        converged correction u^{n+1} - u_p, LearnedStep)."""
+        import torch
+
+        f = self.flow
+        err = torch.empty(1, dtype=torch.float64, device="cuda")
+        mixed = self.switch is not None
+        n32 = n64 = 0
+
+        def rhs(u):
+            nonlocal n32, n64
+            if f.rhs_fp32:
+                n32 += 1
+            else:
+                n64 += 1
+            return f.get_rhs(u)
+
+        f.set_rhs_precision(mixed)
+        r0 = rhs(state)
         up = f.predict(state, r0)
-        inc = torch.linalg.vector_norm(up - state)
-        s_floor = 1e-3 * float(inc) / sqrt(up.numel())
-        use = self.last_rel is not None and self.last_rel < self.gate
+        s_floor = self._s_floor(up, state)
+        use = self.enabled and (self.gate is None or self.last_rel is None
+                                or self.last_rel < self.gate)
         start = up.clone()
         if use:
             self.features(state, up, dprev, s_floor=s_floor)
-            self.net.forward()
-            if self.mode_ok is not None:
-                self.scale.mul_(self.mode_ok)  # no guess for the other modes
+            self.net.replay_forward()
             self.guess(up, start)
-        rn = f.get_rhs(start)
-        cur = f.correct_fused(state, start, r0, rn, err, out=start)
+        rn = rhs(start)
+        cur = f.correct_fused(state, start, rn if self.restart else r0, rn, err, out=start)
         e = float(err.item())
         first = e
         c = 0
+        e_prev = float("inf")
         while e > tol and c < max_iter:
-            rp = rn
-            rn = f.get_rhs(cur)
+            # one way to FP64 for the rest of the step: once below the switch,
+            # or when the FP32 iteration stops contracting (its rounding floor)
+            if mixed and f.rhs_fp32 and (e <= self.switch or e > self.stall * e_prev):
+                f.set_rhs_precision(False)
+            rp, rn = rn, rhs(cur)
             cur = f.correct_fused(state, cur, rp, rn, err, out=cur)
             c += 1
-            e = float(err.item())
+            e_prev, e = e, float(err.item())
+            if self.trace is not None:
+                self.trace.append((c, e, int(f.rhs_fp32)))
+        f.set_rhs_precision(False)
         cur, _ = f.correct_velocity(cur)
         delta = cur - up
-        # learn from this step's pair; measure the guess first
-        self.features(state, up, dprev, target=delta, s_floor=s_floor)
-        self.net.forward()
-        er, rf = self.net.loss()
-        s2 = self.scale.double() ** 2
-        rel = float(torch.sqrt((er.double() * s2).sum()
-                               / (rf.double() * s2).sum().clamp_min(1e-300)))
-        self.last_rel = rel
-        if self.mode_gate is not None:
-            self.mode_ok = (er < (self.mode_gate ** 2) * rf).float()
-        self.net.train(self.train_iters)
-        return cur, delta, LearnedStep(c, e, use, rel, first)
+        rel = None
+        if measure is None:
+            gated_off = self.gate is not None and not use and self.last_rel is not None
+            self._since = self._since + 1 if gated_off else 0
+            measure = self.enabled and (self.train_iters > 0 or (
+                self.gate is not None and (not gated_off or self._since >= self.recheck)))
+            if gated_off and measure:
+                self._since = 0
+        if measure:
+            rel = self.measure(state, up, dprev, delta, s_floor)
+            self.last_rel = rel
+            if self.train_iters:
+                self.net.train(self.train_iters)
+        return cur, delta, LearnedStep(c, e, use, rel, first, n32, n64)
 
 
 def run(flow, state, steps, guess: LearnedGuess, tol=None, max_iter=None):

@@ -285,10 +285,20 @@ int dnsb_couette_autotune(dnsb_couette* ctx, const void* state, int reps, int* c
  * FP32 accumulation); A(m, k) = ta ? A[k lda + m] : A[m lda + k],
  * B(n, k) = tb ? B[k ldb + n] : B[n ldb + k].  Epilogue: + bias[n] (FP32,
  * optional), max(., 0) when relu, times (mask[m ldm + n] > 0) when mask
- * (BF16) is given; written to Cf (FP32) and / or Cb (BF16) at [m ldc + n]. */
+ * (BF16) is given; written to Cf (FP32) and / or Cb (BF16) at [m ldc + n].
+ * With ta = tb = 0, lda and ldb multiples of 8 and 16-byte aligned A, B it
+ * runs on tcgen05 (TMA tiles, TMEM accumulator); other layouts run on
+ * mma.sync.  work (optional, work_elems floats) lets the tcgen05 path split
+ * K when the output tiles cannot fill the GPU: the partial tiles are summed
+ * in a fixed order, so results are the same run to run.  status (optional,
+ * device int): bit 0 is set if a pipeline wait of the tcgen05 kernel gave
+ * up (bounded waits; the call then returns normally with that bit set). */
 int dnsb_mlp_gemm(int ta, int tb, int M, int N, int K, const void* A, int lda, const void* B,
                   int ldb, const float* bias, int relu, const void* mask, int ldm, float* Cf,
-                  void* Cb, int ldc, void* stream);
+                  void* Cb, int ldc, float* work, long long work_elems, int* status,
+                  void* stream);
+/* out[c][r] = A[r][c] for an R x C BF16 matrix (row strides lda, ldo). */
+int dnsb_mlp_transpose(const void* A, int R, int C, int lda, void* out, int ldo, void* stream);
 /* Features of every mode m (spectral layout (3, nz-1, nx/2, ny) complex128):
  * X[m][((F*3 + c)*ny + y)*2 + part] (BF16) with F = 0: (up - un) / s_m,
  * F = 1: dprev / s_m (zero when dprev is NULL), then kx / kx_max,
@@ -305,8 +315,10 @@ int dnsb_learned_guess(dnsb_couette* ctx, const void* up, const float* Y, int ld
  * err[m] = sum_n (Y - T)^2, ref[m] = sum_n T^2. */
 int dnsb_mlp_loss_grad(const float* Y, const float* T, int M, int N, int ld, float* dYf,
                        void* dYb, float* err, float* ref, void* stream);
-/* out[n] = sum_m A[m lda + n]; A is BF16 when bf16 != 0, else FP32. */
-int dnsb_mlp_colsum(const void* A, int bf16, int M, int N, int lda, float* out, void* stream);
+/* out[n] = sum_m A[m lda + n]; A is BF16 when bf16 != 0, else FP32.  Sums
+ * in a fixed order through work (at least min(M, 128) x N floats). */
+int dnsb_mlp_colsum(const void* A, int bf16, int M, int N, int lda, float* out, float* work,
+                    long long work_elems, void* stream);
 /* One Adam update (step >= 1, bias-corrected) of FP32 weights w with
  * moments m, v from grad; wb (BF16, optional) gets the rounded weights. */
 int dnsb_mlp_adam(float* w, float* m, float* v, const float* grad, void* wb, long long n,

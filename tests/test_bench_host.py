@@ -48,18 +48,47 @@ def test_strict_json(capsys):
 
 
 def test_cpu_sample_uses_the_host_threads():
-    """The cpu_baseline leg on the oracle: threads reported as cores, the
-    pool back at one thread afterwards."""
+    """The cpu_baseline leg on the oracle: one full time step timed whole,
+    threads reported as cores, the pool back at one thread afterwards."""
     import bench
     from oracle import parallel
 
     w = bench.WORKLOADS["kolmogorov32"]
-    r = bench.cpu_sample(w, None, bench.initial_state(w, w["seed"]), 3)
+    r = bench.cpu_sample(w, bench.initial_state(w, w["seed"]))
     assert r["kind"] == "port" and r["value"] > 0
     assert r["cores"] == bench.host_threads() and 1 <= r["cores"] <= 32
     assert f"{r['cores']} host threads" in r["sample"]
-    assert r["value_1_thread"] > 0
+    assert "1 full time step" in r["sample"]
     assert parallel.threads() == 1
+
+
+def test_oracle_steps_follow_the_reference_loop():
+    """The reference arm's steps: the oracle's corrector loop stops at the
+    tolerance, like oracle.stepper.run (the restatement of __main__.py)."""
+    import numpy as np
+
+    import bench
+    from oracle.stepper import run
+
+    w = dict(bench.WORKLOADS["kolmogorov32"], nx=8, ny=8, nz=8)
+    S = bench.oracle_setup(w)
+    u0 = bench.initial_state(w, 3)
+    u, iters = bench.oracle_steps(S, u0, 3)
+    ref = run(S, u0, 3)
+    assert iters == ref.corrector_iterations
+    assert np.array_equal(u, ref.state)
+
+
+def test_both_arms_share_the_workload_config():
+    import bench
+
+    for name, w in bench.WORKLOADS.items():
+        tol = w.get("tol", 1e-10)
+        a = bench.workload_config(name, w, tol)
+        assert a == bench.workload_config(name, w, tol) and a["workload"] == name
+        assert "tol" in a and "l2" in a
+    c = bench.workload_config("couette128", bench.WORKLOADS["couette128"], 1e-10)
+    assert c["max_corrector_iterations"] == 60 and "deviation" in c
 
 
 def test_x_pass_flops():

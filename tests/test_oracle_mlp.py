@@ -10,6 +10,7 @@ def test_mlp_oracle_gradients_finite_differences():
 
     assert finite_difference_check(seed=0) < 1e-6
     assert finite_difference_check(seed=1, M=11, K=9, H=5, N=3) < 1e-6
+    assert finite_difference_check(seed=2, M=9, K=6, H=5, N=3, layers=3) < 1e-6
 
 
 def test_bf16_rounding_matches_torch():
