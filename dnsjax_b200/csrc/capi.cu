@@ -781,6 +781,7 @@ struct dnsb_couette {
   double2* Rw = nullptr;
   ImmBatch batch{};
   bool batch_ready = false;
+  int wait_limit = 1 << 20;  // substitution ring: polls before a wait gives up
 
   ImmArgs imm() const {
     ImmArgs a{};
@@ -1015,6 +1016,7 @@ static int bind_batch(dnsb_couette* p) {
   b.paired = p->pair_modes;
   b.max_smem = smax;
   b.status = p->status;
+  b.wait_limit = p->wait_limit;
   b.F = p->Fw;
   b.R = p->Rw;
   p->batch_ready = true;
@@ -1323,6 +1325,20 @@ extern "C" int dnsb_couette_step_graph_create(dnsb_couette* p, void* state, doub
     return rc;
   }
   *out = g;
+  return 0;
+}
+
+extern "C" int dnsb_couette_set_wait_limit(dnsb_couette* p, int polls) {
+  if (!p) return fail(DNSB_ERR_ARG, "null argument");
+  if (polls < 0) return fail(DNSB_ERR_ARG, "polls must be >= 0");
+  p->wait_limit = polls;
+  p->batch.wait_limit = polls;
+  return 0;
+}
+
+extern "C" int dnsb_couette_clear_status(dnsb_couette* p, void* stream) {
+  if (!p) return fail(DNSB_ERR_ARG, "null argument");
+  DNSB_CUDA(cudaMemsetAsync(p->status, 0, sizeof(int), as_stream(stream)));
   return 0;
 }
 

@@ -363,6 +363,7 @@ struct SolveArgs {
   double2* X;  // [ncomp][NM][Ny]
   int* status;
   int NP, NM, Ny, NKX, NZ1, paired, ring, slot_bytes;
+  int wait_limit;  // polls before a ring wait gives up (the drain after it uses kDrainPolls)
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -398,9 +399,11 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
       : "memory");
   return ok != 0;
 }
-// Bounded wait for a ring slot: false if it did not complete.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
-  for (int it = 0; it < (1 << 20); ++it)
+// Bounded wait for a ring slot: false if it did not complete within
+// `limit` polls.
+constexpr int kDrainPolls = 1 << 20;
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int limit) {
+  for (int it = 0; it < limit; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -613,7 +616,7 @@ imm_solve_kernel(SolveArgs a) {
   };
   auto wait_block = [&](int g) {
     if (R == 3) cp_async_wait_2(); else cp_async_wait_1();  // this lane's rows of block g
-    if (!mbar_wait(&bars[g % R], (g / R) & 1)) s_fail = 1;
+    if (!mbar_wait(&bars[g % R], (g / R) & 1, a.wait_limit)) s_fail = 1;
     __syncthreads();
   };
   // The back substitution reads the forward results: its blocks are issued
@@ -716,7 +719,7 @@ imm_solve_kernel(SolveArgs a) {
   if (!ok && tid == 0) {
     // Leave no bulk copy in flight: blocks g .. hi_issued were issued
     // (block g is the one that timed out).
-    for (int h = g; h <= hi_issued; ++h) mbar_wait(&bars[h % R], (h / R) & 1);
+    for (int h = g; h <= hi_issued; ++h) mbar_wait(&bars[h % R], (h / R) & 1, kDrainPolls);
     atomicOr(a.status, 2);
   }
 }
@@ -771,6 +774,7 @@ static cudaError_t solve_launch(const ImmBatch& bt, int op, double2* X, int ncom
   s.paired = bt.paired;
   s.ring = solve_ring(KL, bt.nu, ncomp, bt.max_smem);
   s.slot_bytes = solve_slot_bytes(KL, bt.nu, ncomp);
+  s.wait_limit = bt.wait_limit;
   if (s.ring == 0) return cudaErrorInvalidValue;
   const size_t sm = (size_t)s.ring * s.slot_bytes;
   const int grid = (bt.NP + kTile - 1) / kTile;

@@ -121,6 +121,7 @@ struct ImmBatch {
   int paired;    // mirror mode (nz-1-s, kx) reads item (s, kx)'s factors
   int max_smem;  // per-CTA shared-memory limit of the device
   int* status;   // bit 1: bad pivot, bit 2: a substitution ring wait timed out
+  int wait_limit;  // polls of a ring slot's mbarrier before the wait gives up
   double2* F;
   double2* R;
 };

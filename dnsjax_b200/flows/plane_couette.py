@@ -222,7 +222,16 @@ class PlaneCouetteFlow:
         return {"E'": float(self._scratch[0].item()) / 2}
 
     def check_status(self):
+        """Raises if a bound operator holds an out-of-range pivot or an IMM
+        substitution wait gave up since the status was last cleared."""
         _lib.check(self._L.dnsb_couette_check(self._ctx, _lib.stream_handle()))
+
+    def clear_status(self):
+        _lib.check(self._L.dnsb_couette_clear_status(self._ctx, _lib.stream_handle()))
+
+    def set_wait_limit(self, polls: int):
+        """Polls of a substitution ring slot before the wait gives up."""
+        _lib.check(self._L.dnsb_couette_set_wait_limit(self._ctx, int(polls)))
 
     # -- transforms (operators.py:104-146) -------------------------------------
     def spec_to_phys(self, spec):

@@ -212,6 +212,14 @@ int dnsb_couette_phys_to_spec(dnsb_couette* ctx, const double* phys,
  * followed), DNSB_ERR_CUDA when a bounded wait inside the IMM substitution
  * kernel gave up (its results are then invalid), else 0. */
 int dnsb_couette_check(dnsb_couette* ctx, void* stream);
+/* Failure detection (no counterpart in the reference): the status word stays
+ * set until cleared; the ring waits of the IMM substitution kernel give up
+ * after `polls` polls of a slot's mbarrier (default 2^20; 0 makes every
+ * wait give up at once, which sets the status and invalidates the call's
+ * results but leaves no copy in flight and the context usable).  Step
+ * graphs keep the limit they were captured with. */
+int dnsb_couette_clear_status(dnsb_couette* ctx, void* stream);
+int dnsb_couette_set_wait_limit(dnsb_couette* ctx, int polls);
 
 /* One full plane-Couette time step as a CUDA graph, like
  * dnsb_periodic_step_graph_create: predictor (the IMM iteration with

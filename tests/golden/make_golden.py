@@ -11,9 +11,16 @@ import time.  Inputs are this package's seeded initial fields
 trajectory through the reference's step/corrector loop
 (``__main__.py:125-203``).
 
-Run from the repository root (needs the reference checkout):
+Each case also writes a snapshot file in the reference's npz format from
+the seeded field and loads it back through the reference's own
+``init_state`` (``flows/plane_couette.py:225-248``,
+``flows/monochromatic.py:294-314``), recording the snapshot's array and the
+state the reference read from it.
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+Run from the repository root, given the reference checkout (its path as
+``--ref`` or in ``DNSJAX_REFERENCE``):
+
+    python tests/golden/make_golden.py --ref <reference checkout> [case ...]
 """
 
 from __future__ import annotations
@@ -166,6 +173,17 @@ for it in range(case["steps"]):
     last_error = float(error)
     cs.append(c)
     errs.append(last_error)
+# Snapshot exchange: the reference's snapshot format written from u0 and read
+# back by the reference's own init_state.
+params.init.start_from_laminar = False
+if case["system"] == "plane-couette":
+    snap = {"velocity_phys_nonexpanded": out["phys0"]}
+else:
+    snap = {"velocity_phys": out["phys0"] + np.asarray(flow.base_flow)}
+np.savez("snapshot.npz", **snap)
+out["snapshot_phys"] = next(iter(snap.values()))
+out["snapshot_loaded"] = np.asarray(fm.init_state("snapshot.npz"))
+params.init.start_from_laminar = True
 out["uN"] = np.asarray(state)
 out["iters"] = np.array(cs)
 out["errors"] = np.array(errs)
@@ -209,9 +227,12 @@ def run_case(name: str, case: dict, ref: Path) -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("DNSJAX_REFERENCE"),
+                    help="reference checkout (default: $DNSJAX_REFERENCE)")
     ap.add_argument("cases", nargs="*")
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("give the reference checkout with --ref or DNSJAX_REFERENCE")
     for name in a.cases or CASES:
         run_case(name, CASES[name], Path(a.ref))
 

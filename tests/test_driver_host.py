@@ -85,3 +85,13 @@ def test_oracle_stepper_same_sequence():
     x1, r1, _ = a[0](0.0)
     x2, r2, _ = b[0](0.0)
     assert np.isclose(x1, x2) and f1.calls == f2.calls
+
+
+def test_non_finite_error_ends_the_run():
+    """A NaN correction norm: no corrector iteration (NaN > tol is false), and
+    the loop stops before the next step (not NaN < tol), as
+    __main__.py:125-129 does."""
+    f = FakeFlow(0.5, tol=1e-3, max_iter=3)
+    res = driver.run(f, float("nan"), steps=5, fused=False)
+    assert res.steps == 1 and res.corrector_iterations == [0]
+    assert not res.converged and np.isnan(res.errors[0])

@@ -63,3 +63,37 @@ def test_couette_snapshot_round_trip(tmp_path):
     back = flow.init_state(path)
     d = torch.linalg.vector_norm(back - u) / torch.linalg.vector_norm(u)
     assert float(d) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["kolmogorov_n16", "kolmogorov_tilt30", "waleffe_tilt90",
+                                  "couette_n8_p4", "couette_p6"])
+def test_snapshots_exchange_with_the_reference(tmp_path, name):
+    """Both directions against the reference's own code (golden fixtures made
+    by tests/golden/make_golden.py): this package reads the snapshot file
+    the reference read into the same state the reference's init_state
+    produced, and writes from that state the array the reference's reader
+    takes (the file's contents to rounding)."""
+    import torch
+
+    from conftest import load_golden, package_params, rel_l2
+
+    case, g = load_golden(name)
+    p = package_params(case)
+    p.init.start_from_laminar = False
+    if case["system"] == "plane-couette":
+        from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
+
+        flow, key = PlaneCouetteFlow(p), "velocity_phys_nonexpanded"
+    else:
+        from dnsjax_b200.flows.monochromatic import TriplyPeriodicFlow
+
+        flow, key = TriplyPeriodicFlow(p, ly=case.get("ly")), "velocity_phys"
+    path = tmp_path / "ref_snapshot.npz"
+    np.savez(path, **{key: g["snapshot_phys"]})
+    got = flow.init_state(path).cpu().numpy()
+    assert rel_l2(got, g["snapshot_loaded"]) < 1e-13
+    out = tmp_path / "ours.npz"
+    flow.save_snapshot(out, torch.as_tensor(g["snapshot_loaded"], device="cuda"))
+    with np.load(out) as z:
+        assert list(z.keys()) == [key]
+        assert rel_l2(z[key], g["snapshot_phys"]) < 1e-13

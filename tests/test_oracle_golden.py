@@ -74,3 +74,22 @@ def test_imm_precompute(name):
                                    max(1.0, float(np.abs(g[k]).max())), err_msg=k)
     np.testing.assert_array_equal(S.imm["Lk_piv"], g["Lk_piv"])
     np.testing.assert_array_equal(S.imm["Hk_piv"], g["Hk_piv"])
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_snapshot_read_by_the_reference(name):
+    """The snapshot file the fixture generator wrote from u0 and read back
+    with the reference's own init_state: the oracle's forward transform of
+    the file's array (minus the base flow for the periodic flows) is the
+    state the reference read, and that state is u0 to rounding."""
+    from oracle import fft as F
+
+    case, g = load_golden(name)
+    cfg, S = _setup(case)
+    snap = g["snapshot_phys"]
+    if cfg.system == "plane-couette":
+        spec = F.phys_to_spec_2d(snap, cfg)
+    else:
+        spec = F.phys_to_spec(snap - S.base_flow, cfg)
+    assert rel_l2(spec, g["snapshot_loaded"]) < TOL
+    assert rel_l2(g["snapshot_loaded"], g["u0"]) < 1e-12
