@@ -445,3 +445,29 @@ def run(flow, state, steps, guess: LearnedGuess, tol=None, max_iter=None):
         if not st.error < tol:
             break
     return state, stats
+
+
+def forward_rate(M: int = 8128, sizes=(1550, 640, 640, 774), reps: int = 20) -> dict:
+    """Inference rate of the network's GEMMs at the 128x129x128 sizes: three
+    forward passes, then CUDA-graph replays of the forward timed with CUDA
+    events (``python -c "from dnsjax_b200.learned import forward_rate;
+    print(forward_rate())"``)."""
+    import torch
+
+    net = MLP(M, list(sizes))
+    net.X.normal_()
+    for _ in range(3):
+        net.forward()
+    torch.cuda.synchronize()
+    net.capture_forward()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        net.replay_forward()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    flops = 2.0 * M * sum(sizes[i] * sizes[i + 1] for i in range(len(sizes) - 1))
+    return {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12, "flops": flops,
+            "status": net.pipeline_status()}
