@@ -409,7 +409,7 @@ extern "C" int dnsb_periodic_set_rhs_precision(dnsb_periodic* p, int fp32) {
       return fail(DNSB_ERR_ARG,
                   "FP32 RHS passes need padded sizes in {48, 72, 96, 192} with nx_p = 3 nx / 2");
   }
-  p->rhs_fp32 = fp32 ? 1 : 0;
+  p->rhs_fp32 = fp32 < 0 ? 0 : (fp32 > 2 ? 2 : fp32);
   return 0;
 }
 
@@ -1152,7 +1152,7 @@ extern "C" int dnsb_couette_set_rhs_precision(dnsb_couette* p, int fp32) {
       return fail(DNSB_ERR_ARG,
                   "FP32 RHS passes need padded sizes in {48, 72, 96, 192} with nx_p = 3 nx / 2");
   }
-  p->rhs_fp32 = fp32 ? 1 : 0;
+  p->rhs_fp32 = fp32 < 0 ? 0 : (fp32 > 2 ? 2 : fp32);
   return 0;
 }
 

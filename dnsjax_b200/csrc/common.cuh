@@ -72,6 +72,37 @@ template <typename C>
 __host__ __device__ __forceinline__ C cmake(typename cplx<C>::real x, typename cplx<C>::real y) {
   return cplx<C>::make(x, y);
 }
+// FP32 complex whose register DFTs (dft2/3/4/8, dft_3p) carry compensated
+// (two-sum) accumulation: the FP32 pass buffers and every other operation
+// are those of float2 (same layout); see the compensated DFTs below.
+struct __align__(8) cf2 : public float2 {
+  cf2() = default;
+  __host__ __device__ cf2(float2 v) : float2(v) {}
+};
+template <>
+struct cplx<cf2> {
+  using real = float;
+  __host__ __device__ static cf2 make(float x, float y) { return cf2(make_float2(x, y)); }
+};
+// Element types of a pass kernel instantiated on T: double (FP64), float
+// (FP32), fcomp (FP32 buffers, compensated butterflies).
+struct fcomp {};
+template <typename T>
+struct pass_types {
+  using C = double2;
+  using R = double;
+};
+template <>
+struct pass_types<float> {
+  using C = float2;
+  using R = float;
+};
+template <>
+struct pass_types<fcomp> {
+  using C = cf2;
+  using R = float;
+};
+
 // Conversions between the two precisions.
 __host__ __device__ __forceinline__ double2 to_c(double2 z, double2*) { return z; }
 __host__ __device__ __forceinline__ float2 to_c(double2 z, float2*) {
@@ -150,6 +181,124 @@ __device__ __forceinline__ void dft8(C* v, int sign) {
   v[3] = cadd(e[3], t3);
   v[7] = csub(e[3], t3);
 }
+
+// ---- compensated FP32 butterflies (the cf2 overloads) -----------------------
+// Each FP32 value is carried as h + l: a sum or difference keeps its exact
+// rounding error (Knuth's two-sum) in l, a product by a constant keeps the
+// product's rounding error (from an FMA) and the constant's own FP32 rounding
+// error; l is folded back (h + l, one rounding) when the DFT stores its
+// outputs.  Only the register DFTs are compensated; the twiddle
+// multiplications between stages and the pass buffers stay FP32.
+struct ffv {
+  float h, l;
+};
+__device__ __forceinline__ ffv ff_two_sum(float a, float b) {
+  const float s = a + b;
+  const float bb = s - a;
+  return {s, (a - (s - bb)) + (b - bb)};
+}
+__device__ __forceinline__ ffv ff_add(ffv a, ffv b) {
+  ffv s = ff_two_sum(a.h, b.h);
+  s.l += a.l + b.l;
+  return s;
+}
+__device__ __forceinline__ ffv ff_sub(ffv a, ffv b) {
+  ffv s = ff_two_sum(a.h, -b.h);
+  s.l += a.l - b.l;
+  return s;
+}
+// a (ch + cl): ch the FP32 constant, cl its rounding error
+__device__ __forceinline__ ffv ff_mulc(ffv a, float ch, float cl) {
+  const float p = a.h * ch;
+  return {p, fmaf(a.h, ch, -p) + (a.h * cl + a.l * ch)};
+}
+struct cff {
+  ffv x, y;
+};
+__device__ __forceinline__ cff cff_of(float2 v) { return {{v.x, 0.0f}, {v.y, 0.0f}}; }
+__device__ __forceinline__ cf2 cff_fold(cff v) {
+  return cf2(make_float2(v.x.h + v.x.l, v.y.h + v.y.l));
+}
+__device__ __forceinline__ cff cff_add(cff a, cff b) { return {ff_add(a.x, b.x), ff_add(a.y, b.y)}; }
+__device__ __forceinline__ cff cff_sub(cff a, cff b) { return {ff_sub(a.x, b.x), ff_sub(a.y, b.y)}; }
+__device__ __forceinline__ cff cff_scale(cff a, float ch, float cl) {
+  return {ff_mulc(a.x, ch, cl), ff_mulc(a.y, ch, cl)};
+}
+// i * sign * a (exact)
+__device__ __forceinline__ cff cff_isign(cff a, int sign) {
+  const ffv nx = {-a.y.h, -a.y.l};
+  return sign > 0 ? cff{nx, a.x} : cff{a.y, {-a.x.h, -a.x.l}};
+}
+// FP32 constant and its rounding error, evaluated in double at compile time.
+struct fconst {
+  float h, l;
+};
+__host__ __device__ constexpr fconst fsplit(double c) {
+  return {(float)c, (float)(c - (double)(float)c)};
+}
+constexpr fconst kS3 = fsplit(0.86602540378443864676);  // sin(2 pi / 3)
+constexpr fconst kH8 = fsplit(0.70710678118654752440);  // sqrt(2) / 2
+
+__device__ __forceinline__ void cff_dft2(cff* v) {
+  const cff a = v[0], b = v[1];
+  v[0] = cff_add(a, b);
+  v[1] = cff_sub(a, b);
+}
+__device__ __forceinline__ void cff_dft3(cff* v, int sign) {
+  const cff t1 = cff_add(v[1], v[2]);
+  const cff t2 = cff_sub(v[0], cff_scale(t1, 0.5f, 0.0f));
+  const cff t3 = cff_scale(cff_isign(cff_sub(v[1], v[2]), sign), kS3.h, kS3.l);
+  v[0] = cff_add(v[0], t1);
+  v[1] = cff_add(t2, t3);
+  v[2] = cff_sub(t2, t3);
+}
+__device__ __forceinline__ void cff_dft4(cff* v, int sign) {
+  const cff a = cff_add(v[0], v[2]), b = cff_sub(v[0], v[2]);
+  const cff c = cff_add(v[1], v[3]), d = cff_sub(v[1], v[3]);
+  const cff isd = cff_isign(d, sign);
+  v[0] = cff_add(a, c);
+  v[2] = cff_sub(a, c);
+  v[1] = cff_add(b, isd);
+  v[3] = cff_sub(b, isd);
+}
+__device__ __forceinline__ void cff_dft8(cff* v, int sign) {
+  cff e[4] = {v[0], v[2], v[4], v[6]};
+  cff o[4] = {v[1], v[3], v[5], v[7]};
+  cff_dft4(e, sign);
+  cff_dft4(o, sign);
+  // twiddles w8^q = exp(sign 2 pi i q / 8): (1 + sign i) h, sign i, (-1 + sign i) h
+  const cff t1 = cff_scale(cff_add(o[1], cff_isign(o[1], sign)), kH8.h, kH8.l);
+  const cff t2 = cff_isign(o[2], sign);
+  const cff t3 = cff_scale(cff_sub(cff_isign(o[3], sign), o[3]), kH8.h, kH8.l);
+  v[0] = cff_add(e[0], o[0]);
+  v[4] = cff_sub(e[0], o[0]);
+  v[1] = cff_add(e[1], t1);
+  v[5] = cff_sub(e[1], t1);
+  v[2] = cff_add(e[2], t2);
+  v[6] = cff_sub(e[2], t2);
+  v[3] = cff_add(e[3], t3);
+  v[7] = cff_sub(e[3], t3);
+}
+template <int P>
+__device__ __forceinline__ void cff_dft_small(cff* v, int sign) {
+  if constexpr (P == 2) cff_dft2(v);
+  else if constexpr (P == 3) cff_dft3(v, sign);
+  else if constexpr (P == 4) cff_dft4(v, sign);
+  else cff_dft8(v, sign);
+}
+template <int N>
+__device__ __forceinline__ void cf2_dft(cf2* v, int sign) {
+  cff w[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) w[i] = cff_of(v[i]);
+  cff_dft_small<N>(w, sign);
+#pragma unroll
+  for (int i = 0; i < N; ++i) v[i] = cff_fold(w[i]);
+}
+__device__ __forceinline__ void dft2(cf2* v) { cf2_dft<2>(v, 1); }
+__device__ __forceinline__ void dft3(cf2* v, int sign) { cf2_dft<3>(v, sign); }
+__device__ __forceinline__ void dft4(cf2* v, int sign) { cf2_dft<4>(v, sign); }
+__device__ __forceinline__ void dft8(cf2* v, int sign) { cf2_dft<8>(v, sign); }
 
 // One Stockham radix-R stage over C columns stored as buf[t * C + c].
 template <int R>
@@ -317,10 +466,15 @@ __device__ __forceinline__ void dft_3p_ct(C* v, const C* __restrict__ tw, int TS
 
 // PFA: with 3 and P coprime, the prime-factor form (no twiddles); else the
 // Cooley-Tukey form with the twiddle table.
+template <int N, int SIGN, bool PFA>
+__device__ __forceinline__ void dft_3p_comp(cf2* v, const cf2* __restrict__ tw, int TS);
+
 template <int N, int SIGN, typename C, bool PFA = false>
 __device__ __forceinline__ void dft_3p(C* v, const C* __restrict__ tw, int TS) {
   constexpr int P = N / 3;
-  if constexpr (PFA && P % 3 != 0) {
+  if constexpr (std::is_same<C, cf2>::value) {
+    dft_3p_comp<N, SIGN, PFA>(v, tw, TS);
+  } else if constexpr (PFA && P % 3 != 0) {
     // 3 and P coprime: prime-factor (Good-Thomas) DFT, no twiddles.  Input
     // n = (P n1 + 3 n2) mod N; P-point DFTs over n2, 3-point DFTs over n1;
     // output k = (P (P^-1 mod 3) k1 + 3 (3^-1 mod P) k2) mod N (Chinese
@@ -371,6 +525,58 @@ __device__ __forceinline__ void dft_3p_ct(C* v, const C* __restrict__ tw, int TS
     dft3(b, SIGN);
 #pragma unroll
     for (int k2 = 0; k2 < 3; ++k2) v[k1 + P * k2] = b[k2];
+  }
+}
+
+// The compensated form of dft_3p: the P-point and 3-point DFTs (and, in the
+// Cooley-Tukey form, the twiddle products between them) stay in h + l
+// until the outputs are stored.
+template <int N, int SIGN, bool PFA>
+__device__ __forceinline__ void dft_3p_comp(cf2* v, const cf2* __restrict__ tw, int TS) {
+  constexpr int P = N / 3;
+  cff a[3][P];
+  if constexpr (PFA && P % 3 != 0) {
+    constexpr int A = P * inv_mod(P % 3, 3), B = 3 * inv_mod(3 % P, P);
+    (void)tw;
+    (void)TS;
+#pragma unroll
+    for (int n1 = 0; n1 < 3; ++n1)
+#pragma unroll
+      for (int n2 = 0; n2 < P; ++n2) a[n1][n2] = cff_of(v[(P * n1 + 3 * n2) % N]);
+#pragma unroll
+    for (int n1 = 0; n1 < 3; ++n1) cff_dft_small<P>(a[n1], SIGN);
+#pragma unroll
+    for (int k2 = 0; k2 < P; ++k2) {
+      cff b[3] = {a[0][k2], a[1][k2], a[2][k2]};
+      cff_dft3(b, SIGN);
+#pragma unroll
+      for (int k1 = 0; k1 < 3; ++k1) v[(A * k1 + B * k2) % N] = cff_fold(b[k1]);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+#pragma unroll
+      for (int p = 0; p < P; ++p) a[q][p] = cff_of(v[3 * p + q]);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) cff_dft_small<P>(a[q], SIGN);
+#pragma unroll
+    for (int q = 1; q < 3; ++q)
+#pragma unroll
+      for (int k1 = 1; k1 < P; ++k1) {
+        float2 w = tw[(q * k1) * TS];
+        if (SIGN > 0) w.y = -w.y;
+        // (x + i y)(wx + i wy) with each product's rounding error kept
+        const cff z = a[q][k1];
+        a[q][k1] = {ff_sub(ff_mulc(z.x, w.x, 0.0f), ff_mulc(z.y, w.y, 0.0f)),
+                    ff_add(ff_mulc(z.x, w.y, 0.0f), ff_mulc(z.y, w.x, 0.0f))};
+      }
+#pragma unroll
+    for (int k1 = 0; k1 < P; ++k1) {
+      cff b[3] = {a[0][k1], a[1][k1], a[2][k1]};
+      cff_dft3(b, SIGN);
+#pragma unroll
+      for (int k2 = 0; k2 < 3; ++k2) v[k1 + P * k2] = cff_fold(b[k2]);
+    }
   }
 }
 

@@ -139,7 +139,8 @@ size_t col_pass2_smem(int M) {
 template <int ML, int SIGN, typename T = double, bool OUT32 = false, bool CURL = false>
 __global__ void __launch_bounds__(kC2Threads)
 col_pass2_kernel(ColPassArgs a) {
-  using CT = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+  using CT = typename pass_types<T>::C;
+  using RT = typename pass_types<T>::R;
   constexpr int M = ML, R1 = M / 8, C = kC2Cols;
   extern __shared__ double2 sm_[];
   CT* X = reinterpret_cast<CT*>(sm_);  // [t][C]
@@ -220,7 +221,7 @@ col_pass2_kernel(ColPassArgs a) {
         } else {
           const int sidx = pos_to_stored(t, a.nstored, M);
           if (sidx >= 0) {
-            if (OUT32) out_c[sidx * a.out_ts + c] = cscale(z[i], (T)sc);
+            if (OUT32) out_c[sidx * a.out_ts + c] = cscale(z[i], (RT)sc);
             else out[sidx * a.out_ts + c] = cscale(to_d(z[i]), sc);
           }
         }
@@ -238,7 +239,15 @@ cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
     if (a.fp32 && a.inverse && !a.out32) return cudaErrorInvalidValue;
 #define DNSB_C2(LL)                                                                     \
   case LL:                                                                              \
-    if (a.curl && a.fp32)                                                               \
+    if (a.curl && a.fp32 == 2)                                                          \
+      col_pass2_kernel<LL, 1, fcomp, true, true><<<g2, kC2Threads, sm2, st>>>(a);       \
+    else if (a.fp32 == 2 && a.inverse)                                                  \
+      col_pass2_kernel<LL, 1, fcomp, true><<<g2, kC2Threads, sm2, st>>>(a);             \
+    else if (a.fp32 == 2 && a.out32)                                                    \
+      col_pass2_kernel<LL, -1, fcomp, true><<<g2, kC2Threads, sm2, st>>>(a);            \
+    else if (a.fp32 == 2)                                                               \
+      col_pass2_kernel<LL, -1, fcomp><<<g2, kC2Threads, sm2, st>>>(a);                  \
+    else if (a.curl && a.fp32)                                                          \
       col_pass2_kernel<LL, 1, float, true, true><<<g2, kC2Threads, sm2, st>>>(a);       \
     else if (a.curl)                                                                    \
       col_pass2_kernel<LL, 1, double, false, true><<<g2, kC2Threads, sm2, st>>>(a);     \
@@ -411,6 +420,16 @@ cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
   const int L = (a.nkx * 3 == a.plan.L) ? a.plan.L : -1;
   if (a.variant == 0 && (L == 48 || L == 72 || L == 96 || L == 192)) {
     dim3 g2((a.nrows + kX2Rows - 1) / kX2Rows);
+    if (a.fp32 == 2) {
+      const size_t sm2 = x_pass2_smem(L, a.nkx) / 2;
+      switch (L) {
+        case 48: x_pass2_kernel<48, fcomp><<<g2, kX2Threads, sm2, st>>>(a); break;
+        case 72: x_pass2_kernel<72, fcomp><<<g2, kX2Threads, sm2, st>>>(a); break;
+        case 96: x_pass2_kernel<96, fcomp><<<g2, kX2Threads, sm2, st>>>(a); break;
+        default: x_pass2_kernel<192, fcomp><<<g2, kX2Threads, sm2, st>>>(a); break;
+      }
+      return cudaGetLastError();
+    }
     if (a.fp32) {
       const size_t sm2 = x_pass2_smem(L, a.nkx) / 2;
       switch (L) {
@@ -453,7 +472,8 @@ size_t x_pass2_smem(int M, int nkx) {
 template <int ML, typename T>
 __global__ void __launch_bounds__(kX2Threads)
 x_pass2_kernel(XPassArgs a) {
-  using CT = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+  using CT = typename pass_types<T>::C;
+  using RT = typename pass_types<T>::R;
   constexpr int M = ML, R1 = M / 8, R = kX2Rows, NKX = ML / 3;
   constexpr int CI = 3 * R, CF = 2 * R;
   // Stage outputs carry a skew of XS (X) / 1 (Y) slots per block of R1 (X)
@@ -556,22 +576,22 @@ x_pass2_kernel(XPassArgs a) {
     const bool live = r < nr;
     const int y = s_y[r];
     const int ny = a.ny_grid;
-    const T U0 = live ? (T)a.U[y] : T(0), U1 = live ? (T)a.U[ny + y] : T(0),
-            U2 = live ? (T)a.U[2 * ny + y] : T(0);
-    const T C0 = live ? (T)a.cU[y] : T(0), C1 = live ? (T)a.cU[ny + y] : T(0),
-            C2 = live ? (T)a.cU[2 * ny + y] : T(0);
-    const T N0 = live ? (T)a.nU[y] : T(0), N1 = live ? (T)a.nU[ny + y] : T(0),
-            N2 = live ? (T)a.nU[2 * ny + y] : T(0);
+    const RT U0 = live ? (RT)a.U[y] : RT(0), U1 = live ? (RT)a.U[ny + y] : RT(0),
+            U2 = live ? (RT)a.U[2 * ny + y] : RT(0);
+    const RT C0 = live ? (RT)a.cU[y] : RT(0), C1 = live ? (RT)a.cU[ny + y] : RT(0),
+            C2 = live ? (RT)a.cU[2 * ny + y] : RT(0);
+    const RT N0 = live ? (RT)a.nU[y] : RT(0), N1 = live ? (RT)a.nU[ny + y] : RT(0),
+            N2 = live ? (RT)a.nU[2 * ny + y] : RT(0);
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const T u0 = z[0][i].x, u1 = z[0][i].y, u2 = z[1][i].x;
-      const T w0 = z[1][i].y, w1 = z[2][i].x, w2 = z[2][i].y;
-      const T n0 = u1 * w2 - u2 * w1;
-      const T n1 = u2 * w0 - u0 * w2;
-      const T n2 = u0 * w1 - u1 * w0;
-      const T b0 = (u1 * C2 - u2 * C1) + (U1 * w2 - U2 * w1) + N0;
-      const T b1 = (u2 * C0 - u0 * C2) + (U2 * w0 - U0 * w2) + N1;
-      const T b2 = (u0 * C1 - u1 * C0) + (U0 * w1 - U1 * w0) + N2;
+      const RT u0 = z[0][i].x, u1 = z[0][i].y, u2 = z[1][i].x;
+      const RT w0 = z[1][i].y, w1 = z[2][i].x, w2 = z[2][i].y;
+      const RT n0 = u1 * w2 - u2 * w1;
+      const RT n1 = u2 * w0 - u0 * w2;
+      const RT n2 = u0 * w1 - u1 * w0;
+      const RT b0 = (u1 * C2 - u2 * C1) + (U1 * w2 - U2 * w1) + N0;
+      const RT b1 = (u2 * C0 - u0 * C2) + (U2 * w0 - U0 * w2) + N1;
+      const RT b2 = (u0 * C1 - u1 * C0) + (U0 * w1 - U1 * w0) + N2;
       F0[i] = live ? cmake<CT>(n0 + b0, n1 + b1) : cmake<CT>(0, 0);
       F1[i] = live ? cmake<CT>(n2 + b2, 0) : cmake<CT>(0, 0);
     }
@@ -598,7 +618,7 @@ x_pass2_kernel(XPassArgs a) {
   }
   __syncthreads();
   // Unpack the real-field spectra, truncate to NKX, scale 1/M, store.
-  const T h = (T)0.5 / M;
+  const RT h = (RT)0.5 / M;
   for (int idx = tid; idx < 3 * NKX * R; idx += kX2Threads) {
     int r, k, f;
     if (a.rows_fast) {
@@ -791,7 +811,8 @@ size_t yinv_smem(int My, int NY1, int fp32) {
 template <int ML, typename T = double>
 __global__ void __launch_bounds__(kPassThreads)
 yinv_kernel(YInvArgs a) {
-  using CT = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+  using CT = typename pass_types<T>::C;
+  using RT = typename pass_types<T>::R;
   extern __shared__ double2 sm[];
   const int M = ML > 0 ? ML : a.plan.L;
   const int C = kTile;
@@ -850,6 +871,7 @@ yinv_kernel(YInvArgs a) {
 
 cudaError_t launch_yinv(const YInvArgs& a, cudaStream_t st) {
   dim3 grid((a.NKX + kTile - 1) / kTile, a.NZ1);
+  if (a.fp32 == 2) return cudaErrorInvalidValue;  // compensated: two-stage passes only
   if (a.fp32) {
     const size_t sm = yinv_smem(a.plan.L, a.NY1, 1);
     switch (a.plan.L) {
@@ -879,7 +901,8 @@ size_t yfwd_smem(int My, int NY1, int fp32) {
 template <int ML, typename T = double>
 __global__ void __launch_bounds__(kPassThreads)
 yfwd_kernel(YFwdArgs a) {
-  using CT = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+  using CT = typename pass_types<T>::C;
+  using RT = typename pass_types<T>::R;
   extern __shared__ double2 sm[];
   const int M = ML > 0 ? ML : a.plan.L;
   const int C = kTile;
@@ -939,6 +962,7 @@ yfwd_kernel(YFwdArgs a) {
 
 cudaError_t launch_yfwd(const YFwdArgs& a, cudaStream_t st) {
   dim3 grid((a.NKX + kTile - 1) / kTile, a.NZ1);
+  if (a.fp32 == 2) return cudaErrorInvalidValue;  // compensated: two-stage passes only
   if (a.fp32) {
     const size_t sm = yfwd_smem(a.plan.L, a.NY1, 1);
     switch (a.plan.L) {
@@ -1156,7 +1180,8 @@ __device__ __forceinline__ void zinv2_fill(const ZInvCurlArgs& a, CT* X,
 template <int ML, typename T = double>
 __global__ void __launch_bounds__(kZ2Threads, 4)
 zinv_curl2_kernel(ZInvCurlArgs a) {
-  using CT = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+  using CT = typename pass_types<T>::C;
+  using RT = typename pass_types<T>::R;
   constexpr int M = ML, R1 = M / 8, C = kZ2Cols;
   extern __shared__ double2 sm_[];
   CT* X = reinterpret_cast<CT*>(sm_);  // [t][C]
@@ -1237,6 +1262,16 @@ cudaError_t launch_zinv_curl(const ZInvCurlArgs& a, int span_max,
   if (a.variant == 0 && (L == 48 || L == 72 || L == 96 || L == 192)) {
     const long long ncol = (long long)a.NKX * a.Ny;
     const int grid = (int)((ncol + kZ2Cols - 1) / kZ2Cols);
+    if (a.fp32 == 2) {
+      const size_t sm = zinv_curl2_smem(L) / 2;
+      switch (L) {
+        case 48: zinv_curl2_kernel<48, fcomp><<<grid, kZ2Threads, sm, st>>>(a); break;
+        case 72: zinv_curl2_kernel<72, fcomp><<<grid, kZ2Threads, sm, st>>>(a); break;
+        case 96: zinv_curl2_kernel<96, fcomp><<<grid, kZ2Threads, sm, st>>>(a); break;
+        default: zinv_curl2_kernel<192, fcomp><<<grid, kZ2Threads, sm, st>>>(a); break;
+      }
+      return cudaGetLastError();
+    }
     if (a.fp32) {
       const size_t sm = zinv_curl2_smem(L) / 2;
       switch (L) {

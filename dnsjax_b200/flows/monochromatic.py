@@ -201,6 +201,14 @@ class TriplyPeriodicFlow:
             _lib.stream_handle()))
         return state, None
 
+    def set_rhs_precision(self, fp32: bool, compensated: bool = False) -> None:
+        """FP32 (True) or FP64 (False) RHS passes for the following RHS calls
+        (the ``res.double_precision`` switch); with ``compensated`` the FP32
+        passes' register DFTs carry two-sum compensated accumulation."""
+        mode = (2 if compensated else 1) if fp32 else 0
+        _lib.check(self._L.dnsb_periodic_set_rhs_precision(self._ctx, mode))
+        self.rhs_fp32 = bool(fp32)
+
     def make_step_graph(self, state, tol: float | None = None,
                         max_iter: int | None = None, divergence: bool | None = None):
         """A CUDA graph of one full time step bound to `state` (updated in

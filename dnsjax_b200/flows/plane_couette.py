@@ -176,11 +176,15 @@ class PlaneCouetteFlow:
                                              _lib.ptr(out), _lib.stream_handle()))
         return out
 
-    def set_rhs_precision(self, fp32: bool) -> None:
+    def set_rhs_precision(self, fp32: bool, compensated: bool = False) -> None:
         """FP32 (True) or FP64 (False) RHS passes for the following RHS calls
-        (the ``res.double_precision`` switch, applied per call)."""
-        if bool(fp32) != self.rhs_fp32:
-            _lib.check(self._L.dnsb_couette_set_rhs_precision(self._ctx, int(bool(fp32))))
+        (the ``res.double_precision`` switch, applied per call); with
+        ``compensated`` the FP32 passes' register DFTs carry two-sum
+        compensated accumulation."""
+        mode = (2 if compensated else 1) if fp32 else 0
+        if mode != getattr(self, "_rhs_mode", 1 if self.rhs_fp32 else 0):
+            _lib.check(self._L.dnsb_couette_set_rhs_precision(self._ctx, mode))
+            self._rhs_mode = mode
             self.rhs_fp32 = bool(fp32)
 
     def correct_velocity(self, state):

@@ -84,7 +84,12 @@ int dnsb_periodic_rhs(dnsb_periodic* ctx, const void* state, void* rhs,
  * product run in FP32 on FP32 pass buffers; the state is read, the curl
  * formed and the projection applied in FP64, and the RHS is written in
  * complex128.  Only for padded sizes in {48, 72, 96, 192} with
- * nx_p = 3 nx / 2 (else DNSB_ERR_ARG). */
+ * nx_p = 3 nx / 2 (else DNSB_ERR_ARG).  fp32 = 2: the same FP32 passes with
+ * compensated (two-sum) accumulation in their register DFT butterflies
+ * (each value carried as h + l, the rounding errors of the butterflies'
+ * sums and constant products kept in l and folded back at the DFT's
+ * outputs); the twiddle products between stages and the pass buffers stay
+ * FP32. */
 int dnsb_periodic_set_rhs_precision(dnsb_periodic* ctx, int fp32);
 /* out = (state ldt_1 + rhs) ildt_2       (monochromatic.py:320-333) */
 int dnsb_periodic_predict(dnsb_periodic* ctx, const void* state,
@@ -185,7 +190,9 @@ int dnsb_couette_rhs(dnsb_couette* ctx, const void* state, void* rhs,
  * parameters.py:63, __main__.py:287): fp32 = 1 runs the transforms and the
  * rotational product in FP32 -- the state is read and the RHS written in
  * complex128, the IMM, its banded substitutions and every norm stay FP64;
- * fp32 = 0 (the default) is FP64 throughout.  FP32 needs padded sizes in
+ * fp32 = 0 (the default) is FP64 throughout; fp32 = 2 is fp32 = 1 with
+ * compensated (two-sum) accumulation in the register DFT butterflies, as
+ * for dnsb_periodic_set_rhs_precision.  FP32 needs padded sizes in
  * {48, 72, 96, 192} with nx_p = 3 nx / 2 (DNSB_ERR_ARG otherwise). */
 int dnsb_couette_set_rhs_precision(dnsb_couette* ctx, int fp32);
 /* One influence-matrix iteration (plane_couette.py:376-504):
