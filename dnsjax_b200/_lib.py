@@ -91,6 +91,11 @@ SIGNATURES = {
     "dnsb_couette_spec_to_phys": (c_int, [c_void_p] * 4),
     "dnsb_couette_phys_to_spec": (c_int, [c_void_p] * 4),
     "dnsb_couette_check": (c_int, [c_void_p, c_void_p]),
+    "dnsb_ensemble_create": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int,
+                                     c_void_p]),
+    "dnsb_ensemble_step": (c_int, [c_void_p, c_void_p]),
+    "dnsb_ensemble_status": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "dnsb_ensemble_destroy": (c_int, [c_void_p]),
     "dnsb_couette_clear_status": (c_int, [c_void_p, c_void_p]),
     "dnsb_couette_set_wait_limit": (c_int, [c_void_p, c_int]),
     "dnsb_periodic_set_rhs_precision": (c_int, [c_void_p, c_int]),

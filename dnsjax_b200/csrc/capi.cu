@@ -277,6 +277,74 @@ static ColPassArgs periodic_zfwd(const dnsb_periodic* p) {
   return a;
 }
 
+// y inverse with the curl as a two-stage column pass: state
+// [comp][ky][kz][kx] -> A[f][y][kz][kx] (FP64 fields; the FP32 form sets its
+// flags and table on top).
+static ColPassArgs periodic_ycurl(const dnsb_periodic* p, const void* state) {
+  ColPassArgs yc{};
+  yc.in = (const double2*)state;
+  yc.out = p->A;
+  yc.in_fs = (long long)p->NY1 * p->NZ1 * p->NKX;
+  yc.out_fs = (long long)p->My * p->NZ1 * p->NKX;
+  yc.in_os = p->NKX;
+  yc.out_os = p->NKX;
+  yc.in_ts = (long long)p->NZ1 * p->NKX;
+  yc.out_ts = (long long)p->NZ1 * p->NKX;
+  yc.nI = p->NKX;
+  yc.nstored = p->NY1;
+  yc.inverse = 1;
+  yc.plan = p->py;
+  yc.tw = p->twy;
+  yc.curl = 1;
+  yc.kx = p->kx;
+  yc.ky = p->ky;
+  yc.kz = p->kz;
+  return yc;
+}
+
+// x pass with the rotational product, in place on B[f][y][z][kx].
+static XPassArgs periodic_xpass(const dnsb_periodic* p) {
+  XPassArgs xa{};
+  xa.in = p->B;
+  xa.out = p->B;
+  xa.in_fs = xa.out_fs = (long long)p->My * p->Mz * p->NKX;
+  xa.nrows = p->My * p->Mz;
+  xa.inner_n = p->Mz;
+  xa.so = (long long)p->Mz * p->NKX;
+  xa.si = p->NKX;
+  xa.ks = 1;
+  xa.nkx = p->NKX;
+  xa.y_outer = 1;
+  xa.rows_fast = 0;
+  xa.U = p->U;
+  xa.cU = p->cU;
+  xa.nU = p->nU;
+  xa.ny_grid = p->My;
+  xa.plan = p->px;
+  xa.tw = p->twx;
+  return xa;
+}
+
+// y forward as a two-stage column pass with truncation, A[f][y][kz][kx] ->
+// rhs[comp][ky][kz][kx] (complex128); the projection follows in place.
+static ColPassArgs periodic_yfwd_col(const dnsb_periodic* p, void* rhs) {
+  ColPassArgs yc{};
+  yc.in = p->A;
+  yc.out = (double2*)rhs;
+  yc.in_fs = (long long)p->My * p->NZ1 * p->NKX;
+  yc.out_fs = p->S;
+  yc.in_os = p->NKX;
+  yc.out_os = p->NKX;
+  yc.in_ts = (long long)p->NZ1 * p->NKX;
+  yc.out_ts = (long long)p->NZ1 * p->NKX;
+  yc.nI = p->NKX;
+  yc.nstored = p->NY1;
+  yc.inverse = 0;
+  yc.plan = p->py;
+  yc.tw = p->twy;
+  return yc;
+}
+
 // The five passes of the periodic RHS; bit k of `mask` runs pass k (y
 // inverse, z inverse, x, z forward, y forward), each with its variant.
 static int periodic_rhs_impl(dnsb_periodic* p, const void* state, void* rhs, unsigned mask,
@@ -300,25 +368,9 @@ static int periodic_rhs_impl(dnsb_periodic* p, const void* state, void* rhs, uns
   if ((mask & 1u) && p->var[0] == 0 && fixed(p->My)) {
     // y inverse with the curl as a two-stage column pass: state
     // [comp][ky][kz][kx] -> A[f][y][kz][kx]
-    ColPassArgs yc{};
-    yc.in = (const double2*)state;
-    yc.out = p->A;
-    yc.in_fs = (long long)p->NY1 * p->NZ1 * p->NKX;
-    yc.out_fs = (long long)p->My * p->NZ1 * p->NKX;
-    yc.in_os = p->NKX;
-    yc.out_os = p->NKX;
-    yc.in_ts = (long long)p->NZ1 * p->NKX;
-    yc.out_ts = (long long)p->NZ1 * p->NKX;
-    yc.nI = p->NKX;
-    yc.nstored = p->NY1;
-    yc.inverse = 1;
-    yc.plan = p->py;
+    ColPassArgs yc = periodic_ycurl(p, state);
     yc.tw = yi.tw;
     yc.fp32 = yc.out32 = f32;
-    yc.curl = 1;
-    yc.kx = p->kx;
-    yc.ky = p->ky;
-    yc.kz = p->kz;
     DNSB_LAUNCH(launch_col_pass(yc, 6, p->NZ1, st));
   } else if (mask & 1u) {
     DNSB_LAUNCH(launch_yinv(yi, st));
@@ -328,23 +380,7 @@ static int periodic_rhs_impl(dnsb_periodic* p, const void* state, void* rhs, uns
   if (f32) zi.tw = reinterpret_cast<const double2*>(p->twz32);
   zi.variant = p->var[1];
   if (mask & 2u) DNSB_LAUNCH(launch_col_pass(zi, 6, p->My, st));
-  XPassArgs xa{};
-  xa.in = p->B;
-  xa.out = p->B;
-  xa.in_fs = xa.out_fs = (long long)p->My * p->Mz * p->NKX;
-  xa.nrows = p->My * p->Mz;
-  xa.inner_n = p->Mz;
-  xa.so = (long long)p->Mz * p->NKX;
-  xa.si = p->NKX;
-  xa.ks = 1;
-  xa.nkx = p->NKX;
-  xa.y_outer = 1;
-  xa.rows_fast = 0;
-  xa.U = p->U;
-  xa.cU = p->cU;
-  xa.nU = p->nU;
-  xa.ny_grid = p->My;
-  xa.plan = p->px;
+  XPassArgs xa = periodic_xpass(p);
   xa.tw = f32 ? reinterpret_cast<const double2*>(p->twx32) : p->twx;
   xa.fp32 = f32;
   xa.variant = p->var[2];
@@ -372,19 +408,7 @@ static int periodic_rhs_impl(dnsb_periodic* p, const void* state, void* rhs, uns
   if ((mask & 16u) && p->var[4] == 0 && fixed(p->My)) {
     // y forward as a two-stage column pass with truncation, A[f][y][kz][kx]
     // -> rhs[comp][ky][kz][kx] (complex128), then the projection in place
-    ColPassArgs yc{};
-    yc.in = p->A;
-    yc.out = (double2*)rhs;
-    yc.in_fs = (long long)p->My * p->NZ1 * p->NKX;
-    yc.out_fs = p->S;
-    yc.in_os = p->NKX;
-    yc.out_os = p->NKX;
-    yc.in_ts = (long long)p->NZ1 * p->NKX;
-    yc.out_ts = (long long)p->NZ1 * p->NKX;
-    yc.nI = p->NKX;
-    yc.nstored = p->NY1;
-    yc.inverse = 0;
-    yc.plan = p->py;
+    ColPassArgs yc = periodic_yfwd_col(p, rhs);
     yc.tw = yf.tw;
     yc.fp32 = f32;
     DNSB_LAUNCH(launch_col_pass(yc, 3, p->NZ1, st));
@@ -662,6 +686,394 @@ extern "C" int dnsb_step_graph_status(dnsb_step_graph* g, int* iters, double* er
 extern "C" int dnsb_step_graph_destroy(dnsb_step_graph* g) {
   if (!g) return fail(DNSB_ERR_ARG, "null argument");
   step_graph_free(g);
+  return 0;
+}
+
+// ===========================================================================
+// Ensembles as work lists: one launch per stage for every member
+// ===========================================================================
+namespace dnsb {
+// After a correction of every active member: count the iteration (first: the
+// predictor's correction), keep the errors, and set the loop's condition --
+// and, after iteration A, the IF node's (set_if) -- to "some member iterates
+// again", per member as step_ctl_kernel decides for one trajectory.
+__global__ void ens_ctl_kernel(cudaGraphConditionalHandle h, cudaGraphConditionalHandle h_if,
+                               int set_if, int n, const double* err, const double* tol,
+                               const int* max_iter, int* iters, int* active, double* err_last,
+                               int first) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+    int act = 0;
+    if (first || active[m]) {
+      const int it = first ? 0 : iters[m] + 1;
+      const double e = err[m];
+      iters[m] = it;
+      err_last[m] = e;
+      act = (e > tol[m] && it < max_iter[m]) ? 1 : 0;
+    }
+    active[m] = act;
+    if (act) atomicOr(&any, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    cudaGraphSetConditional(h, any ? 1u : 0u);
+    if (set_if) cudaGraphSetConditional(h_if, any ? 1u : 0u);
+  }
+}
+}  // namespace dnsb
+
+struct dnsb_ensemble {
+  int n = 0;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<void*> bufs;  // device allocations owned by the ensemble
+  long long k_fixed = 0, k_iter = 0;
+  int* iters = nullptr;
+  double* err_last = nullptr;
+};
+
+static void ensemble_free(dnsb_ensemble* e) {
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  for (void* q : e->bufs)
+    if (q) cudaFree(q);
+  delete e;
+}
+
+namespace {
+// One stage's work list on the device: items, their first virtual blocks,
+// the total and the persistent grid.
+struct EnsStage {
+  const void* items = nullptr;
+  const int* base = nullptr;
+  int n = 0, total = 0, grid = 0;
+  size_t smem = 0;
+  int kind = 0;
+};
+
+template <typename T>
+int ens_upload(dnsb_ensemble* e, const std::vector<T>& h, T** d) {
+  *d = nullptr;
+  if (cudaMalloc((void**)d, h.size() * sizeof(T)) != cudaSuccess)
+    return fail(DNSB_ERR_CUDA, "ensemble allocation failed");
+  e->bufs.push_back(*d);
+  if (cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(DNSB_ERR_CUDA, "ensemble upload failed");
+  return 0;
+}
+}  // namespace
+
+// Members: periodic contexts in FP64 with the default pass variants and
+// padded lengths 48, 72, 96 or 192 with nx_p = 3 nx / 2; each bound to its
+// state (updated in place by every step).
+extern "C" int dnsb_ensemble_create(dnsb_periodic* const* ctxs, void* const* states, int n,
+                                    const double* tol, const int* max_iter, int divergence,
+                                    dnsb_ensemble** out) {
+  using namespace dnsb;
+  if (!ctxs || !states || !tol || !max_iter || !out || n < 1)
+    return fail(DNSB_ERR_ARG, "null argument or no members");
+  if (n > 1024) return fail(DNSB_ERR_ARG, "at most 1024 members");
+  for (int m = 0; m < n; ++m) {
+    const dnsb_periodic* p = ctxs[m];
+    if (!p || !states[m]) return fail(DNSB_ERR_ARG, "null member");
+    if (p->rhs_fp32) return fail(DNSB_ERR_ARG, "ensemble members run in FP64");
+    for (int k = 0; k < 5; ++k)
+      if (p->var[k] != 0) return fail(DNSB_ERR_ARG, "ensemble members use the default variants");
+    if (!ens_pass_supported(p->My) || !ens_pass_supported(p->Mz) ||
+        !ens_pass_supported(p->Mx) || 3 * p->NKX != p->Mx)
+      return fail(DNSB_ERR_ARG, "ensemble members need padded lengths 48, 72, 96 or 192 "
+                                "with nx_p = 3 nx / 2");
+  }
+  auto* e = new dnsb_ensemble();
+  e->n = n;
+  int rc = 0;
+  auto alloc = [&](size_t bytes) -> void* {
+    void* q = nullptr;
+    if (!rc && cudaMalloc(&q, bytes) != cudaSuccess)
+      rc = fail(DNSB_ERR_CUDA, "ensemble allocation failed");
+    if (q) e->bufs.push_back(q);
+    return q;
+  };
+  std::vector<double2*> P(n), Ra(n), Rb(n);
+  for (int m = 0; m < n && !rc; ++m) {
+    const size_t b = 3 * (size_t)ctxs[m]->S * sizeof(double2);
+    P[m] = (double2*)alloc(b);
+    Ra[m] = (double2*)alloc(b);
+    Rb[m] = (double2*)alloc(b);
+  }
+  auto* err = (double*)alloc(n * sizeof(double));
+  e->err_last = (double*)alloc(n * sizeof(double));
+  e->iters = (int*)alloc(n * sizeof(int));
+  auto* active = (int*)alloc(n * sizeof(int));
+  double* d_tol = nullptr;
+  int* d_max = nullptr;
+  if (!rc) rc = ens_upload(e, std::vector<double>(tol, tol + n), &d_tol);
+  if (!rc) rc = ens_upload(e, std::vector<int>(max_iter, max_iter + n), &d_max);
+  if (rc) {
+    ensemble_free(e);
+    return rc;
+  }
+  // members ordered by size, largest first, so the persistent CTAs start
+  // on the longest blocks
+  std::vector<int> order(n);
+  for (int m = 0; m < n; ++m) order[m] = m;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return ctxs[a]->S > ctxs[b]->S; });
+  const int smax = max_smem_optin();
+  int maxL = 0, maxNKX = 0;
+  for (int m = 0; m < n; ++m) {
+    maxL = std::max({maxL, ctxs[m]->My, ctxs[m]->Mz, ctxs[m]->Mx});
+    maxNKX = std::max(maxNKX, ctxs[m]->NKX);
+  }
+  // kind 0..3: col (curl), col (inverse), col (forward), x pass
+  auto col_stage = [&](int kind, auto make, int nfields, auto nO) -> EnsStage {
+    EnsStage st;
+    st.kind = kind;
+    std::vector<EnsColItem> items;
+    std::vector<int> base;
+    int total = 0;
+    for (int m : order) {
+      EnsColItem it{};
+      it.a = make(ctxs[m], m);
+      it.member = m;
+      base.push_back(total);
+      total += ens_col_blocks(it.a, nO(ctxs[m]), nfields, &it.gx, &it.gy);
+      items.push_back(it);
+    }
+    EnsColItem* di = nullptr;
+    int* db = nullptr;
+    if (!rc) rc = ens_upload(e, items, &di);
+    if (!rc) rc = ens_upload(e, base, &db);
+    st.items = di;
+    st.base = db;
+    st.n = n;
+    st.total = total;
+    st.smem = ens_col_smem(maxL);
+    st.grid = rc ? 0 : ens_pass_grid(kind, st.smem, total, smax);
+    if (!rc && st.grid <= 0) rc = fail(DNSB_ERR_CUDA, "ensemble pass occupancy");
+    return st;
+  };
+  auto x_stage = [&]() -> EnsStage {
+    EnsStage st;
+    st.kind = 3;
+    std::vector<EnsXItem> items;
+    std::vector<int> base;
+    int total = 0;
+    for (int m : order) {
+      EnsXItem it{};
+      it.a = periodic_xpass(ctxs[m]);
+      it.member = m;
+      base.push_back(total);
+      total += ens_x_blocks(it.a);
+      items.push_back(it);
+    }
+    EnsXItem* di = nullptr;
+    int* db = nullptr;
+    if (!rc) rc = ens_upload(e, items, &di);
+    if (!rc) rc = ens_upload(e, base, &db);
+    st.items = di;
+    st.base = db;
+    st.n = n;
+    st.total = total;
+    st.smem = ens_x_smem(maxL, maxNKX);
+    st.grid = rc ? 0 : ens_pass_grid(3, st.smem, total, smax);
+    if (!rc && st.grid <= 0) rc = fail(DNSB_ERR_CUDA, "ensemble pass occupancy");
+    return st;
+  };
+  auto point_list = [&](auto fill) -> EnsPointItem* {
+    std::vector<EnsPointItem> items;
+    for (int m : order) {
+      EnsPointItem it{};
+      it.a = ctxs[m]->point();
+      it.member = m;
+      fill(it, m);
+      items.push_back(it);
+    }
+    EnsPointItem* d = nullptr;
+    if (!rc) rc = ens_upload(e, items, &d);
+    return d;
+  };
+  // RHS work lists for (in, out) = (state, Ra), (P, Rb), (P, Ra)
+  struct RhsLists {
+    EnsStage yc, zi, x, zf, yf;
+    EnsPointItem* proj = nullptr;
+  } rl[3];
+  for (int c = 0; c < 3; ++c) {
+    auto in_of = [&](int m) -> const void* { return c == 0 ? states[m] : (const void*)P[m]; };
+    auto out_of = [&](int m) -> void* { return c == 1 ? (void*)Rb[m] : (void*)Ra[m]; };
+    rl[c].yc = col_stage(0, [&](const dnsb_periodic* q, int m) { return periodic_ycurl(q, in_of(m)); },
+                         6, [](const dnsb_periodic* q) { return q->NZ1; });
+    rl[c].zi = col_stage(1, [&](const dnsb_periodic* q, int) { return periodic_zinv(q); }, 6,
+                         [](const dnsb_periodic* q) { return q->My; });
+    rl[c].x = x_stage();
+    rl[c].zf = col_stage(2, [&](const dnsb_periodic* q, int) { return periodic_zfwd(q); }, 3,
+                         [](const dnsb_periodic* q) { return q->My; });
+    rl[c].yf = col_stage(2, [&](const dnsb_periodic* q, int m) { return periodic_yfwd_col(q, out_of(m)); },
+                         3, [](const dnsb_periodic* q) { return q->NZ1; });
+    rl[c].proj = point_list([&](EnsPointItem& it, int m) {
+      it.in0 = (const double2*)out_of(m);
+      it.out = (double2*)out_of(m);
+    });
+  }
+  EnsPointItem* pred = point_list([&](EnsPointItem& it, int m) {
+    it.in0 = (const double2*)states[m];
+    it.in1 = Ra[m];
+    it.out = P[m];
+  });
+  // corrections: (prev, next) = (Ra, Rb) and (Rb, Ra)
+  EnsPointItem* corr[2];
+  for (int k = 0; k < 2; ++k)
+    corr[k] = point_list([&](EnsPointItem& it, int m) {
+      it.in0 = P[m];
+      it.in1 = k == 0 ? Ra[m] : Rb[m];
+      it.in2 = k == 0 ? Rb[m] : Ra[m];
+      it.out = P[m];
+      it.partials = ctxs[m]->partials;
+    });
+  EnsPointItem* cv = point_list([&](EnsPointItem& it, int m) {
+    it.in0 = P[m];
+    it.out = (double2*)states[m];
+  });
+  if (rc) {
+    ensemble_free(e);
+    return rc;
+  }
+  int nsm = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int pgrid = std::min(n * kRedBlocks, 4 * nsm);
+
+  auto run_pass = [&](const EnsStage& st, const int* act, cudaStream_t s) {
+    return launch_ens_pass(st.kind, st.items, st.base, st.n, st.total, act, st.grid, st.smem, s);
+  };
+  auto rhs = [&](int c, const int* act, cudaStream_t s) -> cudaError_t {
+    cudaError_t r;
+    const RhsLists& L = rl[c];
+    if ((r = run_pass(L.yc, act, s)) != cudaSuccess) return r;
+    if ((r = run_pass(L.zi, act, s)) != cudaSuccess) return r;
+    if ((r = run_pass(L.x, act, s)) != cudaSuccess) return r;
+    if ((r = run_pass(L.zf, act, s)) != cudaSuccess) return r;
+    if ((r = run_pass(L.yf, act, s)) != cudaSuccess) return r;
+    return launch_ens_point(L.proj, n, act, 2, 1, 0, pgrid, s);
+  };
+  auto correct = [&](int k, const int* act, cudaStream_t s) -> cudaError_t {
+    cudaError_t r = launch_ens_point(corr[k], n, act, 1, 0, 0, pgrid, s);
+    if (r == cudaSuccess) r = launch_ens_finalize(corr[k], n, act, err, s);
+    return r;
+  };
+
+  // the graph: prologue, WHILE { A; IF { B } }, epilogue (as build_step_graph)
+  cudaStream_t s = nullptr, sb = nullptr, si = nullptr;
+  cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  cudaStreamCreateWithFlags(&sb, cudaStreamNonBlocking);
+  cudaStreamCreateWithFlags(&si, cudaStreamNonBlocking);
+  auto ck = [&](cudaError_t r, const char* what) {
+    if (r != cudaSuccess && !rc)
+      rc = fail(DNSB_ERR_CUDA, std::string("ensemble graph: ") + what + ": " +
+                                   cudaGetErrorString(r));
+  };
+  auto add_cond = [&](cudaStream_t st, cudaGraph_t gr, cudaGraphConditionalHandle hd,
+                      cudaGraphConditionalNodeType type) -> cudaGraph_t {
+    if (rc) return nullptr;
+    cudaStreamCaptureStatus cst;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    ck(cudaStreamGetCaptureInfo(st, &cst, nullptr, nullptr, &deps, &ndeps), "capture info");
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hd;
+    cp.conditional.type = type;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if (!rc) ck(cudaGraphAddNode(&node, gr, deps, ndeps, &cp), "conditional node");
+    if (!rc)
+      ck(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies),
+         "capture dependencies");
+    return rc ? nullptr : cp.conditional.phGraph_out[0];
+  };
+  cudaGraph_t graph = nullptr;
+  ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+  cudaStreamCaptureStatus cs;
+  ck(cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, nullptr, nullptr), "capture info");
+  cudaGraphConditionalHandle h = 0, h_if = 0;
+  ck(cudaGraphConditionalHandleCreate(&h, graph, 0, 0), "conditional handle");
+  // prologue: every member
+  ck(rhs(0, nullptr, s), "rhs");
+  ck(launch_ens_point(pred, n, nullptr, 0, 0, 0, pgrid, s), "predict");
+  ck(rhs(1, nullptr, s), "rhs");
+  ck(correct(0, nullptr, s), "correct");
+  ens_ctl_kernel<<<1, 1024, 0, s>>>(h, 0, 0, n, err, d_tol, d_max, e->iters, active,
+                                    e->err_last, 1);
+  ck(cudaGetLastError(), "control kernel");
+  cudaGraph_t bg = add_cond(s, graph, h, cudaGraphCondTypeWhile);
+  if (!rc) {
+    ck(cudaGraphConditionalHandleCreate(&h_if, bg, 0, 0), "conditional handle");
+    ck(cudaStreamBeginCaptureToGraph(sb, bg, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal), "body capture");
+    // iteration A: rhs_next -> Ra, rhs_prev Rb
+    ck(rhs(2, active, sb), "rhs");
+    ck(correct(1, active, sb), "correct");
+    ens_ctl_kernel<<<1, 1024, 0, sb>>>(h, h_if, 1, n, err, d_tol, d_max, e->iters, active,
+                                       e->err_last, 0);
+    ck(cudaGetLastError(), "control kernel");
+    cudaGraph_t ig = add_cond(sb, bg, h_if, cudaGraphCondTypeIf);
+    if (!rc) {
+      ck(cudaStreamBeginCaptureToGraph(si, ig, nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeThreadLocal), "IF body capture");
+      // iteration B: rhs_next -> Rb, rhs_prev Ra
+      ck(rhs(1, active, si), "rhs");
+      ck(correct(0, active, si), "correct");
+      ens_ctl_kernel<<<1, 1024, 0, si>>>(h, 0, 0, n, err, d_tol, d_max, e->iters, active,
+                                         e->err_last, 0);
+      ck(cudaGetLastError(), "control kernel");
+      cudaGraph_t iout = nullptr;
+      ck(cudaStreamEndCapture(si, &iout), "end IF body capture");
+    }
+    cudaGraph_t bout = nullptr;
+    ck(cudaStreamEndCapture(sb, &bout), "end body capture");
+  }
+  ck(launch_ens_point(cv, n, nullptr, 2, divergence, 1, pgrid, s), "correct_velocity");
+  cudaGraph_t done = nullptr;
+  ck(cudaStreamEndCapture(s, &done), "end capture");  // always end the capture
+  if (!rc) ck(cudaGraphInstantiate(&e->exec, done, 0), "instantiate");
+  if (done) cudaGraphDestroy(done);
+  cudaStreamDestroy(s);
+  cudaStreamDestroy(sb);
+  cudaStreamDestroy(si);
+  if (rc) {
+    ensemble_free(e);
+    return rc;
+  }
+  // launches: prologue 2 RHS (6 each) + predict + correct + finalize +
+  // control, epilogue 1; an iteration 6 + 3
+  e->k_fixed = 2 * 6 + 4 + 1;
+  e->k_iter = 6 + 3;
+  *out = e;
+  return 0;
+}
+
+extern "C" int dnsb_ensemble_step(dnsb_ensemble* e, void* stream) {
+  if (!e) return fail(DNSB_ERR_ARG, "null argument");
+  DNSB_CUDA(cudaGraphLaunch(e->exec, as_stream(stream)));
+  return 0;
+}
+
+extern "C" int dnsb_ensemble_status(dnsb_ensemble* e, int* iters, double* errs, void* stream) {
+  if (!e || !iters || !errs) return fail(DNSB_ERR_ARG, "null argument");
+  cudaStream_t st = as_stream(stream);
+  DNSB_CUDA(cudaMemcpyAsync(iters, e->iters, e->n * sizeof(int), cudaMemcpyDeviceToHost, st));
+  DNSB_CUDA(cudaMemcpyAsync(errs, e->err_last, e->n * sizeof(double), cudaMemcpyDeviceToHost,
+                            st));
+  DNSB_CUDA(cudaStreamSynchronize(st));
+  int most = 0;
+  for (int m = 0; m < e->n; ++m) most = std::max(most, iters[m]);
+  g_launches.fetch_add(e->k_fixed + (long long)most * e->k_iter, std::memory_order_relaxed);
+  return 0;
+}
+
+extern "C" int dnsb_ensemble_destroy(dnsb_ensemble* e) {
+  if (!e) return fail(DNSB_ERR_ARG, "null argument");
+  ensemble_free(e);
   return 0;
 }
 

@@ -137,8 +137,7 @@ size_t col_pass2_smem(int M) {
 // spectral state and field f of the 6 is u, v, w (f < 3) or the spectral
 // curl i (k x u) (triply_periodic.py:122-132), formed in FP64 at the load.
 template <int ML, int SIGN, typename T = double, bool OUT32 = false, bool CURL = false>
-__global__ void __launch_bounds__(kC2Threads)
-col_pass2_kernel(ColPassArgs a) {
+__device__ __forceinline__ void col_pass2_body(const ColPassArgs& a, int bx, int by, int bz) {
   using CT = typename pass_types<T>::C;
   using RT = typename pass_types<T>::R;
   constexpr int M = ML, R1 = M / 8, C = kC2Cols;
@@ -146,9 +145,9 @@ col_pass2_kernel(ColPassArgs a) {
   CT* X = reinterpret_cast<CT*>(sm_);  // [t][C]
   CT* tw = X + M * C;
   const int tid = threadIdx.x;
-  const int i0 = blockIdx.x * C;
-  const long long o = blockIdx.y;
-  const long long f = blockIdx.z;
+  const int i0 = bx * C;
+  const long long o = by;
+  const long long f = bz;
   const CT* in = reinterpret_cast<const CT*>(a.in) + f * a.in_fs + o * a.in_os + i0;
   // FP64 output, or (OUT32, FP32 arithmetic) an FP32 pass buffer
   double2* out = a.out + f * a.out_fs + o * a.out_os + i0;
@@ -228,6 +227,15 @@ col_pass2_kernel(ColPassArgs a) {
       }
     }
   }
+}
+
+// Block (bx, by, bz) = (column tile, outer index, field) of the grid
+// ((nI + 15) / 16, nO, nfields); the work-list ensemble kernels call the body
+// with their own block numbering.
+template <int ML, int SIGN, typename T = double, bool OUT32 = false, bool CURL = false>
+__global__ void __launch_bounds__(kC2Threads)
+col_pass2_kernel(ColPassArgs a) {
+  col_pass2_body<ML, SIGN, T, OUT32, CURL>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
@@ -470,8 +478,7 @@ size_t x_pass2_smem(int M, int nkx) {
 // T: the compute type and the element type of the pass buffer (double, or
 // float for the FP32 form of the Couette RHS).
 template <int ML, typename T>
-__global__ void __launch_bounds__(kX2Threads)
-x_pass2_kernel(XPassArgs a) {
+__device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
   using CT = typename pass_types<T>::C;
   using RT = typename pass_types<T>::R;
   constexpr int M = ML, R1 = M / 8, R = kX2Rows, NKX = ML / 3;
@@ -493,7 +500,7 @@ x_pass2_kernel(XPassArgs a) {
   const CT* gtw = reinterpret_cast<const CT*>(a.tw);
   CT* gout = reinterpret_cast<CT*>(a.out);
   const int tid = threadIdx.x;
-  const int r0 = blockIdx.x * R;
+  const int r0 = bx * R;
   const int nr = min(R, a.nrows - r0);
   __shared__ long long s_off[kX2Rows];
   __shared__ int s_y[kX2Rows];
@@ -642,6 +649,139 @@ x_pass2_kernel(XPassArgs a) {
     }
     st_l2(gout + f * a.out_fs + s_off[r] + k * a.ks, v, keep);
   }
+}
+
+template <int ML, typename T>
+__global__ void __launch_bounds__(kX2Threads)
+x_pass2_kernel(XPassArgs a) {
+  x_pass2_body<ML, T>(a, blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// Work-list forms for ensembles (csrc/capi.cu, dnsb_ensemble_*): one launch
+// runs the two-stage pass of every member.  Item k covers the member's blocks
+// base_k .. base_k + blocks_k - 1 of the flattened grid (bx fastest); every
+// CTA walks the virtual blocks blockIdx.x, blockIdx.x + gridDim.x, ... and
+// runs the member's body on its block, so each member computes exactly what
+// its own launch computes.  Members whose `active` flag is 0 are skipped.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int ens_find(const int* __restrict__ base, int n, int vb) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (base[mid] <= vb) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int SIGN, bool CURL>
+__global__ void __launch_bounds__(kC2Threads)
+ens_col_pass2_kernel(const EnsColItem* __restrict__ items, const int* __restrict__ base, int n,
+                     int total, const int* __restrict__ active) {
+  __shared__ int s_k;
+  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+    if (threadIdx.x == 0) s_k = ens_find(base, n, vb);
+    __syncthreads();
+    const int k = s_k;
+    const int m = items[k].member;
+    if (!active || active[m]) {
+      const ColPassArgs a = items[k].a;
+      const int local = vb - base[k], gx = items[k].gx, gy = items[k].gy;
+      const int bx = local % gx, by = (local / gx) % gy, bz = local / (gx * gy);
+      switch (a.plan.L) {
+        case 48: col_pass2_body<48, SIGN, double, false, CURL>(a, bx, by, bz); break;
+        case 72: col_pass2_body<72, SIGN, double, false, CURL>(a, bx, by, bz); break;
+        case 96: col_pass2_body<96, SIGN, double, false, CURL>(a, bx, by, bz); break;
+        default: col_pass2_body<192, SIGN, double, false, CURL>(a, bx, by, bz); break;
+      }
+    }
+    __syncthreads();  // shared memory and s_k are reused by the next block
+  }
+}
+
+__global__ void __launch_bounds__(kX2Threads)
+ens_x_pass2_kernel(const EnsXItem* __restrict__ items, const int* __restrict__ base, int n,
+                   int total, const int* __restrict__ active) {
+  __shared__ int s_k;
+  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+    if (threadIdx.x == 0) s_k = ens_find(base, n, vb);
+    __syncthreads();
+    const int k = s_k;
+    const int m = items[k].member;
+    if (!active || active[m]) {
+      const XPassArgs a = items[k].a;
+      const int bx = vb - base[k];
+      switch (a.plan.L) {
+        case 48: x_pass2_body<48, double>(a, bx); break;
+        case 72: x_pass2_body<72, double>(a, bx); break;
+        case 96: x_pass2_body<96, double>(a, bx); break;
+        default: x_pass2_body<192, double>(a, bx); break;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+bool ens_pass_supported(int L) { return L == 48 || L == 72 || L == 96 || L == 192; }
+
+int ens_col_blocks(const ColPassArgs& a, int nO, int nfields, int* gx, int* gy) {
+  *gx = (a.nI + kC2Cols - 1) / kC2Cols;
+  *gy = nO;
+  return *gx * nO * nfields;
+}
+
+int ens_x_blocks(const XPassArgs& a) { return (a.nrows + kX2Rows - 1) / kX2Rows; }
+
+size_t ens_col_smem(int maxL) { return col_pass2_smem(maxL); }
+size_t ens_x_smem(int maxL, int maxNKX) { return x_pass2_smem(maxL, maxNKX); }
+
+// kind 0: inverse with the curl, 1: inverse, 2: forward (col_pass2); 3: x pass.
+static const void* ens_kernel(int kind) {
+  switch (kind) {
+    case 0: return (const void*)ens_col_pass2_kernel<1, true>;
+    case 1: return (const void*)ens_col_pass2_kernel<1, false>;
+    case 2: return (const void*)ens_col_pass2_kernel<-1, false>;
+    default: return (const void*)ens_x_pass2_kernel;
+  }
+}
+
+// Persistent grid of a work-list pass kernel: resident CTAs per SM x SMs,
+// at most `total`; also raises the kernel's dynamic shared-memory limit.
+int ens_pass_grid(int kind, size_t smem, int total, int max_smem) {
+  const void* f = ens_kernel(kind);
+  if (allow_dynamic_smem(f, max_smem) != cudaSuccess) return 0;
+  int per_sm = 0, dev = 0, nsm = 0;
+  const int threads = kind == 3 ? kX2Threads : kC2Threads;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, threads, smem) != cudaSuccess)
+    return 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return 0;
+  const int g = per_sm * nsm;
+  return g < total ? g : total;
+}
+
+cudaError_t launch_ens_pass(int kind, const void* items, const int* base, int n, int total,
+                            const int* active, int grid, size_t smem, cudaStream_t st) {
+  switch (kind) {
+    case 0:
+      ens_col_pass2_kernel<1, true><<<grid, kC2Threads, smem, st>>>(
+          static_cast<const EnsColItem*>(items), base, n, total, active);
+      break;
+    case 1:
+      ens_col_pass2_kernel<1, false><<<grid, kC2Threads, smem, st>>>(
+          static_cast<const EnsColItem*>(items), base, n, total, active);
+      break;
+    case 2:
+      ens_col_pass2_kernel<-1, false><<<grid, kC2Threads, smem, st>>>(
+          static_cast<const EnsColItem*>(items), base, n, total, active);
+      break;
+    default:
+      ens_x_pass2_kernel<<<grid, kX2Threads, smem, st>>>(static_cast<const EnsXItem*>(items),
+                                                          base, n, total, active);
+  }
+  return cudaGetLastError();
 }
 
 // x pass to physical values only (spec_to_phys of 3 fields).

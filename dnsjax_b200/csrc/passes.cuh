@@ -145,6 +145,28 @@ size_t zinv_curl2_smem(int M);
 cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
                             cudaStream_t st);
 cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st);
+
+// Work lists of the ensemble form (one launch per pass for every member;
+// FP64 two-stage passes, padded lengths 48, 72, 96, 192).
+struct EnsColItem {
+  ColPassArgs a;
+  int gx, gy;  // the member's grid (gx, gy, nfields), flattened bx fastest
+  int member;
+};
+struct EnsXItem {
+  XPassArgs a;
+  int member;
+};
+bool ens_pass_supported(int L);
+int ens_col_blocks(const ColPassArgs& a, int nO, int nfields, int* gx, int* gy);
+int ens_x_blocks(const XPassArgs& a);
+size_t ens_col_smem(int maxL);
+size_t ens_x_smem(int maxL, int maxNKX);
+// kind 0: inverse pass with the spectral curl, 1: inverse, 2: forward
+// (column passes); 3: the x pass.  base[k]: first virtual block of item k.
+int ens_pass_grid(int kind, size_t smem, int total, int max_smem);
+cudaError_t launch_ens_pass(int kind, const void* items, const int* base, int n, int total,
+                            const int* active, int grid, size_t smem, cudaStream_t st);
 cudaError_t launch_x_phys(const XPhysArgs& a, cudaStream_t st);
 // Forward x pass from physical rows (uses XPhysArgs with in_fs = spectral
 // field stride, out_fs = physical field stride).

@@ -28,8 +28,8 @@ __device__ __forceinline__ double block_sum(double v) {
   return v;
 }
 
-__global__ void finalize_kernel(const double* partials, int n, double* out,
-                                double scale, int do_sqrt) {
+__device__ __forceinline__ void finalize_body(const double* partials, int n, double* out,
+                                              double scale, int do_sqrt) {
   double s = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) s += partials[i];
   s = block_sum(s);
@@ -37,6 +37,11 @@ __global__ void finalize_kernel(const double* partials, int n, double* out,
     s *= scale;
     out[0] = do_sqrt ? sqrt(s) : s;
   }
+}
+
+__global__ void finalize_kernel(const double* partials, int n, double* out,
+                                double scale, int do_sqrt) {
+  finalize_body(partials, n, out, scale, do_sqrt);
 }
 
 cudaError_t launch_finalize(const double* partials, int n, double* out,
@@ -48,19 +53,30 @@ cudaError_t launch_finalize(const double* partials, int n, double* out,
 // ---------------------------------------------------------------------------
 // Periodic pointwise kernels (monochromatic.py:320-355, 516-565).
 // ---------------------------------------------------------------------------
-__global__ void periodic_predict_kernel(PeriodicPointArgs a,
-                                        const double2* __restrict__ state,
-                                        const double2* __restrict__ rhs,
-                                        double2* __restrict__ out) {
+// The pointwise bodies run as block vb of a grid of vgrid blocks (the
+// kernels: blockIdx.x, gridDim.x; the work-list ensemble kernels: their own
+// numbering, with the same vgrid, so sums are the same bit for bit).
+__device__ __forceinline__ void periodic_predict_body(const PeriodicPointArgs& a,
+                                                      const double2* __restrict__ state,
+                                                      const double2* __restrict__ rhs,
+                                                      double2* __restrict__ out, int vb,
+                                                      int vgrid) {
   const long long n = 3LL * a.S;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
+  for (long long i = vb * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)vgrid * blockDim.x) {
     const int s = (int)(i % a.S);
     const double l1 = a.ldt_1[s], l2 = a.ildt_2[s];
     const double2 u = state[i], r = rhs[i];
     // (state * ldt_1 + rhs) * ildt_2
     out[i] = cscale(cadd(cscale(u, l1), r), l2);
   }
+}
+
+__global__ void periodic_predict_kernel(PeriodicPointArgs a,
+                                        const double2* __restrict__ state,
+                                        const double2* __restrict__ rhs,
+                                        double2* __restrict__ out) {
+  periodic_predict_body(a, state, rhs, out, blockIdx.x, gridDim.x);
 }
 
 cudaError_t launch_periodic_predict(const PeriodicPointArgs& a,
@@ -70,16 +86,17 @@ cudaError_t launch_periodic_predict(const PeriodicPointArgs& a,
   return cudaGetLastError();
 }
 
-__global__ void periodic_correct_kernel(PeriodicPointArgs a,
-                                        const double2* pred,
-                                        const double2* __restrict__ prev,
-                                        const double2* __restrict__ next,
-                                        double2* pred_out, double2* corr_out,
-                                        double* __restrict__ partials) {
+__device__ __forceinline__ void periodic_correct_body(const PeriodicPointArgs& a,
+                                                      const double2* pred,
+                                                      const double2* __restrict__ prev,
+                                                      const double2* __restrict__ next,
+                                                      double2* pred_out, double2* corr_out,
+                                                      double* __restrict__ partials, int vb,
+                                                      int vgrid) {
   const long long n = 3LL * a.S;
   double acc = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
+  for (long long i = vb * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)vgrid * blockDim.x) {
     const int s = (int)(i % a.S);
     const double l2 = a.ildt_2[s];
     // c * (next - prev) * ildt_2
@@ -90,7 +107,17 @@ __global__ void periodic_correct_kernel(PeriodicPointArgs a,
     acc += km * (corr.x * corr.x + corr.y * corr.y);
   }
   acc = block_sum(acc);
-  if (threadIdx.x == 0 && partials) partials[blockIdx.x] = acc;
+  if (threadIdx.x == 0 && partials) partials[vb] = acc;
+}
+
+__global__ void periodic_correct_kernel(PeriodicPointArgs a,
+                                        const double2* pred,
+                                        const double2* __restrict__ prev,
+                                        const double2* __restrict__ next,
+                                        double2* pred_out, double2* corr_out,
+                                        double* __restrict__ partials) {
+  periodic_correct_body(a, pred, prev, next, pred_out, corr_out, partials, blockIdx.x,
+                        gridDim.x);
 }
 
 cudaError_t launch_periodic_correct(const PeriodicPointArgs& a,
@@ -157,12 +184,11 @@ cudaError_t launch_periodic_stats(const PeriodicPointArgs& a,
 }
 
 // u - grad(inv_lapl div u), then (zero_mean) the mean mode set to zero.
-__global__ void periodic_cv_kernel(PeriodicPointArgs a,
-                                   const double2* in, double2* out,
-                                   int divergence, int zero_mean) {
+__device__ __forceinline__ void periodic_cv_body(const PeriodicPointArgs& a, const double2* in,
+                                                 double2* out, int divergence, int zero_mean,
+                                                 int vb, int vgrid) {
   const int S = a.S;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S;
-       s += gridDim.x * blockDim.x) {
+  for (int s = vb * blockDim.x + threadIdx.x; s < S; s += vgrid * blockDim.x) {
     double2 u0 = in[s], u1 = in[S + s], u2 = in[2 * S + s];
     if (divergence) {
       const int ix = s % a.NKX;
@@ -186,6 +212,12 @@ __global__ void periodic_cv_kernel(PeriodicPointArgs a,
   }
 }
 
+__global__ void periodic_cv_kernel(PeriodicPointArgs a,
+                                   const double2* in, double2* out,
+                                   int divergence, int zero_mean) {
+  periodic_cv_body(a, in, out, divergence, zero_mean, blockIdx.x, gridDim.x);
+}
+
 cudaError_t launch_periodic_correct_velocity(const PeriodicPointArgs& a,
                                              const double2* in, double2* out,
                                              int divergence, cudaStream_t st) {
@@ -198,6 +230,55 @@ cudaError_t launch_periodic_correct_velocity(const PeriodicPointArgs& a,
 cudaError_t launch_periodic_project(const PeriodicPointArgs& a, double2* rhs,
                                    cudaStream_t st) {
   periodic_cv_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(a, rhs, rhs, 1, 0);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Work-list forms for ensembles (csrc/capi.cu, dnsb_ensemble_*): every
+// member's kRedBlocks virtual blocks of the pointwise kernels in one launch,
+// members whose `active` flag is 0 skipped.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool ens_skip(const int* active, int m) {
+  return active && !active[m];
+}
+
+__global__ void __launch_bounds__(kRedThreads)
+ens_point_kernel(const EnsPointItem* __restrict__ items, int n, const int* __restrict__ active,
+                 int op, int divergence, int zero_mean) {
+  const int total = n * kRedBlocks;
+  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+    const int k = vb / kRedBlocks, b = vb % kRedBlocks;
+    const EnsPointItem it = items[k];
+    if (!ens_skip(active, it.member)) {
+      if (op == 0)
+        periodic_predict_body(it.a, it.in0, it.in1, it.out, b, kRedBlocks);
+      else if (op == 1)
+        periodic_correct_body(it.a, it.in0, it.in1, it.in2, it.out, nullptr, it.partials, b,
+                              kRedBlocks);
+      else
+        periodic_cv_body(it.a, it.in0, it.out, divergence, zero_mean, b, kRedBlocks);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(1024)
+ens_finalize_kernel(const EnsPointItem* __restrict__ items, const int* __restrict__ active,
+                    double* err) {
+  const EnsPointItem& it = items[blockIdx.x];
+  if (ens_skip(active, it.member)) return;
+  finalize_body(it.partials, kRedBlocks, err + it.member, 1.0, 1);
+}
+
+cudaError_t launch_ens_point(const EnsPointItem* items, int n, const int* active, int op,
+                             int divergence, int zero_mean, int grid, cudaStream_t st) {
+  ens_point_kernel<<<grid, kRedThreads, 0, st>>>(items, n, active, op, divergence, zero_mean);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ens_finalize(const EnsPointItem* items, int n, const int* active,
+                                double* err, cudaStream_t st) {
+  ens_finalize_kernel<<<n, 1024, 0, st>>>(items, active, err);
   return cudaGetLastError();
 }
 

@@ -29,6 +29,25 @@ struct PeriodicPointArgs {
   double c;
 };
 
+// One member's pointwise call in an ensemble work list: predict (op 0:
+// out = (in0 ldt_1 + in1) ildt_2), correct (op 1: out = in0 + c (in2 - in1)
+// ildt_2, the norm partials into `partials`), correct_velocity / projection
+// (op 2: in0 -> out).
+struct EnsPointItem {
+  PeriodicPointArgs a;
+  const double2* in0;
+  const double2* in1;
+  const double2* in2;
+  double2* out;
+  double* partials;
+  int member;
+};
+cudaError_t launch_ens_point(const EnsPointItem* items, int n, const int* active, int op,
+                             int divergence, int zero_mean, int grid, cudaStream_t st);
+// err[member] = sqrt(sum of the member's kRedBlocks partials), one block each.
+cudaError_t launch_ens_finalize(const EnsPointItem* items, int n, const int* active,
+                                double* err, cudaStream_t st);
+
 cudaError_t launch_periodic_predict(const PeriodicPointArgs& a,
                                     const double2* state, const double2* rhs,
                                     double2* out, cudaStream_t st);

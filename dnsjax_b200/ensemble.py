@@ -1,5 +1,15 @@
 """Ensembles of independent trajectories advanced in lockstep on one GPU.
 
+Three drivers share the per-trajectory semantics below:
+
+* ``worklist=True`` (periodic members, the fastest): one CUDA graph per
+  ensemble step in which every stage is one launch over all members'
+  blocks (``dnsb_ensemble_*``), with a device-controlled corrector loop
+  that runs while any member iterates;
+* ``graphs=True``: one step graph per member, each on its own stream;
+* neither: the host-driven lockstep loop.
+
+
 Each trajectory keeps its own flow context (its own workspace and sizes, so
 resolutions may differ) and runs on its own CUDA stream; every time step
 follows the reference driver's semantics per trajectory
@@ -32,7 +42,8 @@ class Ensemble:
     see timestep.StepGraph), and the host synchronises once per ensemble step to read
     every trajectory's iterations and error."""
 
-    def __init__(self, flows, states, tol=None, max_iter=None, graphs=False, autotune=False):
+    def __init__(self, flows, states, tol=None, max_iter=None, graphs=False, autotune=False,
+                 worklist=False):
         import torch
 
         if len(flows) != len(states):
@@ -58,7 +69,49 @@ class Ensemble:
         self.streams = [torch.cuda.Stream() for _ in self.flows]
         self.graphs = ([f.make_step_graph(s, tol=t, max_iter=m) for f, s, t, m in
                         zip(self.flows, self.states, self.tol, self.max_iter)]
-                       if graphs else None)
+                       if graphs and not worklist else None)
+        self._ens = None
+        if worklist:
+            from . import _lib
+
+            if autotune:
+                raise ValueError("the work-list ensemble runs the default pass variants")
+            L = _lib.lib()
+            n = len(self.flows)
+            for f in self.flows:
+                if not hasattr(f, "make_step_graph") or hasattr(f, "imm"):
+                    raise ValueError("the work-list ensemble is built for the periodic flows")
+            dbg = self.flows[0].params.debug
+            divergence = True if dbg is None else dbg.correct_divergence
+            ctxs = (_lib.C.c_void_p * n)(*[f._ctx.value for f in self.flows])
+            sts = (_lib.C.c_void_p * n)(*[f._check(x) for f, x in zip(self.flows, self.states)])
+            tols = (_lib.C.c_double * n)(*[float(t) for t in self.tol])
+            mis = (_lib.C.c_int * n)(*[int(m) for m in self.max_iter])
+            h = _lib.C.c_void_p()
+            _lib.check(L.dnsb_ensemble_create(ctxs, sts, n, tols, mis, int(divergence),
+                                              _lib.C.byref(h)))
+            self._ens, self._L = h, L
+
+    def close(self):
+        if getattr(self, "_ens", None) is not None and self._ens.value:
+            self._L.dnsb_ensemble_destroy(self._ens)
+            self._ens = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _worklist_step(self) -> EnsembleStep:
+        from . import _lib
+
+        n = len(self.flows)
+        _lib.check(self._L.dnsb_ensemble_step(self._ens, _lib.stream_handle()))
+        its = (_lib.C.c_int * n)()
+        errs = (_lib.C.c_double * n)()
+        _lib.check(self._L.dnsb_ensemble_status(self._ens, its, errs, _lib.stream_handle()))
+        return EnsembleStep(corrector_iterations=list(its), errors=list(errs))
 
     def _graph_step(self) -> EnsembleStep:
         import torch
@@ -80,6 +133,8 @@ class Ensemble:
     def step(self) -> EnsembleStep:
         import torch
 
+        if self._ens is not None:
+            return self._worklist_step()
         if self.graphs is not None:
             return self._graph_step()
 

@@ -128,6 +128,31 @@ int dnsb_step_graph_status(dnsb_step_graph* g, int* iters, double* err,
                            void* stream);
 int dnsb_step_graph_destroy(dnsb_step_graph* g);
 
+/* Ensembles of independent periodic trajectories (the driver's time step,
+ * __main__.py:125-203, for every member; no counterpart for several
+ * trajectories in the reference): one ensemble step is one CUDA graph in
+ * which every stage -- each of the five RHS passes, the projection, the
+ * predictor, the correction with its norm, correct_velocity -- is ONE
+ * launch over all members (a work list of the members' blocks walked by a
+ * persistent grid), and the corrector loop is a device-controlled WHILE
+ * node that runs while any member iterates; a member that has converged or
+ * reached max_iter[m] is skipped.  Every member computes exactly what its
+ * own step graph computes (the same blocks, the same reduction order).
+ * Members: FP64 contexts with the default pass variants and padded lengths
+ * 48, 72, 96 or 192 with nx_p = 3 nx / 2; at most 1024.  states[m] is bound
+ * (advanced in place by every step).  Creation allocates the members'
+ * prediction and RHS buffers and the work lists; stepping allocates
+ * nothing. */
+typedef struct dnsb_ensemble dnsb_ensemble;
+int dnsb_ensemble_create(dnsb_periodic* const* ctxs, void* const* states, int n,
+                         const double* tol, const int* max_iter, int divergence,
+                         dnsb_ensemble** out);
+int dnsb_ensemble_step(dnsb_ensemble* e, void* stream);
+/* Per member: corrector iterations and final corrector error of the last
+ * step (host arrays of n; synchronises `stream`). */
+int dnsb_ensemble_status(dnsb_ensemble* e, int* iters, double* errs, void* stream);
+int dnsb_ensemble_destroy(dnsb_ensemble* e);
+
 /* out_dev[0] = sum k_metric |v|^2, out_dev[1] = sum -lapl |v|^2 (the two
  * reductions of monochromatic.py:433-466). */
 int dnsb_periodic_energy_sums(dnsb_periodic* ctx, const void* v,

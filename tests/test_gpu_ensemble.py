@@ -158,3 +158,65 @@ def test_couette_graph_ensemble_equals_sequential():
                                   f.params.step.max_corrector_iterations)
             assert c == its[k][i]
         assert torch.equal(s, ens.states[i]), i
+
+
+def test_worklist_ensemble_equals_step_graphs():
+    """The work-list ensemble (one launch per stage for all members, the
+    corrector loop on the device while any member iterates) against each
+    member's own step graph: the same states bit for bit and the same
+    iteration counts, over 4 steps of members of three sizes and different
+    Re, including a member with a corrector cap it reaches (max_iter 1)."""
+    import torch
+
+    from dnsjax_b200 import _lib
+
+    spec = [(32, 35.0, 0), (48, 60.0, 1), (64, 42.0, 3), (32, 75.0, 2), (48, 30.0, 4)]
+    built = [member(*s) for s in spec]
+    flows = [f for f, _ in built]
+    caps = [10, 10, 10, 1, 10]
+    states = [torch.as_tensor(u, device="cuda") for _, u in built]
+
+    L = _lib.lib()
+    n = len(flows)
+    ctxs = (_lib.C.c_void_p * n)(*[f._ctx.value for f in flows])
+    sts = (_lib.C.c_void_p * n)(*[f._check(x) for f, x in zip(flows, states)])
+    tols = (_lib.C.c_double * n)(*[1e-10] * n)
+    mis = (_lib.C.c_int * n)(*caps)
+    h = _lib.C.c_void_p()
+    _lib.check(L.dnsb_ensemble_create(ctxs, sts, n, tols, mis, 1, _lib.C.byref(h)))
+    its_w = []
+    for _ in range(4):
+        _lib.check(L.dnsb_ensemble_step(h, _lib.stream_handle()))
+        its = (_lib.C.c_int * n)()
+        errs = (_lib.C.c_double * n)()
+        _lib.check(L.dnsb_ensemble_status(h, its, errs, _lib.stream_handle()))
+        its_w.append(list(its))
+    L.dnsb_ensemble_destroy(h)
+    assert any(k[3] == 1 for k in its_w)  # the capped member stopped at its cap
+    for i, (f, u) in enumerate(built):
+        s = torch.as_tensor(u, device="cuda")
+        g = f.make_step_graph(s, tol=1e-10, max_iter=caps[i])
+        for k in range(4):
+            g.launch()
+            assert g.status()[0] == its_w[k][i], (i, k)
+        g.close()
+        assert torch.equal(s, states[i]), i
+
+
+def test_worklist_ensemble_class():
+    """Ensemble(worklist=True) steps the same states as Ensemble(graphs=True)."""
+    import torch
+
+    from dnsjax_b200.ensemble import Ensemble
+
+    spec = [(32, 35.0, 7), (64, 50.0, 8), (48, 45.0, 9)]
+    built = [member(*s) for s in spec]
+    flows = [f for f, _ in built]
+    a = Ensemble(flows, [torch.as_tensor(u, device="cuda") for _, u in built], worklist=True)
+    b = Ensemble(flows, [torch.as_tensor(u, device="cuda") for _, u in built], graphs=True)
+    for _ in range(3):
+        sa, sb = a.step(), b.step()
+        assert sa.corrector_iterations == sb.corrector_iterations
+    for x, y in zip(a.states, b.states):
+        assert torch.equal(x, y)
+    a.close()
