@@ -3,17 +3,20 @@
 //
 //   C[m][n] = sum_k A[m][k] B[n][k]        A: M x K, B: N x K, both K-contiguous
 //
-// One CTA computes one 128 x 128 tile of C (or, split along K, a partial
-// tile) with six warps:
+// A persistent grid (one CTA per SM) walks the 128 x 128 output tiles (or,
+// split along K, partial tiles); each CTA runs six warps:
 //   warp 0     TMA producer: 128 x 64 tiles of A and B (128-byte swizzle)
 //              into a 6-stage shared-memory ring, completing on the stage's
 //              "full" mbarrier;
-//   warp 1     allocates 128 TMEM columns for the FP32 accumulator; one
+//   warp 1     allocates 256 TMEM columns, two FP32 accumulators; one
 //              elected lane issues tcgen05.mma (M 128, N 128, K 16; 4 per
-//              stage) and releases each stage with tcgen05.commit on its
-//              "empty" mbarrier, then commits the "accumulator ready" one;
+//              stage) into the tile's accumulator, releases each stage with
+//              tcgen05.commit on its "empty" mbarrier and commits the tile's
+//              "accumulator full" one;
 //   warps 2-5  epilogue: tcgen05.ld of their 32 TMEM lanes (rows), bias,
-//              relu, relu-derivative mask, FP32 and / or BF16 stores.
+//              relu, relu-derivative mask, FP32 and / or BF16 stores; the
+//              accumulator is handed back as soon as it is read, so the
+//              next tile's main loop runs under this tile's stores.
 // Split along K (gridDim.z > 1) each CTA stores its raw partial tile in a
 // caller-given workspace and a second kernel sums the partials in a fixed
 // order and applies the epilogue, so results do not depend on scheduling.
@@ -211,31 +214,50 @@ __device__ __forceinline__ void epilogue_store(const TcEpilogue& e, int m, int n
   if (e.Cb) e.Cb[(long long)m * e.ldc + n] = __float2bfloat16(v);
 }
 
-// kps: k-blocks (of 64) per split; work: gridDim.z partial tiles of M x N
-// (row stride N) when split.
+__device__ __forceinline__ void bar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+
+// Persistent form: CTA c takes the work units c, c + gridDim.x, ...; unit u
+// is output tile u / splits, K split u % splits (kps k-blocks of 64 each).
+// The k-block stream of all its units runs through the 6-stage ring without
+// a break, and the accumulator alternates between two 128-column halves of
+// TMEM, so the epilogue of one unit runs under the main loop of the next:
+//   acc_full[b]   MMA -> epilogue: the unit in half b is complete
+//   acc_empty[b]  epilogue -> MMA: half b has been read (one arrive per
+//                 epilogue warp)
+// work: splits partial tiles of M x N (row stride N) when splits > 1.
 __global__ void __launch_bounds__(kTcThreads, 1)
 gemm_tn_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
-                  int M, int N, int K, int kps, TcEpilogue ep, float* work, int* status) {
+                  int M, int N, int K, int kps, int splits, TcEpilogue ep, float* work,
+                  int* status) {
   extern __shared__ uint8_t tc_smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kTcStages];
   __shared__ __align__(8) uint64_t empty_bar[kTcStages];
-  __shared__ __align__(8) uint64_t accum_bar;
+  __shared__ __align__(8) uint64_t acc_full[2];
+  __shared__ __align__(8) uint64_t acc_empty[2];
   __shared__ uint32_t tmem_slot;
 
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.y * kTcBM, n0 = blockIdx.x * kTcBN;
+  const int ntn = (N + kTcBN - 1) / kTcBN, ntm = (M + kTcBM - 1) / kTcBM;
+  const int nunits = ntm * ntn * splits;
   const int nkb = (K + kTcBK - 1) / kTcBK;
-  const int kb0 = blockIdx.z * kps;
-  const int nk = max(0, min(nkb, kb0 + kps) - kb0);
+  auto unit_k = [&](int u, int* kb0) {
+    *kb0 = (u % splits) * kps;
+    return max(0, min(nkb, *kb0 + kps) - *kb0);
+  };
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kTcStages; ++s) {
       bar_init(&full_bar[s], 1);
       bar_init(&empty_bar[s], 1);
     }
-    bar_init(&accum_bar, 1);
+    for (int b = 0; b < 2; ++b) {
+      bar_init(&acc_full[b], 1);
+      bar_init(&acc_empty[b], 4);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapA)) : "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapB)) : "memory");
@@ -243,7 +265,7 @@ gemm_tn_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      su32(&tmem_slot)),
-                 "r"(kTcBN)
+                 "r"(2 * kTcBN)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -254,76 +276,102 @@ gemm_tn_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
 
   if (warp == 0) {
     if (lane == 0) {
-      // producer
-      int issued = 0;
+      // producer: the k-blocks of every unit of this CTA, one stream
+      int g = 0;
       bool ok = true;
-      for (int i = 0; i < nk && ok; ++i) {
-        const int s = i % kTcStages;
-        if (i >= kTcStages) ok = bar_wait(&empty_bar[s], ((i / kTcStages) - 1) & 1, status);
-        if (!ok) break;
-        uint8_t* sa = smem + s * kTcStageBytes;
-        bar_expect_tx(&full_bar[s], kTcStageBytes);
-        const int kx = (kb0 + i) * kTcBK;
-        tma_load_2d(sa, &mapA, kx, m0, &full_bar[s]);
-        tma_load_2d(sa + kTcTileBytes, &mapB, kx, n0, &full_bar[s]);
-        issued = i + 1;
+      for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+        const int tile = u / splits;
+        const int m0 = (tile / ntn) * kTcBM, n0 = (tile % ntn) * kTcBN;
+        int kb0;
+        const int nk = unit_k(u, &kb0);
+        for (int i = 0; i < nk; ++i, ++g) {
+          const int s = g % kTcStages;
+          if (g >= kTcStages) ok = bar_wait(&empty_bar[s], ((g / kTcStages) - 1) & 1, status);
+          if (!ok) break;
+          uint8_t* sa = smem + s * kTcStageBytes;
+          bar_expect_tx(&full_bar[s], kTcStageBytes);
+          const int kx = (kb0 + i) * kTcBK;
+          tma_load_2d(sa, &mapA, kx, m0, &full_bar[s]);
+          tma_load_2d(sa + kTcTileBytes, &mapB, kx, n0, &full_bar[s]);
+        }
       }
       // drain: every issued copy has landed before the CTA can exit
-      for (int i = max(0, issued - kTcStages); i < issued; ++i)
-        bar_wait(&full_bar[i % kTcStages], (i / kTcStages) & 1, status);
+      for (int h = max(0, g - kTcStages); h < g; ++h)
+        bar_wait(&full_bar[h % kTcStages], (h / kTcStages) & 1, status);
     }
   } else if (warp == 1) {
     if (lane == 0) {
       // MMA issuer
+      int g = 0, j = 0;
       bool ok = true;
-      for (int i = 0; i < nk && ok; ++i) {
-        const int s = i % kTcStages;
-        ok = bar_wait(&full_bar[s], (i / kTcStages) & 1, status);
+      for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++j) {
+        const int b = j & 1;
+        if (j >= 2) ok = bar_wait(&acc_empty[b], ((j >> 1) - 1) & 1, status);
         if (!ok) break;
         tc_fence_after();
-        const uint32_t sa = su32(smem + s * kTcStageBytes);
-        const uint32_t sb = sa + kTcTileBytes;
+        const uint32_t acc = tmem + (uint32_t)(b * kTcBN);
+        int kb0;
+        const int nk = unit_k(u, &kb0);
+        for (int i = 0; i < nk && ok; ++i, ++g) {
+          const int s = g % kTcStages;
+          ok = bar_wait(&full_bar[s], (g / kTcStages) & 1, status);
+          if (!ok) break;
+          tc_fence_after();
+          const uint32_t sa = su32(smem + s * kTcStageBytes);
+          const uint32_t sb = sa + kTcTileBytes;
 #pragma unroll
-        for (int kk = 0; kk < kTcBK / 16; ++kk)
-          tc_mma(tmem, kmajor_sw128_desc(sa + kk * 32), kmajor_sw128_desc(sb + kk * 32),
-                 (i > 0 || kk > 0) ? 1u : 0u);
-        tc_commit(&empty_bar[s]);
+          for (int kk = 0; kk < kTcBK / 16; ++kk)
+            tc_mma(acc, kmajor_sw128_desc(sa + kk * 32), kmajor_sw128_desc(sb + kk * 32),
+                   (i > 0 || kk > 0) ? 1u : 0u);
+          tc_commit(&empty_bar[s]);
+        }
+        if (ok) tc_commit(&acc_full[b]);
       }
-      if (ok && nk > 0) tc_commit(&accum_bar);
     }
   } else {
     // epilogue: warps 2..5 own TMEM lanes 32 (warp % 4) .. + 31
     const int q = warp & 3;
-    const int m = m0 + q * 32 + lane;
-    bool ok = nk > 0 && bar_wait(&accum_bar, 0, status);
-    ok = __all_sync(0xffffffffu, ok);  // the TMEM loads below are warp-collective
-    if (ok) {
+    int j = 0;
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x, ++j) {
+      const int b = j & 1;
+      bool ok = bar_wait(&acc_full[b], (j >> 1) & 1, status);
+      ok = __all_sync(0xffffffffu, ok);  // the TMEM loads below are warp-collective
+      if (!ok) break;
       tc_fence_after();
-      const bool split = gridDim.z > 1;
-      float* part = split ? work + (long long)blockIdx.z * M * N : nullptr;
+      const int tile = u / splits;
+      const int m0 = (tile / ntn) * kTcBM, n0 = (tile % ntn) * kTcBN;
+      const int m = m0 + q * 32 + lane;
+      const bool split = splits > 1;
+      float* part = split ? work + (long long)(u % splits) * M * N : nullptr;
       const bool pvec = (N % 4) == 0;
 #pragma unroll 1
       for (int c0 = 0; c0 < kTcBN; c0 += 16) {
         float v[16];
-        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kTcBN + c0), v);
+        if (c0 + 16 == kTcBN) {
+          // the half is read: hand it back to the MMA warp
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) bar_arrive(&acc_empty[b]);
+        }
         const int nb = n0 + c0;
         if (m < M && nb < N) {
           if (split && pvec && nb + 16 <= N) {
             float4* dst = reinterpret_cast<float4*>(part + (long long)m * N + nb);
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-              dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+            for (int jj = 0; jj < 4; ++jj)
+              dst[jj] = make_float4(v[4 * jj], v[4 * jj + 1], v[4 * jj + 2], v[4 * jj + 3]);
           } else if (!split && ep.vec && nb + 16 <= N) {
             epilogue_store16(ep, m, nb, v);
           } else {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              const int n = nb + j;
+            for (int jj = 0; jj < 16; ++jj) {
+              const int n = nb + jj;
               if (n < N) {
                 if (split)
-                  part[(long long)m * N + n] = v[j];
+                  part[(long long)m * N + n] = v[jj];
                 else
-                  epilogue_store(ep, m, n, v[j]);
+                  epilogue_store(ep, m, n, v[jj]);
               }
             }
           }
@@ -336,7 +384,8 @@ gemm_tn_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constan
   if (warp == 1) {
     __syncwarp();
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcBN)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(2 * kTcBN)
                  : "memory");
   }
 }
@@ -467,8 +516,18 @@ cudaError_t launch_tc_gemm(int M, int N, int K, const void* A, int lda, const vo
   }
   const int kps = (nkb + splits - 1) / splits;
   splits = (nkb + kps - 1) / kps;  // every split has at least one k-block
-  const dim3 grid((N + kTcBN - 1) / kTcBN, (M + kTcBM - 1) / kTcBM, splits);
-  gemm_tn_tc_kernel<<<grid, kTcThreads, kTcSmem, st>>>(ma, mb, M, N, K, kps, ep, work, status);
+  // one persistent CTA per SM (the ring takes most of its shared memory)
+  static int nsm = 0;
+  if (!nsm) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      nsm = 148;
+  }
+  const int units = tiles * splits;
+  const int grid = units < nsm ? units : nsm;
+  gemm_tn_tc_kernel<<<grid, kTcThreads, kTcSmem, st>>>(ma, mb, M, N, K, kps, splits, ep, work,
+                                                       status);
   cudaError_t e = cudaGetLastError();
   if (launches) *launches = 1;
   if (e != cudaSuccess || splits == 1) return e;
