@@ -125,6 +125,20 @@ SIGNATURES = {
                                           c_void_p, c_void_p]),
     "dnsb_banded_solve": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int,
                                   c_int, c_int, c_int, c_void_p, c_void_p]),
+    # slab decomposition
+    "dnsb_periodic_create_slab": (c_int, [C.POINTER(PeriodicDesc), c_int, c_int,
+                                          C.POINTER(c_void_p)]),
+    "dnsb_periodic_slab_buffers": (c_int, [c_void_p, C.POINTER(c_void_p), C.POINTER(c_void_p)]),
+    "dnsb_periodic_slab_connect": (c_int, [c_void_p, C.POINTER(c_void_p), C.POINTER(c_void_p)]),
+    "dnsb_periodic_rhs_phase": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "dnsb_couette_create_slab": (c_int, [C.POINTER(CouetteDesc), c_int, c_int,
+                                         C.POINTER(c_void_p)]),
+    "dnsb_couette_slab_buffers": (c_int, [c_void_p, C.POINTER(c_void_p), C.POINTER(c_void_p)]),
+    "dnsb_couette_slab_connect": (c_int, [c_void_p, C.POINTER(c_void_p), C.POINTER(c_void_p)]),
+    "dnsb_couette_rhs_phase": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "dnsb_ipc_handle": (c_int, [c_void_p, c_void_p]),
+    "dnsb_ipc_open": (c_int, [c_void_p, C.POINTER(c_void_p)]),
+    "dnsb_ipc_close": (c_int, [c_void_p]),
 }
 
 

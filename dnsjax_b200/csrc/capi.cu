@@ -91,6 +91,21 @@ int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
 void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 }  // namespace dnsb
 
+// Slab decomposition over several GPUs (the reference's scheme,
+// fft.py:193-392 and sharding.py:107-129): a context of rank `rank` of
+// `nranks` holds the kx modes [rank NKX, (rank + 1) NKX) of the NKXg of the
+// whole problem (its NKX is the local count); the x pass works on a share
+// of Mz / nranks padded-z rows with every kx mode, in Bx.  xdest / kdest:
+// every rank's Bx and kx-sharded pass buffer, as this process addresses
+// them.
+struct SlabState {
+  int nranks = 0, rank = 0, NKXg = 0;
+  double2* Bx = nullptr;
+  double2* xdest[kMaxRanks] = {};
+  double2* kdest[kMaxRanks] = {};
+  bool connected = false;
+};
+
 // ===========================================================================
 // Triply periodic
 // ===========================================================================
@@ -108,6 +123,7 @@ struct dnsb_periodic {
   size_t ws_bytes = 0;
   int rhs_fp32 = 0;  // RHS transforms and product in FP32 (pass buffers float2)
   int var[5] = {0, 0, 0, 0, 0};  // pass variants: y inverse, z inverse, x, z forward, y forward
+  SlabState slab;                 // nranks > 0: a slab context
 
   PeriodicPointArgs point() const {
     PeriodicPointArgs a;
@@ -123,6 +139,7 @@ struct dnsb_periodic {
     a.inv_lapl = inv_lapl;
     a.lapl = lapl;
     a.c = c;
+    a.kx0 = slab.rank == 0 ? 1 : 0;
     return a;
   }
 };
@@ -130,7 +147,7 @@ struct dnsb_periodic {
 static void periodic_free(dnsb_periodic* p) {
   void* ptrs[] = {p->twy, p->twz, p->twx, p->twy32, p->twz32, p->twx32, p->kx, p->ky,
                   p->kz, p->U, p->cU, p->nU, p->ldt1, p->ildt2, p->lapl, p->inv_lapl,
-                  p->A, p->B, p->partials};
+                  p->A, p->B, p->partials, p->slab.Bx};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete p;
@@ -422,11 +439,13 @@ static int periodic_rhs_impl(dnsb_periodic* p, const void* state, void* rhs, uns
 extern "C" int dnsb_periodic_rhs(dnsb_periodic* p, const void* state, void* rhs,
                                  void* stream) {
   if (!p || !state || !rhs) return fail(DNSB_ERR_ARG, "null argument");
+  if (p->slab.nranks) return fail(DNSB_ERR_ARG, "slab context: the RHS runs in phases");
   return periodic_rhs_impl(p, state, rhs, 31u, as_stream(stream));
 }
 
 extern "C" int dnsb_periodic_set_rhs_precision(dnsb_periodic* p, int fp32) {
   if (!p) return fail(DNSB_ERR_ARG, "null argument");
+  if (fp32 && p->slab.nranks) return fail(DNSB_ERR_ARG, "slab contexts run the FP64 passes");
   if (fp32) {
     auto fixed = [](int L) { return L == 48 || L == 72 || L == 96 || L == 192; };
     if (!fixed(p->My) || !fixed(p->Mz) || !fixed(p->Mx) || 3 * p->NKX != p->Mx)
@@ -459,8 +478,11 @@ extern "C" int dnsb_periodic_correct(dnsb_periodic* p, const void* pred,
       p->point(), (const double2*)pred, (const double2*)rhs_prev,
       (const double2*)rhs_next, (double2*)pred_out, (double2*)corr_out,
       err_dev ? p->partials : nullptr, st));
+  // A slab rank returns its share of the squared norm (summed over the ranks
+  // by the caller, who takes the square root).
   if (err_dev)
-    DNSB_LAUNCH(launch_finalize(p->partials, kRedBlocks, err_dev, 1.0, 1, st));
+    DNSB_LAUNCH(launch_finalize(p->partials, kRedBlocks, err_dev, 1.0, p->slab.nranks ? 0 : 1,
+                                st));
   return 0;
 }
 
@@ -469,7 +491,8 @@ extern "C" int dnsb_periodic_norm(dnsb_periodic* p, const void* v,
   if (!p || !v || !out_dev) return fail(DNSB_ERR_ARG, "null argument");
   cudaStream_t st = as_stream(stream);
   DNSB_LAUNCH(launch_periodic_norm2(p->point(), (const double2*)v, p->partials, st));
-  DNSB_LAUNCH(launch_finalize(p->partials, kRedBlocks, out_dev, 1.0, 1, st));
+  DNSB_LAUNCH(launch_finalize(p->partials, kRedBlocks, out_dev, 1.0, p->slab.nranks ? 0 : 1,
+                              st));
   return 0;
 }
 
@@ -635,6 +658,7 @@ extern "C" int dnsb_periodic_step_graph_create(dnsb_periodic* p, void* state, do
                                                int max_iter, int divergence,
                                                dnsb_step_graph** out) {
   if (!p || !state || !out) return fail(DNSB_ERR_ARG, "null argument");
+  if (p->slab.nranks) return fail(DNSB_ERR_ARG, "slab contexts step through the host loop");
   const size_t n = 3 * (size_t)p->S;
   dnsb_step_graph* g = new_step_graph(n);
   if (!g) return fail(DNSB_ERR_CUDA, "step graph allocation failed");
@@ -779,6 +803,7 @@ extern "C" int dnsb_ensemble_create(dnsb_periodic* const* ctxs, void* const* sta
     if (p->rhs_fp32) return fail(DNSB_ERR_ARG, "ensemble members run in FP64");
     for (int k = 0; k < 5; ++k)
       if (p->var[k] != 0) return fail(DNSB_ERR_ARG, "ensemble members use the default variants");
+    if (p->slab.nranks) return fail(DNSB_ERR_ARG, "ensemble members are whole contexts");
     if (!ens_pass_supported(p->My) || !ens_pass_supported(p->Mz) ||
         !ens_pass_supported(p->Mx) || 3 * p->NKX != p->Mx)
       return fail(DNSB_ERR_ARG, "ensemble members need padded lengths 48, 72, 96 or 192 "
@@ -1194,6 +1219,7 @@ struct dnsb_couette {
   ImmBatch batch{};
   bool batch_ready = false;
   int wait_limit = 1 << 20;  // substitution ring: polls before a wait gives up
+  SlabState slab;            // nranks > 0: a slab context
 
   ImmArgs imm() const {
     ImmArgs a{};
@@ -1227,6 +1253,7 @@ struct dnsb_couette {
     a.status = status;
     a.ab_row0 = ab_row0;
     a.pair_modes = pair_modes;
+    a.kx0 = slab.rank == 0 ? 1 : 0;
     return a;
   }
 };
@@ -1234,7 +1261,7 @@ struct dnsb_couette {
 static void couette_free(dnsb_couette* p) {
   void* ptrs[] = {p->twz, p->twx, p->twz32, p->twx32, p->kx, p->kz, p->d1w, p->d2w, p->d1wT, p->d2wT, p->d1j0,
                   p->d2j0, p->U, p->cU, p->nU, p->simpson, p->B, p->partials,
-                  p->status, p->fac, p->dp, p->Fw, p->Rw};
+                  p->status, p->fac, p->dp, p->Fw, p->Rw, p->slab.Bx};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete p;
@@ -1553,11 +1580,13 @@ static int couette_rhs_impl(dnsb_couette* p, const void* state, void* rhs, unsig
 extern "C" int dnsb_couette_rhs(dnsb_couette* p, const void* state, void* rhs,
                                 void* stream) {
   if (!p || !state || !rhs) return fail(DNSB_ERR_ARG, "null argument");
+  if (p->slab.nranks) return fail(DNSB_ERR_ARG, "slab context: the RHS runs in phases");
   return couette_rhs_impl(p, state, rhs, 7u, as_stream(stream));
 }
 
 extern "C" int dnsb_couette_set_rhs_precision(dnsb_couette* p, int fp32) {
   if (!p) return fail(DNSB_ERR_ARG, "null argument");
+  if (fp32 && p->slab.nranks) return fail(DNSB_ERR_ARG, "slab contexts run the FP64 passes");
   if (fp32) {
     auto fixed = [](int L) { return L == 48 || L == 72 || L == 96 || L == 192; };
     if (!fixed(p->Mz) || !fixed(p->Mx) || 3 * p->NKX != p->Mx)
@@ -1596,8 +1625,10 @@ extern "C" int dnsb_couette_imm(dnsb_couette* p, const void* vel_n,
                            (double2*)vel_new, (double2*)corr_out,
                            err_dev ? p->partials : nullptr, st));
   }
+  // A slab rank returns its share of the squared norm.
   if (err_dev)
-    DNSB_LAUNCH(launch_finalize(p->partials, p->NM, err_dev, 1.0 / p->ly, 1, st));
+    DNSB_LAUNCH(launch_finalize(p->partials, p->NM, err_dev, 1.0 / p->ly,
+                                p->slab.nranks ? 0 : 1, st));
   return 0;
 }
 
@@ -1607,7 +1638,7 @@ static int couette_norm_impl(dnsb_couette* p, const void* v, double* out_dev,
   cudaStream_t st = as_stream(stream);
   DNSB_LAUNCH(launch_couette_norm2(p->imm(), (const double2*)v, p->partials, st));
   DNSB_LAUNCH(launch_finalize(p->partials, kRedBlocks, out_dev, 1.0 / p->ly,
-                              do_sqrt, st));
+                              p->slab.nranks ? 0 : do_sqrt, st));
   return 0;
 }
 
@@ -1707,6 +1738,7 @@ extern "C" int dnsb_couette_phys_to_spec(dnsb_couette* p, const double* phys,
 extern "C" int dnsb_couette_step_graph_create(dnsb_couette* p, void* state, double tol,
                                               int max_iter, dnsb_step_graph** out) {
   if (!p || !state || !out) return fail(DNSB_ERR_ARG, "null argument");
+  if (p->slab.nranks) return fail(DNSB_ERR_ARG, "slab contexts step through the host loop");
   if (!p->bound) return fail(DNSB_ERR_ARG, "IMM operators not bound");
   const size_t n = 3 * (size_t)p->NM * p->Ny;
   dnsb_step_graph* g = new_step_graph(n);
@@ -1820,6 +1852,7 @@ int tune_one(int* var, int k, const int* variants, int nv, int reps, cudaStream_
 
 extern "C" int dnsb_periodic_set_variants(dnsb_periodic* p, const int* var) {
   if (!p || !var) return fail(DNSB_ERR_ARG, "null argument");
+  if (p->slab.nranks) return fail(DNSB_ERR_ARG, "slab contexts run the default pass variants");
   for (int k = 0; k < 5; ++k)
     if (var[k] < 0 || var[k] > 2 || (p->rhs_fp32 && var[k] != 0))
       return fail(DNSB_ERR_ARG, "pass variants are 0, 1 or 2 (0 only in FP32)");
@@ -1829,6 +1862,8 @@ extern "C" int dnsb_periodic_set_variants(dnsb_periodic* p, const int* var) {
 
 extern "C" int dnsb_couette_set_variants(dnsb_couette* p, const int* var) {
   if (!p || !var) return fail(DNSB_ERR_ARG, "null argument");
+  if (p->slab.nranks && (var[0] || var[1] || var[2]))
+    return fail(DNSB_ERR_ARG, "slab contexts run the default pass variants");
   for (int k = 0; k < 4; ++k)
     if (var[k] < 0 || var[k] > 2 || (k < 3 && p->rhs_fp32 && var[k] != 0))
       return fail(DNSB_ERR_ARG, "variants are 0, 1 or 2 (passes: 0 only in FP32)");
@@ -1842,6 +1877,7 @@ extern "C" int dnsb_periodic_autotune(dnsb_periodic* p, const void* state, int r
                                       int* chosen, float* ms, void* stream) {
   if (!p || !state || !chosen || !ms) return fail(DNSB_ERR_ARG, "null argument");
   if (reps < 1) return fail(DNSB_ERR_ARG, "reps must be positive");
+  if (p->slab.nranks) return fail(DNSB_ERR_ARG, "slab contexts run the default pass variants");
   cudaStream_t st = as_stream(stream);
   for (int i = 0; i < 15; ++i) ms[i] = -1.0f;
   double2* rhs = nullptr;
@@ -1866,6 +1902,7 @@ extern "C" int dnsb_couette_autotune(dnsb_couette* p, const void* state, int rep
                                      float* ms, void* stream) {
   if (!p || !state || !chosen || !ms) return fail(DNSB_ERR_ARG, "null argument");
   if (reps < 1) return fail(DNSB_ERR_ARG, "reps must be positive");
+  if (p->slab.nranks) return fail(DNSB_ERR_ARG, "slab contexts run the default pass variants");
   cudaStream_t st = as_stream(stream);
   for (int i = 0; i < 12; ++i) ms[i] = -1.0f;
   const size_t n = 3 * (size_t)p->NM * p->Ny;
@@ -2032,5 +2069,302 @@ extern "C" int dnsb_banded_solve(const double* ab, const int* ipiv, double* b,
   if (nmodes == 0) return 0;
   DNSB_LAUNCH(launch_banded_solve(ab, ipiv, b, nmodes, ny, kl, ku, ncols,
                                   status_dev, as_stream(stream)));
+  return 0;
+}
+
+// ===========================================================================
+// Slab decomposition over several GPUs (fft.py:193-392, sharding.py:107-129
+// of the reference).  Spectral arrays are sharded on kx; between the column
+// passes and the x pass the padded grid is sharded on z.  The two passes
+// that feed the other layout (the z inverse, the x pass) store every output
+// straight into the receive buffer of the rank that owns it, through that
+// rank's pointer (peer memory over NVLink, or a buffer of the same GPU when
+// the ranks are emulated in one process): the exchange is fused into the
+// pass kernels.  The RHS runs in three phases; between them the caller
+// makes every rank's previous phase complete before any rank starts the
+// next one (a collective on the stream, or plain stream order when the
+// ranks share one).
+// ===========================================================================
+static bool slab_sizes_ok(int nx_p, int nz_p, int nkxg, int nranks, int rank,
+                          const char** why) {
+  auto fixed = [](int L) { return L == 48 || L == 72 || L == 96 || L == 192; };
+  if (nranks < 1 || nranks > kMaxRanks || rank < 0 || rank >= nranks) {
+    *why = "nranks must be 1..8 and 0 <= rank < nranks";
+    return false;
+  }
+  if (nkxg % nranks || nz_p % nranks) {
+    *why = "nx/2 and nz_p must be multiples of nranks";
+    return false;
+  }
+  if (!fixed(nx_p) || !fixed(nz_p) || 3 * nkxg != nx_p) {
+    *why = "slab passes need padded sizes in {48, 72, 96, 192} with nx_p = 3 nx / 2";
+    return false;
+  }
+  return true;
+}
+
+extern "C" int dnsb_periodic_create_slab(const dnsb_periodic_desc* d, int nranks, int rank,
+                                         dnsb_periodic** out) {
+  if (!d || !out || !d->kx || !d->ldt_1 || !d->ildt_2) return fail(DNSB_ERR_ARG, "null argument");
+  *out = nullptr;
+  const int nkxg = d->nx / 2;
+  const char* why = nullptr;
+  if (!slab_sizes_ok(d->nx_p, d->nz_p, nkxg, nranks, rank, &why)) return fail(DNSB_ERR_ARG, why);
+  auto fixed = [](int L) { return L == 48 || L == 72 || L == 96 || L == 192; };
+  if (!fixed(d->ny_p)) return fail(DNSB_ERR_ARG, "slab passes need ny_p in {48, 72, 96, 192}");
+  // This rank's kx columns of the per-mode coefficients ([ky][kz][kx]).
+  const int nkx = nkxg / nranks, ny1 = d->ny - 1, nz1 = d->nz - 1;
+  std::vector<double> l1((size_t)ny1 * nz1 * nkx), l2(l1.size());
+  for (size_t r = 0; r < (size_t)ny1 * nz1; ++r)
+    for (int ix = 0; ix < nkx; ++ix) {
+      l1[r * nkx + ix] = d->ldt_1[r * nkxg + (size_t)rank * nkx + ix];
+      l2[r * nkx + ix] = d->ildt_2[r * nkxg + (size_t)rank * nkx + ix];
+    }
+  dnsb_periodic_desc ld = *d;
+  ld.nx = 2 * nkx;
+  ld.kx = d->kx + (size_t)rank * nkx;
+  ld.ldt_1 = l1.data();
+  ld.ildt_2 = l2.data();
+  dnsb_periodic* p = nullptr;
+  int rc = dnsb_periodic_create(&ld, &p);
+  if (rc) return rc;
+  p->slab.nranks = nranks;
+  p->slab.rank = rank;
+  p->slab.NKXg = nkxg;
+  const size_t nx = 6ull * p->My * (p->Mz / nranks) * nkxg;
+  if (cudaMalloc(&p->slab.Bx, nx * sizeof(double2)) != cudaSuccess) {
+    periodic_free(p);
+    return fail(DNSB_ERR_CUDA, "slab buffer allocation failed");
+  }
+  p->ws_bytes += nx * sizeof(double2);
+  *out = p;
+  return 0;
+}
+
+extern "C" int dnsb_couette_create_slab(const dnsb_couette_desc* d, int nranks, int rank,
+                                        dnsb_couette** out) {
+  if (!d || !out || !d->kx) return fail(DNSB_ERR_ARG, "null argument");
+  *out = nullptr;
+  const int nkxg = d->nx / 2;
+  const char* why = nullptr;
+  if (!slab_sizes_ok(d->nx_p, d->nz_p, nkxg, nranks, rank, &why)) return fail(DNSB_ERR_ARG, why);
+  const int nkx = nkxg / nranks;
+  dnsb_couette_desc ld = *d;
+  ld.nx = 2 * nkx;
+  ld.kx = d->kx + (size_t)rank * nkx;
+  dnsb_couette* p = nullptr;
+  int rc = dnsb_couette_create(&ld, &p);
+  if (rc) return rc;
+  p->slab.nranks = nranks;
+  p->slab.rank = rank;
+  p->slab.NKXg = nkxg;
+  const size_t nx = 6ull * (p->Mz / nranks) * nkxg * p->Ny;
+  if (cudaMalloc(&p->slab.Bx, nx * sizeof(double2)) != cudaSuccess) {
+    couette_free(p);
+    return fail(DNSB_ERR_CUDA, "slab buffer allocation failed");
+  }
+  p->ws_bytes += nx * sizeof(double2);
+  *out = p;
+  return 0;
+}
+
+static int slab_buffers(const SlabState& s, double2* B, void** bx, void** bk) {
+  if (!s.nranks) return fail(DNSB_ERR_ARG, "not a slab context");
+  if (!bx || !bk) return fail(DNSB_ERR_ARG, "null argument");
+  *bx = s.Bx;
+  *bk = B;
+  return 0;
+}
+
+static int slab_connect(SlabState& s, void* const* bx, void* const* bk) {
+  if (!s.nranks) return fail(DNSB_ERR_ARG, "not a slab context");
+  if (!bx || !bk) return fail(DNSB_ERR_ARG, "null argument");
+  for (int r = 0; r < s.nranks; ++r)
+    if (!bx[r] || !bk[r]) return fail(DNSB_ERR_ARG, "null rank buffer");
+  for (int r = 0; r < s.nranks; ++r) {
+    s.xdest[r] = (double2*)bx[r];
+    s.kdest[r] = (double2*)bk[r];
+  }
+  s.connected = true;
+  return 0;
+}
+
+extern "C" int dnsb_periodic_slab_buffers(dnsb_periodic* p, void** bx, void** bk) {
+  if (!p) return fail(DNSB_ERR_ARG, "null argument");
+  return slab_buffers(p->slab, p->B, bx, bk);
+}
+
+extern "C" int dnsb_periodic_slab_connect(dnsb_periodic* p, void* const* bx, void* const* bk) {
+  if (!p) return fail(DNSB_ERR_ARG, "null argument");
+  return slab_connect(p->slab, bx, bk);
+}
+
+extern "C" int dnsb_couette_slab_buffers(dnsb_couette* p, void** bx, void** bk) {
+  if (!p) return fail(DNSB_ERR_ARG, "null argument");
+  return slab_buffers(p->slab, p->B, bx, bk);
+}
+
+extern "C" int dnsb_couette_slab_connect(dnsb_couette* p, void* const* bx, void* const* bk) {
+  if (!p) return fail(DNSB_ERR_ARG, "null argument");
+  return slab_connect(p->slab, bx, bk);
+}
+
+static int slab_ready(const SlabState& s, int fp32, const int* var, int nvar) {
+  if (!s.nranks) return fail(DNSB_ERR_ARG, "not a slab context");
+  if (!s.connected) return fail(DNSB_ERR_ARG, "slab context not connected");
+  if (fp32) return fail(DNSB_ERR_ARG, "slab contexts run the FP64 passes");
+  for (int k = 0; k < nvar; ++k)
+    if (var[k] != 0) return fail(DNSB_ERR_ARG, "slab contexts run the default pass variants");
+  return 0;
+}
+
+// Phase 0: y inverse with the curl, z inverse into every rank's Bx (its
+// padded-z share).  Phase 1: the x pass with the product over this rank's
+// Bx into every rank's pass buffer (its kx share).  Phase 2: z forward, y
+// forward and the projection into `rhs`.
+extern "C" int dnsb_periodic_rhs_phase(dnsb_periodic* p, const void* state, void* rhs,
+                                       int phase, void* stream) {
+  if (!p || !state || !rhs) return fail(DNSB_ERR_ARG, "null argument");
+  int rc = slab_ready(p->slab, p->rhs_fp32, p->var, 5);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  const SlabState& s = p->slab;
+  const int mzl = p->Mz / s.nranks;
+  if (phase == 0) {
+    rc = periodic_rhs_impl(p, state, rhs, 1u, st);
+    if (rc) return rc;
+    ColPassArgs zi = periodic_zinv(p);
+    for (int r = 0; r < s.nranks; ++r) zi.slab.buf[r] = s.xdest[r];
+    zi.slab.blk = mzl;
+    zi.slab.fs = (long long)p->My * mzl * s.NKXg;
+    zi.out_os = (long long)mzl * s.NKXg;
+    zi.slab.ts = s.NKXg;
+    zi.slab.off = (long long)s.rank * p->NKX;
+    DNSB_LAUNCH(launch_col_pass(zi, 6, p->My, st));
+    return 0;
+  }
+  if (phase == 1) {
+    XPassArgs xa{};
+    xa.in = xa.out = s.Bx;
+    xa.in_fs = xa.out_fs = (long long)p->My * mzl * s.NKXg;
+    xa.nrows = p->My * mzl;
+    xa.inner_n = mzl;
+    xa.so = (long long)mzl * s.NKXg;
+    xa.si = s.NKXg;
+    xa.ks = 1;
+    xa.nkx = s.NKXg;
+    xa.y_outer = 1;
+    xa.rows_fast = 0;
+    xa.U = p->U;
+    xa.cU = p->cU;
+    xa.nU = p->nU;
+    xa.ny_grid = p->My;
+    xa.plan = p->px;
+    xa.tw = p->twx;
+    for (int r = 0; r < s.nranks; ++r) xa.slab.buf[r] = s.kdest[r];
+    xa.slab.blk = p->NKX;
+    xa.slab.fs = (long long)p->My * p->Mz * p->NKX;
+    xa.slab.so = (long long)p->Mz * p->NKX;
+    xa.slab.si = p->NKX;
+    xa.slab.oo = 0;
+    xa.slab.io = s.rank * mzl;
+    xa.slab.ks = 1;
+    DNSB_LAUNCH(launch_x_pass(xa, st));
+    return 0;
+  }
+  if (phase == 2) return periodic_rhs_impl(p, state, rhs, 8u | 16u, st);
+  return fail(DNSB_ERR_ARG, "phase must be 0, 1 or 2");
+}
+
+// Phase 0: z inverse with the FD curl into every rank's Bx.  Phase 1: the x
+// pass over this rank's Bx into every rank's pass buffer.  Phase 2: z
+// forward into `rhs`.
+extern "C" int dnsb_couette_rhs_phase(dnsb_couette* p, const void* state, void* rhs, int phase,
+                                      void* stream) {
+  if (!p || !state || !rhs) return fail(DNSB_ERR_ARG, "null argument");
+  int rc = slab_ready(p->slab, p->rhs_fp32, p->var, 3);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  const SlabState& s = p->slab;
+  const int mzl = p->Mz / s.nranks;
+  if (phase == 0) {
+    ZInvCurlArgs zi{};
+    zi.u = (const double2*)state;
+    zi.out = p->B;
+    zi.NZ1 = p->NZ1;
+    zi.NKX = p->NKX;
+    zi.Ny = p->Ny;
+    zi.curl = 1;
+    zi.s1 = p->s1;
+    zi.d1_j0 = p->d1j0;
+    zi.d1_w = p->d1w;
+    zi.d1_wT = p->d1wT;
+    zi.kx = p->kx;
+    zi.kz = p->kz;
+    zi.plan = p->pz;
+    zi.tw = p->twz;
+    for (int r = 0; r < s.nranks; ++r) zi.slab.buf[r] = s.xdest[r];
+    zi.slab.blk = mzl;
+    zi.slab.fs = (long long)mzl * s.NKXg * p->Ny;
+    zi.slab.ts = (long long)s.NKXg * p->Ny;
+    zi.slab.off = (long long)s.rank * p->NKX * p->Ny;
+    DNSB_LAUNCH(launch_zinv_curl(zi, p->span_max, st));
+    return 0;
+  }
+  if (phase == 1) {
+    XPassArgs xa{};
+    xa.in = xa.out = s.Bx;
+    xa.in_fs = xa.out_fs = (long long)mzl * s.NKXg * p->Ny;
+    xa.nrows = mzl * p->Ny;
+    xa.inner_n = p->Ny;
+    xa.so = (long long)s.NKXg * p->Ny;
+    xa.si = 1;
+    xa.ks = p->Ny;
+    xa.nkx = s.NKXg;
+    xa.y_outer = 0;
+    xa.rows_fast = 1;
+    xa.U = p->U;
+    xa.cU = p->cU;
+    xa.nU = p->nU;
+    xa.ny_grid = p->Ny;
+    xa.plan = p->px;
+    xa.tw = p->twx;
+    for (int r = 0; r < s.nranks; ++r) xa.slab.buf[r] = s.kdest[r];
+    xa.slab.blk = p->NKX;
+    xa.slab.fs = (long long)p->Mz * p->NKX * p->Ny;
+    xa.slab.so = (long long)p->NKX * p->Ny;
+    xa.slab.si = 1;
+    xa.slab.oo = s.rank * mzl;
+    xa.slab.io = 0;
+    xa.slab.ks = p->Ny;
+    DNSB_LAUNCH(launch_x_pass(xa, st));
+    return 0;
+  }
+  if (phase == 2) return couette_rhs_impl(p, state, rhs, 4u, st);
+  return fail(DNSB_ERR_ARG, "phase must be 0, 1 or 2");
+}
+
+// CUDA IPC of a device allocation (the slab buffers of another process's
+// rank): a 64-byte handle, opened with peer access.
+extern "C" int dnsb_ipc_handle(const void* dev_ptr, void* handle) {
+  if (!dev_ptr || !handle) return fail(DNSB_ERR_ARG, "null argument");
+  cudaIpcMemHandle_t h;
+  DNSB_CUDA(cudaIpcGetMemHandle(&h, const_cast<void*>(dev_ptr)));
+  static_assert(sizeof(h) == 64, "CUDA IPC handles are 64 bytes");
+  std::memcpy(handle, &h, sizeof(h));
+  return 0;
+}
+
+extern "C" int dnsb_ipc_open(const void* handle, void** dev_ptr) {
+  if (!handle || !dev_ptr) return fail(DNSB_ERR_ARG, "null argument");
+  cudaIpcMemHandle_t h;
+  std::memcpy(&h, handle, sizeof(h));
+  DNSB_CUDA(cudaIpcOpenMemHandle(dev_ptr, h, cudaIpcMemLazyEnablePeerAccess));
+  return 0;
+}
+
+extern "C" int dnsb_ipc_close(void* dev_ptr) {
+  if (!dev_ptr) return fail(DNSB_ERR_ARG, "null argument");
+  DNSB_CUDA(cudaIpcCloseMemHandle(dev_ptr));
   return 0;
 }

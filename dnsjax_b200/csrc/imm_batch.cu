@@ -305,7 +305,7 @@ imm_stage6_kernel(ImmArgs a, const double2* __restrict__ R, const double2* vel_j
   const double2 a2 = make_double2(-(Mi[2] * dw0.x + Mi[3] * dw1.x),
                                   -(Mi[2] * dw0.y + Mi[3] * dw1.y));
   // Stage 6: assemble, store, correction norm
-  const double km = (ix == 0) ? 1.0 : 2.0;
+  const double km = (ix == 0 && a.kx0) ? 1.0 : 2.0;
   double acc = 0.0;
 #pragma unroll
   for (int k = 0; k < YM; ++k) {

@@ -136,7 +136,8 @@ size_t col_pass2_smem(int M) {
 // OUT32 (FP32 only) an FP32 pass buffer.  CURL (inverse): `in` is the FP64
 // spectral state and field f of the 6 is u, v, w (f < 3) or the spectral
 // curl i (k x u) (triply_periodic.py:122-132), formed in FP64 at the load.
-template <int ML, int SIGN, typename T = double, bool OUT32 = false, bool CURL = false>
+template <int ML, int SIGN, typename T = double, bool OUT32 = false, bool CURL = false,
+          bool SLAB = false>
 __device__ __forceinline__ void col_pass2_body(const ColPassArgs& a, int bx, int by, int bz) {
   using CT = typename pass_types<T>::C;
   using RT = typename pass_types<T>::R;
@@ -215,8 +216,16 @@ __device__ __forceinline__ void col_pass2_body(const ColPassArgs& a, int bx, int
       for (int i = 0; i < 8; ++i) {
         const int t = k + R1 * i;
         if (SIGN > 0) {
-          if (OUT32) out_c[t * a.out_ts + c] = z[i];
-          else out[t * a.out_ts + c] = to_d(z[i]);
+          if constexpr (SLAB) {
+            // position t belongs to rank t / blk (its padded-z share)
+            const int q = t / a.slab.blk;
+            a.slab.buf[q][f * a.slab.fs + o * a.out_os + (t - q * a.slab.blk) * a.slab.ts +
+                          a.slab.off + i0 + c] = to_d(z[i]);
+          } else if (OUT32) {
+            out_c[t * a.out_ts + c] = z[i];
+          } else {
+            out[t * a.out_ts + c] = to_d(z[i]);
+          }
         } else {
           const int sidx = pos_to_stored(t, a.nstored, M);
           if (sidx >= 0) {
@@ -232,10 +241,11 @@ __device__ __forceinline__ void col_pass2_body(const ColPassArgs& a, int bx, int
 // Block (bx, by, bz) = (column tile, outer index, field) of the grid
 // ((nI + 15) / 16, nO, nfields); the work-list ensemble kernels call the body
 // with their own block numbering.
-template <int ML, int SIGN, typename T = double, bool OUT32 = false, bool CURL = false>
+template <int ML, int SIGN, typename T = double, bool OUT32 = false, bool CURL = false,
+          bool SLAB = false>
 __global__ void __launch_bounds__(kC2Threads)
 col_pass2_kernel(ColPassArgs a) {
-  col_pass2_body<ML, SIGN, T, OUT32, CURL>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  col_pass2_body<ML, SIGN, T, OUT32, CURL, SLAB>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
@@ -245,9 +255,13 @@ cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
     dim3 g2((a.nI + kC2Cols - 1) / kC2Cols, nO, nfields);
     const size_t sm2 = a.fp32 ? col_pass2_smem(L) / 2 : col_pass2_smem(L);
     if (a.fp32 && a.inverse && !a.out32) return cudaErrorInvalidValue;
+    const bool slab = a.slab.buf[0] != nullptr;
+    if (slab && (a.fp32 || a.curl || !a.inverse)) return cudaErrorInvalidValue;
 #define DNSB_C2(LL)                                                                     \
   case LL:                                                                              \
-    if (a.curl && a.fp32 == 2)                                                          \
+    if (slab)                                                                           \
+      col_pass2_kernel<LL, 1, double, false, false, true><<<g2, kC2Threads, sm2, st>>>(a); \
+    else if (a.curl && a.fp32 == 2)                                                     \
       col_pass2_kernel<LL, 1, fcomp, true, true><<<g2, kC2Threads, sm2, st>>>(a);       \
     else if (a.fp32 == 2 && a.inverse)                                                  \
       col_pass2_kernel<LL, 1, fcomp, true><<<g2, kC2Threads, sm2, st>>>(a);             \
@@ -274,7 +288,8 @@ cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
 #undef DNSB_C2
     return cudaGetLastError();
   }
-  if (a.fp32 || a.curl) return cudaErrorInvalidValue;  // two-stage compile-time passes only
+  // two-stage compile-time passes only
+  if (a.fp32 || a.curl || a.slab.buf[0]) return cudaErrorInvalidValue;
   dim3 grid((a.nI + kTile - 1) / kTile, nO, nfields);
   size_t sm = col_pass_smem(a.plan.L);
   DNSB_DISPATCH_V(a.variant, a.plan.L, col_pass_kernel, grid, sm, st, a);
@@ -419,15 +434,27 @@ x_pass_kernel(XPassArgs a) {
   }
 }
 
-template <int ML, typename T = double>
+template <int ML, typename T = double, bool SLAB = false>
 __global__ void __launch_bounds__(kX2Threads) x_pass2_kernel(XPassArgs a);
 
 cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
   dim3 grid((a.nrows + kXRows - 1) / kXRows);
   // The compile-time variants assume nx/2 = M/3 (3/2 oversampling).
   const int L = (a.nkx * 3 == a.plan.L) ? a.plan.L : -1;
+  const bool slab = a.slab.buf[0] != nullptr;
+  if (slab && (a.fp32 || a.variant != 0 || L < 0)) return cudaErrorInvalidValue;
   if (a.variant == 0 && (L == 48 || L == 72 || L == 96 || L == 192)) {
     dim3 g2((a.nrows + kX2Rows - 1) / kX2Rows);
+    if (slab) {
+      const size_t sm2 = x_pass2_smem(L, a.nkx);
+      switch (L) {
+        case 48: x_pass2_kernel<48, double, true><<<g2, kX2Threads, sm2, st>>>(a); break;
+        case 72: x_pass2_kernel<72, double, true><<<g2, kX2Threads, sm2, st>>>(a); break;
+        case 96: x_pass2_kernel<96, double, true><<<g2, kX2Threads, sm2, st>>>(a); break;
+        default: x_pass2_kernel<192, double, true><<<g2, kX2Threads, sm2, st>>>(a); break;
+      }
+      return cudaGetLastError();
+    }
     if (a.fp32 == 2) {
       const size_t sm2 = x_pass2_smem(L, a.nkx) / 2;
       switch (L) {
@@ -477,7 +504,7 @@ size_t x_pass2_smem(int M, int nkx) {
 
 // T: the compute type and the element type of the pass buffer (double, or
 // float for the FP32 form of the Couette RHS).
-template <int ML, typename T>
+template <int ML, typename T, bool SLAB = false>
 __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
   using CT = typename pass_types<T>::C;
   using RT = typename pass_types<T>::R;
@@ -503,12 +530,16 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
   const int r0 = bx * R;
   const int nr = min(R, a.nrows - r0);
   __shared__ long long s_off[kX2Rows];
+  __shared__ long long s_doff[kX2Rows];  // SLAB: the row in the destination layout
   __shared__ int s_y[kX2Rows];
   if (tid < R) {
     const int row = r0 + tid;
     const int outer = row / a.inner_n, inner = row % a.inner_n;
     s_off[tid] = (long long)outer * a.so + (long long)inner * a.si;
     s_y[tid] = a.y_outer ? outer : inner;
+    if (SLAB)
+      s_doff[tid] = (long long)(outer + a.slab.oo) * a.slab.so +
+                    (long long)(inner + a.slab.io) * a.slab.si;
   }
   for (int i = tid; i < M; i += kX2Threads) cp_async_elem(tw + i, gtw + i);
   __syncthreads();
@@ -647,14 +678,20 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
     } else {
       v = cmake<CT>((Z.x + Zm.x) * h, (Z.y - Zm.y) * h);
     }
-    st_l2(gout + f * a.out_fs + s_off[r] + k * a.ks, v, keep);
+    if constexpr (SLAB) {
+      // mode k belongs to rank k / blk (its kx share)
+      const int q = k / a.slab.blk;
+      a.slab.buf[q][f * a.slab.fs + s_doff[r] + (k - q * a.slab.blk) * a.slab.ks] = to_d(v);
+    } else {
+      st_l2(gout + f * a.out_fs + s_off[r] + k * a.ks, v, keep);
+    }
   }
 }
 
-template <int ML, typename T>
+template <int ML, typename T, bool SLAB>
 __global__ void __launch_bounds__(kX2Threads)
 x_pass2_kernel(XPassArgs a) {
-  x_pass2_body<ML, T>(a, blockIdx.x);
+  x_pass2_body<ML, T, SLAB>(a, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1317,7 +1354,7 @@ __device__ __forceinline__ void zinv2_fill(const ZInvCurlArgs& a, CT* X,
 // T: the compute type and the element type of the output pass buffer
 // (double, or float for the FP32 form of the Couette RHS); the state is
 // read, and the curl's fill computed, in FP64.
-template <int ML, typename T = double>
+template <int ML, typename T = double, bool SLAB = false>
 __global__ void __launch_bounds__(kZ2Threads, 4)
 zinv_curl2_kernel(ZInvCurlArgs a) {
   using CT = typename pass_types<T>::C;
@@ -1388,8 +1425,16 @@ zinv_curl2_kernel(ZInvCurlArgs a) {
       dft8(z, 1);
       if (c < nq) {
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
-          st_l2(gout + f * fs + (long long)(k + R1 * i) * ncol + q0 + c, z[i], keep);
+        for (int i = 0; i < 8; ++i) {
+          if constexpr (SLAB) {
+            // position t belongs to rank t / blk (its padded-z share)
+            const int t = k + R1 * i, r = t / a.slab.blk;
+            a.slab.buf[r][f * a.slab.fs + (long long)(t - r * a.slab.blk) * a.slab.ts +
+                          a.slab.off + q0 + c] = to_d(z[i]);
+          } else {
+            st_l2(gout + f * fs + (long long)(k + R1 * i) * ncol + q0 + c, z[i], keep);
+          }
+        }
       }
     }
     __syncthreads();  // X is refilled by the next field
@@ -1399,9 +1444,22 @@ zinv_curl2_kernel(ZInvCurlArgs a) {
 cudaError_t launch_zinv_curl(const ZInvCurlArgs& a, int span_max,
                              cudaStream_t st) {
   const int L = a.plan.L;
-  if (a.variant == 0 && (L == 48 || L == 72 || L == 96 || L == 192)) {
+  const bool slab = a.slab.buf[0] != nullptr;
+  const bool fixed = L == 48 || L == 72 || L == 96 || L == 192;
+  if (slab && (a.fp32 || a.variant != 0 || !fixed)) return cudaErrorInvalidValue;
+  if (a.variant == 0 && fixed) {
     const long long ncol = (long long)a.NKX * a.Ny;
     const int grid = (int)((ncol + kZ2Cols - 1) / kZ2Cols);
+    if (slab) {
+      const size_t sm = zinv_curl2_smem(L);
+      switch (L) {
+        case 48: zinv_curl2_kernel<48, double, true><<<grid, kZ2Threads, sm, st>>>(a); break;
+        case 72: zinv_curl2_kernel<72, double, true><<<grid, kZ2Threads, sm, st>>>(a); break;
+        case 96: zinv_curl2_kernel<96, double, true><<<grid, kZ2Threads, sm, st>>>(a); break;
+        default: zinv_curl2_kernel<192, double, true><<<grid, kZ2Threads, sm, st>>>(a); break;
+      }
+      return cudaGetLastError();
+    }
     if (a.fp32 == 2) {
       const size_t sm = zinv_curl2_smem(L) / 2;
       switch (L) {
@@ -1450,6 +1508,14 @@ cudaError_t set_pass_attributes(int max_smem) {
                        (const void*)zinv_curl2_kernel<72, float>,
                        (const void*)zinv_curl2_kernel<96, float>,
                        (const void*)zinv_curl2_kernel<192, float>,
+                       (const void*)zinv_curl2_kernel<48, double, true>,
+                       (const void*)zinv_curl2_kernel<72, double, true>,
+                       (const void*)zinv_curl2_kernel<96, double, true>,
+                       (const void*)zinv_curl2_kernel<192, double, true>,
+                       (const void*)x_pass2_kernel<48, double, true>,
+                       (const void*)x_pass2_kernel<72, double, true>,
+                       (const void*)x_pass2_kernel<96, double, true>,
+                       (const void*)x_pass2_kernel<192, double, true>,
                        (const void*)x_pass2_kernel<48>, (const void*)x_pass2_kernel<72>,
                        (const void*)x_pass2_kernel<96>, (const void*)x_pass2_kernel<192>,
                        (const void*)x_pass2_kernel<48, float>, (const void*)x_pass2_kernel<72, float>,
@@ -1467,7 +1533,8 @@ cudaError_t set_pass_attributes(int max_smem) {
       (const void*)col_pass2_kernel<L, 1, float, true>,                             \
       (const void*)col_pass2_kernel<L, -1, float, true>,                            \
       (const void*)col_pass2_kernel<L, 1, float, true, true>,                       \
-      (const void*)col_pass2_kernel<L, 1, double, false, true>
+      (const void*)col_pass2_kernel<L, 1, double, false, true>,                     \
+      (const void*)col_pass2_kernel<L, 1, double, false, false, true>
                        DNSB_F32_PASSES(48), DNSB_F32_PASSES(72), DNSB_F32_PASSES(96),
                        DNSB_F32_PASSES(192)};
 #undef DNSB_F32_PASSES

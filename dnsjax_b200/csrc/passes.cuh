@@ -19,6 +19,21 @@ constexpr int kX2Rows = 4;       // physical rows per CTA in the two-stage x pas
 constexpr int kX2Threads = 128;
 size_t x_pass2_smem(int M, int nkx);
 
+// Slab exchange (the reference's slab scheme over several GPUs): a pass
+// that feeds the other layout stores each output straight into the
+// buffer of the rank that owns it, through that rank's pointer (peer
+// memory, or a buffer of this GPU when the ranks are emulated on one).
+constexpr int kMaxRanks = 8;
+struct SlabDest {
+  double2* buf[kMaxRanks];  // receive buffer of each rank (null: no slab store)
+  int blk;                  // extent of the split coordinate per rank
+  long long fs, ts;         // destination field / split-coordinate strides
+  long long off;            // offset of this rank's share in every destination
+  long long so, si;         // x pass: destination row (outer + oo, inner + io)
+  int oo, io;
+  long long ks;             // x pass: destination kx stride
+};
+
 // Generic strided column pass: element (f, o, t, i) at
 // base + f*fs + o*os + t*ts + i, with i the contiguous inner index.
 struct ColPassArgs {
@@ -41,6 +56,10 @@ struct ColPassArgs {
   const double* kx;
   const double* ky;
   const double* kz;
+  // Slab store (inverse, FP64 two-stage pass): position t goes to
+  // slab.buf[t / blk] + f*fs + o*out_os + (t % blk)*ts + off + i, instead of
+  // out + f*out_fs + o*out_os + t*out_ts + i.
+  SlabDest slab;
 };
 
 // x pass.  Rows are (outer, inner) pairs; row r = outer * inner_n + inner
@@ -63,6 +82,10 @@ struct XPassArgs {
   int fp32;            // pass buffer and arithmetic in FP32 (compile-time sizes)
   int variant;         // 0: two-stage register pass when compiled for L, 1: Stockham
                        // stages (compile-time plan when compiled for L), 2: runtime plan
+  // Slab store (FP64 two-stage pass): mode k of field f of row (outer,
+  // inner) goes to slab.buf[k / blk] + f*fs + (outer + oo)*so +
+  // (inner + io)*si + (k % blk)*ks, instead of into `out`.
+  SlabDest slab;
 };
 
 // x pass to physical space only (3 fields -> real [c] at row offsets
@@ -130,6 +153,9 @@ struct ZInvCurlArgs {
   int fp32;            // output pass buffer and FFT in FP32 (compile-time sizes)
   int variant;         // 0: two-stage register pass when compiled for L, 1: Stockham
                        // stages (compile-time plan when compiled for L), 2: runtime plan
+  // Slab store (FP64 two-stage pass): position t of column q goes to
+  // slab.buf[t / blk] + f*fs + (t % blk)*ts + off + q.
+  SlabDest slab;
 };
 
 constexpr int kZTile = 8;  // y values per CTA in the Couette z passes

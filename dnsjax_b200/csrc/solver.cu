@@ -103,7 +103,7 @@ __device__ __forceinline__ void periodic_correct_body(const PeriodicPointArgs& a
     const double2 corr = cscale(cscale(csub(next[i], prev[i]), a.c), l2);
     pred_out[i] = cadd(pred[i], corr);
     if (corr_out) corr_out[i] = corr;
-    const double km = (s % a.NKX == 0) ? 1.0 : 2.0;
+    const double km = (s % a.NKX == 0 && a.kx0) ? 1.0 : 2.0;
     acc += km * (corr.x * corr.x + corr.y * corr.y);
   }
   acc = block_sum(acc);
@@ -140,7 +140,7 @@ __global__ void periodic_norm2_kernel(PeriodicPointArgs a,
        i += (long long)gridDim.x * blockDim.x) {
     const int s = (int)(i % a.S);
     const double2 z = v[i];
-    const double km = (s % a.NKX == 0) ? 1.0 : 2.0;
+    const double km = (s % a.NKX == 0 && a.kx0) ? 1.0 : 2.0;
     acc += km * (z.x * z.x + z.y * z.y);
   }
   acc = block_sum(acc);
@@ -164,7 +164,7 @@ __global__ void periodic_stats_kernel(PeriodicPointArgs a,
     const int s = (int)(i % a.S);
     const double2 z = v[i];
     const double m2 = z.x * z.x + z.y * z.y;
-    e += ((s % a.NKX == 0) ? 1.0 : 2.0) * m2;
+    e += ((s % a.NKX == 0 && a.kx0) ? 1.0 : 2.0) * m2;
     ens += -a.lapl[s] * m2;
   }
   e = block_sum(e);
@@ -203,7 +203,7 @@ __device__ __forceinline__ void periodic_cv_body(const PeriodicPointArgs& a, con
       u1 = cadd(u1, make_double2(-g1.x, -g1.y));
       u2 = cadd(u2, make_double2(-g2.x, -g2.y));
     }
-    if (s == 0 && zero_mean) {
+    if (s == 0 && zero_mean && a.kx0) {
       u0 = u1 = u2 = make_double2(0.0, 0.0);
     }
     out[s] = u0;
@@ -461,7 +461,7 @@ imm_kernel(ImmArgs a, const double2* __restrict__ vel_n,
   const double2 a2 = make_double2(-(Mi[2] * dw0.x + Mi[3] * dw1.x),
                                   -(Mi[2] * dw0.y + Mi[3] * dw1.y));
   // Stage 6: assemble, store, correction norm
-  const double km = (ix == 0) ? 1.0 : 2.0;
+  const double km = (ix == 0 && a.kx0) ? 1.0 : 2.0;
   const double* v1 = a.v1 + mo;
   const double* v2 = a.v2 + mo;
   const double* q1 = a.q1 + mo;
@@ -511,7 +511,7 @@ __global__ void couette_norm2_kernel(ImmArgs a, const double2* __restrict__ v,
        i += (long long)gridDim.x * blockDim.x) {
     const int y = (int)(i % a.Ny);
     const int m = (int)((i / a.Ny) % NM);
-    const double km = (m % a.NKX == 0) ? 1.0 : 2.0;
+    const double km = (m % a.NKX == 0 && a.kx0) ? 1.0 : 2.0;
     const double2 z = v[i];
     acc += a.simpson[y] * km * (z.x * z.x + z.y * z.y);
   }

@@ -27,6 +27,7 @@ struct PeriodicPointArgs {
   const double* inv_lapl;
   const double* lapl;
   double c;
+  int kx0;  // 1: local kx index 0 is the kx = 0 mode (weight 1 in the norms; else 2)
 };
 
 // One member's pointwise call in an ensemble work list: predict (op 0:
@@ -99,6 +100,7 @@ struct ImmArgs {
   int* status;            // set nonzero on a pivot index out of range
   int ab_row0;            // first ab row with a nonzero entry in any mode
   int pair_modes;         // 1: (s, kx) and (nz-1-s, kx) share LU factors
+  int kx0;                // 1: local kx index 0 is the kx = 0 mode (norm weight 1)
 };
 
 constexpr int kImmWarps = 4;  // modes per CTA (one warp each)

@@ -22,7 +22,13 @@ from ..timestep import StepGraph, make_fused_stepper, make_stepper
 
 
 class TriplyPeriodicFlow:
-    def __init__(self, p: Parameters, ly: float | None = None):
+    """``slab=(nranks, rank)`` makes this flow one rank's share of a slab
+    decomposition (see dnsjax_b200.slab): its tensors hold the kx modes
+    [rank nx/2/nranks, (rank+1) nx/2/nranks), as the reference's kx-sharded
+    arrays do (sharding.py:107-129)."""
+
+    def __init__(self, p: Parameters, ly: float | None = None,
+                 slab: tuple[int, int] | None = None):
         import torch
 
         L = _lib.lib()
@@ -45,7 +51,11 @@ class TriplyPeriodicFlow:
         self.dt = p.step.dt
         self.c = p.step.implicitness
         self.fourier = f = Fourier.build(r.nx, r.ny, r.nz, p.geo.lx, self.ly, p.geo.lz)
-        self.spec_shape = (3, r.ny - 1, r.nz - 1, r.nx // 2)
+        self.nranks, self.rank = (0, 0) if slab is None else (int(slab[0]), int(slab[1]))
+        nkx = r.nx // 2 // max(self.nranks, 1)
+        self.kx_range = (self.rank * nkx, (self.rank + 1) * nkx)
+        self.spec_shape = (3, r.ny - 1, r.nz - 1, nkx)
+        self.kx_axis = 3
         self.phys_shape = (3, self.ny_p, self.nz_p, self.nx_p)
         self._setup_base_flow(d)
 
@@ -69,7 +79,11 @@ class TriplyPeriodicFlow:
             c_d(hold["U"]), c_d(hold["cU"]), c_d(hold["nU"]),
             c_d(hold["l1"]), c_d(hold["l2"]))
         h = _lib.C.c_void_p()
-        _lib.check(L.dnsb_periodic_create(_lib.C.byref(desc), _lib.C.byref(h)))
+        if self.nranks:
+            _lib.check(L.dnsb_periodic_create_slab(_lib.C.byref(desc), self.nranks, self.rank,
+                                                   _lib.C.byref(h)))
+        else:
+            _lib.check(L.dnsb_periodic_create(_lib.C.byref(desc), _lib.C.byref(h)))
         self._ctx = h
         self._L = L
         if self.rhs_fp32:
@@ -156,6 +170,26 @@ class TriplyPeriodicFlow:
         out = self._new() if out is None else out
         _lib.check(self._L.dnsb_periodic_rhs(
             self._ctx, self._check(state), self._check(out), _lib.stream_handle()))
+        return out
+
+    # -- slab decomposition (dnsjax_b200.slab) -----------------------------------
+    def slab_buffers(self):
+        """This rank's receive buffers (device pointers): the padded-z share
+        the z inverse fills, and the pass buffer the x pass fills."""
+        bx, bk = _lib.C.c_void_p(), _lib.C.c_void_p()
+        _lib.check(self._L.dnsb_periodic_slab_buffers(self._ctx, _lib.C.byref(bx),
+                                                      _lib.C.byref(bk)))
+        return bx.value, bk.value
+
+    def slab_connect(self, bx, bk) -> None:
+        """Every rank's receive buffers, as this process addresses them."""
+        arr = _lib.C.c_void_p * len(bx)
+        _lib.check(self._L.dnsb_periodic_slab_connect(self._ctx, arr(*bx), arr(*bk)))
+
+    def rhs_phase(self, state, out, phase: int):
+        _lib.check(self._L.dnsb_periodic_rhs_phase(
+            self._ctx, self._check(state), self._check(out), int(phase),
+            _lib.stream_handle()))
         return out
 
     def predict(self, state, rhs, out=None):

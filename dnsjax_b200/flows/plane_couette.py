@@ -27,8 +27,14 @@ from ..timestep import StepGraph, make_fused_stepper, make_stepper
 
 
 class PlaneCouetteFlow:
+    """``slab=(nranks, rank)`` makes this flow one rank's share of a slab
+    decomposition (see dnsjax_b200.slab): its tensors and IMM operators hold
+    the kx modes [rank nx/2/nranks, (rank+1) nx/2/nranks), as the reference's
+    kx-sharded arrays do (sharding.py:107-129); ``imm``, when given, is the
+    whole problem's."""
+
     def __init__(self, p: Parameters, imm: dict | None = None, ly: float | None = None,
-                 precompute: str = "gpu"):
+                 precompute: str = "gpu", slab: tuple[int, int] | None = None):
         import torch
 
         L = _lib.lib()
@@ -58,7 +64,12 @@ class PlaneCouetteFlow:
         nU = np.zeros((3, ny))
         nU[1] = self.ys * 1.0
         self.base_flow, self.curl_base_flow, self.nonlin_base_flow = U, cU, nU
-        self.spec_shape = (3, r.nz - 1, r.nx // 2, ny)
+        self.nranks, self.rank = (0, 0) if slab is None else (int(slab[0]), int(slab[1]))
+        nkx = r.nx // 2 // max(self.nranks, 1)
+        self.kx_range = k0, k1 = (self.rank * nkx, (self.rank + 1) * nkx)
+        kx_local = self.fourier.kx_global[k0:k1]
+        self.spec_shape = (3, r.nz - 1, nkx, ny)
+        self.kx_axis = 2
         self.phys_shape = (3, ny, self.nz_p, self.nx_p)
         self.simpson = simpson_weights(self.ys)
 
@@ -77,7 +88,11 @@ class PlaneCouetteFlow:
             c_d(hold["j02"], _lib.C.c_int), c_d(hold["w2"]),
             c_d(hold["U"]), c_d(hold["cU"]), c_d(hold["nU"]))
         h = _lib.C.c_void_p()
-        _lib.check(L.dnsb_couette_create(_lib.C.byref(desc), _lib.C.byref(h)))
+        if self.nranks:
+            _lib.check(L.dnsb_couette_create_slab(_lib.C.byref(desc), self.nranks, self.rank,
+                                                  _lib.C.byref(h)))
+        else:
+            _lib.check(L.dnsb_couette_create(_lib.C.byref(desc), _lib.C.byref(h)))
         self._ctx = h
         self._L = L
         if self.rhs_fp32:
@@ -86,16 +101,19 @@ class PlaneCouetteFlow:
         # Influence-matrix data (cartesian.py:575-801): given, or computed
         # once here -- on the GPU ("gpu") or on the host as the reference
         # does ("host").
+        # A slab rank computes (or takes) the operators of its kx modes only.
         if imm is None:
             if precompute == "gpu":
-                imm = precompute_imm_gpu(self.fourier.kx_global, self.fourier.kz_global,
+                imm = precompute_imm_gpu(kx_local, self.fourier.kz_global,
                                          self.p, self.dt, self.c, self.nu, self.D1, self.D2)
             elif precompute == "host":
-                imm = precompute_imm(self.ys, self.fourier.kx_global,
+                imm = precompute_imm(self.ys, kx_local,
                                      self.fourier.kz_global, self.p, self.dt,
                                      self.c, self.nu, self.D1, self.D2)
             else:
                 raise ValueError(f"precompute must be 'gpu' or 'host', got {precompute!r}")
+        elif self.nranks:
+            imm = {k: v[:, k0:k1] for k, v in imm.items()}
 
         def to_dev(a, dt_np, dt_t):
             if isinstance(a, torch.Tensor):
@@ -137,6 +155,26 @@ class PlaneCouetteFlow:
         out = self._new() if out is None else out
         _lib.check(self._L.dnsb_couette_rhs(
             self._ctx, self._check(state), self._check(out), _lib.stream_handle()))
+        return out
+
+    # -- slab decomposition (dnsjax_b200.slab) -----------------------------------
+    def slab_buffers(self):
+        """This rank's receive buffers (device pointers): the padded-z share
+        the z inverse fills, and the pass buffer the x pass fills."""
+        bx, bk = _lib.C.c_void_p(), _lib.C.c_void_p()
+        _lib.check(self._L.dnsb_couette_slab_buffers(self._ctx, _lib.C.byref(bx),
+                                                     _lib.C.byref(bk)))
+        return bx.value, bk.value
+
+    def slab_connect(self, bx, bk) -> None:
+        """Every rank's receive buffers, as this process addresses them."""
+        arr = _lib.C.c_void_p * len(bx)
+        _lib.check(self._L.dnsb_couette_slab_connect(self._ctx, arr(*bx), arr(*bk)))
+
+    def rhs_phase(self, state, out, phase: int):
+        _lib.check(self._L.dnsb_couette_rhs_phase(
+            self._ctx, self._check(state), self._check(out), int(phase),
+            _lib.stream_handle()))
         return out
 
     def imm_iteration(self, vel_n, vel_j, nl_n, nl_j, out=None, corr=None,

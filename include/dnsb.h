@@ -408,6 +408,53 @@ int dnsb_banded_solve(const double* ab, const int* ipiv, double* b,
                       int nmodes, int ny, int kl, int ku, int ncols,
                       int* status_dev, void* stream);
 
+/* ------------------------------------------------------------------ */
+/* Slab decomposition over several GPUs: the reference's multi-device  */
+/* scheme (fft.py:193-392, sharding.py:107-129; jax shard_map with a   */
+/* reshard between the column passes and the x pass).                  */
+/*   A slab context of rank r of nranks holds the kx modes             */
+/*   [r nx/2/nranks, (r+1) nx/2/nranks) of every spectral array (its   */
+/*   tensors are the reference's shards: (3, ny-1, nz-1, nx/2/nranks)   */
+/*   periodic, (3, nz-1, nx/2/nranks, ny) Couette).  desc is the whole  */
+/*   problem's; the context keeps its share of kx, ldt_1, ildt_2.      */
+/*   Between the column passes and the x pass the padded grid is       */
+/*   sharded on z (nz_p / nranks rows per rank).  The z inverse and    */
+/*   the x pass store every output straight into the receive buffer    */
+/*   of the rank that owns it (the exchange is fused into those        */
+/*   kernels): dnsb_*_slab_buffers gives this rank's two receive       */
+/*   buffers, dnsb_*_slab_connect takes every rank's, as this process  */
+/*   addresses them (dnsb_ipc_open of another process's handles, or    */
+/*   the buffers of other contexts on the same GPU).                   */
+/*   dnsb_*_rhs_phase(phase = 0, 1, 2) is the RHS: the caller makes     */
+/*   every rank's phase k complete before any rank starts phase k+1    */
+/*   (a collective on the stream, or the order of one stream).         */
+/*   The corrector's err_dev and dnsb_*_norm return this rank's share  */
+/*   of the squared norm: the caller sums the shares over the ranks    */
+/*   and takes the square root.  The mean mode (kx = 0) lives on rank  */
+/*   0.  Slab contexts run the FP64 two-stage passes (padded sizes in  */
+/*   {48, 72, 96, 192}, nx_p = 3 nx / 2, nx/2 and nz_p multiples of    */
+/*   nranks, nranks <= 8), step through the host loop (no step graph,  */
+/*   no autotune) and refuse dnsb_*_rhs.                               */
+/* ------------------------------------------------------------------ */
+int dnsb_periodic_create_slab(const dnsb_periodic_desc* desc, int nranks, int rank,
+                              dnsb_periodic** out);
+int dnsb_periodic_slab_buffers(dnsb_periodic* ctx, void** bx, void** bk);
+int dnsb_periodic_slab_connect(dnsb_periodic* ctx, void* const* bx, void* const* bk);
+int dnsb_periodic_rhs_phase(dnsb_periodic* ctx, const void* state, void* rhs, int phase,
+                            void* stream);
+int dnsb_couette_create_slab(const dnsb_couette_desc* desc, int nranks, int rank,
+                             dnsb_couette** out);
+int dnsb_couette_slab_buffers(dnsb_couette* ctx, void** bx, void** bk);
+int dnsb_couette_slab_connect(dnsb_couette* ctx, void* const* bx, void* const* bk);
+int dnsb_couette_rhs_phase(dnsb_couette* ctx, const void* state, void* rhs, int phase,
+                           void* stream);
+/* CUDA IPC of a device allocation made by this library (the slab      */
+/* receive buffers): a 64-byte handle; dnsb_ipc_open maps it with peer */
+/* access in another process, dnsb_ipc_close unmaps it.                */
+int dnsb_ipc_handle(const void* dev_ptr, void* handle);
+int dnsb_ipc_open(const void* handle, void** dev_ptr);
+int dnsb_ipc_close(void* dev_ptr);
+
 #ifdef __cplusplus
 }
 #endif
