@@ -1233,6 +1233,94 @@ def run_reference(a, w, rank, world):
     })
 
 
+def run_slab(a, w, rank, world):
+    """One trajectory over the slab decomposition (dnsjax_b200.slab): under
+    torchrun one rank per GPU (NCCL barriers between the RHS phases, CUDA IPC
+    receive buffers), or with --slab-emulate P every rank on this GPU.  The
+    host-driven reference loop; strong scaling (the whole job is one
+    trajectory)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from dnsjax_b200 import _lib, driver
+    from dnsjax_b200.replicas import max_over_ranks
+    from dnsjax_b200.slab import Slab, TorchComm
+
+    if w["system"] not in ("plane-couette", "kolmogorov"):
+        raise SystemExit("--parallel slab runs the plane-Couette and Kolmogorov workloads")
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    emulate = a.slab_emulate > 0
+    comm = None
+    if not emulate:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29533")
+        dist.init_process_group("nccl", rank=rank, world_size=world,
+                                timeout=datetime.timedelta(seconds=300))
+        comm = TorchComm()
+    nranks = a.slab_emulate if emulate else world
+    p = params_for(w, fp64=True)
+    if w["system"] == "plane-couette":
+        from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
+
+        def make(**k):
+            return PlaneCouetteFlow(p, **k)
+    else:
+        from dnsjax_b200.flows.monochromatic import TriplyPeriodicFlow
+
+        def make(**k):
+            return TriplyPeriodicFlow(p, ly=w["ly"], **k)
+    slab = Slab(make, nranks, comm=comm)
+    tol, mi = (w["tol"] if a.tol is None else a.tol), w["max_iter"]
+    u0 = slab.scatter(torch.as_tensor(initial_state(w, w["seed"]), device="cuda"))
+    st = slab.make_stepper()
+    states = [u.clone() for u in u0]
+    for _ in range(a.warmup):
+        states, c, e = driver.step(slab, st, states, tol, mi)
+
+    def barrier():
+        if comm is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    iters = []
+    ms = 0.0
+    n0 = _lib.launch_count()
+    for seg in segments(a.steps):
+        states = [u.clone() for u in u0]
+        barrier()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(seg):
+            states, c, e = driver.step(slab, st, states, tol, mi)
+            iters.append(c)
+        t1.record()
+        barrier()
+        ms += max_over_ranks(t0.elapsed_time(t1), dist if comm is not None else None, "cuda")
+    launches = _lib.launch_count() - n0
+    slab.close()
+    if comm is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    value = a.steps / (ms / 1e3)
+    emit({"metric": "steps/s of one trajectory (slab decomposition)", "value": value,
+          "unit": "steps/s", "n_gpus": 1 if emulate else world, "steps": a.steps,
+          "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
+          "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+          "data": "synthetic (seeded divergence-free spectral field)",
+          "config": dict(workload_config(a.workload, w, tol),
+                         parallelism=(f"slab over {nranks} ranks emulated on one GPU"
+                                      if emulate else f"slab over {world} GPUs")),
+          "diagnostics": {"driver": "host-driven reference loop",
+                          "corrector_iterations_per_step": sum(iters) / len(iters),
+                          "last_error": e},
+          "gpu_launches": launches})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1254,12 +1342,19 @@ def main():
                     help="keep the default pass variants instead of timing them first")
     ap.add_argument("--tol", type=float, default=None,
                     help="corrector tolerance of the timed run (default: the workload's)")
+    ap.add_argument("--parallel", default="replicas", choices=["replicas", "slab"],
+                    help="replicas: one independent trajectory per GPU; slab: one "
+                         "trajectory over every GPU (the reference's slab decomposition)")
+    ap.add_argument("--slab-emulate", type=int, default=0, metavar="P",
+                    help="with --parallel slab: P slab ranks emulated on this one GPU")
     a = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     w = WORKLOADS[a.workload]
     if a.impl == "reference":
         run_reference(a, w, rank, world)
+    elif a.parallel == "slab":
+        run_slab(a, w, rank, world)
     elif w["system"] == "ensemble":
         run_ensemble(a, w, rank, world)
     elif a.form.startswith("learned"):

@@ -194,3 +194,45 @@ def test_slab_refusals():
     # nz_p = 48 is not a multiple of 5 ranks; nx/2 = 16 is not either
     with pytest.raises(_lib.DnsbError, match="multiples of nranks"):
         PlaneCouetteFlow(p, slab=(5, 0))
+
+
+def _bench(args, env_extra=None):
+    import json
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    env = dict(os.environ)
+    env.update(env_extra or {})
+    r = subprocess.run([sys.executable, str(root / "bench.py"), *args], cwd=root, env=env,
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def test_bench_slab_emulated():
+    """bench.py --parallel slab with 4 ranks emulated on this GPU."""
+    out = _bench(["--parallel", "slab", "--slab-emulate", "4", "--workload", "couette64",
+                  "--steps", "3", "--warmup", "1"])
+    assert out["value"] > 0 and out["scaling"] == "strong"
+    assert "emulated" in out["config"]["parallelism"]
+    assert out["diagnostics"]["last_error"] <= 1e-10
+
+
+def test_bench_slab_one_process_nccl():
+    """bench.py --parallel slab as one torch.distributed rank (NCCL barriers,
+    the CUDA IPC export of the receive buffers)."""
+    import socket
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    out = _bench(["--parallel", "slab", "--workload", "couette64", "--steps", "3",
+                  "--warmup", "1"],
+                 {"RANK": "0", "WORLD_SIZE": "1", "LOCAL_RANK": "0",
+                  "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    assert out["value"] > 0 and out["n_gpus"] == 1
+    assert out["config"]["parallelism"] == "slab over 1 GPUs"
