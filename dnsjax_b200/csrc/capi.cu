@@ -540,6 +540,10 @@ struct dnsb_step_graph {
   double2 *P = nullptr, *Ra = nullptr, *Rb = nullptr;
   double* err = nullptr;  // [0] corrector error, [1] error of the last step
   int* ctl = nullptr;     // corrector iterations of the last step
+  // pinned host copies read by dnsb_step_graph_status (a copy into pageable
+  // memory would not be asynchronous and could queue behind other copies)
+  int* h_ctl = nullptr;
+  double* h_err = nullptr;
 };
 
 static void step_graph_free(dnsb_step_graph* g) {
@@ -547,6 +551,8 @@ static void step_graph_free(dnsb_step_graph* g) {
   void* ptrs[] = {g->P, g->Ra, g->Rb, g->err, g->ctl};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  if (g->h_ctl) cudaFreeHost(g->h_ctl);
+  if (g->h_err) cudaFreeHost(g->h_err);
   delete g;
 }
 
@@ -647,7 +653,8 @@ static dnsb_step_graph* new_step_graph(size_t n) {
   auto* g = new dnsb_step_graph();
   if (cudaMalloc(&g->P, n * sizeof(double2)) || cudaMalloc(&g->Ra, n * sizeof(double2)) ||
       cudaMalloc(&g->Rb, n * sizeof(double2)) || cudaMalloc(&g->err, 2 * sizeof(double)) ||
-      cudaMalloc(&g->ctl, sizeof(int))) {
+      cudaMalloc(&g->ctl, sizeof(int)) || cudaMallocHost(&g->h_ctl, sizeof(int)) ||
+      cudaMallocHost(&g->h_err, sizeof(double))) {
     step_graph_free(g);
     return nullptr;
   }
@@ -700,9 +707,11 @@ extern "C" int dnsb_step_graph_status(dnsb_step_graph* g, int* iters, double* er
                                       void* stream) {
   if (!g || !iters || !err) return fail(DNSB_ERR_ARG, "null argument");
   cudaStream_t st = as_stream(stream);
-  DNSB_CUDA(cudaMemcpyAsync(iters, g->ctl, sizeof(int), cudaMemcpyDeviceToHost, st));
-  DNSB_CUDA(cudaMemcpyAsync(err, g->err + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+  DNSB_CUDA(cudaMemcpyAsync(g->h_ctl, g->ctl, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DNSB_CUDA(cudaMemcpyAsync(g->h_err, g->err + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
   DNSB_CUDA(cudaStreamSynchronize(st));
+  *iters = *g->h_ctl;
+  *err = *g->h_err;
   g_launches.fetch_add(g->k_fixed + (long long)*iters * g->k_iter, std::memory_order_relaxed);
   return 0;
 }

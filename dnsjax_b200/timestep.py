@@ -87,6 +87,63 @@ class StepGraph:
 
         _lib.check(self._L.dnsb_step_graph_launch(self._h, _lib.stream_handle(stream)))
 
+    def run_host(self, host_in, host_out, chunks: int = 4):
+        """One step from pinned host memory to pinned host memory: the state
+        copied in, the step graph launched, the new state copied out, all
+        ordered on the current stream's timeline without host waits.
+
+        The copies move in ``chunks`` pieces on two copy streams.  When
+        ``host_in`` is the ``host_out`` of the previous call (a trajectory
+        that round-trips through the host every step), piece i of this
+        copy-in starts as soon as piece i of the previous copy-out has
+        landed, so the two directions of the link overlap instead of
+        running one after the other.  ``host_out`` is complete once
+        ``wait_host()`` has ordered the current stream after the copy-out
+        and that stream has been synchronized."""
+        import torch
+
+        main = torch.cuda.current_stream()
+        if getattr(self, "_copy_streams", None) is None:
+            self._copy_streams = (torch.cuda.Stream(), torch.cuda.Stream())
+            self._out_events, self._out_ptr = [], None
+        s_in, s_out = self._copy_streams
+        d = self.state.view(-1)
+        hi, ho = host_in.view(-1), host_out.view(-1)
+        n = d.numel()
+        bounds = [(n * i) // chunks for i in range(chunks + 1)]
+        # host_in still being written by the previous copy-out: piece by
+        # piece when the pieces match, else after all of it
+        chained = self._out_ptr == host_in.data_ptr()
+        per_piece = chained and len(self._out_events) == chunks
+        if chained and not per_piece:
+            s_in.wait_event(self._out_events[-1])
+        s_in.wait_stream(main)  # the previous step's graph no longer reads the state
+        for i in range(chunks):
+            a, b = bounds[i], bounds[i + 1]
+            if per_piece:
+                s_in.wait_event(self._out_events[i])
+            with torch.cuda.stream(s_in):
+                d[a:b].copy_(hi[a:b], non_blocking=True)
+        main.wait_stream(s_in)
+        self.launch(main)
+        s_out.wait_stream(main)
+        events = []
+        for i in range(chunks):
+            a, b = bounds[i], bounds[i + 1]
+            with torch.cuda.stream(s_out):
+                ho[a:b].copy_(d[a:b], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(s_out)
+            events.append(ev)
+        self._out_events, self._out_ptr = events, host_out.data_ptr()
+
+    def wait_host(self) -> None:
+        """Orders the current stream after the last run_host copy-out."""
+        import torch
+
+        if getattr(self, "_out_events", None):
+            torch.cuda.current_stream().wait_event(self._out_events[-1])
+
     def status(self, stream=None):
         from . import _lib
 

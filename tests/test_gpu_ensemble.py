@@ -82,6 +82,32 @@ def test_step_graph_equals_driver():
     assert c == 2 and torch.equal(s3_eager, s3)
 
 
+def test_step_graph_host_round_trip():
+    """run_host: the state copied in from pinned host memory and out again
+    every step, the copy-out of one step overlapping the copy-in of the
+    next, gives the device-resident steps bit for bit."""
+    import torch
+
+    f, u = member(32, 40.0, 5)
+    s_dev = torch.as_tensor(u, device="cuda")
+    g_dev = f.make_step_graph(s_dev)
+    f2, _ = member(32, 40.0, 5)
+    s_bound = torch.empty_like(s_dev)
+    g_host = f2.make_step_graph(s_bound)
+    a = torch.empty(s_dev.shape, dtype=s_dev.dtype, pin_memory=True)
+    b = torch.empty_like(a, pin_memory=True)
+    a.copy_(torch.as_tensor(u))
+    for chunks in (8, 3):
+        for _ in range(3):
+            g_dev.launch()
+            g_host.run_host(a, b, chunks=chunks)
+            assert g_host.status() == g_dev.status()
+            a, b = b, a
+    g_host.wait_host()
+    torch.cuda.synchronize()
+    assert torch.equal(a, s_dev.cpu())
+
+
 def test_graph_ensemble_equals_sequential():
     import torch
 
