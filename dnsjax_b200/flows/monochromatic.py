@@ -275,17 +275,34 @@ class TriplyPeriodicFlow:
 
     def get_stats(self, state) -> dict:
         """E, I, D, E' (monochromatic.py:433-505)."""
+        return self.stats_from_sums(self.stats_sums(state))
+
+    def stats_sums(self, state):
+        """The sums get_stats needs, over this flow's modes (a slab rank's
+        share; the shares add up over the ranks): sum k_metric |u|^2, the
+        enstrophy sum, and the forcing's projection on the forced modes this
+        flow holds."""
         _lib.check(self._L.dnsb_periodic_energy_sums(
             self._ctx, self._check(state), _lib.ptr(self._scratch),
             _lib.stream_handle()))
         norm2, ens_sum = (float(v) for v in self._scratch.tolist())
+        proj = 0.0
+        if self.system in monochromatic_systems:
+            k0, k1 = self.kx_range
+            c, iy, iz, ix = (np.array(i) for i in self.forced_modes)
+            mine = (ix >= k0) & (ix < k1)
+            if mine.any():
+                vals = state[(c[mine], iy[mine], iz[mine], ix[mine] - k0)].cpu().numpy()
+                proj = float(np.sum(np.conj(self.unit_force[mine] * self.force_amplitude)
+                                    * vals).real)
+        return norm2, ens_sum, proj
+
+    def stats_from_sums(self, sums) -> dict:
+        norm2, ens_sum, proj = sums
         ep = norm2 / 2
         re = self.re
         if self.system in monochromatic_systems:
-            idx = tuple(np.array(i) for i in self.forced_modes)
-            vals = state[idx].cpu().numpy()
-            inp = float(np.sum(np.conj(self.unit_force * self.force_amplitude)
-                               * vals).real) + self.input_lam
+            inp = proj + self.input_lam
             energy = ep - self.ekin_lam + inp / self.force_amplitude
         else:
             # The reference reads flow.unit_force here, which only forced

@@ -258,10 +258,17 @@ class PlaneCouetteFlow:
 
     def get_stats(self, state) -> dict:
         """plane_couette.py:591-613: E' = ||u||^2 / 2."""
+        return self.stats_from_sums(self.stats_sums(state))
+
+    def stats_sums(self, state):
+        """||u||^2 over this flow's modes (a slab rank's share)."""
         _lib.check(self._L.dnsb_couette_norm2(
             self._ctx, self._check(state), _lib.ptr(self._scratch),
             _lib.stream_handle()))
-        return {"E'": float(self._scratch[0].item()) / 2}
+        return (float(self._scratch[0].item()),)
+
+    def stats_from_sums(self, sums) -> dict:
+        return {"E'": sums[0] / 2}
 
     def check_status(self):
         """Raises if a bound operator holds an out-of-range pivot or an IMM

@@ -236,22 +236,14 @@ class Slab:
 
         return predict_and_correct, iterate_correction
 
-    def energy(self, states) -> float:
-        """E' = ||u||^2 / 2 over every rank (the reference's get_stats E')."""
+    def get_stats(self, states) -> dict:
+        """The flow's get_stats over every rank: each rank's sums
+        (stats_sums), added over the ranks, then the reference's formulas."""
         import torch
 
-        shares = []
-        for f, s in zip(self.flows, states):
-            sh = torch.empty(1, dtype=torch.float64, device=self.device)
-            if hasattr(f, "imm_iteration"):  # plane Couette: Simpson in y, / ly
-                _lib.check(f._L.dnsb_couette_norm2(f._ctx, f._check(s), _lib.ptr(sh),
-                                                   _lib.stream_handle()))
-            else:
-                _lib.check(f._L.dnsb_periodic_norm(f._ctx, f._check(s), _lib.ptr(sh),
-                                                   _lib.stream_handle()))
-            shares.append(sh)
-        acc = shares[0].clone()
-        for sh in shares[1:]:
-            acc += sh
-        self.comm.sum_(acc)
-        return float(acc.item()) / 2
+        tot = None
+        for f, st in zip(self.flows, states):
+            sh = torch.tensor(f.stats_sums(st), dtype=torch.float64, device=self.device)
+            tot = sh if tot is None else tot + sh
+        self.comm.sum_(tot)
+        return self.flows[0].stats_from_sums(tuple(float(v) for v in tot.tolist()))

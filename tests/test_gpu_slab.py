@@ -161,7 +161,11 @@ def test_periodic_slab_steps_32():
     _compare_runs(whole, slab, u0, 10)
 
 
-def test_slab_energy_matches_whole():
+def test_slab_stats_match_whole():
+    """get_stats over the ranks: each rank's sums added over the ranks give
+    the whole flow's E' (Couette) and E, I, D, E' (Kolmogorov, whose forced
+    modes live on the rank holding kx = 0)."""
+    from dnsjax_b200.flows.monochromatic import TriplyPeriodicFlow
     from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
     from dnsjax_b200.slab import Slab
 
@@ -170,8 +174,16 @@ def test_slab_energy_matches_whole():
     slab = Slab(lambda **k: PlaneCouetteFlow(p, **k), 4)
     u = dev(u0)
     e_w = whole.get_stats(u)["E'"]
-    e_s = slab.energy(slab.scatter(u))
+    e_s = slab.get_stats(slab.scatter(u))["E'"]
     assert abs(e_s - e_w) <= 1e-13 * e_w
+    p, u0 = periodic_case(32, 40.0, 0.01, 1e-2, 0)
+    whole = TriplyPeriodicFlow(p)
+    slab = Slab(lambda **k: TriplyPeriodicFlow(p, **k), 2)
+    u = dev(u0)
+    sw = whole.get_stats(u)
+    ss = slab.get_stats(slab.scatter(u))
+    for k in ("E", "I", "D", "E'"):
+        assert abs(ss[k] - sw[k]) <= 1e-12 * abs(sw[k]) + 1e-15, k
 
 
 def test_slab_refusals():
