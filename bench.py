@@ -1128,11 +1128,15 @@ def run_ensemble(a, w, rank, world):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(a.steps):
-        for x, h in zip(ens.states, host):  # the graphs are bound to these buffers
-            x.copy_(h, non_blocking=True)
-        ens.step()
-        for h, x in zip(host, ens.states):
-            h.copy_(x, non_blocking=True)
+        if ens.graphs is not None:
+            # member i's copy in, step graph, copy out on its own stream
+            ens.step_host(host, host)
+        else:
+            for x, h in zip(ens.states, host):
+                x.copy_(h, non_blocking=True)
+            ens.step()
+            for h, x in zip(host, ens.states):
+                h.copy_(x, non_blocking=True)
     e1.record()
     barrier()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")

@@ -2,11 +2,13 @@
 
 Three drivers share the per-trajectory semantics below:
 
-* ``worklist=True`` (periodic members, the fastest): one CUDA graph per
-  ensemble step in which every stage is one launch over all members'
-  blocks (``dnsb_ensemble_*``), with a device-controlled corrector loop
-  that runs while any member iterates;
-* ``graphs=True``: one step graph per member, each on its own stream;
+* ``worklist=True`` (periodic members): one CUDA graph per ensemble step
+  in which every stage is one launch over all members' blocks
+  (``dnsb_ensemble_*``), with a device-controlled corrector loop that runs
+  while any member iterates;
+* ``graphs=True``: one step graph per member, each on its own stream (the
+  fastest measured: members' stages overlap freely, and each member's pass
+  buffers stay in L2 between its passes);
 * neither: the host-driven lockstep loop.
 
 
@@ -120,6 +122,34 @@ class Ensemble:
         for g, st in zip(self.graphs, self.streams):
             st.wait_event(ready)
             g.launch(st)
+        for st in self.streams:
+            torch.cuda.current_stream().wait_stream(st)
+        torch.cuda.synchronize()
+        res = EnsembleStep()
+        for g, st in zip(self.graphs, self.streams):
+            it, e = g.status(st)
+            res.corrector_iterations.append(it)
+            res.errors.append(e)
+        return res
+
+    def step_host(self, host_in, host_out) -> EnsembleStep:
+        """One ensemble step from pinned host memory to pinned host memory
+        (``host_in[i]`` / ``host_out[i]``: member i's state, which may be the
+        same buffer): member i's copy-in, step graph and copy-out run in that
+        order on member i's stream, so the copies of some members overlap the
+        steps of others.  Needs the step-graph form (``graphs=True``)."""
+        import torch
+
+        if self.graphs is None:
+            raise ValueError("step_host runs the step-graph form (graphs=True)")
+        ready = torch.cuda.current_stream().record_event()
+        for g, st, x, hi, ho in zip(self.graphs, self.streams, self.states, host_in, host_out):
+            st.wait_event(ready)
+            with torch.cuda.stream(st):
+                x.copy_(hi, non_blocking=True)  # the graph is bound to x
+            g.launch(st)
+            with torch.cuda.stream(st):
+                ho.copy_(x, non_blocking=True)
         for st in self.streams:
             torch.cuda.current_stream().wait_stream(st)
         torch.cuda.synchronize()

@@ -129,6 +129,31 @@ def test_graph_ensemble_equals_sequential():
         assert torch.equal(s, ens.states[i]), i
 
 
+def test_graph_ensemble_host_round_trip():
+    """step_host (each member's state in from pinned host memory and out
+    again on its own stream) gives the device-resident steps bit for bit."""
+    import torch
+
+    from dnsjax_b200.ensemble import Ensemble
+
+    spec = [(32, 35.0, 0), (48, 60.0, 1)]
+    built = [member(*s) for s in spec]
+    dev = Ensemble([f for f, _ in built], [torch.as_tensor(u, device="cuda") for _, u in built],
+                   graphs=True)
+    built2 = [member(*s) for s in spec]
+    hst = Ensemble([f for f, _ in built2],
+                   [torch.empty(u.shape, dtype=torch.complex128, device="cuda") for _, u in built2],
+                   graphs=True)
+    host = [torch.as_tensor(u).pin_memory() for _, u in built2]
+    for _ in range(2):
+        a = dev.step()
+        b = hst.step_host(host, host)
+        assert a.corrector_iterations == b.corrector_iterations
+    torch.cuda.synchronize()
+    for x, h in zip(dev.states, host):
+        assert torch.equal(x.cpu(), h)
+
+
 def couette_member(n, re, seed):
     from dnsjax_b200 import initial
     from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
