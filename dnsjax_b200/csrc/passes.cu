@@ -435,7 +435,7 @@ x_pass_kernel(XPassArgs a) {
 }
 
 template <int ML, typename T = double, bool SLAB = false>
-__global__ void __launch_bounds__(kX2Threads) x_pass2_kernel(XPassArgs a);
+__global__ void __launch_bounds__(kX2Threads, 5) x_pass2_kernel(XPassArgs a);
 
 cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
   dim3 grid((a.nrows + kXRows - 1) / kXRows);
@@ -496,10 +496,16 @@ cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
 // thread (the 8 positions k + R1 i a radix-8 output holds are the inputs of
 // the forward radix-8 stage); forward radix-R1 stage; unpack and store.
 // ---------------------------------------------------------------------------
+// One work region holds, in turn, the staged half spectra, the inverse
+// stage-A output, the forward stage-1 output and the stage-C output: each
+// stage reads its input into registers, waits for every thread, then writes
+// its output over it.
 size_t x_pass2_smem(int M, int nkx) {
   const size_t S = (size_t)6 * nkx * kX2Rows, Y = (size_t)M * 2 * kX2Rows + M / 8;
   const size_t X = (size_t)M * 3 * kX2Rows + 4 * 8;  // + the stage-A skew
-  return sizeof(double2) * ((S > Y ? S : Y) + X + M);
+  size_t W = S > Y ? S : Y;
+  W = W > X ? W : X;
+  return sizeof(double2) * (W + M);
 }
 
 // T: the compute type and the element type of the pass buffer (double, or
@@ -515,14 +521,19 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
   // different bank groups on both the store and the next stage's load.
   constexpr int XS = 4;
   static_assert(R == 4, "the stage-A lane map assumes 4 rows");
-  constexpr int SZ_S = 6 * NKX * R, SZ_Y = M * CF + R1;
+  constexpr int SZ_S = 6 * NKX * R, SZ_Y = M * CF + R1, SZ_X = M * CI + XS * 8;
   constexpr int SZ_SY = SZ_S > SZ_Y ? SZ_S : SZ_Y;
+  constexpr int SZ_W = SZ_SY > SZ_X ? SZ_SY : SZ_X;
+  // every stage has at most one item per thread, so a thread can hold its
+  // item's inputs in registers across the barrier before the in-place write
+  static_assert(8 * CI <= kX2Threads && R1 * R <= kX2Threads && 8 * CF <= kX2Threads,
+                "one item per thread in every stage");
   extern __shared__ double2 sm_[];
   CT* sm = reinterpret_cast<CT*>(sm_);
   CT* S = sm;                 // staged half spectra, S[(f*NKX + k)*R + r]
-  CT* Y = sm;                 // forward stage-1 output [t][CF] (after S dies)
-  CT* X = sm + SZ_SY;         // inverse stage-A output [t][CI]; later [t][CF]
-  CT* tw = X + M * CI + XS * 8;
+  CT* X = sm;                 // inverse stage-A output [t][CI] (over S); later [t][CF]
+  CT* Y = sm;                 // forward stage-1 output [t][CF] (over X)
+  CT* tw = sm + SZ_W;
   const CT* gin = reinterpret_cast<const CT*>(a.in);
   const CT* gtw = reinterpret_cast<const CT*>(a.tw);
   CT* gout = reinterpret_cast<CT*>(a.out);
@@ -565,94 +576,115 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
   cp_async_wait_all();
   __syncthreads();
   // Stage A: inverse radix R1 (Ns = 1) on Z = A + iB, built on the fly.
-  for (int it = tid; it < 8 * CI; it += kX2Threads) {
+  {
     // lanes of a quarter warp: 4 rows x 2 parities of j, one field pair
+    const int it = tid;
+    const bool act = it < 8 * CI;
     const int r = it & 3, rest = it >> 3;
     const int pr = rest % 3, j = ((it >> 2) & 1) + 2 * (rest / 3);
     const int col = 3 * r + pr;
-    const CT* A = S + (2 * pr) * NKX * R + r;
-    const CT* B = S + (2 * pr + 1) * NKX * R + r;
     CT v[R1];
+    if (act) {
+      const CT* A = S + (2 * pr) * NKX * R + r;
+      const CT* B = S + (2 * pr + 1) * NKX * R + r;
 #pragma unroll
-    for (int i = 0; i < R1; ++i) {
-      const int t = j + 8 * i;
-      CT z = cmake<CT>(0, 0);
-      if (t == 0) {
-        z = cmake<CT>(A[0].x, B[0].x);
-      } else if (t < NKX) {
-        const CT av = A[t * R], bv = B[t * R];
-        z = cmake<CT>(av.x - bv.y, av.y + bv.x);
-      } else if (M - t < NKX) {
-        const CT av = A[(M - t) * R], bv = B[(M - t) * R];
-        z = cmake<CT>(av.x + bv.y, -av.y + bv.x);
+      for (int i = 0; i < R1; ++i) {
+        const int t = j + 8 * i;
+        CT z = cmake<CT>(0, 0);
+        if (t == 0) {
+          z = cmake<CT>(A[0].x, B[0].x);
+        } else if (t < NKX) {
+          const CT av = A[t * R], bv = B[t * R];
+          z = cmake<CT>(av.x - bv.y, av.y + bv.x);
+        } else if (M - t < NKX) {
+          const CT av = A[(M - t) * R], bv = B[(M - t) * R];
+          z = cmake<CT>(av.x + bv.y, -av.y + bv.x);
+        }
+        v[i] = z;
       }
-      v[i] = z;
     }
-    dft_3p<R1, 1, CT, true>(v, tw, 8);
+    __syncthreads();  // S read by every thread before X is written over it
+    if (act) {
+      dft_3p<R1, 1, CT, true>(v, tw, 8);
 #pragma unroll
-    for (int i = 0; i < R1; ++i) X[(j * R1 + i) * CI + col + XS * j] = v[i];
+      for (int i = 0; i < R1; ++i) X[(j * R1 + i) * CI + col + XS * j] = v[i];
+    }
   }
   __syncthreads();
   // Stage B: inverse radix 8 (Ns = R1) -> physical values at t = k + R1 i;
   // rotational product there; forward radix-8 stage (Ns = 1) on the same t.
-  for (int it = tid; it < R1 * R; it += kX2Threads) {
+  {
+    const int it = tid;
+    const bool act = it < R1 * R;
     const int r = it % R, k = it / R;
-    CT z[3][8];
-#pragma unroll
-    for (int pr = 0; pr < 3; ++pr) {
-#pragma unroll
-      for (int i = 0; i < 8; ++i) z[pr][i] = X[(k + R1 * i) * CI + 3 * r + pr + XS * i];
-#pragma unroll
-      for (int i = 1; i < 8; ++i) {
-        CT w = tw[i * k];
-        w.y = -w.y;
-        z[pr][i] = cmul(z[pr][i], w);
-      }
-      dft8(z[pr], 1);
-    }
     CT F0[8], F1[8];
-    const bool live = r < nr;
-    const int y = s_y[r];
-    const int ny = a.ny_grid;
-    const RT U0 = live ? (RT)a.U[y] : RT(0), U1 = live ? (RT)a.U[ny + y] : RT(0),
-            U2 = live ? (RT)a.U[2 * ny + y] : RT(0);
-    const RT C0 = live ? (RT)a.cU[y] : RT(0), C1 = live ? (RT)a.cU[ny + y] : RT(0),
-            C2 = live ? (RT)a.cU[2 * ny + y] : RT(0);
-    const RT N0 = live ? (RT)a.nU[y] : RT(0), N1 = live ? (RT)a.nU[ny + y] : RT(0),
-            N2 = live ? (RT)a.nU[2 * ny + y] : RT(0);
+    if (act) {
+      CT z[3][8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const RT u0 = z[0][i].x, u1 = z[0][i].y, u2 = z[1][i].x;
-      const RT w0 = z[1][i].y, w1 = z[2][i].x, w2 = z[2][i].y;
-      const RT n0 = u1 * w2 - u2 * w1;
-      const RT n1 = u2 * w0 - u0 * w2;
-      const RT n2 = u0 * w1 - u1 * w0;
-      const RT b0 = (u1 * C2 - u2 * C1) + (U1 * w2 - U2 * w1) + N0;
-      const RT b1 = (u2 * C0 - u0 * C2) + (U2 * w0 - U0 * w2) + N1;
-      const RT b2 = (u0 * C1 - u1 * C0) + (U0 * w1 - U1 * w0) + N2;
-      F0[i] = live ? cmake<CT>(n0 + b0, n1 + b1) : cmake<CT>(0, 0);
-      F1[i] = live ? cmake<CT>(n2 + b2, 0) : cmake<CT>(0, 0);
+      for (int pr = 0; pr < 3; ++pr) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) z[pr][i] = X[(k + R1 * i) * CI + 3 * r + pr + XS * i];
+#pragma unroll
+        for (int i = 1; i < 8; ++i) {
+          CT w = tw[i * k];
+          w.y = -w.y;
+          z[pr][i] = cmul(z[pr][i], w);
+        }
+        dft8(z[pr], 1);
+      }
+      const bool live = r < nr;
+      const int y = s_y[r];
+      const int ny = a.ny_grid;
+      const RT U0 = live ? (RT)a.U[y] : RT(0), U1 = live ? (RT)a.U[ny + y] : RT(0),
+              U2 = live ? (RT)a.U[2 * ny + y] : RT(0);
+      const RT C0 = live ? (RT)a.cU[y] : RT(0), C1 = live ? (RT)a.cU[ny + y] : RT(0),
+              C2 = live ? (RT)a.cU[2 * ny + y] : RT(0);
+      const RT N0 = live ? (RT)a.nU[y] : RT(0), N1 = live ? (RT)a.nU[ny + y] : RT(0),
+              N2 = live ? (RT)a.nU[2 * ny + y] : RT(0);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const RT u0 = z[0][i].x, u1 = z[0][i].y, u2 = z[1][i].x;
+        const RT w0 = z[1][i].y, w1 = z[2][i].x, w2 = z[2][i].y;
+        const RT n0 = u1 * w2 - u2 * w1;
+        const RT n1 = u2 * w0 - u0 * w2;
+        const RT n2 = u0 * w1 - u1 * w0;
+        const RT b0 = (u1 * C2 - u2 * C1) + (U1 * w2 - U2 * w1) + N0;
+        const RT b1 = (u2 * C0 - u0 * C2) + (U2 * w0 - U0 * w2) + N1;
+        const RT b2 = (u0 * C1 - u1 * C0) + (U0 * w1 - U1 * w0) + N2;
+        F0[i] = live ? cmake<CT>(n0 + b0, n1 + b1) : cmake<CT>(0, 0);
+        F1[i] = live ? cmake<CT>(n2 + b2, 0) : cmake<CT>(0, 0);
+      }
+      dft8(F0, -1);
+      dft8(F1, -1);
     }
-    dft8(F0, -1);
-    dft8(F1, -1);
+    __syncthreads();  // X read by every thread before Y is written over it
+    if (act) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      Y[(k * 8 + i) * CF + 2 * r + k] = F0[i];
-      Y[(k * 8 + i) * CF + 2 * r + 1 + k] = F1[i];
+      for (int i = 0; i < 8; ++i) {
+        Y[(k * 8 + i) * CF + 2 * r + k] = F0[i];
+        Y[(k * 8 + i) * CF + 2 * r + 1 + k] = F1[i];
+      }
     }
   }
   __syncthreads();
   // Stage C: forward radix R1 (Ns = 8), natural order into X[t][CF].
-  for (int it = tid; it < 8 * CF; it += kX2Threads) {
+  {
+    const int it = tid;
+    const bool act = it < 8 * CF;
     const int col = it % CF, j = it / CF;
     CT v[R1];
+    if (act) {
 #pragma unroll
-    for (int i = 0; i < R1; ++i) v[i] = Y[(j + 8 * i) * CF + col + i];
+      for (int i = 0; i < R1; ++i) v[i] = Y[(j + 8 * i) * CF + col + i];
+    }
+    __syncthreads();  // Y read by every thread before X is written over it
+    if (act) {
 #pragma unroll
-    for (int i = 1; i < R1; ++i) v[i] = cmul(v[i], tw[i * j]);
-    dft_3p<R1, -1, CT, true>(v, tw, 8);
+      for (int i = 1; i < R1; ++i) v[i] = cmul(v[i], tw[i * j]);
+      dft_3p<R1, -1, CT, true>(v, tw, 8);
 #pragma unroll
-    for (int i = 0; i < R1; ++i) X[(j + 8 * i) * CF + col] = v[i];
+      for (int i = 0; i < R1; ++i) X[(j + 8 * i) * CF + col] = v[i];
+    }
   }
   __syncthreads();
   // Unpack the real-field spectra, truncate to NKX, scale 1/M, store.
@@ -689,7 +721,7 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
 }
 
 template <int ML, typename T, bool SLAB>
-__global__ void __launch_bounds__(kX2Threads)
+__global__ void __launch_bounds__(kX2Threads, 5)
 x_pass2_kernel(XPassArgs a) {
   x_pass2_body<ML, T, SLAB>(a, blockIdx.x);
 }

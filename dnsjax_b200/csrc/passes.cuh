@@ -16,7 +16,7 @@ constexpr int kTile = 8;     // columns per CTA in the column passes
 constexpr int kXRows = 4;    // physical rows per CTA in the x pass
 constexpr int kPassThreads = 256;
 constexpr int kX2Rows = 4;       // physical rows per CTA in the two-stage x pass
-constexpr int kX2Threads = 128;
+constexpr int kX2Threads = 96;   // one item per thread in every stage
 size_t x_pass2_smem(int M, int nkx);
 
 // Slab exchange (the reference's slab scheme over several GPUs): a pass
