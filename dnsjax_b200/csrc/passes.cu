@@ -248,6 +248,15 @@ col_pass2_kernel(ColPassArgs a) {
   col_pass2_body<ML, SIGN, T, OUT32, CURL, SLAB>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
+// The FP64 pass held to 128 registers, so 4 CTAs fit per SM instead of 3
+// (ColPassArgs::occ4: the periodic flows' column passes, measured faster so;
+// the Couette z forward measured slower).
+template <int ML, int SIGN, bool CURL>
+__global__ void __launch_bounds__(kC2Threads, 4)
+col_pass2_occ4_kernel(ColPassArgs a) {
+  col_pass2_body<ML, SIGN, double, false, CURL, false>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
                             cudaStream_t st) {
   const int L = a.plan.L;
@@ -271,6 +280,12 @@ cudaError_t launch_col_pass(const ColPassArgs& a, int nfields, int nO,
       col_pass2_kernel<LL, -1, fcomp><<<g2, kC2Threads, sm2, st>>>(a);                  \
     else if (a.curl && a.fp32)                                                          \
       col_pass2_kernel<LL, 1, float, true, true><<<g2, kC2Threads, sm2, st>>>(a);       \
+    else if (a.occ4 && !a.fp32 && a.curl)                                               \
+      col_pass2_occ4_kernel<LL, 1, true><<<g2, kC2Threads, sm2, st>>>(a);               \
+    else if (a.occ4 && !a.fp32 && a.inverse)                                            \
+      col_pass2_occ4_kernel<LL, 1, false><<<g2, kC2Threads, sm2, st>>>(a);              \
+    else if (a.occ4 && !a.fp32)                                                         \
+      col_pass2_occ4_kernel<LL, -1, false><<<g2, kC2Threads, sm2, st>>>(a);             \
     else if (a.curl)                                                                    \
       col_pass2_kernel<LL, 1, double, false, true><<<g2, kC2Threads, sm2, st>>>(a);     \
     else if (a.fp32 && a.inverse)                                                       \
@@ -1560,6 +1575,13 @@ cudaError_t set_pass_attributes(int max_smem) {
                        (const void*)col_pass2_kernel<72, 1>, (const void*)col_pass2_kernel<72, -1>,
                        (const void*)col_pass2_kernel<96, 1>, (const void*)col_pass2_kernel<96, -1>,
                        (const void*)col_pass2_kernel<192, 1>, (const void*)col_pass2_kernel<192, -1>,
+#define DNSB_OCC4_PASSES(L)                                                         \
+  (const void*)col_pass2_occ4_kernel<L, 1, true>,                                   \
+      (const void*)col_pass2_occ4_kernel<L, 1, false>,                              \
+      (const void*)col_pass2_occ4_kernel<L, -1, false>
+                       DNSB_OCC4_PASSES(48), DNSB_OCC4_PASSES(72), DNSB_OCC4_PASSES(96),
+                       DNSB_OCC4_PASSES(192),
+#undef DNSB_OCC4_PASSES
 #define DNSB_F32_PASSES(L)                                                          \
   (const void*)yinv_kernel<L, float>, (const void*)yfwd_kernel<L, float>,           \
       (const void*)col_pass2_kernel<L, 1, float, true>,                             \

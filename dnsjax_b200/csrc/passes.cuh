@@ -56,6 +56,7 @@ struct ColPassArgs {
   const double* kx;
   const double* ky;
   const double* kz;
+  int occ4;  // FP64 two-stage pass held to 4 CTAs per SM (128 registers)
   // Slab store (inverse, FP64 two-stage pass): position t goes to
   // slab.buf[t / blk] + f*fs + o*out_os + (t % blk)*ts + off + i, instead of
   // out + f*out_fs + o*out_os + t*out_ts + i.
