@@ -30,8 +30,19 @@ __device__ __forceinline__ double block_sum(double v) {
 
 __device__ __forceinline__ void finalize_body(const double* partials, int n, double* out,
                                               double scale, int do_sqrt) {
+  // each thread adds its partials in index order; the loads of eight at a
+  // time are issued together (the sum is the plain loop's, bit for bit)
   double s = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s += partials[i];
+  const int bd = blockDim.x;
+  int i = threadIdx.x;
+  for (; i + 7 * bd < n; i += 8 * bd) {
+    double v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = partials[i + k * bd];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += v[k];
+  }
+  for (; i < n; i += bd) s += partials[i];
   s = block_sum(s);
   if (threadIdx.x == 0) {
     s *= scale;
