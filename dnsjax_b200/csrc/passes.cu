@@ -450,7 +450,8 @@ x_pass_kernel(XPassArgs a) {
 }
 
 template <int ML, typename T = double, bool SLAB = false>
-__global__ void __launch_bounds__(kX2Threads, 5) x_pass2_kernel(XPassArgs a);
+__global__ void __launch_bounds__(kX2Threads, std::is_same<T, float>::value ? 8 : 5)
+x_pass2_kernel(XPassArgs a);
 
 cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
   dim3 grid((a.nrows + kXRows - 1) / kXRows);
@@ -736,7 +737,7 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
 }
 
 template <int ML, typename T, bool SLAB>
-__global__ void __launch_bounds__(kX2Threads, 5)
+__global__ void __launch_bounds__(kX2Threads, std::is_same<T, float>::value ? 8 : 5)
 x_pass2_kernel(XPassArgs a) {
   x_pass2_body<ML, T, SLAB>(a, blockIdx.x);
 }
