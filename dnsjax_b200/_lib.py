@@ -78,6 +78,14 @@ SIGNATURES = {
     "dnsb_step_graph_launch": (c_int, [c_void_p, c_void_p]),
     "dnsb_step_graph_status": (c_int, [c_void_p, P_int, P_double, c_void_p]),
     "dnsb_step_graph_destroy": (c_int, [c_void_p]),
+    "dnsb_couette_mixed_graph_create": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p,
+                                                c_double, c_int, c_int, c_double, c_double,
+                                                c_int, C.POINTER(c_void_p)]),
+    "dnsb_mixed_graph_predict": (c_int, [c_void_p, c_void_p]),
+    "dnsb_mixed_graph_correct": (c_int, [c_void_p, c_void_p]),
+    "dnsb_mixed_graph_status": (c_int, [c_void_p, P_int, P_double, P_double, P_int, P_int,
+                                        c_void_p]),
+    "dnsb_mixed_graph_destroy": (c_int, [c_void_p]),
     "dnsb_periodic_spec_to_phys": (c_int, [c_void_p] * 4),
     "dnsb_periodic_phys_to_spec": (c_int, [c_void_p] * 4),
     "dnsb_couette_create": (c_int, [C.POINTER(CouetteDesc), C.POINTER(c_void_p)]),

@@ -560,6 +560,33 @@ static void step_graph_free(dnsb_step_graph* g) {
   delete g;
 }
 
+// Adds a conditional node of `type` to graph `gr` after the work captured so
+// far on `st` (which captures into `gr`), makes it the stream's dependency,
+// and returns the node's body graph (nullptr and rc set on failure).
+static cudaGraph_t add_cond_node(cudaStream_t st, cudaGraph_t gr, cudaGraphConditionalHandle hd,
+                                 cudaGraphConditionalNodeType type, int& rc) {
+  if (rc) return nullptr;
+  auto ck = [&](cudaError_t e, const char* what) {
+    if (e != cudaSuccess && !rc)
+      rc = fail(DNSB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  };
+  cudaStreamCaptureStatus cst;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  ck(cudaStreamGetCaptureInfo(st, &cst, nullptr, nullptr, &deps, &ndeps), "capture info");
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = hd;
+  cp.conditional.type = type;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node = nullptr;
+  if (!rc) ck(cudaGraphAddNode(&node, gr, deps, ndeps, &cp), "conditional node");
+  if (!rc)
+    ck(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies),
+       "capture dependencies");
+  return rc ? nullptr : cp.conditional.phGraph_out[0];
+}
+
 // Captures prologue (predictor and first correction, error into g->err),
 // the corrector iterations `body(stream, 0)` (A) and `body(stream, 1)` (B)
 // inside the WHILE node, and `epilogue`, with the control kernel after the
@@ -577,27 +604,9 @@ static int build_step_graph(dnsb_step_graph* g, double tol, int max_iter,
     if (e != cudaSuccess && !rc)
       rc = fail(DNSB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
   };
-  // Adds a conditional node of `type` after the work captured so far on
-  // `st` (in graph `gr`), makes it the stream's dependency, and returns its
-  // body graph.
   auto add_cond = [&](cudaStream_t st, cudaGraph_t gr, cudaGraphConditionalHandle hd,
-                      cudaGraphConditionalNodeType type) -> cudaGraph_t {
-    if (rc) return nullptr;
-    cudaStreamCaptureStatus cst;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    ck(cudaStreamGetCaptureInfo(st, &cst, nullptr, nullptr, &deps, &ndeps), "capture info");
-    cudaGraphNodeParams cp = {};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = hd;
-    cp.conditional.type = type;
-    cp.conditional.size = 1;
-    cudaGraphNode_t node = nullptr;
-    if (!rc) ck(cudaGraphAddNode(&node, gr, deps, ndeps, &cp), "conditional node");
-    if (!rc)
-      ck(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies),
-         "capture dependencies");
-    return rc ? nullptr : cp.conditional.phGraph_out[0];
+                      cudaGraphConditionalNodeType type) {
+    return add_cond_node(st, gr, hd, type, rc);
   };
   cudaGraph_t graph = nullptr;
   ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
@@ -1011,23 +1020,8 @@ extern "C" int dnsb_ensemble_create(dnsb_periodic* const* ctxs, void* const* sta
                                    cudaGetErrorString(r));
   };
   auto add_cond = [&](cudaStream_t st, cudaGraph_t gr, cudaGraphConditionalHandle hd,
-                      cudaGraphConditionalNodeType type) -> cudaGraph_t {
-    if (rc) return nullptr;
-    cudaStreamCaptureStatus cst;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    ck(cudaStreamGetCaptureInfo(st, &cst, nullptr, nullptr, &deps, &ndeps), "capture info");
-    cudaGraphNodeParams cp = {};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = hd;
-    cp.conditional.type = type;
-    cp.conditional.size = 1;
-    cudaGraphNode_t node = nullptr;
-    if (!rc) ck(cudaGraphAddNode(&node, gr, deps, ndeps, &cp), "conditional node");
-    if (!rc)
-      ck(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies),
-         "capture dependencies");
-    return rc ? nullptr : cp.conditional.phGraph_out[0];
+                      cudaGraphConditionalNodeType type) {
+    return add_cond_node(st, gr, hd, type, rc);
   };
   cudaGraph_t graph = nullptr;
   ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
@@ -1597,15 +1591,19 @@ extern "C" int dnsb_couette_rhs(dnsb_couette* p, const void* state, void* rhs,
   return couette_rhs_impl(p, state, rhs, 7u, as_stream(stream));
 }
 
+// The FP32 passes are compiled for padded lengths 48, 72, 96 and 192 with
+// 3/2 oversampling in x.
+static bool couette_fp32_sizes(const dnsb_couette* p) {
+  auto fixed = [](int L) { return L == 48 || L == 72 || L == 96 || L == 192; };
+  return fixed(p->Mz) && fixed(p->Mx) && 3 * p->NKX == p->Mx;
+}
+
 extern "C" int dnsb_couette_set_rhs_precision(dnsb_couette* p, int fp32) {
   if (!p) return fail(DNSB_ERR_ARG, "null argument");
   if (fp32 && p->slab.nranks) return fail(DNSB_ERR_ARG, "slab contexts run the FP64 passes");
-  if (fp32) {
-    auto fixed = [](int L) { return L == 48 || L == 72 || L == 96 || L == 192; };
-    if (!fixed(p->Mz) || !fixed(p->Mx) || 3 * p->NKX != p->Mx)
-      return fail(DNSB_ERR_ARG,
-                  "FP32 RHS passes need padded sizes in {48, 72, 96, 192} with nx_p = 3 nx / 2");
-  }
+  if (fp32 && !couette_fp32_sizes(p))
+    return fail(DNSB_ERR_ARG,
+                "FP32 RHS passes need padded sizes in {48, 72, 96, 192} with nx_p = 3 nx / 2");
   p->rhs_fp32 = fp32 < 0 ? 0 : (fp32 > 2 ? 2 : fp32);
   return 0;
 }
@@ -1782,6 +1780,284 @@ extern "C" int dnsb_couette_step_graph_create(dnsb_couette* p, void* state, doub
     return rc;
   }
   *out = g;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// The restarted, mixed-precision corrector step as two CUDA graphs (no
+// counterpart in the reference: the device form of the learned corrector
+// step of dnsjax_b200.learned, whose corrector is the reference's
+// iterate_correction, plane_couette.py:522-540, started from a guessed
+// iterate).
+//   "predict": the RHS of u^n (into Rb) and the predictor (the IMM
+//     iteration with (u^n, u^n, N^n, N^n)) into `up`, copied into the
+//     iterate `cur`.  Between the two launches the caller may overwrite
+//     `cur` with a guessed start.
+//   "correct": the first correction from `cur` (restart != 0: the start's
+//     own RHS in both RHS slots; else N^n as the previous RHS), then the
+//     corrector iterations in a WHILE node while error > tol and iterations
+//     < max_iter, as in build_step_graph, and the converged iterate copied
+//     into `state`.
+// With mixed != 0 the RHS runs at precision mode `mixed` (1 FP32, 2 FP32
+// with compensated butterflies) until the error after a correction is at or
+// below switch_tol, or the iteration stops contracting (error > stall x the
+// previous error); from then on it runs in FP64 for the rest of the step.
+// The control kernel makes that choice on the device after every
+// correction, and each iteration selects one of two IF nodes holding the RHS
+// passes captured at each precision.
+// ---------------------------------------------------------------------------
+namespace dnsb {
+struct MixedCtl {
+  int it;         // corrector iterations of the step so far
+  int fp32;       // the next RHS runs at the reduced precision
+  int n32, n64;   // RHS evaluations of the step at reduced precision / FP64
+  double e_prev;  // error of the previous correction (+inf before the first)
+  double first;   // error of the first correction
+  double err;     // error of the latest correction
+};
+
+__global__ void mixed_init_kernel(MixedCtl* c, int mixed) {
+  c->it = 0;
+  c->fp32 = mixed ? 1 : 0;
+  c->n32 = mixed ? 2 : 0;  // the RHS of u^n and of the start
+  c->n64 = mixed ? 0 : 2;
+  c->e_prev = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+  c->first = 0.0;
+  c->err = 0.0;
+}
+
+// After a correction: count the iteration (first: the start's correction),
+// keep the errors, choose the next RHS's precision, and set the loop's
+// condition (and, after iteration A, the IF node's) to "iterate again".
+__global__ void mixed_ctl_kernel(cudaGraphConditionalHandle h, cudaGraphConditionalHandle h_if,
+                                 int set_if, const double* err, MixedCtl* c, double tol,
+                                 int max_iter, double switch_tol, double stall, int first) {
+  const int it = first ? 0 : c->it + 1;
+  const double e = err[0];
+  const unsigned cont = (e > tol && it < max_iter) ? 1u : 0u;
+  if (first) c->first = e;
+  if (c->fp32 && (e <= switch_tol || e > stall * c->e_prev)) c->fp32 = 0;
+  c->e_prev = e;
+  c->it = it;
+  c->err = e;
+  cudaGraphSetConditional(h, cont);
+  if (set_if) cudaGraphSetConditional(h_if, cont);
+}
+
+// Top of a corrector iteration of the mixed form: run the RHS of the chosen
+// precision (one of the two IF nodes) and count it.
+__global__ void mixed_prec_kernel(cudaGraphConditionalHandle h32, cudaGraphConditionalHandle h64,
+                                  MixedCtl* c) {
+  const int f = c->fp32;
+  if (f)
+    c->n32 += 1;
+  else
+    c->n64 += 1;
+  cudaGraphSetConditional(h32, f ? 1u : 0u);
+  cudaGraphSetConditional(h64, f ? 0u : 1u);
+}
+}  // namespace dnsb
+
+struct dnsb_mixed_graph {
+  cudaGraphExec_t pre = nullptr, post = nullptr;
+  long long k_pre = 0, k_post = 0, k_iter = 0;  // kernels per graph / per iteration
+  int mixed = 0;
+  double2 *Ra = nullptr, *Rb = nullptr;
+  double* err = nullptr;
+  dnsb::MixedCtl* ctl = nullptr;
+  dnsb::MixedCtl* h_ctl = nullptr;  // pinned copy read by dnsb_mixed_graph_status
+};
+
+static void mixed_graph_free(dnsb_mixed_graph* g) {
+  if (g->pre) cudaGraphExecDestroy(g->pre);
+  if (g->post) cudaGraphExecDestroy(g->post);
+  void* ptrs[] = {g->Ra, g->Rb, g->err, g->ctl};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  if (g->h_ctl) cudaFreeHost(g->h_ctl);
+  delete g;
+}
+
+extern "C" int dnsb_couette_mixed_graph_create(dnsb_couette* p, void* state, void* up,
+                                               void* cur, double tol, int max_iter, int mixed,
+                                               double switch_tol, double stall, int restart,
+                                               dnsb_mixed_graph** out) {
+  if (!p || !state || !up || !cur || !out) return fail(DNSB_ERR_ARG, "null argument");
+  if (state == up || state == cur || up == cur)
+    return fail(DNSB_ERR_ARG, "state, up and cur must be distinct buffers");
+  if (p->slab.nranks) return fail(DNSB_ERR_ARG, "slab contexts step through the host loop");
+  if (!p->bound) return fail(DNSB_ERR_ARG, "IMM operators not bound");
+  if (mixed < 0 || mixed > 2) return fail(DNSB_ERR_ARG, "mixed must be 0, 1 or 2");
+  if (mixed && !couette_fp32_sizes(p))
+    return fail(DNSB_ERR_ARG,
+                "FP32 RHS passes need padded sizes in {48, 72, 96, 192} with nx_p = 3 nx / 2");
+  const size_t n = 3 * (size_t)p->NM * p->Ny;
+  auto* g = new dnsb_mixed_graph();
+  g->mixed = mixed;
+  if (cudaMalloc(&g->Ra, n * sizeof(double2)) || cudaMalloc(&g->Rb, n * sizeof(double2)) ||
+      cudaMalloc(&g->err, sizeof(double)) || cudaMalloc(&g->ctl, sizeof(dnsb::MixedCtl)) ||
+      cudaMallocHost(&g->h_ctl, sizeof(dnsb::MixedCtl))) {
+    mixed_graph_free(g);
+    return fail(DNSB_ERR_CUDA, "mixed step graph allocation failed");
+  }
+  const int keep = p->rhs_fp32;
+  // the RHS passes of one precision (the context's own setting is restored)
+  auto rhs = [&](const void* in, void* o, int prec, cudaStream_t s) {
+    p->rhs_fp32 = prec;
+    const int r = couette_rhs_impl(p, in, o, 7u, s);
+    p->rhs_fp32 = keep;
+    return r;
+  };
+  cudaStream_t s = nullptr, sb = nullptr, si = nullptr, sp = nullptr;
+  cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  cudaStreamCreateWithFlags(&sb, cudaStreamNonBlocking);
+  cudaStreamCreateWithFlags(&si, cudaStreamNonBlocking);
+  cudaStreamCreateWithFlags(&sp, cudaStreamNonBlocking);
+  int rc = 0;
+  auto ck = [&](cudaError_t e, const char* what) {
+    if (e != cudaSuccess && !rc)
+      rc = fail(DNSB_ERR_CUDA, std::string("mixed step graph: ") + what + ": " +
+                                   cudaGetErrorString(e));
+  };
+  const long long c0 = g_launches.load();
+
+  // -- predict
+  cudaGraph_t done = nullptr;
+  ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+  dnsb::mixed_init_kernel<<<1, 1, 0, s>>>(g->ctl, mixed);
+  ck(cudaGetLastError(), "init kernel");
+  if (!rc) rc = rhs(state, g->Rb, mixed, s);
+  if (!rc) rc = dnsb_couette_imm(p, state, state, g->Rb, g->Rb, up, nullptr, nullptr, s);
+  ck(cudaMemcpyAsync(cur, up, n * sizeof(double2), cudaMemcpyDeviceToDevice, s), "copy");
+  g->k_pre = g_launches.load() - c0 + 1;  // + the init kernel
+  ck(cudaStreamEndCapture(s, &done), "end capture");  // always end the capture
+  if (!rc) ck(cudaGraphInstantiate(&g->pre, done, 0), "instantiate");
+  if (done) cudaGraphDestroy(done);
+  done = nullptr;
+
+  // -- correct
+  // one corrector iteration captured on `st` into graph `gr`: the RHS of
+  // `cur` into nx (both precisions behind IF nodes in the mixed form), then
+  // the correction with rhs_prev pv
+  long long k_rhs = 0, k_imm = 0;
+  auto iteration = [&](cudaStream_t st, cudaGraph_t gr, double2* nx, double2* pv) {
+    if (rc) return;
+    if (mixed) {
+      cudaGraphConditionalHandle h32 = 0, h64 = 0;
+      ck(cudaGraphConditionalHandleCreate(&h32, gr, 0, 0), "conditional handle");
+      ck(cudaGraphConditionalHandleCreate(&h64, gr, 0, 0), "conditional handle");
+      dnsb::mixed_prec_kernel<<<1, 1, 0, st>>>(h32, h64, g->ctl);
+      ck(cudaGetLastError(), "precision kernel");
+      for (int f = 0; f < 2 && !rc; ++f) {
+        cudaGraph_t ib = add_cond_node(st, gr, f ? h64 : h32, cudaGraphCondTypeIf, rc);
+        if (rc) break;
+        ck(cudaStreamBeginCaptureToGraph(sp, ib, nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal), "RHS capture");
+        const long long a = g_launches.load();
+        if (!rc) rc = rhs(cur, nx, f ? 0 : mixed, sp);
+        k_rhs = g_launches.load() - a;
+        cudaGraph_t o = nullptr;
+        ck(cudaStreamEndCapture(sp, &o), "end RHS capture");
+      }
+    } else {
+      const long long a = g_launches.load();
+      rc = rhs(cur, nx, 0, st);
+      k_rhs = g_launches.load() - a;
+    }
+    const long long b = g_launches.load();
+    if (!rc) rc = dnsb_couette_imm(p, state, cur, pv, nx, cur, nullptr, g->err, st);
+    k_imm = g_launches.load() - b;
+  };
+  ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t graph = nullptr;
+  ck(cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, nullptr, nullptr), "capture info");
+  cudaGraphConditionalHandle h = 0, h_if = 0;
+  ck(cudaGraphConditionalHandleCreate(&h, graph, 0, 0), "conditional handle");
+  const long long c1 = g_launches.load();
+  if (!rc) rc = rhs(cur, g->Ra, mixed, s);
+  if (!rc) rc = dnsb_couette_imm(p, state, cur, restart ? g->Ra : g->Rb, g->Ra, cur, nullptr,
+                                 g->err, s);
+  dnsb::mixed_ctl_kernel<<<1, 1, 0, s>>>(h, 0, 0, g->err, g->ctl, tol, max_iter, switch_tol,
+                                         stall, 1);
+  ck(cudaGetLastError(), "control kernel");
+  g->k_post = g_launches.load() - c1 + 1;  // + the control kernel
+  cudaGraph_t bg = add_cond_node(s, graph, h, cudaGraphCondTypeWhile, rc);
+  if (!rc) {
+    ck(cudaGraphConditionalHandleCreate(&h_if, bg, 0, 0), "conditional handle");
+    ck(cudaStreamBeginCaptureToGraph(sb, bg, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal), "body capture");
+    iteration(sb, bg, g->Rb, g->Ra);  // A: rhs_next -> Rb, rhs_prev Ra
+    dnsb::mixed_ctl_kernel<<<1, 1, 0, sb>>>(h, h_if, 1, g->err, g->ctl, tol, max_iter,
+                                            switch_tol, stall, 0);
+    ck(cudaGetLastError(), "control kernel");
+    cudaGraph_t ig = add_cond_node(sb, bg, h_if, cudaGraphCondTypeIf, rc);
+    if (!rc) {
+      ck(cudaStreamBeginCaptureToGraph(si, ig, nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeThreadLocal), "IF body capture");
+      iteration(si, ig, g->Ra, g->Rb);  // B: rhs_next -> Ra, rhs_prev Rb
+      dnsb::mixed_ctl_kernel<<<1, 1, 0, si>>>(h, 0, 0, g->err, g->ctl, tol, max_iter,
+                                              switch_tol, stall, 0);
+      ck(cudaGetLastError(), "control kernel");
+      cudaGraph_t iout = nullptr;
+      ck(cudaStreamEndCapture(si, &iout), "end IF body capture");
+    }
+    cudaGraph_t bout = nullptr;
+    ck(cudaStreamEndCapture(sb, &bout), "end body capture");
+  }
+  ck(cudaMemcpyAsync(state, cur, n * sizeof(double2), cudaMemcpyDeviceToDevice, s), "copy");
+  ck(cudaStreamEndCapture(s, &done), "end capture");
+  if (!rc) ck(cudaGraphInstantiate(&g->post, done, 0), "instantiate");
+  if (done) cudaGraphDestroy(done);
+  // a mixed iteration: precision kernel, one RHS, the IMM, the control kernel
+  g->k_iter = (mixed ? 1 : 0) + k_rhs + k_imm + 1;
+  g_launches.fetch_sub(g_launches.load() - c0, std::memory_order_relaxed);
+  cudaStreamDestroy(s);
+  cudaStreamDestroy(sb);
+  cudaStreamDestroy(si);
+  cudaStreamDestroy(sp);
+  if (rc) {
+    mixed_graph_free(g);
+    return rc;
+  }
+  *out = g;
+  return 0;
+}
+
+extern "C" int dnsb_mixed_graph_predict(dnsb_mixed_graph* g, void* stream) {
+  if (!g) return fail(DNSB_ERR_ARG, "null argument");
+  DNSB_CUDA(cudaGraphLaunch(g->pre, as_stream(stream)));
+  return 0;
+}
+
+extern "C" int dnsb_mixed_graph_correct(dnsb_mixed_graph* g, void* stream) {
+  if (!g) return fail(DNSB_ERR_ARG, "null argument");
+  DNSB_CUDA(cudaGraphLaunch(g->post, as_stream(stream)));
+  return 0;
+}
+
+extern "C" int dnsb_mixed_graph_status(dnsb_mixed_graph* g, int* iters, double* err,
+                                       double* first_err, int* n32, int* n64, void* stream) {
+  if (!g || !iters || !err) return fail(DNSB_ERR_ARG, "null argument");
+  cudaStream_t st = as_stream(stream);
+  DNSB_CUDA(cudaMemcpyAsync(g->h_ctl, g->ctl, sizeof(dnsb::MixedCtl), cudaMemcpyDeviceToHost,
+                            st));
+  DNSB_CUDA(cudaStreamSynchronize(st));
+  const dnsb::MixedCtl c = *g->h_ctl;
+  *iters = c.it;
+  *err = c.err;
+  if (first_err) *first_err = c.first;
+  // the FP64 form has no precision kernel: every RHS of the step is FP64
+  if (n32) *n32 = g->mixed ? c.n32 : 0;
+  if (n64) *n64 = g->mixed ? c.n64 : 2 + c.it;
+  g_launches.fetch_add(g->k_pre + g->k_post + (long long)c.it * g->k_iter,
+                       std::memory_order_relaxed);
+  return 0;
+}
+
+extern "C" int dnsb_mixed_graph_destroy(dnsb_mixed_graph* g) {
+  if (!g) return fail(DNSB_ERR_ARG, "null argument");
+  mixed_graph_free(g);
   return 0;
 }
 

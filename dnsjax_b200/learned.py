@@ -27,6 +27,11 @@ N(u^n) in the first slot).  With ``switch`` set (the mixed form), the RHS
 runs in FP32 until the correction norm falls below ``switch`` and in FP64
 from then on within the step, so the iteration ends at an FP64 fixed point
 while its early iterations cost less.
+
+``LearnedStepGraph`` (``LearnedGuess.make_step_graph``) is the same step with
+the corrector on the device: the predictor and the corrector loop are CUDA
+graphs, the precision switch is decided by a control kernel after every
+correction, and the host synchronises once per step.
 """
 
 from __future__ import annotations
@@ -366,6 +371,28 @@ class LearnedGuess:
         return losses
 
     # -- one time step -----------------------------------------------------------
+    def make_step_graph(self, state, tol: float, max_iter: int) -> "LearnedStepGraph":
+        """The graph form of ``step`` bound to ``state`` (see
+        LearnedStepGraph); ``switch``, ``stall`` and ``restart`` are fixed
+        when it is made."""
+        return LearnedStepGraph(self, state, tol, max_iter)
+
+    def _plan(self):
+        """(use the guess, measure it, steps since the last measurement) for
+        the next step: the guess is used while its latest measured error is
+        below the gate; while gated off it is re-measured every ``recheck``
+        steps; with online training every step is measured.  Depends only on
+        earlier steps, so a caller can know it before the step runs."""
+        use = self.enabled and (self.gate is None or self.last_rel is None
+                                or self.last_rel < self.gate)
+        gated_off = self.gate is not None and not use and self.last_rel is not None
+        since = self._since + 1 if gated_off else 0
+        measure = self.enabled and (self.train_iters > 0 or (
+            self.gate is not None and (not gated_off or since >= self.recheck)))
+        if gated_off and measure:
+            since = 0
+        return use, measure, since
+
     def step(self, state, dprev, tol, max_iter, measure: bool | None = None):
         """One time step started from the guessed state; returns (new state,
         converged correction u^{n+1} - u_p, LearnedStep)."""
@@ -384,12 +411,13 @@ class LearnedGuess:
                 n64 += 1
             return f.get_rhs(u)
 
+        use, planned, since = self._plan()
+        if measure is None:
+            measure, self._since = planned, since
         f.set_rhs_precision(mixed)
         r0 = rhs(state)
         up = f.predict(state, r0)
         s_floor = self._s_floor(up, state)
-        use = self.enabled and (self.gate is None or self.last_rel is None
-                                or self.last_rel < self.gate)
         start = up.clone()
         if use:
             self.features(state, up, dprev, s_floor=s_floor)
@@ -416,19 +444,123 @@ class LearnedGuess:
         cur, _ = f.correct_velocity(cur)
         delta = cur - up
         rel = None
-        if measure is None:
-            gated_off = self.gate is not None and not use and self.last_rel is not None
-            self._since = self._since + 1 if gated_off else 0
-            measure = self.enabled and (self.train_iters > 0 or (
-                self.gate is not None and (not gated_off or self._since >= self.recheck)))
-            if gated_off and measure:
-                self._since = 0
         if measure:
             rel = self.measure(state, up, dprev, delta, s_floor)
             self.last_rel = rel
             if self.train_iters:
                 self.net.train(self.train_iters)
         return cur, delta, LearnedStep(c, e, use, rel, first, n32, n64)
+
+
+class LearnedStepGraph:
+    """``LearnedGuess.step`` with the corrector on the device: two CUDA
+    graphs per step (``dnsb_couette_mixed_graph_create``) bound to
+    ``state``, which every ``step()`` advances in place.
+
+    The first graph runs the RHS of u^n and the predictor; when the guess is
+    used, the features, the network's forward pass and the guessed start
+    are launched between the two graphs on the same stream; the second graph
+    runs the restarted first correction, the corrector loop (FP32 RHS until
+    the switch, then FP64, chosen on the device after every correction) and
+    copies the converged state into ``state``.  A step synchronises the host
+    once (the status), plus once more on steps that use or measure the guess
+    (the scale floor of the features).  The states, iteration counts and
+    gating decisions are those of ``LearnedGuess.step`` bit for bit.
+    ``reset()`` forgets the previous step's correction (as ``dprev=None``)."""
+
+    def __init__(self, guess: LearnedGuess, state, tol: float, max_iter: int):
+        import torch
+
+        f = guess.flow
+        self.lg, self.flow, self.state = guess, f, state
+        self.up, self.cur = f._new(), f._new()
+        self._d = (torch.empty_like(state), torch.empty_like(state))
+        self._un = None
+        self._dprev = None
+        self._k = 0
+        mixed = guess.switch is not None
+        h = _lib.C.c_void_p()
+        _lib.check(f._L.dnsb_couette_mixed_graph_create(
+            f._ctx, f._check(state), f._check(self.up), f._check(self.cur), float(tol),
+            int(max_iter), 1 if mixed else 0, float(guess.switch) if mixed else 0.0,
+            float(guess.stall), 1 if guess.restart else 0, _lib.C.byref(h)))
+        self._h = h
+
+    def reset(self) -> None:
+        self._dprev = None
+
+    def snapshot(self):
+        """Copies of the bound state and the previous step's correction."""
+        return (self.state.clone(), None if self._dprev is None else self._dprev.clone())
+
+    def restore(self, snap) -> None:
+        state, dprev = snap
+        self.state.copy_(state)
+        if dprev is None:
+            self._dprev = None
+        else:
+            self._dprev = self._d[self._k]
+            self._dprev.copy_(dprev)
+
+    def step(self, measure: bool | None = None) -> LearnedStep:
+        import torch
+
+        lg, f, L = self.lg, self.flow, self.flow._L
+        stream = _lib.stream_handle()
+        use, planned, since = lg._plan()
+        if measure is None:
+            measure, lg._since = planned, since
+        _lib.check(L.dnsb_mixed_graph_predict(self._h, stream))
+        s_floor = lg._s_floor(self.up, self.state) if (use or measure) else 0.0
+        if measure:
+            if self._un is None:
+                self._un = torch.empty_like(self.state)
+            self._un.copy_(self.state)
+        if use:
+            lg.features(self.state, self.up, self._dprev, s_floor=s_floor)
+            lg.net.replay_forward()
+            lg.guess(self.up, self.cur)
+        _lib.check(L.dnsb_mixed_graph_correct(self._h, stream))
+        it, err, first = _lib.C.c_int(), _lib.C.c_double(), _lib.C.c_double()
+        n32, n64 = _lib.C.c_int(), _lib.C.c_int()
+        _lib.check(L.dnsb_mixed_graph_status(self._h, _lib.C.byref(it), _lib.C.byref(err),
+                                             _lib.C.byref(first), _lib.C.byref(n32),
+                                             _lib.C.byref(n64), stream))
+        rel = None
+        delta = None
+        if measure:
+            delta = self._delta()
+            rel = lg.measure(self._un, self.up, self._dprev, delta, s_floor)
+            lg.last_rel = rel
+            if lg.train_iters:
+                lg.net.train(lg.train_iters)
+        nuse, nmeasure, _ = lg._plan()
+        if nuse or nmeasure:
+            self._dprev = delta if delta is not None else self._delta()
+        else:
+            self._dprev = None
+        return LearnedStep(it.value, err.value, use, rel, first.value, n32.value, n64.value)
+
+    def _delta(self):
+        """u^{n+1} - u_p of the step just run, in the buffer the previous
+        step's correction does not occupy."""
+        import torch
+
+        self._k ^= 1
+        out = self._d[self._k]
+        torch.sub(self.state, self.up, out=out)
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.flow._L.dnsb_mixed_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def run(flow, state, steps, guess: LearnedGuess, tol=None, max_iter=None):

@@ -264,6 +264,35 @@ int dnsb_couette_set_wait_limit(dnsb_couette* ctx, int polls);
 int dnsb_couette_step_graph_create(dnsb_couette* ctx, void* state, double tol,
                                    int max_iter, dnsb_step_graph** out);
 
+/* The restarted, mixed-precision corrector step as two CUDA graphs (no
+ * counterpart in the reference: the device form of the learned corrector
+ * step, dnsjax_b200.learned.LearnedGuess.step, whose corrector is
+ * iterate_correction, plane_couette.py:522-540, from a guessed start).
+ * Bound to three distinct complex128 (3, nz-1, nx/2, ny) buffers:
+ *   dnsb_mixed_graph_predict: RHS of `state` (u^n), the predictor
+ *     (plane_couette.py:507-519) into `up`, copied into `cur`; the caller
+ *     may then overwrite `cur` with a guessed start;
+ *   dnsb_mixed_graph_correct: the first correction from `cur` (restart != 0:
+ *     the start's RHS in both RHS slots, else N^n as the previous RHS), the
+ *     corrector loop on the device while error > tol and iterations <
+ *     max_iter (__main__.py:166-180), and `cur` copied into `state`.
+ * mixed = 0: every RHS in FP64.  mixed = 1 (FP32) or 2 (FP32, compensated
+ * butterflies): the RHS runs at that precision until the error after a
+ * correction is <= switch_tol or > stall x the previous error, then in FP64
+ * for the rest of the step (needs the FP32 pass sizes of
+ * dnsb_couette_set_rhs_precision).  status: corrector iterations after the
+ * first correction, the last and the first error, and the RHS evaluations at
+ * reduced precision / FP64 of the last step (synchronises `stream`). */
+typedef struct dnsb_mixed_graph dnsb_mixed_graph;
+int dnsb_couette_mixed_graph_create(dnsb_couette* ctx, void* state, void* up, void* cur,
+                                    double tol, int max_iter, int mixed, double switch_tol,
+                                    double stall, int restart, dnsb_mixed_graph** out);
+int dnsb_mixed_graph_predict(dnsb_mixed_graph* g, void* stream);
+int dnsb_mixed_graph_correct(dnsb_mixed_graph* g, void* stream);
+int dnsb_mixed_graph_status(dnsb_mixed_graph* g, int* iters, double* err, double* first_err,
+                            int* n32, int* n64, void* stream);
+int dnsb_mixed_graph_destroy(dnsb_mixed_graph* g);
+
 /* Allocation-free Couette norm (no counterpart in the reference; it exists
  * for callers that cannot allocate device memory, such as an XLA FFI handler
  * working inside memory its framework owns).  Computes what dnsb_couette_norm computes, from the field alone

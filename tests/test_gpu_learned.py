@@ -15,6 +15,11 @@ gains over the method without it.
   guessed start converges every step to the tolerance, stays within 1e-8 of
   the plain trajectory, and the corrector iterations with and without the
   guess are recorded.
+* The graph form of the learned step (LearnedStepGraph: the corrector loop
+  and the FP32 -> FP64 switch on the device) gives the host-driven step's
+  states bit for bit, with the same iteration counts, RHS precisions,
+  first errors and gating decisions: mixed with the gate, mixed with the
+  guess applied every step, FP64 without the network, and an iteration cap.
 """
 
 import json
@@ -227,3 +232,57 @@ def test_learned_couette_run(tmp_path):
                   pretrain_losses=[losses[0], losses[-1]], parameters=lg.net.parameters)
     (tmp_path / "learned_gain.json").write_text(json.dumps(record))
     print(json.dumps(record))
+
+
+@pytest.mark.parametrize("form", ["mixed-gated", "mixed-guess", "fp64-no-network", "mixed-cap"])
+def test_learned_step_graph_equals_host_step(form):
+    import torch
+
+    from dnsjax_b200 import initial, learned
+    from dnsjax_b200.flows.plane_couette import PlaneCouetteFlow
+    from dnsjax_b200.parameters import Parameters
+
+    p = Parameters(phys=dict(system="plane-couette", re=400.0),
+                   geo=dict(lx=2 * pi, lz=pi), res=dict(nx=32, ny=33, nz=32, fd_order=4),
+                   step=dict(dt=0.02, corrector_tolerance=1e-10, max_corrector_iterations=60))
+    flow = PlaneCouetteFlow(p)
+    mixed = form.startswith("mixed")
+    lg = learned.LearnedGuess(flow, hidden=(64, 64), seed=0,
+                              switch=1e-5 if mixed else None,
+                              gate=None if form == "mixed-guess" else 0.9)
+    u = initial.couette_field(32, 33, 32, 2 * pi, pi, 4, 11, 8.0, 1e-3)
+    lg.collect(torch.as_tensor(u, device="cuda"), 6, 1e-10, 60)
+    lg.pretrain(5)
+    lg.enabled = form != "fp64-no-network"
+    tol = 1e-8 if mixed else 1e-10
+    mi = 2 if form == "mixed-cap" else 60
+    u0 = initial.couette_field(32, 33, 32, 2 * pi, pi, 4, 1, 8.0, 1e-3)
+    n = 12
+
+    lg.last_rel, lg._since = None, 0
+    s, dprev, host = torch.as_tensor(u0, device="cuda"), None, []
+    for _ in range(n):
+        s, dprev, st = lg.step(s, dprev, tol, mi)
+        host.append(st)
+
+    lg.last_rel, lg._since = None, 0
+    g_state = torch.as_tensor(u0, device="cuda")
+    g = lg.make_step_graph(g_state, tol, mi)
+    dev = [g.step() for _ in range(n)]
+    g.close()
+    for k, (a, b) in enumerate(zip(host, dev)):
+        assert a.corrector_iterations == b.corrector_iterations, k
+        assert a.error == b.error and a.first_correction == b.first_correction, k
+        assert (a.rhs_fp32, a.rhs_fp64) == (b.rhs_fp32, b.rhs_fp64), k
+        assert a.guessed == b.guessed and a.guess_rel_error == b.guess_rel_error, k
+    assert torch.equal(s, g_state)
+    if form == "mixed-cap":
+        assert all(x.corrector_iterations <= 2 for x in dev)
+    if mixed:
+        assert all(x.rhs_fp32 >= 2 for x in dev)
+    else:
+        assert all(x.rhs_fp32 == 0 for x in dev)
+    if form == "mixed-gated":
+        assert dev[0].guessed and dev[0].guess_rel_error is not None
+    if form == "mixed-guess":
+        assert all(x.guessed for x in dev)
