@@ -420,13 +420,20 @@ def run_ours(a, w, rank, world):
 
     graph = None
     graph_check = None
+    unroll = None
     if a.driver == "graph":
         # Headline pass: every step is one step-graph launch (predictor,
         # corrector loop on the device, correct_velocity) over the same K
         # steps the eager pass took (from the same state); the host reads
         # iterations and error per step.
+        # Couette graphs hold the eager pass's median iteration count as
+        # straight-line kernels ahead of the device-controlled loop.
         gstate = snap.clone()
-        graph = flow.make_step_graph(gstate, tol=tol, max_iter=mi)
+        if hasattr(flow, "set_graph_unroll"):
+            unroll = int(statistics.median(iters))
+            graph = flow.make_step_graph(gstate, tol=tol, max_iter=mi, unroll=unroll)
+        else:
+            graph = flow.make_step_graph(gstate, tol=tol, max_iter=mi)
         for _ in range(a.warmup):
             graph.launch()
             graph.status()
@@ -556,6 +563,7 @@ def run_ours(a, w, rank, world):
                                      "host-driven loop; per-op events of this pass give "
                                      "op_ms and the roofline"},
             "graph_vs_eager": graph_check,
+            "graph_unroll": unroll,
             "corrector_iterations_per_step": sum(iters) / len(iters),
             "last_error": last_err,
             "grid_points_steps_per_s": value * grid_points(w),
@@ -666,12 +674,19 @@ def plain_graph_rate(flow, w, u0, mi, warmup, steps, tol=None):
     import torch
 
     state = torch.as_tensor(u0, device="cuda")
-    graph = flow.make_step_graph(state, tol=w["tol"] if tol is None else tol, max_iter=mi)
+    t = w["tol"] if tol is None else tol
+    graph = flow.make_step_graph(state, tol=t, max_iter=mi)
+    its_w = []
     for i in range(warmup):
         if i and i % SEGMENT == 0:
             state.copy_(torch.as_tensor(u0, device="cuda"))
         graph.launch()
-        graph.status()
+        its_w.append(graph.status()[0])
+    if its_w and hasattr(flow, "set_graph_unroll"):
+        # the warm-up's median iteration count as straight-line kernels
+        graph.close()
+        graph = flow.make_step_graph(state, tol=t, max_iter=mi,
+                                     unroll=int(statistics.median(its_w)))
     snap = state.clone()
     ms, its = 0.0, 0
     for seg in segments(steps):
@@ -742,12 +757,17 @@ def metric_form(a, w, flow, u0, mi):
         lg.last_rel, lg._since = None, 0
         u = dev0()
         g = lg.make_step_graph(u, tol, mi)
+        its_w = []
         for i in range(a.warmup):
             if i and i % SEGMENT == 0:
                 u.copy_(dev0())
                 g.reset()
-            g.step()
+            its_w.append(g.step().corrector_iterations)
         snap = g.snapshot()
+        if its_w:
+            # the warm-up's median iteration count as straight-line kernels
+            g.close()
+            g = lg.make_step_graph(u, tol, mi, unroll=int(statistics.median(its_w)))
         ms, out = 0.0, []
         for seg in segs:
             g.restore(snap)

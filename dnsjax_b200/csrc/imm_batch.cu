@@ -126,6 +126,7 @@ __global__ void __launch_bounds__(32 * kStageWarps)
 imm_stage01_kernel(ImmArgs a, const double2* __restrict__ vel_n,
                    const double2* __restrict__ nl_n, const double2* __restrict__ nl_j,
                    double2* __restrict__ F) {
+  if (a.skip && *a.skip) return;
   constexpr int S1 = KL + 1, S2 = KL + 2, YM = kSYM;
   extern __shared__ double2 sm[];
   const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
@@ -197,6 +198,7 @@ __global__ void __launch_bounds__(32 * kStageWarps)
 imm_stage3_kernel(ImmArgs a, const double2* __restrict__ vel_n,
                   const double2* __restrict__ nl_n, const double2* __restrict__ nl_j,
                   const double2* __restrict__ P, double2* __restrict__ R) {
+  if (a.skip && *a.skip) return;
   constexpr int S1 = KL + 1, S2 = KL + 2, YM = kSYM;
   extern __shared__ double2 sm[];
   const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
@@ -267,6 +269,7 @@ __global__ void __launch_bounds__(32 * kStageWarps)
 imm_stage6_kernel(ImmArgs a, const double2* __restrict__ R, const double2* vel_j,
                   double2* vel_new, double2* __restrict__ corr_out,
                   double* __restrict__ partials) {
+  if (a.skip && *a.skip) return;
   constexpr int S1 = KL + 1, YM = kSYM;
   const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
   const int NKX = a.NKX, Ny = a.Ny, NM = a.NZ1 * a.NKX;
@@ -364,6 +367,7 @@ struct SolveArgs {
   int* status;
   int NP, NM, Ny, NKX, NZ1, paired, ring, slot_bytes;
   int wait_limit;  // polls before a ring wait gives up (the drain after it uses kDrainPolls)
+  const int* skip;  // non-null and *skip != 0: return at once (ImmArgs::skip)
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -540,6 +544,7 @@ __device__ __forceinline__ void tile_bwd_block(double2* const (&col)[NCP], int j
 template <int KL, int NU>
 __global__ void __launch_bounds__(96)
 imm_solve_kernel(SolveArgs a) {
+  if (a.skip && *a.skip) return;  // before any barrier is set up
   constexpr int NCP = 1;  // components per thread (one warp per component)
   constexpr int W = KL + 1, WB = NU + 1, NUP = (NU + 2) & ~1;
   constexpr int LB = W * KL * kTile * 8, PB = W * kTile, UB = WB * NUP * kTile * 8;
@@ -759,8 +764,9 @@ bool imm_batch_fits(int kl, int nu, int max_smem) {
 
 template <int KL>
 static cudaError_t solve_launch(const ImmBatch& bt, int op, double2* X, int ncomp, int NM,
-                                int Ny, int NKX, int NZ1, cudaStream_t st) {
+                                int Ny, int NKX, int NZ1, const int* skip, cudaStream_t st) {
   SolveArgs s{};
+  s.skip = skip;
   s.facL = bt.facL[op];
   s.facU = bt.facU[op];
   s.dp = bt.dp[op];
@@ -796,11 +802,11 @@ static cudaError_t pipeline(const ImmArgs& a, const ImmBatch& bt, const double2*
   cudaError_t e;
   imm_stage01_kernel<K><<<grid, 32 * kStageWarps, sm, st>>>(a, vel_n, nl_n, nl_j, bt.F);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  e = solve_launch<K>(bt, 0, bt.F, 1, NM, Ny, a.NKX, a.NZ1, st);
+  e = solve_launch<K>(bt, 0, bt.F, 1, NM, Ny, a.NKX, a.NZ1, a.skip, st);
   if (e != cudaSuccess) return e;
   imm_stage3_kernel<K><<<grid, 32 * kStageWarps, sm, st>>>(a, vel_n, nl_n, nl_j, bt.F, bt.R);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  e = solve_launch<K>(bt, 1, bt.R, 3, NM, Ny, a.NKX, a.NZ1, st);
+  e = solve_launch<K>(bt, 1, bt.R, 3, NM, Ny, a.NKX, a.NZ1, a.skip, st);
   if (e != cudaSuccess) return e;
   imm_stage6_kernel<K><<<grid, 32 * kStageWarps, 0, st>>>(a, bt.R, vel_j, vel_new, corr_out,
                                                           partials);

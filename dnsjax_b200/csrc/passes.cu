@@ -245,6 +245,7 @@ template <int ML, int SIGN, typename T = double, bool OUT32 = false, bool CURL =
           bool SLAB = false>
 __global__ void __launch_bounds__(kC2Threads)
 col_pass2_kernel(ColPassArgs a) {
+  if (a.skip && *a.skip) return;
   col_pass2_body<ML, SIGN, T, OUT32, CURL, SLAB>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
@@ -254,6 +255,7 @@ col_pass2_kernel(ColPassArgs a) {
 template <int ML, int SIGN, bool CURL>
 __global__ void __launch_bounds__(kC2Threads, 4)
 col_pass2_occ4_kernel(ColPassArgs a) {
+  if (a.skip && *a.skip) return;
   col_pass2_body<ML, SIGN, double, false, CURL, false>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
@@ -739,6 +741,7 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
 template <int ML, typename T, bool SLAB>
 __global__ void __launch_bounds__(kX2Threads, std::is_same<T, float>::value ? 8 : 5)
 x_pass2_kernel(XPassArgs a) {
+  if (a.skip && *a.skip) return;
   x_pass2_body<ML, T, SLAB>(a, blockIdx.x);
 }
 
@@ -1405,6 +1408,7 @@ __device__ __forceinline__ void zinv2_fill(const ZInvCurlArgs& a, CT* X,
 template <int ML, typename T = double, bool SLAB = false>
 __global__ void __launch_bounds__(kZ2Threads, 4)
 zinv_curl2_kernel(ZInvCurlArgs a) {
+  if (a.skip && *a.skip) return;
   using CT = typename pass_types<T>::C;
   using RT = typename pass_types<T>::R;
   constexpr int M = ML, R1 = M / 8, C = kZ2Cols;

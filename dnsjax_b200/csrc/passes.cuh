@@ -61,6 +61,9 @@ struct ColPassArgs {
   // slab.buf[t / blk] + f*fs + o*out_os + (t % blk)*ts + off + i, instead of
   // out + f*out_fs + o*out_os + t*out_ts + i.
   SlabDest slab;
+  // Unrolled step-graph iterations: when non-null and *skip != 0 (the
+  // corrector loop ended earlier in the step), the kernel returns at once.
+  const int* skip = nullptr;
 };
 
 // x pass.  Rows are (outer, inner) pairs; row r = outer * inner_n + inner
@@ -87,6 +90,9 @@ struct XPassArgs {
   // inner) goes to slab.buf[k / blk] + f*fs + (outer + oo)*so +
   // (inner + io)*si + (k % blk)*ks, instead of into `out`.
   SlabDest slab;
+  // Unrolled step-graph iterations: when non-null and *skip != 0 (the
+  // corrector loop ended earlier in the step), the kernel returns at once.
+  const int* skip = nullptr;
 };
 
 // x pass to physical space only (3 fields -> real [c] at row offsets
@@ -157,6 +163,9 @@ struct ZInvCurlArgs {
   // Slab store (FP64 two-stage pass): position t of column q goes to
   // slab.buf[t / blk] + f*fs + (t % blk)*ts + off + q.
   SlabDest slab;
+  // Unrolled step-graph iterations: when non-null and *skip != 0 (the
+  // corrector loop ended earlier in the step), the kernel returns at once.
+  const int* skip = nullptr;
 };
 
 constexpr int kZTile = 8;  // y values per CTA in the Couette z passes

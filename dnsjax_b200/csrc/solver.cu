@@ -51,13 +51,14 @@ __device__ __forceinline__ void finalize_body(const double* partials, int n, dou
 }
 
 __global__ void finalize_kernel(const double* partials, int n, double* out,
-                                double scale, int do_sqrt) {
+                                double scale, int do_sqrt, const int* skip) {
+  if (skip && *skip) return;
   finalize_body(partials, n, out, scale, do_sqrt);
 }
 
 cudaError_t launch_finalize(const double* partials, int n, double* out,
-                            double scale, int do_sqrt, cudaStream_t st) {
-  finalize_kernel<<<1, 1024, 0, st>>>(partials, n, out, scale, do_sqrt);
+                            double scale, int do_sqrt, cudaStream_t st, const int* skip) {
+  finalize_kernel<<<1, 1024, 0, st>>>(partials, n, out, scale, do_sqrt, skip);
   return cudaGetLastError();
 }
 

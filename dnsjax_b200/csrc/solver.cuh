@@ -13,7 +13,8 @@ constexpr int kRedBlocks = 592;  // 4 x 148 SMs; fixed so sums are reproducible
 
 // out[0] = scale * sum(partials[0..n)), sqrt'ed if do_sqrt.
 cudaError_t launch_finalize(const double* partials, int n, double* out,
-                            double scale, int do_sqrt, cudaStream_t st);
+                            double scale, int do_sqrt, cudaStream_t st,
+                            const int* skip = nullptr);
 
 // ---- periodic pointwise ----------------------------------------------------
 struct PeriodicPointArgs {
@@ -101,6 +102,9 @@ struct ImmArgs {
   int ab_row0;            // first ab row with a nonzero entry in any mode
   int pair_modes;         // 1: (s, kx) and (nz-1-s, kx) share LU factors
   int kx0;                // 1: local kx index 0 is the kx = 0 mode (norm weight 1)
+  // Unrolled step-graph iterations (the batched pipeline): when non-null and
+  // *skip != 0, every kernel of the call returns at once.
+  const int* skip = nullptr;
 };
 
 constexpr int kImmWarps = 4;  // modes per CTA (one warp each)

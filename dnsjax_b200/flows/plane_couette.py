@@ -229,15 +229,37 @@ class PlaneCouetteFlow:
         """plane_couette.py:575-582: pass-through."""
         return state, None
 
+    def set_graph_unroll(self, n: int) -> None:
+        """Corrector iterations that step graphs made afterwards hold as
+        straight-line kernels ahead of the device-controlled loop (see
+        dnsb_couette_set_graph_unroll); the states are the same bit for bit,
+        the iterations within the unrolled count enter no conditional node."""
+        _lib.check(self._L.dnsb_couette_set_graph_unroll(self._ctx, int(n)))
+        self._graph_unroll = int(n)
+
+    def _with_unroll(self, unroll, make):
+        """make() with the graph unroll set to `unroll` (None: the current
+        setting), the setting restored afterwards."""
+        if unroll is None:
+            return make()
+        prev = getattr(self, "_graph_unroll", 0)
+        self.set_graph_unroll(unroll)
+        try:
+            return make()
+        finally:
+            self.set_graph_unroll(prev)
+
     def make_step_graph(self, state, tol: float | None = None,
-                        max_iter: int | None = None):
+                        max_iter: int | None = None, unroll: int | None = None):
         """A CUDA graph of one full time step bound to `state` (updated in
-        place by every launch); see StepGraph."""
+        place by every launch); see StepGraph.  ``unroll``: corrector
+        iterations held as straight-line kernels (set_graph_unroll)."""
         st = self.params.step
         tol = st.corrector_tolerance if tol is None else tol
         max_iter = st.max_corrector_iterations if max_iter is None else max_iter
-        return StepGraph(self._L, state, lambda h: self._L.dnsb_couette_step_graph_create(
-            self._ctx, self._check(state), float(tol), int(max_iter), h))
+        return self._with_unroll(unroll, lambda: StepGraph(
+            self._L, state, lambda h: self._L.dnsb_couette_step_graph_create(
+                self._ctx, self._check(state), float(tol), int(max_iter), h)))
 
     # -- variants of the passes (no counterpart in the reference) ----------------
     def autotune(self, state, reps: int = 5) -> dict:

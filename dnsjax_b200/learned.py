@@ -371,11 +371,14 @@ class LearnedGuess:
         return losses
 
     # -- one time step -----------------------------------------------------------
-    def make_step_graph(self, state, tol: float, max_iter: int) -> "LearnedStepGraph":
+    def make_step_graph(self, state, tol: float, max_iter: int,
+                        unroll: int | None = None) -> "LearnedStepGraph":
         """The graph form of ``step`` bound to ``state`` (see
         LearnedStepGraph); ``switch``, ``stall`` and ``restart`` are fixed
-        when it is made."""
-        return LearnedStepGraph(self, state, tol, max_iter)
+        when it is made; ``unroll`` corrector iterations are held as
+        straight-line kernels (PlaneCouetteFlow.set_graph_unroll)."""
+        return self.flow._with_unroll(
+            unroll, lambda: LearnedStepGraph(self, state, tol, max_iter))
 
     def _plan(self):
         """(use the guess, measure it, steps since the last measurement) for

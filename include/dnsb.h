@@ -264,6 +264,18 @@ int dnsb_couette_set_wait_limit(dnsb_couette* ctx, int polls);
 int dnsb_couette_step_graph_create(dnsb_couette* ctx, void* state, double tol,
                                    int max_iter, dnsb_step_graph** out);
 
+/* Corrector iterations that step graphs captured afterwards on this context
+ * (dnsb_couette_step_graph_create, dnsb_couette_mixed_graph_create) hold as
+ * straight-line kernels before the WHILE node (no counterpart in the
+ * reference).  Every entry into a conditional node's body leaves the GPU idle
+ * for tens of microseconds; the unrolled iterations enter none, and once the
+ * loop has ended their kernels return at once.  n in [0, 64] (capped at the
+ * graph's max_iter); it applies when the context runs the two-stage passes at
+ * the compiled sizes and the batched IMM (the defaults there), else graphs
+ * are captured without unrolling.  The states and iteration counts are those
+ * of the graphs without unrolling, bit for bit. */
+int dnsb_couette_set_graph_unroll(dnsb_couette* ctx, int n);
+
 /* The restarted, mixed-precision corrector step as two CUDA graphs (no
  * counterpart in the reference: the device form of the learned corrector
  * step, dnsjax_b200.learned.LearnedGuess.step, whose corrector is

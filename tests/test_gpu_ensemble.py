@@ -190,6 +190,35 @@ def test_couette_step_graph_equals_driver():
     assert g2.status()[0] == 0
 
 
+@pytest.mark.parametrize("unroll,max_iter", [(1, 60), (2, 60), (5, 60), (64, 60), (5, 2)])
+def test_couette_step_graph_unrolled(unroll, max_iter):
+    """Corrector iterations held as straight-line kernels ahead of the WHILE
+    node (fewer, as many as, and more than the step needs; odd and even
+    counts; a cap below the unrolled count): the host loop's states bit for
+    bit and its iteration counts."""
+    import torch
+
+    from dnsjax_b200 import driver
+
+    f, u = couette_member(64, 400.0, 2)
+    s_eager = torch.as_tensor(u, device="cuda")
+    s_graph = torch.as_tensor(u, device="cuda")
+    g = f.make_step_graph(s_graph, max_iter=max_iter, unroll=unroll)
+    st = f.make_stepper()
+    its = []
+    for _ in range(3):
+        s_eager, c, e = driver.step(f, st, s_eager, f.params.step.corrector_tolerance, max_iter)
+        g.launch()
+        it, err = g.status()
+        assert it == c and err == e
+        its.append(it)
+    f.check_status()
+    assert torch.equal(s_eager, s_graph)
+    if max_iter == 2:
+        assert its == [2, 2, 2]
+    g.close()
+
+
 def test_couette_graph_ensemble_equals_sequential():
     import torch
 

@@ -19,7 +19,8 @@ gains over the method without it.
   and the FP32 -> FP64 switch on the device) gives the host-driven step's
   states bit for bit, with the same iteration counts, RHS precisions,
   first errors and gating decisions: mixed with the gate, mixed with the
-  guess applied every step, FP64 without the network, and an iteration cap.
+  guess applied every step, FP64 without the network, and an iteration cap,
+  with and without corrector iterations held as straight-line kernels.
 """
 
 import json
@@ -234,8 +235,11 @@ def test_learned_couette_run(tmp_path):
     print(json.dumps(record))
 
 
-@pytest.mark.parametrize("form", ["mixed-gated", "mixed-guess", "fp64-no-network", "mixed-cap"])
-def test_learned_step_graph_equals_host_step(form):
+@pytest.mark.parametrize("form,unroll", [("mixed-gated", 0), ("mixed-guess", 0),
+                                         ("fp64-no-network", 0), ("mixed-cap", 0),
+                                         ("mixed-gated", 3), ("fp64-no-network", 2),
+                                         ("mixed-cap", 5), ("mixed-guess", 64)])
+def test_learned_step_graph_equals_host_step(form, unroll):
     import torch
 
     from dnsjax_b200 import initial, learned
@@ -267,7 +271,7 @@ def test_learned_step_graph_equals_host_step(form):
 
     lg.last_rel, lg._since = None, 0
     g_state = torch.as_tensor(u0, device="cuda")
-    g = lg.make_step_graph(g_state, tol, mi)
+    g = lg.make_step_graph(g_state, tol, mi, unroll=unroll)
     dev = [g.step() for _ in range(n)]
     g.close()
     for k, (a, b) in enumerate(zip(host, dev)):
