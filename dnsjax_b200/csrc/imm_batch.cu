@@ -4,13 +4,14 @@
 // dgbtrs-'N' substitution of src/dnsjax/geometries/cartesian.py:360-441.
 //
 //   stages 0-1   one warp per (kz, kx) mode: d_hat = div u^n, then f_hat
-//                (D1 / D2 along y from shared memory) -> F      [NM][Ny]
+//   (+ 3)        (D1 / D2 along y from shared memory) -> F      [NM][Ny],
+//                and in the same pass the part of stage 3 that does not
+//                need p_P, Q = H_k^- u^n + c N_j + (1-c) N_n -> R [3][NM][Ny]
 //   L_k solve    p_P = L_k^-1 f_hat in place in F: a CTA per 16 items, one
 //                warp per component, lane = side * 16 + item (side 1 is the
 //                mirror mode (nz-1-s, kx) of item (s, kx) when it shares the
 //                item's factors), each lane one complex column
-//   stage 3      one warp per mode: R = H_k^- u^n - grad p_P + c N_j +
-//                (1-c) N_n -> R                                  [3][NM][Ny]
+//   stage 3      one warp per mode: R = Q - grad p_P (interior rows)
 //   H_k solve    as the L_k solve, three components, in place in R
 //   stages 4-6   one warp per mode: wall divergence, influence-matrix
 //                weights, u^{j+1}, the correction and its Simpson norm
@@ -36,8 +37,8 @@ constexpr int kSYM = 5;         // y values per lane: y = lane + 32 k, Ny <= 160
 // L2 residency of the workspaces F and R (K Ny and 3 K Ny complex, 67 MB at
 // 128x129x128, each touched about three times per call): their writes and
 // the substitutions' accesses carry an evict_last policy, and their last
-// reads (F in stage 3, R in stage 6) evict_first, so the streamed inputs do
-// not push them out of the 126 MB L2 between the kernels of one call
+// reads (F in the gradient kernel, R in stage 6) evict_first, so the streamed
+// inputs do not push them out of the 126 MB L2 between the kernels of one call
 // (l2_keep / l2_drop and the hinted accesses are in common.cuh).
 
 // Banded stencil row y applied to x: sum_m w[m][y] x[j0[y] + m], with the
@@ -119,13 +120,15 @@ cudaError_t launch_imm_repack(const double* ab, const int* piv, int Ny, int kl, 
 }
 
 // ---------------------------------------------------------------------------
-// Stages 0-1: f_hat -> F.
+// Stages 0-1 and the pressure-free part of stage 3, in one pass over the
+// inputs: f_hat -> F, and Q = H_k^- u^n + c N_j + (1-c) N_n -> R (wall rows
+// zero), so u^n, N_j and N_n are read once per call.
 // ---------------------------------------------------------------------------
 template <int KL>
 __global__ void __launch_bounds__(32 * kStageWarps)
-imm_stage01_kernel(ImmArgs a, const double2* __restrict__ vel_n,
-                   const double2* __restrict__ nl_n, const double2* __restrict__ nl_j,
-                   double2* __restrict__ F) {
+imm_stage013_kernel(ImmArgs a, const double2* __restrict__ vel_n,
+                    const double2* __restrict__ nl_n, const double2* __restrict__ nl_j,
+                    double2* __restrict__ F, double2* __restrict__ R) {
   if (a.skip && *a.skip) return;
   constexpr int S1 = KL + 1, S2 = KL + 2, YM = kSYM;
   extern __shared__ double2 sm[];
@@ -133,93 +136,22 @@ imm_stage01_kernel(ImmArgs a, const double2* __restrict__ vel_n,
   const int NKX = a.NKX, Ny = a.Ny, NM = a.NZ1 * a.NKX;
   const int m = blockIdx.x * kStageWarps + wq;
   if (m >= NM) return;  // no CTA-wide barrier below
-  double2* T = sm + wq * 4 * Ny;  // v^n, N^j_v, N^n_v
-  double2* D = T + 3 * Ny;        // d_hat^n
+  double2* T = sm + wq * 6 * Ny;  // u^n, v^n, w^n, N^j_v, N^n_v, d_hat^n
+  double2* D = T + 5 * Ny;
   const long long CS = (long long)NM * Ny, mo = (long long)m * Ny;
-  for (int y = lane; y < Ny; y += 32) {
-    cp_async16(T + y, vel_n + CS + mo + y);
-    cp_async16(T + Ny + y, nl_j + CS + mo + y);
-    cp_async16(T + 2 * Ny + y, nl_n + CS + mo + y);
-  }
-  cp_async_commit();
-  const int iz = m / NKX, ix = m % NKX;
-  const double kx = a.kx[ix], kz = a.kz[iz];
-  const double k2 = kx * kx + kz * kz;
-  const double c = a.c, dt = a.dt, omc = 1.0 - c, omc_nu = omc * a.nu;
-  const unsigned long long keep = l2_keep();
-  double2 ua[YM], wa[YM], uj[YM], wj[YM], un[YM], wn[YM];
-#pragma unroll
-  for (int k = 0; k < YM; ++k) {
-    const int y = lane + 32 * k;
-    if (y < Ny) {
-      ua[k] = vel_n[mo + y];
-      wa[k] = vel_n[2 * CS + mo + y];
-      uj[k] = nl_j[mo + y];
-      wj[k] = nl_j[2 * CS + mo + y];
-      un[k] = nl_n[mo + y];
-      wn[k] = nl_n[2 * CS + mo + y];
-    }
-  }
-  cp_async_wait_all();
-  __syncwarp();
-  // Stage 0: d_hat^n = div u^n
-#pragma unroll
-  for (int k = 0; k < YM; ++k) {
-    const int y = lane + 32 * k;
-    if (y < Ny)
-      D[y] = cadd(cadd(cik(kx, ua[k]), band_row<S1>(T, a.d1_j0, a.d1_wT, Ny, y)), cik(kz, wa[k]));
-  }
-  __syncwarp();
-  // Stage 1: f_hat (wall rows zero)
-#pragma unroll
-  for (int k = 0; k < YM; ++k) {
-    const int y = lane + 32 * k;
-    if (y >= Ny) continue;
-    double2 fy = make_double2(0.0, 0.0);
-    if (y > 0 && y < Ny - 1) {
-      const double2 divNj =
-          cadd(cadd(cik(kx, uj[k]), band_row<S1>(T + Ny, a.d1_j0, a.d1_wT, Ny, y)), cik(kz, wj[k]));
-      const double2 divNn =
-          cadd(cadd(cik(kx, un[k]), band_row<S1>(T + 2 * Ny, a.d1_j0, a.d1_wT, Ny, y)), cik(kz, wn[k]));
-      const double2 dy = D[y];
-      const double2 Lkd = csub(band_row<S2>(D, a.d2_j0, a.d2_wT, Ny, y), cscale(dy, k2));
-      const double2 dd = make_double2(dy.x / dt, dy.y / dt);
-      fy = cadd(cadd(cadd(dd, cscale(divNj, c)), cscale(divNn, omc)), cscale(Lkd, omc_nu));
-    }
-    st_l2(F + mo + y, fy, keep);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Stage 3: R -> R (3 components).
-// ---------------------------------------------------------------------------
-template <int KL>
-__global__ void __launch_bounds__(32 * kStageWarps)
-imm_stage3_kernel(ImmArgs a, const double2* __restrict__ vel_n,
-                  const double2* __restrict__ nl_n, const double2* __restrict__ nl_j,
-                  const double2* __restrict__ P, double2* __restrict__ R) {
-  if (a.skip && *a.skip) return;
-  constexpr int S1 = KL + 1, S2 = KL + 2, YM = kSYM;
-  extern __shared__ double2 sm[];
-  const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
-  const int NKX = a.NKX, Ny = a.Ny, NM = a.NZ1 * a.NKX;
-  const int m = blockIdx.x * kStageWarps + wq;
-  if (m >= NM) return;
-  double2* T = sm + wq * 4 * Ny;  // u^n, v^n, w^n
-  double2* Pp = T + 3 * Ny;       // p_P
-  const long long CS = (long long)NM * Ny, mo = (long long)m * Ny;
-  const unsigned long long keep = l2_keep(), drop = l2_drop();
   for (int y = lane; y < Ny; y += 32) {
     cp_async16(T + y, vel_n + mo + y);
     cp_async16(T + Ny + y, vel_n + CS + mo + y);
     cp_async16(T + 2 * Ny + y, vel_n + 2 * CS + mo + y);
-    cp_async16_l2(Pp + y, P + mo + y, drop);
+    cp_async16(T + 3 * Ny + y, nl_j + CS + mo + y);
+    cp_async16(T + 4 * Ny + y, nl_n + CS + mo + y);
   }
   cp_async_commit();
   const int iz = m / NKX, ix = m % NKX;
   const double kx = a.kx[ix], kz = a.kz[iz];
   const double k2 = kx * kx + kz * kz;
-  const double c = a.c, omc = 1.0 - c, omc_nu = omc * a.nu, idt = 1.0 / a.dt;
+  const double c = a.c, dt = a.dt, omc = 1.0 - c, omc_nu = omc * a.nu, idt = 1.0 / dt;
+  const unsigned long long keep = l2_keep();
   double2 nj[3][YM], nn[3][YM];
 #pragma unroll
   for (int k = 0; k < YM; ++k) {
@@ -234,16 +166,33 @@ imm_stage3_kernel(ImmArgs a, const double2* __restrict__ vel_n,
   }
   cp_async_wait_all();
   __syncwarp();
+  // Stage 0: d_hat^n = div u^n
+#pragma unroll
+  for (int k = 0; k < YM; ++k) {
+    const int y = lane + 32 * k;
+    if (y < Ny)
+      D[y] = cadd(cadd(cik(kx, T[y]), band_row<S1>(T + Ny, a.d1_j0, a.d1_wT, Ny, y)),
+                  cik(kz, T[2 * Ny + y]));
+  }
+  __syncwarp();
 #pragma unroll
   for (int k = 0; k < YM; ++k) {
     const int y = lane + 32 * k;
     if (y >= Ny) continue;
-    double2 ru = make_double2(0.0, 0.0), rv = ru, rw = ru;
+    double2 fy = make_double2(0.0, 0.0), qu = fy, qv = fy, qw = fy;
     if (y > 0 && y < Ny - 1) {
-      const double2 p = Pp[y];
-      const double2 dxp = cik(kx, p);
-      const double2 dyp = band_row<S1>(Pp, a.d1_j0, a.d1_wT, Ny, y);
-      const double2 dzp = cik(kz, p);
+      // Stage 1: f_hat
+      const double2 divNj = cadd(cadd(cik(kx, nj[0][k]),
+                                      band_row<S1>(T + 3 * Ny, a.d1_j0, a.d1_wT, Ny, y)),
+                                 cik(kz, nj[2][k]));
+      const double2 divNn = cadd(cadd(cik(kx, nn[0][k]),
+                                      band_row<S1>(T + 4 * Ny, a.d1_j0, a.d1_wT, Ny, y)),
+                                 cik(kz, nn[2][k]));
+      const double2 dy = D[y];
+      const double2 Lkd = csub(band_row<S2>(D, a.d2_j0, a.d2_wT, Ny, y), cscale(dy, k2));
+      const double2 dd = make_double2(dy.x / dt, dy.y / dt);
+      fy = cadd(cadd(cadd(dd, cscale(divNj, c)), cscale(divNn, omc)), cscale(Lkd, omc_nu));
+      // Stage 3 without the pressure gradient
       const double2 u = T[y], v = T[Ny + y], w = T[2 * Ny + y];
       const double2 D2u = band_row<S2>(T, a.d2_j0, a.d2_wT, Ny, y);
       const double2 D2v = band_row<S2>(T + Ny, a.d2_j0, a.d2_wT, Ny, y);
@@ -251,13 +200,57 @@ imm_stage3_kernel(ImmArgs a, const double2* __restrict__ vel_n,
       const double2 hu = cadd(cscale(u, idt), cscale(csub(D2u, cscale(u, k2)), omc_nu));
       const double2 hv = cadd(cscale(v, idt), cscale(csub(D2v, cscale(v, k2)), omc_nu));
       const double2 hw = cadd(cscale(w, idt), cscale(csub(D2w, cscale(w, k2)), omc_nu));
-      ru = cadd(cadd(csub(hu, dxp), cscale(nj[0][k], c)), cscale(nn[0][k], omc));
-      rv = cadd(cadd(csub(hv, dyp), cscale(nj[1][k], c)), cscale(nn[1][k], omc));
-      rw = cadd(cadd(csub(hw, dzp), cscale(nj[2][k], c)), cscale(nn[2][k], omc));
+      qu = cadd(cadd(hu, cscale(nj[0][k], c)), cscale(nn[0][k], omc));
+      qv = cadd(cadd(hv, cscale(nj[1][k], c)), cscale(nn[1][k], omc));
+      qw = cadd(cadd(hw, cscale(nj[2][k], c)), cscale(nn[2][k], omc));
     }
-    st_l2(R + mo + y, ru, keep);
-    st_l2(R + CS + mo + y, rv, keep);
-    st_l2(R + 2 * CS + mo + y, rw, keep);
+    st_l2(F + mo + y, fy, keep);
+    st_l2(R + mo + y, qu, keep);
+    st_l2(R + CS + mo + y, qv, keep);
+    st_l2(R + 2 * CS + mo + y, qw, keep);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stage 3's pressure gradient: R -= grad p_P on the interior rows (the wall
+// rows of R stay zero), p_P = L_k^-1 f_hat from the L_k substitution in F.
+// ---------------------------------------------------------------------------
+template <int KL>
+__global__ void __launch_bounds__(32 * kStageWarps)
+imm_grad_kernel(ImmArgs a, const double2* __restrict__ P, double2* __restrict__ R) {
+  if (a.skip && *a.skip) return;
+  constexpr int S1 = KL + 1, YM = kSYM;
+  extern __shared__ double2 sm[];
+  const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+  const int NKX = a.NKX, Ny = a.Ny, NM = a.NZ1 * a.NKX;
+  const int m = blockIdx.x * kStageWarps + wq;
+  if (m >= NM) return;
+  double2* Pp = sm + wq * Ny;
+  const long long CS = (long long)NM * Ny, mo = (long long)m * Ny;
+  const unsigned long long keep = l2_keep(), drop = l2_drop();
+  for (int y = lane; y < Ny; y += 32) cp_async16_l2(Pp + y, P + mo + y, drop);
+  cp_async_commit();
+  const int iz = m / NKX, ix = m % NKX;
+  const double kx = a.kx[ix], kz = a.kz[iz];
+  double2 q[3][YM];
+#pragma unroll
+  for (int k = 0; k < YM; ++k) {
+    const int y = lane + 32 * k;
+    if (y > 0 && y < Ny - 1) {
+#pragma unroll
+      for (int cpt = 0; cpt < 3; ++cpt) q[cpt][k] = ld_l2(R + cpt * CS + mo + y, keep);
+    }
+  }
+  cp_async_wait_all();
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < YM; ++k) {
+    const int y = lane + 32 * k;
+    if (y <= 0 || y >= Ny - 1) continue;
+    const double2 p = Pp[y];
+    st_l2(R + mo + y, csub(q[0][k], cik(kx, p)), keep);
+    st_l2(R + CS + mo + y, csub(q[1][k], band_row<S1>(Pp, a.d1_j0, a.d1_wT, Ny, y)), keep);
+    st_l2(R + 2 * CS + mo + y, csub(q[2][k], cik(kz, p)), keep);
   }
 }
 
@@ -733,7 +726,11 @@ imm_solve_kernel(SolveArgs a) {
 // Host side.
 // ---------------------------------------------------------------------------
 size_t imm_batch_stage_smem(int Ny) {
-  return sizeof(double2) * (size_t)(4 * Ny * kStageWarps);
+  return sizeof(double2) * (size_t)(6 * Ny * kStageWarps);
+}
+
+static size_t imm_batch_grad_smem(int Ny) {
+  return sizeof(double2) * (size_t)(Ny * kStageWarps);
 }
 
 bool imm_batch_supported(int kl, int ny) {
@@ -800,11 +797,11 @@ static cudaError_t pipeline(const ImmArgs& a, const ImmBatch& bt, const double2*
   const int grid = (NM + kStageWarps - 1) / kStageWarps;
   const size_t sm = imm_batch_stage_smem(Ny);
   cudaError_t e;
-  imm_stage01_kernel<K><<<grid, 32 * kStageWarps, sm, st>>>(a, vel_n, nl_n, nl_j, bt.F);
+  imm_stage013_kernel<K><<<grid, 32 * kStageWarps, sm, st>>>(a, vel_n, nl_n, nl_j, bt.F, bt.R);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   e = solve_launch<K>(bt, 0, bt.F, 1, NM, Ny, a.NKX, a.NZ1, a.skip, st);
   if (e != cudaSuccess) return e;
-  imm_stage3_kernel<K><<<grid, 32 * kStageWarps, sm, st>>>(a, vel_n, nl_n, nl_j, bt.F, bt.R);
+  imm_grad_kernel<K><<<grid, 32 * kStageWarps, imm_batch_grad_smem(Ny), st>>>(a, bt.F, bt.R);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   e = solve_launch<K>(bt, 1, bt.R, 3, NM, Ny, a.NKX, a.NZ1, a.skip, st);
   if (e != cudaSuccess) return e;
@@ -829,10 +826,10 @@ cudaError_t launch_imm_batch(const ImmArgs& a, const ImmBatch& bt, const double2
 
 cudaError_t set_imm_batch_attributes(int max_smem) {
   const void* fns[] = {
-      (const void*)imm_stage01_kernel<2>, (const void*)imm_stage01_kernel<4>,
-      (const void*)imm_stage01_kernel<6>, (const void*)imm_stage01_kernel<8>,
-      (const void*)imm_stage3_kernel<2>,  (const void*)imm_stage3_kernel<4>,
-      (const void*)imm_stage3_kernel<6>,  (const void*)imm_stage3_kernel<8>,
+      (const void*)imm_stage013_kernel<2>, (const void*)imm_stage013_kernel<4>,
+      (const void*)imm_stage013_kernel<6>, (const void*)imm_stage013_kernel<8>,
+      (const void*)imm_grad_kernel<2>,     (const void*)imm_grad_kernel<4>,
+      (const void*)imm_grad_kernel<6>,     (const void*)imm_grad_kernel<8>,
 #define DNSB_SOLVE_FNS(K) \
   (const void*)imm_solve_kernel<K, K + 1>, (const void*)imm_solve_kernel<K, 2 * K>
       DNSB_SOLVE_FNS(2), DNSB_SOLVE_FNS(4), DNSB_SOLVE_FNS(6), DNSB_SOLVE_FNS(8)};
