@@ -151,7 +151,7 @@ def step_roofline(w, iters, steps_per_s_per_gpu, peak, fp32=False):
 # DRAM bytes (read + write) of one call, summed over the call's kernels, from
 # an ncu capture of the current kernels on this workload (profiles/); a
 # workload without a current capture reports traffic null.
-MEASURED_TRAFFIC = {"couette128": {"rhs": 428398592, "imm": 586905856,
+MEASURED_TRAFFIC = {"couette128": {"rhs": 429060864, "imm": 546556160,
                                   "source": "profiles/couette128_step_dram_ncu.md"}}
 
 
