@@ -79,6 +79,7 @@ SIGNATURES = {
     "dnsb_step_graph_status": (c_int, [c_void_p, P_int, P_double, c_void_p]),
     "dnsb_step_graph_destroy": (c_int, [c_void_p]),
     "dnsb_couette_set_graph_unroll": (c_int, [c_void_p, c_int]),
+    "dnsb_periodic_set_graph_unroll": (c_int, [c_void_p, c_int]),
     "dnsb_couette_mixed_graph_create": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p,
                                                 c_double, c_int, c_int, c_double, c_double,
                                                 c_int, C.POINTER(c_void_p)]),

@@ -124,6 +124,10 @@ struct dnsb_periodic {
   int rhs_fp32 = 0;  // RHS transforms and product in FP32 (pass buffers float2)
   int var[5] = {0, 0, 0, 0, 0};  // pass variants: y inverse, z inverse, x, z forward, y forward
   SlabState slab;                 // nranks > 0: a slab context
+  int graph_unroll = 0;           // corrector iterations step graphs capture unrolled
+  // set only while a step graph captures an unrolled iteration: the device
+  // flag that makes the iteration's kernels return at once
+  const int* skip = nullptr;
 
   PeriodicPointArgs point() const {
     PeriodicPointArgs a;
@@ -140,6 +144,7 @@ struct dnsb_periodic {
     a.lapl = lapl;
     a.c = c;
     a.kx0 = slab.rank == 0 ? 1 : 0;
+    a.skip = skip;
     return a;
   }
 };
@@ -390,6 +395,7 @@ static int periodic_rhs_impl(dnsb_periodic* p, const void* state, void* rhs, uns
     // y inverse with the curl as a two-stage column pass: state
     // [comp][ky][kz][kx] -> A[f][y][kz][kx]
     ColPassArgs yc = periodic_ycurl(p, state);
+    yc.skip = p->skip;
     yc.tw = yi.tw;
     yc.fp32 = yc.out32 = f32;
     DNSB_LAUNCH(launch_col_pass(yc, 6, p->NZ1, st));
@@ -397,16 +403,19 @@ static int periodic_rhs_impl(dnsb_periodic* p, const void* state, void* rhs, uns
     DNSB_LAUNCH(launch_yinv(yi, st));
   }
   ColPassArgs zi = periodic_zinv(p);
+  zi.skip = p->skip;
   zi.fp32 = zi.out32 = f32;
   if (f32) zi.tw = reinterpret_cast<const double2*>(p->twz32);
   zi.variant = p->var[1];
   if (mask & 2u) DNSB_LAUNCH(launch_col_pass(zi, 6, p->My, st));
   XPassArgs xa = periodic_xpass(p);
+  xa.skip = p->skip;
   xa.tw = f32 ? reinterpret_cast<const double2*>(p->twx32) : p->twx;
   xa.fp32 = f32;
   xa.variant = p->var[2];
   if (mask & 4u) DNSB_LAUNCH(launch_x_pass(xa, st));
   ColPassArgs zf = periodic_zfwd(p);
+  zf.skip = p->skip;
   zf.fp32 = zf.out32 = f32;
   if (f32) zf.tw = reinterpret_cast<const double2*>(p->twz32);
   zf.variant = p->var[3];
@@ -430,6 +439,7 @@ static int periodic_rhs_impl(dnsb_periodic* p, const void* state, void* rhs, uns
     // y forward as a two-stage column pass with truncation, A[f][y][kz][kx]
     // -> rhs[comp][ky][kz][kx] (complex128), then the projection in place
     ColPassArgs yc = periodic_yfwd_col(p, rhs);
+    yc.skip = p->skip;
     yc.tw = yf.tw;
     yc.fp32 = f32;
     DNSB_LAUNCH(launch_col_pass(yc, 3, p->NZ1, st));
@@ -486,7 +496,7 @@ extern "C" int dnsb_periodic_correct(dnsb_periodic* p, const void* pred,
   // by the caller, who takes the square root).
   if (err_dev)
     DNSB_LAUNCH(launch_finalize(p->partials, kRedBlocks, err_dev, 1.0, p->slab.nranks ? 0 : 1,
-                                st));
+                                st, p->skip));
   return 0;
 }
 
@@ -697,6 +707,27 @@ static dnsb_step_graph* new_step_graph(size_t n) {
   return g;
 }
 
+// Corrector iterations a periodic step graph captures unrolled: the
+// context's setting, when every kernel of an iteration checks the skip flag
+// (the two-stage passes at the compiled sizes, the y forward as a column
+// pass plus the projection), at most max_iter; otherwise none.
+static int periodic_unroll(const dnsb_periodic* p, int max_iter) {
+  auto fixed = [](int L) { return L == 48 || L == 72 || L == 96 || L == 192; };
+  if (p->graph_unroll <= 0 || !fixed(p->My) || !fixed(p->Mz) || !fixed(p->Mx) ||
+      3 * p->NKX != p->Mx)
+    return 0;
+  for (int k = 0; k < 5; ++k)
+    if (p->var[k] != 0) return 0;
+  return std::min(p->graph_unroll, std::max(max_iter, 0));
+}
+
+extern "C" int dnsb_periodic_set_graph_unroll(dnsb_periodic* p, int n) {
+  if (!p) return fail(DNSB_ERR_ARG, "null argument");
+  if (n < 0 || n > 64) return fail(DNSB_ERR_ARG, "unroll must be in [0, 64]");
+  p->graph_unroll = n;
+  return 0;
+}
+
 extern "C" int dnsb_periodic_step_graph_create(dnsb_periodic* p, void* state, double tol,
                                                int max_iter, int divergence,
                                                dnsb_step_graph** out) {
@@ -714,17 +745,20 @@ extern "C" int dnsb_periodic_step_graph_create(dnsb_periodic* p, void* state, do
   };
   // one corrector iteration: A (parity 0) rhs_next -> Ra with rhs_prev Rb,
   // B (parity 1) the other way round
-  auto body = [&](cudaStream_t s, int parity, const int*) {
+  auto body = [&](cudaStream_t s, int parity, const int* skip) {
     double2* nx = parity ? g->Rb : g->Ra;
     double2* pv = parity ? g->Ra : g->Rb;
+    p->skip = skip;
     int rc = dnsb_periodic_rhs(p, g->P, nx, s);
     if (!rc) rc = dnsb_periodic_correct(p, g->P, pv, nx, g->P, nullptr, g->err, s);
+    p->skip = nullptr;
     return rc;
   };
   auto epilogue = [&](cudaStream_t s) {
     return dnsb_periodic_correct_velocity(p, g->P, state, divergence, s);
   };
-  const int rc = build_step_graph(g, tol, max_iter, prologue, body, epilogue);
+  const int rc = build_step_graph(g, tol, max_iter, prologue, body, epilogue,
+                                 periodic_unroll(p, max_iter));
   if (rc) {
     step_graph_free(g);
     return rc;

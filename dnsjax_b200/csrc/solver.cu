@@ -128,6 +128,7 @@ __global__ void periodic_correct_kernel(PeriodicPointArgs a,
                                         const double2* __restrict__ next,
                                         double2* pred_out, double2* corr_out,
                                         double* __restrict__ partials) {
+  if (a.skip && *a.skip) return;
   periodic_correct_body(a, pred, prev, next, pred_out, corr_out, partials, blockIdx.x,
                         gridDim.x);
 }
@@ -227,6 +228,7 @@ __device__ __forceinline__ void periodic_cv_body(const PeriodicPointArgs& a, con
 __global__ void periodic_cv_kernel(PeriodicPointArgs a,
                                    const double2* in, double2* out,
                                    int divergence, int zero_mean) {
+  if (a.skip && *a.skip) return;
   periodic_cv_body(a, in, out, divergence, zero_mean, blockIdx.x, gridDim.x);
 }
 

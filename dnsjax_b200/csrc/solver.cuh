@@ -29,6 +29,10 @@ struct PeriodicPointArgs {
   const double* lapl;
   double c;
   int kx0;  // 1: local kx index 0 is the kx = 0 mode (weight 1 in the norms; else 2)
+  // Unrolled step-graph iterations: when non-null and *skip != 0, the
+  // correct and projection kernels return at once (the work-list forms
+  // ignore it).
+  const int* skip = nullptr;
 };
 
 // One member's pointwise call in an ensemble work list: predict (op 0:

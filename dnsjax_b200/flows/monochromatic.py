@@ -243,18 +243,39 @@ class TriplyPeriodicFlow:
         _lib.check(self._L.dnsb_periodic_set_rhs_precision(self._ctx, mode))
         self.rhs_fp32 = bool(fp32)
 
+    def set_graph_unroll(self, n: int) -> None:
+        """Corrector iterations that step graphs made afterwards hold as
+        straight-line kernels ahead of the device-controlled loop (see
+        dnsb_periodic_set_graph_unroll); the states are the same bit for
+        bit."""
+        _lib.check(self._L.dnsb_periodic_set_graph_unroll(self._ctx, int(n)))
+        self._graph_unroll = int(n)
+
     def make_step_graph(self, state, tol: float | None = None,
-                        max_iter: int | None = None, divergence: bool | None = None):
+                        max_iter: int | None = None, divergence: bool | None = None,
+                        unroll: int | None = None):
         """A CUDA graph of one full time step bound to `state` (updated in
-        place by every launch); see StepGraph."""
+        place by every launch); see StepGraph.  ``unroll``: corrector
+        iterations held as straight-line kernels (set_graph_unroll)."""
         st = self.params.step
         if divergence is None:
             dbg = self.params.debug
             divergence = True if dbg is None else dbg.correct_divergence
         tol = st.corrector_tolerance if tol is None else tol
         max_iter = st.max_corrector_iterations if max_iter is None else max_iter
-        return StepGraph(self._L, state, lambda h: self._L.dnsb_periodic_step_graph_create(
-            self._ctx, self._check(state), float(tol), int(max_iter), int(divergence), h))
+
+        def make():
+            return StepGraph(self._L, state, lambda h: self._L.dnsb_periodic_step_graph_create(
+                self._ctx, self._check(state), float(tol), int(max_iter), int(divergence), h))
+
+        if unroll is None:
+            return make()
+        prev = getattr(self, "_graph_unroll", 0)
+        self.set_graph_unroll(unroll)
+        try:
+            return make()
+        finally:
+            self.set_graph_unroll(prev)
 
     # -- variants of the passes (no counterpart in the reference) ----------------
     def autotune(self, state, reps: int = 5) -> dict:

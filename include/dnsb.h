@@ -127,6 +127,13 @@ int dnsb_step_graph_launch(dnsb_step_graph* g, void* stream);
 int dnsb_step_graph_status(dnsb_step_graph* g, int* iters, double* err,
                            void* stream);
 int dnsb_step_graph_destroy(dnsb_step_graph* g);
+/* Corrector iterations that periodic step graphs captured afterwards on this
+ * context hold as straight-line kernels ahead of the WHILE node (no
+ * counterpart in the reference; see dnsb_couette_set_graph_unroll).  n in
+ * [0, 64] (capped at the graph's max_iter); it applies when the context runs
+ * the two-stage passes at the compiled sizes (every pass variant 0), else
+ * graphs are captured without unrolling. */
+int dnsb_periodic_set_graph_unroll(dnsb_periodic* ctx, int n);
 
 /* Ensembles of independent periodic trajectories (the driver's time step,
  * __main__.py:125-203, for every member; no counterpart for several

@@ -82,6 +82,30 @@ def test_step_graph_equals_driver():
     assert c == 2 and torch.equal(s3_eager, s3)
 
 
+@pytest.mark.parametrize("unroll,max_iter", [(1, 10), (2, 10), (3, 10), (64, 10), (4, 2)])
+def test_step_graph_unrolled(unroll, max_iter):
+    """Periodic step graphs with corrector iterations held as straight-line
+    kernels (fewer, as many and more than the step needs; a cap below the
+    unrolled count): the host loop's states and iteration counts."""
+    import torch
+
+    from dnsjax_b200 import driver
+
+    f, u = member(48, 60.0, 1)
+    s_eager = torch.as_tensor(u, device="cuda")
+    s_graph = torch.as_tensor(u, device="cuda")
+    g = f.make_step_graph(s_graph, max_iter=max_iter, unroll=unroll)
+    st = f.make_stepper()
+    for _ in range(3):
+        s_eager, c, e = driver.step(f, st, s_eager, f.params.step.corrector_tolerance, max_iter)
+        g.launch()
+        it, err = g.status()
+        assert it == c and err == e
+        assert it <= max_iter
+    assert torch.equal(s_eager, s_graph)
+    g.close()
+
+
 def test_step_graph_host_round_trip():
     """run_host: the state copied in from pinned host memory and out again
     every step, the copy-out of one step overlapping the copy-in of the
