@@ -45,7 +45,7 @@ class Ensemble:
     every trajectory's iterations and error."""
 
     def __init__(self, flows, states, tol=None, max_iter=None, graphs=False, autotune=False,
-                 worklist=False):
+                 worklist=False, unroll=None):
         import torch
 
         if len(flows) != len(states):
@@ -69,9 +69,9 @@ class Ensemble:
                     self.tuning[key] = f.autotune(st)
         self.steppers = [f.make_stepper() for f in self.flows]
         self.streams = [torch.cuda.Stream() for _ in self.flows]
-        self.graphs = ([f.make_step_graph(s, tol=t, max_iter=m) for f, s, t, m in
-                        zip(self.flows, self.states, self.tol, self.max_iter)]
-                       if graphs and not worklist else None)
+        self.graphs = None
+        if graphs and not worklist:
+            self.set_unroll(unroll)
         self._ens = None
         if worklist:
             from . import _lib
@@ -159,6 +159,15 @@ class Ensemble:
             res.corrector_iterations.append(it)
             res.errors.append(e)
         return res
+
+    def set_unroll(self, unroll) -> None:
+        """(Re)captures every member's step graph with ``unroll`` corrector
+        iterations held as straight-line kernels (None: the flows' own
+        setting; see make_step_graph)."""
+        for g in self.graphs or []:
+            g.close()
+        self.graphs = [f.make_step_graph(s, tol=t, max_iter=m, unroll=unroll)
+                       for f, s, t, m in zip(self.flows, self.states, self.tol, self.max_iter)]
 
     def step(self) -> EnsembleStep:
         import torch
