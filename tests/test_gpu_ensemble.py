@@ -132,7 +132,8 @@ def test_step_graph_host_round_trip():
     assert torch.equal(a, s_dev.cpu())
 
 
-def test_graph_ensemble_equals_sequential():
+@pytest.mark.parametrize("unroll", [None, 2])
+def test_graph_ensemble_equals_sequential(unroll):
     import torch
 
     from dnsjax_b200 import driver
@@ -141,7 +142,7 @@ def test_graph_ensemble_equals_sequential():
     spec = [(32, 35.0, 0), (48, 60.0, 1), (64, 42.0, 3)]
     built = [member(*s) for s in spec]
     ens = Ensemble([f for f, _ in built], [torch.as_tensor(u, device="cuda") for _, u in built],
-                   graphs=True)
+                   graphs=True, unroll=unroll)
     its = [ens.step().corrector_iterations for _ in range(3)]
     for i, (f, u) in enumerate(built):
         st = f.make_stepper()
