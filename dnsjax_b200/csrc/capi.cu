@@ -1891,7 +1891,8 @@ extern "C" int dnsb_couette_step_graph_create(dnsb_couette* p, void* state, doub
 // With mixed != 0 the RHS runs at precision mode `mixed` (1 FP32, 2 FP32
 // with compensated butterflies) until the error after a correction is at or
 // below switch_tol, or the iteration stops contracting (error > stall x the
-// previous error); from then on it runs in FP64 for the rest of the step.
+// error two corrections back: the errors fall in pairs); from then on it
+// runs in FP64 for the rest of the step.
 // The control kernel makes that choice on the device after every
 // correction, and each iteration selects one of two IF nodes holding the RHS
 // passes captured at each precision.
@@ -1901,7 +1902,8 @@ struct MixedCtl {
   int it;         // corrector iterations of the step so far
   int fp32;       // the next RHS runs at the reduced precision
   int n32, n64;   // RHS evaluations of the step at reduced precision / FP64
-  double e_prev;  // error of the previous correction (+inf before the first)
+  double e_prev;   // error of the previous correction (+inf before the first)
+  double e_prev2;  // and of the one before it
   double first;   // error of the first correction
   double err;     // error of the latest correction
 };
@@ -1912,6 +1914,7 @@ __global__ void mixed_init_kernel(MixedCtl* c, int mixed) {
   c->n32 = mixed ? 2 : 0;  // the RHS of u^n and of the start
   c->n64 = mixed ? 0 : 2;
   c->e_prev = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+  c->e_prev2 = c->e_prev;
   c->first = 0.0;
   c->err = 0.0;
 }
@@ -1934,7 +1937,8 @@ __global__ void mixed_ctl_kernel(cudaGraphConditionalHandle h, cudaGraphConditio
   const double e = err[0];
   const unsigned cont = (e > tol && it < max_iter) ? 1u : 0u;
   if (first) c->first = e;
-  if (c->fp32 && (e <= switch_tol || e > stall * c->e_prev)) c->fp32 = 0;
+  if (c->fp32 && (e <= switch_tol || e > stall * c->e_prev2)) c->fp32 = 0;
+  c->e_prev2 = c->e_prev;
   c->e_prev = e;
   c->it = it;
   c->err = e;

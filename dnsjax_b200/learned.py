@@ -268,7 +268,11 @@ class LearnedGuess:
         self.NM = (flow.nz - 1) * (flow.nx // 2)
         self.net = MLP(self.NM, [12 * self.ny + 2, *hidden, 6 * self.ny], lr=lr, seed=seed)
         self.restart, self.switch, self.gate = restart, switch, gate
-        self.stall = 0.8      # FP32 iterations stop when e > stall * previous e
+        # FP32 iterations stop when e > stall * the error two corrections
+        # back: the corrector's errors fall in pairs (from the seeded
+        # 128x129x128 field, FP64 or FP32 alike: 3.3e-4, 6.4e-6, 6.4e-6,
+        # 4.7e-7, 2.4e-7), so a pause of one iteration is not the FP32 floor
+        self.stall = 0.8
         self.recheck = 8      # while gated off, measure the guess every recheck steps
         self.trace = None     # list: (iteration, error, fp32) of every correction
         self._since = 0
@@ -431,16 +435,17 @@ class LearnedGuess:
         e = float(err.item())
         first = e
         c = 0
-        e_prev = float("inf")
+        e_prev = e_prev2 = float("inf")
         while e > tol and c < max_iter:
             # one way to FP64 for the rest of the step: once below the switch,
-            # or when the FP32 iteration stops contracting (its rounding floor)
-            if mixed and f.rhs_fp32 and (e <= self.switch or e > self.stall * e_prev):
+            # or when the FP32 iteration stops contracting over two
+            # corrections (its rounding floor)
+            if mixed and f.rhs_fp32 and (e <= self.switch or e > self.stall * e_prev2):
                 f.set_rhs_precision(False)
             rp, rn = rn, rhs(cur)
             cur = f.correct_fused(state, cur, rp, rn, err, out=cur)
             c += 1
-            e_prev, e = e, float(err.item())
+            e_prev2, e_prev, e = e_prev, e, float(err.item())
             if self.trace is not None:
                 self.trace.append((c, e, int(f.rhs_fp32)))
         f.set_rhs_precision(False)

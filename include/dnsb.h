@@ -297,7 +297,8 @@ int dnsb_couette_set_graph_unroll(dnsb_couette* ctx, int n);
  *     max_iter (__main__.py:166-180), and `cur` copied into `state`.
  * mixed = 0: every RHS in FP64.  mixed = 1 (FP32) or 2 (FP32, compensated
  * butterflies): the RHS runs at that precision until the error after a
- * correction is <= switch_tol or > stall x the previous error, then in FP64
+ * correction is <= switch_tol or > stall x the error two corrections back
+ * (the corrector's errors fall in pairs), then in FP64
  * for the rest of the step (needs the FP32 pass sizes of
  * dnsb_couette_set_rhs_precision).  status: corrector iterations after the
  * first correction, the last and the first error, and the RHS evaluations at

@@ -19,8 +19,10 @@ gains over the method without it.
   and the FP32 -> FP64 switch on the device) gives the host-driven step's
   states bit for bit, with the same iteration counts, RHS precisions,
   first errors and gating decisions: mixed with the gate, mixed with the
-  guess applied every step, FP64 without the network, and an iteration cap,
-  with and without corrector iterations held as straight-line kernels.
+  guess applied every step, FP64 without the network, an iteration cap, and
+  a tolerance below the FP32 floor (the stall test moves every step to
+  FP64), with and without corrector iterations held as straight-line
+  kernels.
 """
 
 import json
@@ -237,8 +239,9 @@ def test_learned_couette_run(tmp_path):
 
 @pytest.mark.parametrize("form,unroll", [("mixed-gated", 0), ("mixed-guess", 0),
                                          ("fp64-no-network", 0), ("mixed-cap", 0),
-                                         ("mixed-gated", 3), ("fp64-no-network", 2),
-                                         ("mixed-cap", 5), ("mixed-guess", 64)])
+                                         ("mixed-stall", 0), ("mixed-gated", 3),
+                                         ("fp64-no-network", 2), ("mixed-cap", 5),
+                                         ("mixed-guess", 64), ("mixed-stall", 6)])
 def test_learned_step_graph_equals_host_step(form, unroll):
     import torch
 
@@ -251,14 +254,18 @@ def test_learned_step_graph_equals_host_step(form, unroll):
                    step=dict(dt=0.02, corrector_tolerance=1e-10, max_corrector_iterations=60))
     flow = PlaneCouetteFlow(p)
     mixed = form.startswith("mixed")
+    # mixed-stall: the switch at a tolerance below the FP32 rounding floor,
+    # so only the stall test (no contraction over two corrections) moves the
+    # iteration to FP64
+    stall_only = form == "mixed-stall"
     lg = learned.LearnedGuess(flow, hidden=(64, 64), seed=0,
-                              switch=1e-5 if mixed else None,
+                              switch=(1e-11 if stall_only else 1e-5) if mixed else None,
                               gate=None if form == "mixed-guess" else 0.9)
     u = initial.couette_field(32, 33, 32, 2 * pi, pi, 4, 11, 8.0, 1e-3)
     lg.collect(torch.as_tensor(u, device="cuda"), 6, 1e-10, 60)
     lg.pretrain(5)
     lg.enabled = form != "fp64-no-network"
-    tol = 1e-8 if mixed else 1e-10
+    tol = (1e-11 if stall_only else 1e-8) if mixed else 1e-10
     mi = 2 if form == "mixed-cap" else 60
     u0 = initial.couette_field(32, 33, 32, 2 * pi, pi, 4, 1, 8.0, 1e-3)
     n = 12
@@ -290,3 +297,5 @@ def test_learned_step_graph_equals_host_step(form, unroll):
         assert dev[0].guessed and dev[0].guess_rel_error is not None
     if form == "mixed-guess":
         assert all(x.guessed for x in dev)
+    if stall_only:
+        assert all(x.rhs_fp64 > 0 for x in dev)  # every step finished in FP64
