@@ -21,8 +21,9 @@ gains over the method without it.
   first errors and gating decisions: mixed with the gate, mixed with the
   guess applied every step, FP64 without the network, an iteration cap, and
   a tolerance below the FP32 floor (the stall test moves every step to
-  FP64), with and without corrector iterations held as straight-line
-  kernels.
+  FP64), and the first correction without the restart (N(u^n) in the
+  previous-RHS slot), with and without corrector iterations held as
+  straight-line kernels.
 """
 
 import json
@@ -239,7 +240,8 @@ def test_learned_couette_run(tmp_path):
 
 @pytest.mark.parametrize("form,unroll", [("mixed-gated", 0), ("mixed-guess", 0),
                                          ("fp64-no-network", 0), ("mixed-cap", 0),
-                                         ("mixed-stall", 0), ("mixed-gated", 3),
+                                         ("mixed-stall", 0), ("mixed-norestart", 0),
+                                         ("mixed-norestart", 3), ("mixed-gated", 3),
                                          ("fp64-no-network", 2), ("mixed-cap", 5),
                                          ("mixed-guess", 64), ("mixed-stall", 6)])
 def test_learned_step_graph_equals_host_step(form, unroll):
@@ -260,7 +262,8 @@ def test_learned_step_graph_equals_host_step(form, unroll):
     stall_only = form == "mixed-stall"
     lg = learned.LearnedGuess(flow, hidden=(64, 64), seed=0,
                               switch=(1e-11 if stall_only else 1e-5) if mixed else None,
-                              gate=None if form == "mixed-guess" else 0.9)
+                              gate=None if form == "mixed-guess" else 0.9,
+                              restart=form != "mixed-norestart")
     u = initial.couette_field(32, 33, 32, 2 * pi, pi, 4, 11, 8.0, 1e-3)
     lg.collect(torch.as_tensor(u, device="cuda"), 6, 1e-10, 60)
     lg.pretrain(5)
