@@ -24,9 +24,10 @@ same to within the tolerance.  With ``restart`` (the default) the guessed
 state is treated as the previous iterate, so its own RHS fills both RHS
 slots of the first correction (the reference's predict_and_correct keeps
 N(u^n) in the first slot).  With ``switch`` set (the mixed form), the RHS
-runs in FP32 until the correction norm falls below ``switch`` and in FP64
-from then on within the step, so the iteration ends at an FP64 fixed point
-while its early iterations cost less.
+runs in FP32 until the correction norm falls below ``switch`` or the FP32
+iteration stops contracting, and in FP64 from then on within the step; with
+the switch at the tolerance, the FP32 RHS carries the whole iteration unless
+it stagnates above the tolerance.
 
 ``LearnedStepGraph`` (``LearnedGuess.make_step_graph``) is the same step with
 the corrector on the device: the predictor and the corrector loop are CUDA
