@@ -519,7 +519,8 @@ cudaError_t launch_x_pass(const XPassArgs& a, cudaStream_t st) {
 // stage reads its input into registers, waits for every thread, then writes
 // its output over it.
 size_t x_pass2_smem(int M, int nkx) {
-  const size_t S = (size_t)6 * nkx * kX2Rows, Y = (size_t)M * 2 * kX2Rows + M / 8;
+  // the stage-B output: M / 8 blocks of 8 * CF + 16 slots (CF = 2 rows x 4)
+  const size_t S = (size_t)6 * nkx * kX2Rows, Y = (size_t)(M / 8) * (8 * 2 * kX2Rows + 16);
   const size_t X = (size_t)M * 3 * kX2Rows + 4 * 8;  // + the stage-A skew
   size_t W = S > Y ? S : Y;
   W = W > X ? W : X;
@@ -534,12 +535,19 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
   using RT = typename pass_types<T>::R;
   constexpr int M = ML, R1 = M / 8, R = kX2Rows, NKX = ML / 3;
   constexpr int CI = 3 * R, CF = 2 * R;
-  // Stage outputs carry a skew of XS (X) / 1 (Y) slots per block of R1 (X)
-  // / 8 (Y) positions, so the 8 lanes of a 16-byte shared access hit 8
-  // different bank groups on both the store and the next stage's load.
+  // Shared-memory layouts keep the stages' accesses free of bank conflicts
+  // for 16-byte (FP64, 8 lanes per 128-byte wavefront) and 8-byte (FP32, 16
+  // lanes) elements alike:
+  //  * the stage-A output carries a skew of XS slots per block of R1
+  //    positions;
+  //  * the stage-B output, position t = 8 k + i, lives in blocks of YB
+  //    slots (a multiple of 16, so the banks depend on the skew alone), with
+  //    a skew of (k & 1) + 8 ((k >> 1) & 1) slots per block.
   constexpr int XS = 4;
+  constexpr int YB = 8 * CF + 16;
   static_assert(R == 4, "the stage-A lane map assumes 4 rows");
-  constexpr int SZ_S = 6 * NKX * R, SZ_Y = M * CF + R1, SZ_X = M * CI + XS * 8;
+  static_assert(YB % 16 == 0 && YB >= 8 * CF + 10, "stage-B blocks hold their skew");
+  constexpr int SZ_S = 6 * NKX * R, SZ_Y = R1 * YB, SZ_X = M * CI + XS * 8;
   constexpr int SZ_SY = SZ_S > SZ_Y ? SZ_S : SZ_Y;
   constexpr int SZ_W = SZ_SY > SZ_X ? SZ_SY : SZ_X;
   // every stage has at most one item per thread, so a thread can hold its
@@ -595,11 +603,15 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
   __syncthreads();
   // Stage A: inverse radix R1 (Ns = 1) on Z = A + iB, built on the fly.
   {
-    // lanes of a quarter warp: 4 rows x 2 parities of j, one field pair
+    // lanes of a half warp: 4 rows x 4 values of j, one field pair, where
+    // the stage-A output's stride per j (R1 CI + XS slots) spreads the four
+    // j over the banks; else (M = 72) 4 rows x 2 values of j x 2 pairs
+    constexpr bool J4 = (R1 * CI + XS) % 16 != 0;
     const int it = tid;
     const bool act = it < 8 * CI;
-    const int r = it & 3, rest = it >> 3;
-    const int pr = rest % 3, j = ((it >> 2) & 1) + 2 * (rest / 3);
+    const int r = it & 3, rest = J4 ? it >> 4 : it >> 3;
+    const int pr = rest % 3;
+    const int j = J4 ? ((it >> 2) & 3) + 4 * (rest / 3) : ((it >> 2) & 1) + 2 * (rest / 3);
     const int col = 3 * r + pr;
     CT v[R1];
     if (act) {
@@ -677,10 +689,11 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
     }
     __syncthreads();  // X read by every thread before Y is written over it
     if (act) {
+      CT* yk = Y + k * YB + (k & 1) + 8 * ((k >> 1) & 1);
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        Y[(k * 8 + i) * CF + 2 * r + k] = F0[i];
-        Y[(k * 8 + i) * CF + 2 * r + 1 + k] = F1[i];
+        yk[i * CF + 2 * r] = F0[i];
+        yk[i * CF + 2 * r + 1] = F1[i];
       }
     }
   }
@@ -692,8 +705,10 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
     const int col = it % CF, j = it / CF;
     CT v[R1];
     if (act) {
+      // position t = j + 8 i is entry j of stage-B block i
 #pragma unroll
-      for (int i = 0; i < R1; ++i) v[i] = Y[(j + 8 * i) * CF + col + i];
+      for (int i = 0; i < R1; ++i)
+        v[i] = Y[i * YB + (i & 1) + 8 * ((i >> 1) & 1) + j * CF + col];
     }
     __syncthreads();  // Y read by every thread before X is written over it
     if (act) {
