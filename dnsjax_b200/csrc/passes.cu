@@ -542,12 +542,17 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
   //    positions;
   //  * the stage-B output, position t = 8 k + i, lives in blocks of YB
   //    slots (a multiple of 16, so the banks depend on the skew alone), with
-  //    a skew of (k & 1) + 8 ((k >> 1) & 1) slots per block.
+  //    a skew of (k & 1) + 8 ((k >> 1) & 1) slots per block;
+  //  * the stage-C output's row t starts at slot 9 t for 16-byte elements,
+  //    which the final unpack reads without conflicts (8-byte elements keep
+  //    rows of CF slots: a skew of t / 2 measured slower there).
   constexpr int XS = 4;
   constexpr int YB = 8 * CF + 16;
   static_assert(R == 4, "the stage-A lane map assumes 4 rows");
   static_assert(YB % 16 == 0 && YB >= 8 * CF + 10, "stage-B blocks hold their skew");
   constexpr int SZ_S = 6 * NKX * R, SZ_Y = R1 * YB, SZ_X = M * CI + XS * 8;
+  static_assert(9 * M <= SZ_X, "the stage-C rows fit the work region");
+  auto xrow = [](int t) { return sizeof(CT) == 16 ? 9 * t : CF * t; };
   constexpr int SZ_SY = SZ_S > SZ_Y ? SZ_S : SZ_Y;
   constexpr int SZ_W = SZ_SY > SZ_X ? SZ_SY : SZ_X;
   // every stage has at most one item per thread, so a thread can hold its
@@ -716,7 +721,7 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
       for (int i = 1; i < R1; ++i) v[i] = cmul(v[i], tw[i * j]);
       dft_3p<R1, -1, CT, true>(v, tw, 8);
 #pragma unroll
-      for (int i = 0; i < R1; ++i) X[(j + 8 * i) * CF + col] = v[i];
+      for (int i = 0; i < R1; ++i) X[xrow(j + 8 * i) + col] = v[i];
     }
   }
   __syncthreads();
@@ -735,8 +740,8 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
     }
     if (r >= nr) continue;
     const int col = 2 * r + (f == 2 ? 1 : 0);
-    const CT Z = X[k * CF + col];
-    const CT Zm = X[((M - k) % M) * CF + col];
+    const CT Z = X[xrow(k) + col];
+    const CT Zm = X[xrow((M - k) % M) + col];
     CT v;
     if (f == 1) {
       v = cmake<CT>((Z.y + Zm.y) * h, (Zm.x - Z.x) * h);
