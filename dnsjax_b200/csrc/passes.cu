@@ -543,16 +543,19 @@ __device__ __forceinline__ void x_pass2_body(const XPassArgs& a, int bx) {
   //  * the stage-B output, position t = 8 k + i, lives in blocks of YB
   //    slots (a multiple of 16, so the banks depend on the skew alone), with
   //    a skew of (k & 1) + 8 ((k >> 1) & 1) slots per block;
-  //  * the stage-C output's row t starts at slot 9 t for 16-byte elements,
-  //    which the final unpack reads without conflicts (8-byte elements keep
-  //    rows of CF slots: a skew of t / 2 measured slower there).
+  //  * the stage-C output's row t starts at slot 9 t, which the final
+  //    unpack reads without conflicts, rows or modes fastest (for 8-byte
+  //    elements unpacked rows fastest, rows of CF slots measured faster).
   constexpr int XS = 4;
   constexpr int YB = 8 * CF + 16;
   static_assert(R == 4, "the stage-A lane map assumes 4 rows");
   static_assert(YB % 16 == 0 && YB >= 8 * CF + 10, "stage-B blocks hold their skew");
   constexpr int SZ_S = 6 * NKX * R, SZ_Y = R1 * YB, SZ_X = M * CI + XS * 8;
   static_assert(9 * M <= SZ_X, "the stage-C rows fit the work region");
-  auto xrow = [](int t) { return sizeof(CT) == 16 ? 9 * t : CF * t; };
+  // 9 slots per row, except 8-byte elements unpacked rows fastest (CF:
+  // 1% faster there); the mapping is fixed per launch
+  const int xstride = (sizeof(CT) == 16 || !a.rows_fast) ? 9 : CF;
+  auto xrow = [xstride](int t) { return xstride * t; };
   constexpr int SZ_SY = SZ_S > SZ_Y ? SZ_S : SZ_Y;
   constexpr int SZ_W = SZ_SY > SZ_X ? SZ_SY : SZ_X;
   // every stage has at most one item per thread, so a thread can hold its
