@@ -169,18 +169,34 @@ __device__ __forceinline__ void col_pass2_body(const ColPassArgs& a, int bx, int
           const int sidx = pos_to_stored(t, a.nstored, M);
           if (sidx >= 0) {
             if constexpr (CURL) {
+              // f is the same for the whole CTA: load only the components
+              // the field needs
               const double2* st = reinterpret_cast<const double2*>(a.in) + o * a.in_os + i0 +
                                   (long long)sidx * a.in_ts + c;
-              const double2 u = st[0], vv = st[a.in_fs], w = st[2 * a.in_fs];
-              const double kx = a.kx[i0 + c], ky = a.ky[sidx], kz = a.kz[o];
+              const long long fs = a.in_fs;
               double2 q;
               switch (f) {
-                case 0: q = u; break;
-                case 1: q = vv; break;
-                case 2: q = w; break;
-                case 3: q = ci(make_double2(ky * w.x - kz * vv.x, ky * w.y - kz * vv.y)); break;
-                case 4: q = ci(make_double2(kz * u.x - kx * w.x, kz * u.y - kx * w.y)); break;
-                default: q = ci(make_double2(kx * vv.x - ky * u.x, kx * vv.y - ky * u.y)); break;
+                case 0: q = st[0]; break;
+                case 1: q = st[fs]; break;
+                case 2: q = st[2 * fs]; break;
+                case 3: {
+                  const double2 vv = st[fs], w = st[2 * fs];
+                  const double ky = a.ky[sidx], kz = a.kz[o];
+                  q = ci(make_double2(ky * w.x - kz * vv.x, ky * w.y - kz * vv.y));
+                  break;
+                }
+                case 4: {
+                  const double2 u = st[0], w = st[2 * fs];
+                  const double kx = a.kx[i0 + c], kz = a.kz[o];
+                  q = ci(make_double2(kz * u.x - kx * w.x, kz * u.y - kx * w.y));
+                  break;
+                }
+                default: {
+                  const double2 u = st[0], vv = st[fs];
+                  const double kx = a.kx[i0 + c], ky = a.ky[sidx];
+                  q = ci(make_double2(kx * vv.x - ky * u.x, kx * vv.y - ky * u.y));
+                  break;
+                }
               }
               z = to_c(q, (CT*)nullptr);
             } else {
