@@ -1478,7 +1478,8 @@ zinv_curl2_kernel(ZInvCurlArgs a) {
   // Half of the pass buffer's lines stay in L2 for the x pass that reads
   // them next (all of them would not fit beside the rest).
   const unsigned long long keep = l2_keep_half();
-  for (int f = 0; f < nf; ++f) {
+  // the fields of this CTA: blockIdx.y, blockIdx.y + gridDim.y, ...
+  for (int f = blockIdx.y; f < nf; f += gridDim.y) {
     switch (f) {
       case 0: zinv2_fill<M, 0>(a, X, U, V, Wc, ncol, y, kx, live); break;
       case 1: zinv2_fill<M, 1>(a, X, U, V, Wc, ncol, y, kx, live); break;
@@ -1540,7 +1541,8 @@ cudaError_t launch_zinv_curl(const ZInvCurlArgs& a, int span_max,
   if (slab && (a.fp32 || a.variant != 0 || !fixed)) return cudaErrorInvalidValue;
   if (a.variant == 0 && fixed) {
     const long long ncol = (long long)a.NKX * a.Ny;
-    const int grid = (int)((ncol + kZ2Cols - 1) / kZ2Cols);
+    // one field per CTA along y
+    const dim3 grid((unsigned)((ncol + kZ2Cols - 1) / kZ2Cols), a.curl ? 6 : 3);
     if (slab) {
       const size_t sm = zinv_curl2_smem(L);
       switch (L) {
