@@ -8,6 +8,9 @@
   single RHS / predictor / corrector calls against the oracle, plus
   size-independent properties (transform round trip, no-slip walls and zero
   wall divergence after the influence-matrix solve).
+* The RHS at the other compiled padded lengths (72 and 96: 48^3 and 64^3
+  grids) for both flows against the oracle, and the FP32 RHS against the
+  FP64 one at padded length 72.
 """
 
 from math import pi
@@ -180,3 +183,34 @@ def test_kolmogorov_rhs_sizes(n):
     u0 = initial.periodic_field(n, n, n, 2 * pi, 2 * pi, 2 * pi, n,
                                 initial.kolmogorov_spectrum_cfg0, 1e-2)
     assert rel_l2(host(flow.get_rhs(dev(u0))), orc.get_rhs(u0)) < 1e-12
+
+
+@pytest.mark.parametrize("n", [48, 64])
+def test_couette_rhs_sizes(n):
+    """Padded lengths 72 and 96 of the two-stage Couette passes (the x pass
+    unpacking rows fastest) against the oracle."""
+    from dnsjax_b200 import initial
+
+    flow, orc = couette(n, n + 1, n, 4, 400.0, 0.02)
+    u0 = initial.couette_field(n, n + 1, n, 2 * pi, pi, 4, n, 8.0, 1e-3)
+    assert rel_l2(host(flow.get_rhs(dev(u0))), orc.get_rhs(u0)) < 1e-12
+
+
+def test_fp32_rhs_48():
+    """The FP32 RHS passes at padded length 72 (48^3 grids) against the FP64
+    RHS, both flows (the FP32 pass buffers' rounding: ~1e-7 relative)."""
+    from dnsjax_b200 import initial
+
+    flow, _ = couette(48, 49, 48, 4, 400.0, 0.02)
+    u = dev(initial.couette_field(48, 49, 48, 2 * pi, pi, 4, 5, 8.0, 1e-3))
+    r64 = host(flow.get_rhs(u))
+    flow.set_rhs_precision(True)
+    r32 = host(flow.get_rhs(u))
+    assert rel_l2(r32, r64) < 2e-6
+    pflow, _ = kolmogorov(48, 60.0, 0.01)
+    u = dev(initial.periodic_field(48, 48, 48, 2 * pi, 2 * pi, 2 * pi, 7,
+                                   initial.kolmogorov_spectrum_cfg0, 1e-2))
+    r64 = host(pflow.get_rhs(u))
+    pflow.set_rhs_precision(True)
+    r32 = host(pflow.get_rhs(u))
+    assert rel_l2(r32, r64) < 2e-6
