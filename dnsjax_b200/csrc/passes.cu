@@ -1445,7 +1445,7 @@ __device__ __forceinline__ void zinv2_fill(const ZInvCurlArgs& a, CT* X,
 // (double, or float for the FP32 form of the Couette RHS); the state is
 // read, and the curl's fill computed, in FP64.
 template <int ML, typename T = double, bool SLAB = false>
-__global__ void __launch_bounds__(kZ2Threads, 4)
+__global__ void __launch_bounds__(kZ2Threads, std::is_same<T, float>::value ? 6 : 4)
 zinv_curl2_kernel(ZInvCurlArgs a) {
   if (a.skip && *a.skip) return;
   using CT = typename pass_types<T>::C;
